@@ -1,0 +1,330 @@
+#!/usr/bin/env python
+"""Benchmark of the Nyström operator application on B200.
+
+Workload (the single-GPU configuration the headline metric is quoted on):
+3D Helmholtz single layer, k = 10, FP64 complex, matrix-free, on the unit
+sphere meshed by 10,368 quadratic triangles with the 6-point VR rule
+(N = 62,208 nodes), plus its DIM correction (6 nonzeros per row) applied as a
+CSR SpMV fused into the pair kernel's epilogue.  Density: complex Gaussian,
+seed 1.  One step = one y = (A + δS) σ over all N² node pairs.
+
+value   kernel-pairs/s (G) with σ and y resident in HBM; L2 flushed between
+        steps (a 256 MiB write, untimed), each step timed with CUDA events on
+        the library's stream.
+e2e     the same metric through the public API (GpuOperator.mul with pinned
+        host buffers): host->device copy of σ, the apply, device->host copy
+        of y, every step.
+gmres   (extra key) time to ||b - Lx|| <= 1e-10 ||b|| for the 3D Laplace
+        combined field ½I + D + S on the (1, 0.7, 0.5) ellipsoid, N = 200,934,
+        plain FP64 GMRES versus FP32-inner / FP64-outer refinement.
+
+--impl reference times the reference's CPU algorithm for the same step
+(Inti's on-the-fly row sums, restated in C++ as the oracle) on all host
+cores, each step a bounded sample of rows scaled to the metric.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "inti.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "G kernel-pairs/s (Helmholtz SL, FP64, N=62208, DIM-corrected matvec)"
+UNIT = "Gpairs/s"
+# Algorithmic flops per pair (FMA = 2 flops; special functions counted apart)
+FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10}
+# DRAM bytes (read + write) of one pair-kernel launch on this workload, from
+# the ncu capture summarised in profiles/pair_forward_helmholtz_sl_fp64_p2sphere62k.md
+PAIR_TRAFFIC_BYTES = None
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def build_c2(ctx):
+    import inti_b200 as inti
+
+    q = inti.p2_sphere_quadrature(36)
+    op = inti.Helmholtz(k=10.0, dim=3)
+    t0 = time.perf_counter()
+    dS, _ = inti.bdim_correction(op, q, q, ctx=ctx)
+    t_dim = time.perf_counter() - t0
+    S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, "fp64", ctx)
+    r = np.random.default_rng(1)
+    sigma = (r.standard_normal(len(q)) + 1j * r.standard_normal(len(q))) / np.sqrt(2)
+    return q, S, sigma, t_dim
+
+
+def cpu_sample(q, sigma, seconds: float, nthreads: int) -> dict:
+    """The oracle's on-the-fly FP64 row sums on a bounded sample of rows."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle as O
+
+    n = len(q)
+    args = (O.HELMHOLTZ, O.SL, 10.0, q.coords, q.normals, q.coords, q.normals, q.weights, sigma)
+    t0 = time.perf_counter()
+    rows0 = max(8 * nthreads, 32)
+    O.apply_rows_block(*args, 0, rows0, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    rows = int(min(n, max(rows0, rows0 * seconds / max(dt, 1e-6))))
+    t0 = time.perf_counter()
+    O.apply_rows_block(*args, 0, rows, nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    return {"value": rows * n / dt / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{rows} of {n} target rows x {n} sources (C++ FP64 restatement of Inti's "
+                      f"on-the-fly row sums), {dt:.1f} s"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import inti_b200.geometry as G
+    import oracle as O
+
+    q = G.p2_sphere_quadrature(36)
+    r = np.random.default_rng(1)
+    sigma = (r.standard_normal(len(q)) + 1j * r.standard_normal(len(q))) / np.sqrt(2)
+    nt = host_cores()
+    n = len(q)
+    budget = max(60.0 / max(args.steps + args.warmup, 1), 2.0)  # whole run within a few minutes
+    sargs = (O.HELMHOLTZ, O.SL, 10.0, q.coords, q.normals, q.coords, q.normals, q.weights, sigma)
+    t0 = time.perf_counter()
+    O.apply_rows_block(*sargs, 0, 8 * nt, nthreads=nt)
+    rate = 8 * nt / (time.perf_counter() - t0)
+    rows = int(min(n, max(8 * nt, rate * budget)))
+    for _ in range(args.warmup):
+        O.apply_rows_block(*sargs, 0, min(rows, 8 * nt), nthreads=nt)
+    times = []
+    for s in range(args.steps):
+        row0 = (s * rows) % max(n - rows, 1)
+        t0 = time.perf_counter()
+        O.apply_rows_block(*sargs, row0, rows, nthreads=nt)
+        times.append(time.perf_counter() - t0)
+    per = statistics.mean(times)
+    value = rows * n / per / 1e9
+    full_ms = per * (n / rows) * 1e3
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "helmholtz3d_sl_k10_p2sphere_N62208_dim", "n": n, "nnz_per_row": 6},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
+                         "sample": f"{rows} target rows x {n} sources per step (scaled to a full step)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def gmres_c3(ctx) -> dict:
+    """Combined-field Laplace solve on the ellipsoid (N = 200,934)."""
+    import inti_b200 as inti
+
+    q = inti.ellipsoid_quadrature(61, 5)
+    op = inti.Laplace(dim=3)
+    t0 = time.perf_counter()
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    t_setup = time.perf_counter() - t0
+    r = np.random.default_rng(8)
+    src = r.uniform(-1, 1, (64, 3))
+    src = src[np.sum((src / np.array([0.5, 0.35, 0.25])) ** 2, 1) < 1][:8]  # inside the 0.5-scaled ellipsoid
+    c = r.standard_normal(len(src))
+    d = np.linalg.norm(q.coords[:, None, :] - src[None, :, :], axis=2)
+    b = (c[None, :] / (4 * np.pi * d)).sum(1)
+    L = 0.5 * inti.I + D + S
+    out = {"workload": "laplace3d_cfie(0.5I+D+S)_ellipsoid_N200934_dim", "n": len(q), "rtol": 1e-10,
+           "setup_s": t_setup}
+    for mode in ("fp64", "mixed"):
+        x, st = inti.gmres(L, b, rtol=1e-10, restart=100, maxiter=500, mode=mode)
+        out[mode] = {"seconds": st["seconds"], "iterations": st["iterations"], "outer": st["outer"],
+                     "fp64_applies": st["fp64_applies"], "fp32_applies": st["fp32_applies"],
+                     "relres_fp64": st["relres"], "converged": bool(st["converged"])}
+    if out["fp64"]["converged"] and out["mixed"]["converged"]:
+        out["mixed_speedup_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    return out
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-gmres", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    import inti_b200 as inti
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    ctx = inti.Context(local)
+    peaks = ctx.measure_peaks()
+    q, S, sigma, t_dim = build_c2(ctx)
+    n = len(q)
+    pairs = float(n) * n
+    stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
+    dev = torch.device(f"cuda:{local}")
+    xs = torch.from_numpy(sigma.view(np.float64).copy()).to(dev)
+    ys = torch.zeros(2 * n, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            S.apply_device(xs.data_ptr(), ys.data_ptr())
+        stream.synchronize()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        clocks = Clocks(local)
+        launches0 = ctx.launch_count
+        ctx.set_profiling(True)
+        evs = []
+        for _ in range(args.steps):
+            flush.zero_()  # untimed: evicts L2 between steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            S.apply_device(xs.data_ptr(), ys.data_ptr())
+            e1.record(stream)
+            evs.append((e0, e1))
+        stream.synchronize()
+        torch.cuda.synchronize(dev)
+        step_ms = [a.elapsed_time(b) for a, b in evs]
+        pair_ms, pair_launches = ctx.profile("pair")
+        epi_ms, _ = ctx.profile("epilogue")
+        pack_ms, _ = ctx.profile("pack")
+        ctx.set_profiling(False)
+        launches = ctx.launch_count - launches0
+        clk = clocks.stop()
+    ms = sum(step_ms) / len(step_ms)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * pairs / (ms * 1e-3) / 1e9
+
+    # e2e through the public API with pinned host buffers
+    hx = torch.from_numpy(sigma.copy()).pin_memory().numpy()
+    hy = torch.zeros(n, dtype=torch.complex128).pin_memory().numpy()
+    for _ in range(2):
+        S.mul(hy, hx)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S.mul(hy, hx)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = {"value": world * pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
+           "d2h_bytes_per_step": 16 * n, "ms_per_step": e2e_s * 1e3}
+
+    # roofline of the dominant kernel (the pair kernel)
+    kern_ms = pair_ms / max(pair_launches, 1)
+    achieved = pairs * FLOPS_PER_PAIR["helmholtz_sl"] / (kern_ms * 1e-3) / 1e12
+    peak = peaks["fp64_flops"] / 1e12
+    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": PAIR_TRAFFIC_BYTES,
+                "kernel": "pair_forward<Helmholtz,SL,3,double>", "kernel_ms": kern_ms,
+                "flops_per_pair": FLOPS_PER_PAIR["helmholtz_sl"],
+                "peak_source": "FP64 FMA throughput measured in this run (inti_measure_peaks)",
+                "share_of_step": pair_ms / max(sum(step_ms), 1e-9),
+                "other_kernels_ms": {"pack": pack_ms / args.steps, "epilogue": epi_ms / args.steps}}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "helmholtz3d_sl_k10_p2sphere_N62208_dim", "n": n, "nnz_per_row": 6,
+                   "precision": "fp64", "parallelism": f"replicas{world}", "l2": "flushed between steps",
+                   "dim_setup_s": t_dim},
+        "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk,
+        "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_sample(q, sigma, args.cpu_seconds, host_cores())
+    if not args.no_gmres and world == 1:
+        line["gmres"] = gmres_c3(ctx)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

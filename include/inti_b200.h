@@ -1,0 +1,214 @@
+/*
+ * inti_b200.h — C ABI of libinti_b200.so, the B200 (sm_100a) implementation
+ * of Inti.jl's Nyström operator application.
+ *
+ * The library replaces, for one GPU, the product that Inti.jl evaluates on
+ * the CPU:
+ *
+ *     y = alpha * (A_K * x + C * x) + beta * y,
+ *     (A_K)_ij = K(x_i, y_j) * w_j        (src/nystrom.jl:93-96)
+ *
+ * with K one of the Laplace / Helmholtz single-layer, double-layer,
+ * adjoint-double-layer or hypersingular kernels (src/kernels.jl:137-204,
+ * 347-413) evaluated on the fly over all target/source node pairs (never
+ * stored), and C a sparse DIM/BDIM/VDIM correction (src/bdim.jl:193-194,
+ * src/vdim.jl:127) applied as a CSR SpMV.  It also builds the BDIM
+ * correction on the GPU, runs GMRES (plain FP64 or FP32-inner / FP64-outer
+ * refinement) and evaluates adjoints and shape gradients.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (INTI_OK = 0).  On failure
+ *    inti_last_error(ctx) returns a message; no C++ exception crosses this
+ *    boundary.  Error categories mirror the ArgumentError / ErrorException
+ *    split of the Julia side (src/nystrom.jl:81-84, src/utils.jl:192-194).
+ *  - Arrays are plain host pointers unless `on_device` is set, in which case
+ *    they are device pointers on the context's device.  The library never
+ *    keeps a caller's pointer past the call.
+ *  - Coordinates / normals: dim x n, column-major (= array-of-structs
+ *    x0 y0 [z0] x1 y1 ...), the layout of Julia's Matrix{Float64}(dim, n) and
+ *    of Vector{SVector{dim,Float64}}.
+ *  - Complex data (Helmholtz) is interleaved (re, im) doubles: ComplexF64.
+ *  - Indices are 0-based.  inti_csr_create_from_csc accepts Julia's 1-based
+ *    SparseMatrixCSC arrays directly.
+ *  - One context per device and stream.  Calls on one context are serialised
+ *    by an internal lock; different contexts are independent.
+ */
+#ifndef INTI_B200_H
+#define INTI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define INTI_B200_ABI_VERSION 1
+
+typedef struct inti_ctx inti_ctx;
+typedef struct inti_quad inti_quad;
+typedef struct inti_csr inti_csr;
+typedef struct inti_op inti_op;
+
+/* status codes */
+enum {
+  INTI_OK = 0,
+  INTI_E_ARG = 1,         /* invalid argument (ArgumentError) */
+  INTI_E_SHAPE = 2,       /* dimension mismatch (DimensionMismatch) */
+  INTI_E_CUDA = 3,        /* CUDA runtime failure */
+  INTI_E_NONFINITE = 4,   /* NaN/Inf found in an input */
+  INTI_E_TIMEOUT = 5,     /* a device-side bounded wait ran out */
+  INTI_E_NOMEM = 6,       /* device allocation failed */
+  INTI_E_UNSUPPORTED = 7, /* combination not implemented */
+  INTI_E_NOCONV = 8,      /* iterative solver did not reach tolerance */
+  INTI_E_STATE = 9        /* handle used with the wrong context/state */
+};
+
+/* differential operators (src/kernels.jl:118, 310) */
+enum { INTI_LAPLACE = 0, INTI_HELMHOLTZ = 1 };
+/* kernels (src/kernels.jl:52-112) */
+enum { INTI_SL = 0, INTI_DL = 1, INTI_ADL = 2, INTI_HS = 3 };
+/* arithmetic of the pair evaluation */
+enum {
+  INTI_FP64 = 0, /* FP64 pairs and accumulation */
+  INTI_FP32C = 1 /* FP32 pairs, compensated (two-sum) accumulation; FP64 correction SpMV */
+};
+/* element type of densities / correction values */
+enum { INTI_F64 = 0, INTI_C128 = 1 };
+/* inti_memcpy directions */
+enum { INTI_H2D = 0, INTI_D2H = 1, INTI_D2D = 2 };
+/* GMRES modes */
+enum { INTI_GMRES_FP64 = 0, INTI_GMRES_MIXED = 1 };
+
+int inti_version(void);
+
+/* ---- context ----------------------------------------------------------- */
+/* stream: a cudaStream_t to run on, or NULL for a library-owned stream. */
+int inti_ctx_create(int device, void* stream, inti_ctx** out);
+int inti_ctx_destroy(inti_ctx* ctx);
+/* Message of the last failure on ctx (or of the calling thread when ctx is
+ * NULL, e.g. after inti_ctx_create failed).  Valid until the next call. */
+const char* inti_last_error(const inti_ctx* ctx);
+int inti_ctx_synchronize(inti_ctx* ctx);
+/* The cudaStream_t every launch of ctx goes to. */
+void* inti_ctx_stream(inti_ctx* ctx);
+/* Number of library kernels launched on ctx so far. */
+int64_t inti_ctx_launch_count(const inti_ctx* ctx);
+/* Per-kernel device timing with CUDA events recorded on ctx's stream around
+ * each launch (off by default; enabling clears earlier records). */
+int inti_ctx_set_profiling(inti_ctx* ctx, int enable);
+/* Total device milliseconds and launch count recorded for one kernel class
+ * ("pack", "pair", "epilogue", "csr", "transpose", "dim", "gmres") since
+ * profiling was enabled.  Synchronises the stream. */
+int inti_ctx_profile(inti_ctx* ctx, const char* kernel, double* total_ms, int64_t* launches);
+
+/* ---- device buffers, for callers without a CUDA allocator --------------- */
+int inti_dev_alloc(inti_ctx* ctx, int64_t bytes, void** ptr);
+int inti_dev_free(inti_ctx* ctx, void* ptr);
+/* Stream-ordered copy on ctx's stream; synchronous when host memory is
+ * involved. */
+int inti_memcpy(inti_ctx* ctx, void* dst, const void* src, int64_t bytes, int direction);
+
+/* ---- quadrature (replaces Inti.Quadrature's node arrays,
+ *      src/quadrature.jl:7-11, 65-70) ------------------------------------ */
+/* normals may be NULL (bare target points, src/quadrature.jl:50); weights may
+ * be NULL for target-only sets (taken as 1).  nq > 0 declares that element e
+ * owns the contiguous nodes e*nq .. e*nq+nq-1 (etype2qtags,
+ * src/quadrature.jl:160); 0 means no element structure. */
+int inti_quad_create(inti_ctx* ctx, int dim, int64_t n, const double* coords,
+                     const double* normals, const double* weights, int32_t nq,
+                     inti_quad** out);
+int inti_quad_destroy(inti_quad* q);
+int64_t inti_quad_size(const inti_quad* q);
+
+/* ---- sparse correction (replaces SparseMatrixCSC δS/δD,
+ *      src/bdim.jl:193-194, src/api.jl:170-185) -------------------------- */
+int inti_csr_create(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz, const int64_t* rowptr,
+                    const int32_t* col, const double* val, int dtype, inti_csr** out);
+/* From Julia's 1-based CSC arrays (colptr length n+1, rowval/nzval length
+ * nnz); the transposition to CSR keeps the pattern bit-exactly. */
+int inti_csr_create_from_csc(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz,
+                             const int64_t* colptr1, const int64_t* rowval1,
+                             const double* nzval, int dtype, inti_csr** out);
+int inti_csr_info(const inti_csr* c, int64_t* m, int64_t* n, int64_t* nnz, int* dtype);
+/* Copies the CSR arrays to host buffers sized m+1, nnz, nnz*(1|2). */
+int inti_csr_download(const inti_csr* c, int64_t* rowptr, int32_t* col, double* val);
+/* y = alpha*C*x + beta*y (alpha/beta: 2 doubles, re and im). */
+int inti_csr_apply(inti_csr* c, const double* x, double* y, const double* alpha,
+                   const double* beta, int on_device);
+int inti_csr_destroy(inti_csr* c);
+
+/* ---- operator (replaces IntegralOperator + its LinearMap sum with the
+ *      correction, src/nystrom.jl:67-96, src/api.jl:179-184) ------------- */
+/* k_re/k_im: Helmholtz wavenumber (ignored for Laplace).  correction may be
+ * NULL.  The operator keeps references to target, source and correction:
+ * destroy it before them. */
+int inti_op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
+                   const inti_quad* target, const inti_quad* source,
+                   const inti_csr* correction, int precision, inti_op** out);
+int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype);
+/* Y = alpha*(A*X + C*X) + beta*Y for nrhs columns (leading dimensions ldx,
+ * ldy in elements).  alpha, beta: 2 doubles each (re, im); NULL means 1, 0.
+ * beta = 0 does not read Y. */
+int inti_op_apply(inti_op* op, const double* x, int64_t ldx, double* y, int64_t ldy,
+                  int32_t nrhs, const double* alpha, const double* beta, int on_device);
+/* Y = alpha*(A^T*X + C^T*X) + beta*Y: the transpose (not conjugate) apply,
+ * the density gradient of the adjoint method. */
+int inti_op_apply_transpose(inti_op* op, const double* x, int64_t ldx, double* y,
+                            int64_t ldy, int32_t nrhs, const double* alpha,
+                            const double* beta, int on_device);
+/* Dense column-major m x n matrix of A (without the correction), the GPU
+ * counterpart of assemble_matrix (src/nystrom.jl:103-124). */
+int inti_op_assemble(inti_op* op, double* out, int on_device);
+int inti_op_destroy(inti_op* op);
+
+/* ---- BDIM correction on the GPU (src/bdim.jl:50-196, target === source) -- */
+/* green_multiplier: n values or NULL for -1/2 (on the surface,
+ * src/nystrom.jl:196-207).  derivative = 1 builds the ADL/HS corrections.
+ * Outputs two CSR handles (δS, δD) with the element-block pattern of
+ * src/quadrature.jl:250-256. */
+int inti_dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im,
+                        const inti_quad* q, int derivative, const double* green_multiplier,
+                        inti_csr** dS, inti_csr** dD);
+
+/* ---- GMRES on L = shift*I + sum_t coef_t * op_t ------------------------- */
+typedef struct {
+  int32_t iterations;       /* total Krylov iterations (all restarts, all solves) */
+  int32_t outer;            /* refinement steps (MIXED) or restarts + 1 (FP64) */
+  int32_t fp64_applies;     /* applications of the FP64 operator */
+  int32_t fp32_applies;     /* applications of the FP32C operator */
+  int32_t converged;        /* 1 if relres <= rtol */
+  int32_t reserved;
+  double relres;            /* ||b - L x|| / ||b||, FP64 residual */
+  double seconds;           /* device time of the solve */
+} inti_gmres_stats;
+
+/* coefs: nterms complex pairs; shift: one complex pair.  All ops must share
+ * the same source/target quadrature and be FP64 operators; MIXED mode runs
+ * the inner solves with FP32C twins built internally.  b/x: n values
+ * (complex if any operator or coefficient is).  x is the initial guess on
+ * input.  history (nullable, maxiter+1 doubles) receives relative residuals
+ * per iteration. */
+int inti_gmres(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const double* coefs,
+               const double* shift, const double* b, double* x, double rtol,
+               int32_t restart, int32_t maxiter, int32_t mode, int on_device,
+               double* history, inti_gmres_stats* stats);
+
+/* ---- adjoint: gradients of J(u), u = A sigma (Laplace, on-the-fly) ------ */
+/* Given the cotangent g = dJ/du (m values) and the density sigma (n values),
+ * returns dJ/dsigma (n), dJ/dcoords (dim x n), dJ/dnormals (dim x n) and
+ * dJ/dweights (n) of the source quadrature; any output may be NULL.  Tiles
+ * of the kernel are recomputed, nothing m x n is stored. */
+int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, double* dsigma,
+                         double* dcoords, double* dnormals, double* dweights, int on_device);
+
+/* ---- measured peaks for the roofline ------------------------------------ */
+/* Sustained throughput of dependent-free FP64 FMA, FP32 FMA and MUFU rsqrt
+ * on this device, in operations per second (FMA counted as 2 flops). */
+int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops,
+                       double* mufu_ops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INTI_B200_H */

@@ -1,0 +1,175 @@
+// Internal declarations shared by the CUDA translation units of
+// libinti_b200.so.  Nothing here is part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/inti_b200.h"
+
+namespace inti {
+
+// src/utils.jl:235 — pairs closer than this are the excluded self-pair.  The
+// kernels compare the squared distance with its square.
+constexpr double kSamePointTol = 1.0e-14;
+constexpr double kSamePointTol2 = 1.0e-28;
+constexpr double kPi = 3.14159265358979323846;
+
+// An error carrying an ABI status code; caught at the C boundary.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define INTI_CUDA(call)                                                              \
+  do {                                                                               \
+    cudaError_t _e = (call);                                                         \
+    if (_e != cudaSuccess)                                                           \
+      throw ::inti::Error(INTI_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
+  } while (0)
+
+// Device allocation owned by a handle.
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void ensure(size_t nbytes) {
+    if (nbytes <= bytes && p) return;
+    release();
+    if (nbytes == 0) nbytes = 16;
+    cudaError_t e = cudaMalloc(&p, nbytes);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw Error(INTI_E_NOMEM, std::string("cudaMalloc(") + std::to_string(nbytes) +
+                                    "): " + cudaGetErrorString(e));
+    }
+    bytes = nbytes;
+  }
+  template <class T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+
+}  // namespace inti
+
+struct inti_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int num_sms = 148;
+  std::recursive_mutex mu;
+  std::string last_error;
+  int64_t launches = 0;
+  inti::DevBuf err_flag;  // device int: nonzero when a bounded wait ran out
+  // per-kernel-class event timing (inti_ctx_set_profiling)
+  bool profiling = false;
+  struct Span {
+    std::string name;
+    cudaEvent_t a, b;
+  };
+  std::vector<Span> spans;
+  std::map<std::string, std::pair<double, int64_t>> prof_totals;
+};
+
+struct inti_quad {
+  inti_ctx* ctx = nullptr;
+  int dim = 3;
+  int64_t n = 0;
+  int32_t nq = 0;
+  bool has_normals = false;
+  // device copies: coords/normals dim x n (AoS), weights n
+  inti::DevBuf coords, normals, weights;
+  std::vector<double> h_coords, h_normals, h_weights;  // host copies for setup work
+};
+
+struct inti_csr {
+  inti_ctx* ctx = nullptr;
+  int64_t m = 0, n = 0, nnz = 0;
+  int dtype = INTI_F64;
+  inti::DevBuf rowptr, col, val;
+};
+
+namespace inti {
+
+// Records a CUDA event pair around the launches issued in its scope when the
+// context is profiling.
+struct ProfScope {
+  inti_ctx* ctx;
+  cudaEvent_t b = nullptr;
+  const char* name;
+  ProfScope(inti_ctx* c, const char* n) : ctx(c), name(n) {
+    if (!ctx->profiling) return;
+    cudaEvent_t a;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+      b = nullptr;
+      return;
+    }
+    cudaEventRecord(a, ctx->stream);
+    ctx->spans.push_back({name, a, b});
+  }
+  ~ProfScope() {
+    if (b) cudaEventRecord(b, ctx->stream);
+  }
+};
+
+// Launch plumbing implemented in the .cu files.
+enum Pde { LAPLACE = INTI_LAPLACE, HELMHOLTZ = INTI_HELMHOLTZ };
+enum Kind { SL = INTI_SL, DL = INTI_DL, ADL = INTI_ADL, HS = INTI_HS };
+
+// Per-apply description of the pair product A*x for one right-hand side.
+struct PairLaunch {
+  int pde, kind, dim, precision;
+  double k;
+  int64_t m, n;
+  const double* tcoords;   // dim x m
+  const double* tnormals;  // dim x m or null
+  const double* scoords;   // dim x n
+  const double* snormals;  // dim x n or null
+  const double* sweights;  // n
+  const double* x;         // density, n (x2 complex)
+  void* packed;            // scratch: packed source records (n padded)
+  void* partial;           // scratch: split x m accumulators
+  int split;               // number of source chunks (computed by plan)
+  int64_t n_tiles;         // padded source tiles
+  int* err_flag;
+};
+
+// Source records per tile (must match the kernel template parameter).
+int pair_tile(int precision);
+// Bytes of one packed source record.
+int pair_record_bytes(int pde, int kind, int dim, int precision);
+// Bytes of one partial accumulator per target per split.
+int pair_partial_bytes(int pde, int precision);
+// Choose the split for a problem on this device.
+int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
+                    int64_t n);
+// Enqueue pack + pair kernels (results in L.partial); returns launches.
+int pair_launch(inti_ctx* ctx, const PairLaunch& L);
+// y = alpha*(scale*sum_s partial + C x) + beta*y; complex when cplx.
+int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x,
+                  double* y, const double* alpha, const double* beta);
+// Dense assembly of A.
+int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out);
+// Transpose apply partials: y_j = sum_i K(x_i,y_j) w_j x_i.
+int pair_transpose_launch(inti_ctx* ctx, const PairLaunch& L);
+
+// CSR: y = alpha*C*x + beta*y (alpha/beta complex pairs); transpose via col scatter.
+int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, const double* alpha,
+              const double* beta);
+
+}  // namespace inti

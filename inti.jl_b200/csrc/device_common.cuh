@@ -1,0 +1,151 @@
+// Device-side helpers shared by the kernels: the Laplace / Helmholtz kernel
+// values in FP64 (generic form, used off the hot loop), the bulk-copy (TMA)
+// and mbarrier primitives with bounded waits, and warp reductions.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "common.h"
+
+namespace inti {
+
+// ---------------------------------------------------------------------------
+// Generic kernel values K(x, y) with the reference's constants
+// (src/kernels.jl:137-204 Laplace, :347-413 Helmholtz 3D); zero when
+// |x - y| <= 1e-14 (src/utils.jl:235).  Returned as (re, im).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ double dotd(const double* a, const double* b) {
+  double s = a[0] * b[0];
+#pragma unroll
+  for (int i = 1; i < DIM; ++i) s = fma(a[i], b[i], s);
+  return s;
+}
+
+template <int PDE, int KIND, int DIM>
+__device__ __forceinline__ double2 kernel_value(const double* x, const double* nx,
+                                                const double* y, const double* ny, double k) {
+  double r[DIM];
+#pragma unroll
+  for (int i = 0; i < DIM; ++i) r[i] = x[i] - y[i];
+  const double d2 = dotd<DIM>(r, r);
+  if (!(d2 > kSamePointTol2)) return make_double2(0.0, 0.0);
+  const double d = sqrt(d2);
+  if (PDE == LAPLACE) {
+    if (KIND == SL) {
+      if (DIM == 2) return make_double2(-log(d) / (2 * kPi), 0.0);
+      return make_double2(1.0 / (4 * kPi) / d, 0.0);
+    } else if (KIND == DL) {
+      const double c = DIM == 2 ? 1.0 / (2 * kPi) / d2 : 1.0 / (4 * kPi) / (d2 * d);
+      return make_double2(c * dotd<DIM>(r, ny), 0.0);
+    } else if (KIND == ADL) {
+      const double c = DIM == 2 ? -1.0 / (2 * kPi) / d2 : -1.0 / (4 * kPi) / (d2 * d);
+      return make_double2(c * dotd<DIM>(r, nx), 0.0);
+    } else {
+      const double id2 = 1.0 / d2;
+      const double nxdny = dotd<DIM>(nx, ny), rdnx = dotd<DIM>(r, nx), rdny = dotd<DIM>(r, ny);
+      if (DIM == 2) return make_double2(id2 / (2 * kPi) * (nxdny - 2 * rdnx * rdny * id2), 0.0);
+      return make_double2(id2 / (4 * kPi * d) * (nxdny - 3 * rdnx * rdny * id2), 0.0);
+    }
+  } else {
+    double s, c;
+    sincos(k * d, &s, &c);
+    const double inv4pi = 1.0 / (4 * kPi);
+    if (KIND == SL) {
+      const double g = inv4pi / d;
+      return make_double2(g * c, g * s);
+    }
+    // e^{ikd} (1/d - ik) = (c/d + k s) + i (s/d - k c)
+    const double id = 1.0 / d;
+    const double er = c * id + k * s, ei = s * id - k * c;
+    if (KIND == DL || KIND == ADL) {
+      const double rn = KIND == DL ? dotd<3>(r, ny) : -dotd<3>(r, nx);
+      const double g = inv4pi / d2 * rn;
+      return make_double2(g * er, g * ei);
+    }
+    // HS: a (r.nx)(r.ny) + b nx.ny
+    const double rdnx = dotd<3>(r, nx), rdny = dotd<3>(r, ny), nxdny = dotd<3>(nx, ny);
+    const double id2 = 1.0 / d2;
+    // b = e^{ikd} id2/(4pi) (1/d - ik)
+    const double br = er * id2 * inv4pi, bi = ei * id2 * inv4pi;
+    // a = e^{ikd} id2^2/(4 pi d) (3(ikd - 1) + k^2 d^2)
+    const double fr = -3.0 + k * k * d2, fi = 3.0 * k * d;
+    const double sa = id2 * id2 * inv4pi * id;
+    const double ar = sa * (c * fr - s * fi), ai = sa * (c * fi + s * fr);
+    const double t = rdnx * rdny;
+    return make_double2(ar * t + br * nxdny, ai * t + bi * nxdny);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Bulk asynchronous copies global -> shared (cp.async.bulk, the TMA engine)
+// completed on an mbarrier, with waits bounded by an iteration limit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// dst (shared) and src (global) 16-byte aligned, bytes a multiple of 16.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes,
+                                              uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Upper bound on polls of one barrier phase (each poll may suspend the
+// thread for a hardware-chosen interval); far beyond any healthy copy.
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+// Error codes written to the context's device flag.
+constexpr int kErrWaitTimeout = 1;
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+}  // namespace inti

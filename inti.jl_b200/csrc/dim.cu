@@ -1,0 +1,477 @@
+// Boundary density-interpolation (BDIM) correction built on the GPU, for
+// target === source (src/bdim.jl:50-196 with the X === Y branch of
+// etype_to_nearest_points, src/quadrature.jl:249-256):
+//
+//  1. ns = ceil(3*nq) monopole centres on a circle/sphere of radius
+//     1.5*|bbox diagonal|/2 about the bounding-box centre (bdim.jl:79-92,
+//     utils.jl:142-171) — host, O(n).
+//  2. traces g0[j,k] = G(y_j, xs_k), g1[j,k] = ADL(y_j, xs_k) (bdim.jl:94-103).
+//  3. Theta = mu*B(x) + S*g1 - D*g0 (bdim.jl:104-118): a multi-right-hand-side
+//     pair product over all node pairs, S and D being the uncorrected Nystrom
+//     operators (entries K*w), evaluated on the fly and never stored.
+//  4. per element: Householder QR of M^T = [g0[el,:]; g1[el,:]]^T (ns x 2nq)
+//     and least squares for each of the element's nq nodes (bdim.jl:154-185);
+//     one warp per element, lane l owning row l.
+//  5. values dS[i, e*nq+a] = -W[nq+a], dD[i, e*nq+a] = W[a] (bdim.jl:176-179)
+//     written straight into CSR arrays with the element-block pattern.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.h"
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace inti {
+
+// Scalar abstraction: double (Laplace) or double2 (Helmholtz).
+template <bool CPLX>
+struct S;
+template <>
+struct S<false> {
+  using T = double;
+  static __device__ __forceinline__ T from(double2 v) { return v.x; }
+  static __device__ __forceinline__ T zero() { return 0.0; }
+  static __device__ __forceinline__ T one() { return 1.0; }
+  static __device__ __forceinline__ T mul(T a, T b) { return a * b; }
+  static __device__ __forceinline__ T cmul(T a, T b) { return a * b; }  // conj(a)*b
+  static __device__ __forceinline__ T add(T a, T b) { return a + b; }
+  static __device__ __forceinline__ T sub(T a, T b) { return a - b; }
+  static __device__ __forceinline__ T scale(T a, double s) { return a * s; }
+  static __device__ __forceinline__ double abs2(T a) { return a * a; }
+  static __device__ __forceinline__ double re(T a) { return a; }
+  static __device__ __forceinline__ double im(T) { return 0.0; }
+  static __device__ __forceinline__ T conj(T a) { return a; }
+  static __device__ __forceinline__ T div(T a, T b) { return a / b; }
+  static __device__ __forceinline__ T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
+  static __device__ __forceinline__ T wsum(T v) { return warp_sum(v); }
+  static __device__ __forceinline__ T neg(T a) { return -a; }
+};
+template <>
+struct S<true> {
+  using T = double2;
+  static __device__ __forceinline__ T from(double2 v) { return v; }
+  static __device__ __forceinline__ T zero() { return make_double2(0.0, 0.0); }
+  static __device__ __forceinline__ T one() { return make_double2(1.0, 0.0); }
+  static __device__ __forceinline__ T mul(T a, T b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+  }
+  static __device__ __forceinline__ T cmul(T a, T b) {
+    return make_double2(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
+  }
+  static __device__ __forceinline__ T add(T a, T b) { return make_double2(a.x + b.x, a.y + b.y); }
+  static __device__ __forceinline__ T sub(T a, T b) { return make_double2(a.x - b.x, a.y - b.y); }
+  static __device__ __forceinline__ T scale(T a, double s) { return make_double2(a.x * s, a.y * s); }
+  static __device__ __forceinline__ double abs2(T a) { return a.x * a.x + a.y * a.y; }
+  static __device__ __forceinline__ double re(T a) { return a.x; }
+  static __device__ __forceinline__ double im(T a) { return a.y; }
+  static __device__ __forceinline__ T conj(T a) { return make_double2(a.x, -a.y); }
+  static __device__ __forceinline__ T div(T a, T b) {
+    const double d = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+  }
+  static __device__ __forceinline__ T shfl(T v, int src) {
+    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+  }
+  static __device__ __forceinline__ T wsum(T v) { return make_double2(warp_sum(v.x), warp_sum(v.y)); }
+  static __device__ __forceinline__ T neg(T a) { return make_double2(-a.x, -a.y); }
+};
+
+// ---------------------------------------------------------------------------
+// 2. traces: g0/g1 are n x ns, row-major (ns contiguous per node).
+// ---------------------------------------------------------------------------
+template <int PDE, int DIM>
+__global__ void dim_traces(int64_t n, int ns, const double* __restrict__ x,
+                           const double* __restrict__ nrm, const double* __restrict__ xs, double k,
+                           double2* __restrict__ g0, double2* __restrict__ g1) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * ns) return;
+  const int64_t j = t / ns;
+  const int kk = (int)(t % ns);
+  g0[t] = kernel_value<PDE, SL, DIM>(x + DIM * j, nrm + DIM * j, xs + DIM * kk, nullptr, k);
+  g1[t] = kernel_value<PDE, ADL, DIM>(x + DIM * j, nrm + DIM * j, xs + DIM * kk, nullptr, k);
+}
+
+// ---------------------------------------------------------------------------
+// 3. Theta partials: for targets i (one per thread) and a chunk of sources,
+//    acc[k] = sum_j (K_S(x_i,y_j) w_j) g1[j,k] - (K_D(x_i,y_j) w_j) g0[j,k].
+//    Source data and trace rows are staged in shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kThetaBlock = 128;
+constexpr int kThetaTile = 32;
+
+template <int PDE, int DIM, bool DERIV, int NS>
+__global__ void __launch_bounds__(kThetaBlock) dim_theta(
+    int64_t n, int ns, const double* __restrict__ x, const double* __restrict__ nrm,
+    const double* __restrict__ w, const double2* __restrict__ g0, const double2* __restrict__ g1,
+    double k, int tiles_per_split, double2* __restrict__ partial) {
+  constexpr bool CPLX = PDE == HELMHOLTZ;
+  using Sc = S<CPLX>;
+  using T = typename Sc::T;
+  constexpr int KS = DERIV ? ADL : SL;
+  constexpr int KD = DERIV ? HS : DL;
+  __shared__ double sx[kThetaTile * DIM], sn[kThetaTile * DIM], sw[kThetaTile];
+  __shared__ T s0[kThetaTile * NS], s1[kThetaTile * NS];
+  const int64_t i = blockIdx.x * (int64_t)kThetaBlock + threadIdx.x;
+  const int64_t ii = min(i, n - 1);
+  double xi[DIM], ni[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    xi[c] = x[DIM * ii + c];
+    ni[c] = nrm[DIM * ii + c];
+  }
+  T acc[NS];
+#pragma unroll
+  for (int q = 0; q < NS; ++q) acc[q] = Sc::zero();
+  const int64_t ntile = (n + kThetaTile - 1) / kThetaTile;
+  const int64_t t0 = (int64_t)blockIdx.y * tiles_per_split;
+  const int64_t t1 = min(ntile, t0 + tiles_per_split);
+  for (int64_t t = t0; t < t1; ++t) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < kThetaTile; q += kThetaBlock) {
+      const int64_t j = t * kThetaTile + q;
+      const bool in = j < n;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        sx[q * DIM + c] = in ? x[DIM * j + c] : 0.0;
+        sn[q * DIM + c] = in ? nrm[DIM * j + c] : 0.0;
+      }
+      sw[q] = in ? w[j] : 0.0;
+    }
+    for (int q = threadIdx.x; q < kThetaTile * NS; q += kThetaBlock) {
+      const int a = q / NS, kk = q % NS;
+      const int64_t j = t * kThetaTile + a;
+      const bool in = j < n && kk < ns;
+      s0[q] = in ? Sc::from(g0[j * ns + kk]) : Sc::zero();
+      s1[q] = in ? Sc::from(g1[j * ns + kk]) : Sc::zero();
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int a = 0; a < kThetaTile; ++a) {
+      const double wj = sw[a];
+      const T sv = Sc::scale(Sc::from(kernel_value<PDE, KS, DIM>(xi, ni, &sx[a * DIM], &sn[a * DIM], k)), wj);
+      const T dv = Sc::scale(Sc::from(kernel_value<PDE, KD, DIM>(xi, ni, &sx[a * DIM], &sn[a * DIM], k)), wj);
+#pragma unroll
+      for (int q = 0; q < NS; ++q)
+        acc[q] = Sc::sub(Sc::add(acc[q], Sc::mul(sv, s1[a * NS + q])), Sc::mul(dv, s0[a * NS + q]));
+    }
+  }
+  if (i < n) {
+    double2* out = partial + ((int64_t)blockIdx.y * n + i) * ns;
+#pragma unroll
+    for (int q = 0; q < NS; ++q)
+      if (q < ns) out[q] = make_double2(Sc::re(acc[q]), Sc::im(acc[q]));
+  }
+}
+
+// theta[i,k] = mu_i * B(x_i, xs_k) + sum_s partial[s][i][k]
+template <int PDE, int DIM, bool DERIV>
+__global__ void dim_theta_reduce(int64_t n, int ns, int split, const double* __restrict__ x,
+                                 const double* __restrict__ nrm, const double* __restrict__ xs,
+                                 const double* __restrict__ mu, double k,
+                                 const double2* __restrict__ partial, double2* __restrict__ theta) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (t >= n * ns) return;
+  const int64_t i = t / ns;
+  const int kk = (int)(t % ns);
+  const double2 b = kernel_value<PDE, DERIV ? ADL : SL, DIM>(x + DIM * i, nrm + DIM * i,
+                                                             xs + DIM * kk, nullptr, k);
+  const double m = mu ? mu[i] : -0.5;
+  double sr = m * b.x, si = m * b.y;
+  for (int s = 0; s < split; ++s) {
+    const double2 v = partial[(int64_t)s * n * ns + t];
+    sr += v.x;
+    si += v.y;
+  }
+  theta[t] = make_double2(sr, si);
+}
+
+// ---------------------------------------------------------------------------
+// 4-5. per-element least squares.  Lane l owns row l of A = M^T (ns x 2NQ):
+// A[l][a] = g0[e*nq+a][l], A[l][NQ+a] = g1[e*nq+a][l].  Householder vectors
+// follow the LAPACK xLARFG convention (H = I - tau v v^H, v_k = 1, real beta).
+// ---------------------------------------------------------------------------
+template <bool CPLX, int NQ>
+__global__ void dim_lsq(int64_t nel, int ns, const double2* __restrict__ g0,
+                        const double2* __restrict__ g1, const double2* __restrict__ theta,
+                        double* __restrict__ dS, double* __restrict__ dD) {
+  using Sc = S<CPLX>;
+  using T = typename Sc::T;
+  constexpr int NC = 2 * NQ;
+  const int lane = threadIdx.x & 31;
+  const int64_t e = blockIdx.x * (int64_t)(blockDim.x / 32) + threadIdx.x / 32;
+  if (e >= nel) return;  // whole warp leaves together
+  const bool row = lane < ns;
+  T A[NC];
+#pragma unroll
+  for (int a = 0; a < NQ; ++a) {
+    const int64_t j = e * NQ + a;
+    A[a] = row ? Sc::from(g0[j * ns + lane]) : Sc::zero();
+    A[NQ + a] = row ? Sc::from(g1[j * ns + lane]) : Sc::zero();
+  }
+  T tau[NC];
+#pragma unroll
+  for (int kc = 0; kc < NC; ++kc) {
+    // x = A[kc:, kc]; alpha = A[kc][kc]
+    const T alpha = Sc::shfl(A[kc], kc);
+    const double xn2 = warp_sum((row && lane > kc) ? Sc::abs2(A[kc]) : 0.0);
+    if (xn2 == 0.0 && Sc::im(alpha) == 0.0) {
+      tau[kc] = Sc::zero();
+      continue;
+    }
+    const double nrm = sqrt(Sc::abs2(alpha) + xn2);
+    const double beta = Sc::re(alpha) >= 0 ? -nrm : nrm;
+    T tk;
+    if (CPLX) {
+      tk = Sc::from(make_double2((beta - Sc::re(alpha)) / beta, -Sc::im(alpha) / beta));
+    } else {
+      tk = Sc::from(make_double2((beta - Sc::re(alpha)) / beta, 0.0));
+    }
+    tau[kc] = tk;
+    const T ab = Sc::sub(alpha, Sc::from(make_double2(beta, 0.0)));
+    if (lane > kc) A[kc] = Sc::div(A[kc], ab);
+    if (lane == kc) A[kc] = Sc::from(make_double2(beta, 0.0));
+    // trailing columns: s = conj(tau) * (A[kc][j] + sum_{l>kc} conj(v_l) A[l][j])
+#pragma unroll
+    for (int j = kc + 1; j < NC; ++j) {
+      T contrib = (row && lane > kc) ? Sc::cmul(A[kc], A[j]) : Sc::zero();
+      if (lane == kc) contrib = A[j];
+      const T s = Sc::cmul(tk, Sc::wsum(contrib));
+      if (lane == kc) A[j] = Sc::sub(A[j], s);
+      if (row && lane > kc) A[j] = Sc::sub(A[j], Sc::mul(s, A[kc]));
+    }
+  }
+  // solve for each of the element's own nodes (targets)
+  for (int t = 0; t < NQ; ++t) {
+    const int64_t i = e * NQ + t;
+    T b = row ? Sc::from(theta[i * ns + lane]) : Sc::zero();
+#pragma unroll
+    for (int kc = 0; kc < NC; ++kc) {
+      T contrib = (row && lane > kc) ? Sc::cmul(A[kc], b) : Sc::zero();
+      if (lane == kc) contrib = b;
+      const T s = Sc::cmul(tau[kc], Sc::wsum(contrib));
+      if (lane == kc) b = Sc::sub(b, s);
+      if (row && lane > kc) b = Sc::sub(b, Sc::mul(s, A[kc]));
+    }
+    // back substitution R W = (Q^H b)[0:NC]; lane c holds row c of R
+    T W[NC];
+#pragma unroll
+    for (int c = NC - 1; c >= 0; --c) {
+      T s = b;
+#pragma unroll
+      for (int j = c + 1; j < NC; ++j) s = Sc::sub(s, Sc::mul(A[j], W[j]));
+      const T wc = Sc::div(s, A[c]);
+      W[c] = Sc::shfl(wc, c);
+    }
+    if (lane < NQ) {
+      // row i of the CSR holds columns e*NQ .. e*NQ+NQ-1 in order
+      T vS = Sc::zero(), vD = Sc::zero();
+#pragma unroll
+      for (int a = 0; a < NQ; ++a)
+        if (a == lane) {
+          vS = Sc::neg(W[NQ + a]);
+          vD = W[a];
+        }
+      const int64_t p = i * NQ + lane;
+      if (CPLX) {
+        dS[2 * p] = Sc::re(vS);
+        dS[2 * p + 1] = Sc::im(vS);
+        dD[2 * p] = Sc::re(vD);
+        dD[2 * p + 1] = Sc::im(vD);
+      } else {
+        dS[p] = Sc::re(vS);
+        dD[p] = Sc::re(vD);
+      }
+    }
+  }
+}
+
+__global__ void block_pattern(int64_t n, int nq, int64_t* rowptr, int32_t* col) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i > n) return;
+  rowptr[i] = i * nq;
+  if (i == n) return;
+  const int64_t e = i / nq;
+  for (int a = 0; a < nq; ++a) col[i * nq + a] = (int32_t)(e * nq + a);
+}
+
+// ---------------------------------------------------------------------------
+// host driver
+// ---------------------------------------------------------------------------
+template <int NS, class F>
+static bool ns_bucket(int ns, F&& f) {
+  if (ns <= NS) {
+    f(std::integral_constant<int, NS>());
+    return true;
+  }
+  return false;
+}
+
+template <class F>
+static void nq_dispatch(int nq, F&& f) {
+  switch (nq) {
+    case 1: return f(std::integral_constant<int, 1>());
+    case 2: return f(std::integral_constant<int, 2>());
+    case 3: return f(std::integral_constant<int, 3>());
+    case 4: return f(std::integral_constant<int, 4>());
+    case 5: return f(std::integral_constant<int, 5>());
+    case 6: return f(std::integral_constant<int, 6>());
+    case 7: return f(std::integral_constant<int, 7>());
+    case 8: return f(std::integral_constant<int, 8>());
+    case 9: return f(std::integral_constant<int, 9>());
+    case 10: return f(std::integral_constant<int, 10>());
+  }
+  throw Error(INTI_E_UNSUPPORTED, "DIM correction supports 1..10 nodes per element");
+}
+
+void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
+                    int derivative, const double* green_multiplier, inti_csr** dS,
+                    inti_csr** dD) {
+  if (!q) throw Error(INTI_E_ARG, "quadrature is NULL");
+  if (q->ctx != ctx) throw Error(INTI_E_STATE, "quadrature belongs to another context");
+  if (!q->has_normals) throw Error(INTI_E_ARG, "DIM needs a quadrature with normals");
+  if (q->nq <= 0) throw Error(INTI_E_ARG, "DIM needs the element structure (nq > 0)");
+  if (pde != INTI_LAPLACE && pde != INTI_HELMHOLTZ) throw Error(INTI_E_ARG, "unknown pde");
+  if (pde == INTI_HELMHOLTZ && q->dim != 3) throw Error(INTI_E_UNSUPPORTED, "Helmholtz is 3D only");
+  if (pde == INTI_HELMHOLTZ && k_im != 0.0) throw Error(INTI_E_UNSUPPORTED, "complex wavenumbers are not implemented");
+  const int dim = q->dim;
+  const int64_t n = q->n;
+  const int nq = q->nq;
+  const int64_t nel = n / nq;
+  const int ns = (int)std::ceil(3.0 * nq);  // bdim.jl:79-80
+  if (ns > 32) throw Error(INTI_E_UNSUPPORTED, "ns > 32");
+  const bool cplx = pde == INTI_HELMHOLTZ;
+  if (green_multiplier)
+    for (int64_t i = 0; i < n; ++i)
+      if (!std::isfinite(green_multiplier[i])) throw Error(INTI_E_NONFINITE, "green_multiplier contains NaN/Inf");
+
+  // 1. monopole centres (bdim.jl:82-92; utils.jl:142-171)
+  double lc[3] = {INFINITY, INFINITY, INFINITY}, hc[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t j = 0; j < n; ++j)
+    for (int c = 0; c < dim; ++c) {
+      lc[c] = std::min(lc[c], q->h_coords[dim * j + c]);
+      hc[c] = std::max(hc[c], q->h_coords[dim * j + c]);
+    }
+  double xc[3] = {0, 0, 0}, diag2 = 0.0;
+  for (int c = 0; c < dim; ++c) {
+    xc[c] = (lc[c] + hc[c]) / 2;
+    diag2 += (hc[c] - lc[c]) * (hc[c] - lc[c]);
+  }
+  const double R = 1.5 * std::sqrt(diag2) / 2;
+  std::vector<double> xs((size_t)ns * dim);
+  if (dim == 2) {
+    for (int i = 0; i < ns; ++i) {
+      xs[2 * i] = R * std::cos(2 * kPi * i / ns) + xc[0];
+      xs[2 * i + 1] = R * std::sin(2 * kPi * i / ns) + xc[1];
+    }
+  } else {
+    const double phi = kPi * (3 - std::sqrt(5.0));
+    for (int i = 1; i <= ns; ++i) {
+      const double ytmp = 1 - ((double)(i - 1) / (double)(ns - 1)) * 2;
+      const double radius = std::sqrt(1 - ytmp * ytmp);
+      const double theta = phi * i;
+      xs[3 * (i - 1)] = std::cos(theta) * radius * R + xc[0];
+      xs[3 * (i - 1) + 1] = ytmp * R + xc[1];
+      xs[3 * (i - 1) + 2] = std::sin(theta) * radius * R + xc[2];
+    }
+  }
+  DevBuf d_xs, d_mu, g0, g1, theta, part;
+  d_xs.ensure(sizeof(double) * xs.size());
+  INTI_CUDA(cudaMemcpyAsync(d_xs.p, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice, ctx->stream));
+  if (green_multiplier) {
+    d_mu.ensure(sizeof(double) * n);
+    INTI_CUDA(cudaMemcpyAsync(d_mu.p, green_multiplier, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  g0.ensure(sizeof(double2) * n * ns);
+  g1.ensure(sizeof(double2) * n * ns);
+  theta.ensure(sizeof(double2) * n * ns);
+  const double* X = q->coords.as<double>();
+  const double* NR = q->normals.as<double>();
+  const double* W = q->weights.as<double>();
+
+  auto run = [&](auto pde_c, auto dim_c) {
+    constexpr int P = decltype(pde_c)::value;
+    constexpr int D = decltype(dim_c)::value;
+    const int64_t tot = n * ns;
+    dim_traces<P, D><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
+        n, ns, X, NR, d_xs.as<double>(), k_re, g0.as<double2>(), g1.as<double2>());
+    ctx->launches++;
+    // Theta split over sources so the grid covers the device
+    const int64_t blocks = (n + kThetaBlock - 1) / kThetaBlock;
+    const int64_t ntile = (n + kThetaTile - 1) / kThetaTile;
+    const int64_t want = (int64_t)ctx->num_sms * 6;
+    int split = (int)std::max<int64_t>(1, std::min<int64_t>({ntile, (want + blocks - 1) / blocks, 64}));
+    const int tps = (int)((ntile + split - 1) / split);
+    split = (int)((ntile + tps - 1) / tps);
+    part.ensure(sizeof(double2) * (size_t)split * n * ns);
+    auto theta_go = [&](auto nsb, auto deriv_c) {
+      constexpr int NSB = decltype(nsb)::value;
+      constexpr bool DV = decltype(deriv_c)::value;
+      dim3 grid((unsigned)blocks, (unsigned)split);
+      ProfScope pd(ctx, "dim");
+      dim_theta<P, D, DV, NSB><<<grid, kThetaBlock, 0, ctx->stream>>>(
+          n, ns, X, NR, W, g0.as<double2>(), g1.as<double2>(), k_re, tps, part.as<double2>());
+      ctx->launches++;
+      dim_theta_reduce<P, D, DV><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
+          n, ns, split, X, NR, d_xs.as<double>(), green_multiplier ? d_mu.as<double>() : nullptr,
+          k_re, part.as<double2>(), theta.as<double2>());
+      ctx->launches++;
+    };
+    auto by_ns = [&](auto deriv_c) {
+      if (ns_bucket<8>(ns, [&](auto b) { theta_go(b, deriv_c); })) return;
+      if (ns_bucket<16>(ns, [&](auto b) { theta_go(b, deriv_c); })) return;
+      if (ns_bucket<24>(ns, [&](auto b) { theta_go(b, deriv_c); })) return;
+      ns_bucket<32>(ns, [&](auto b) { theta_go(b, deriv_c); });
+    };
+    if (derivative)
+      by_ns(std::true_type());
+    else
+      by_ns(std::false_type());
+  };
+  if (pde == INTI_LAPLACE && dim == 2)
+    run(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, 2>());
+  else if (pde == INTI_LAPLACE)
+    run(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, 3>());
+  else
+    run(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, 3>());
+  INTI_CUDA(cudaGetLastError());
+
+  // output CSR handles with the element-block pattern
+  const int comps = cplx ? 2 : 1;
+  const int64_t nnz = n * nq;
+  std::unique_ptr<inti_csr> cS(new inti_csr()), cD(new inti_csr());
+  for (auto* c : {cS.get(), cD.get()}) {
+    c->ctx = ctx;
+    c->m = n;
+    c->n = n;
+    c->nnz = nnz;
+    c->dtype = cplx ? INTI_C128 : INTI_F64;
+    c->rowptr.ensure(sizeof(int64_t) * (n + 1));
+    c->col.ensure(sizeof(int32_t) * nnz);
+    c->val.ensure(sizeof(double) * comps * nnz);
+  }
+  block_pattern<<<(unsigned)((n + 1 + 255) / 256), 256, 0, ctx->stream>>>(n, nq, cS->rowptr.as<int64_t>(), cS->col.as<int32_t>());
+  ctx->launches++;
+  INTI_CUDA(cudaMemcpyAsync(cD->rowptr.p, cS->rowptr.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, ctx->stream));
+  INTI_CUDA(cudaMemcpyAsync(cD->col.p, cS->col.p, sizeof(int32_t) * nnz, cudaMemcpyDeviceToDevice, ctx->stream));
+  nq_dispatch(nq, [&](auto nqc) {
+    constexpr int NQ = decltype(nqc)::value;
+    const int warps = 4;
+    const unsigned grid = (unsigned)((nel + warps - 1) / warps);
+    if (cplx)
+      dim_lsq<true, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(nel, ns, g0.as<double2>(), g1.as<double2>(),
+                                                              theta.as<double2>(), cS->val.as<double>(), cD->val.as<double>());
+    else
+      dim_lsq<false, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(nel, ns, g0.as<double2>(), g1.as<double2>(),
+                                                               theta.as<double2>(), cS->val.as<double>(), cD->val.as<double>());
+    ctx->launches++;
+  });
+  INTI_CUDA(cudaGetLastError());
+  sync_and_check(ctx);
+  *dS = cS.release();
+  *dD = cD.release();
+}
+
+}  // namespace inti

@@ -1,0 +1,57 @@
+// Operator handle and the functions the C ABI layer calls into.  Internal.
+#pragma once
+
+#include <memory>
+
+#include "common.h"
+
+struct inti_op {
+  inti_ctx* ctx = nullptr;
+  int pde = INTI_LAPLACE, kind = INTI_SL, dim = 3, precision = INTI_FP64;
+  double k = 0.0;
+  const inti_quad* target = nullptr;
+  const inti_quad* source = nullptr;
+  const inti_csr* corr = nullptr;
+  std::unique_ptr<inti_csr> corrT;  // transposed correction, built on first A^T apply
+  // scratch owned by the operator
+  inti::DevBuf packed;    // packed source records, n_tiles * tile
+  inti::DevBuf partial;   // split x m accumulators
+  inti::DevBuf xbuf, ybuf;  // staging for host-pointer applies
+  inti::DevBuf tpartial;  // transpose: tsplit x n double2
+  int split = 1;
+  int tsplit = 1;
+  int64_t n_tiles = 1;
+};
+
+namespace inti {
+
+void sync_and_check(inti_ctx* ctx);
+PairLaunch make_launch(inti_op* op, const double* xdev);
+void op_apply_device(inti_op* op, const double* x, double* y, const double* alpha,
+                     const double* beta);
+void op_apply_transpose_device(inti_op* op, const double* x, double* y, const double* alpha,
+                               const double* beta);
+inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
+                   const inti_quad* target, const inti_quad* source, const inti_csr* correction,
+                   int precision);
+void op_prepare_transpose(inti_op* op);
+void transpose_epilogue(inti_ctx* ctx, int64_t n, int split, const void* partial,
+                        const inti_csr* corrT, const double* x, double* y, const double* alpha,
+                        const double* beta, bool cplx);
+inti_csr* csr_create_host(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz,
+                          const int64_t* rowptr, const int32_t* col, const double* val,
+                          int dtype);
+std::unique_ptr<inti_csr> csr_transpose(inti_ctx* ctx, const inti_csr* c);
+
+void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
+                    int derivative, const double* green_multiplier, inti_csr** dS,
+                    inti_csr** dD);
+void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const double* coefs,
+                 const double* shift, const double* b, double* x, double rtol, int32_t restart,
+                 int32_t maxiter, int32_t mode, int on_device, double* history,
+                 inti_gmres_stats* stats);
+void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsigma,
+                  double* dcoords, double* dnormals, double* dweights, int on_device);
+void measure_peaks(inti_ctx* ctx, double* fp64, double* fp32, double* mufu);
+
+}  // namespace inti

@@ -1,0 +1,785 @@
+// On-the-fly Nyström pair product y = A x, A_ij = K(x_i, y_j) w_j
+// (src/nystrom.jl:93-96 entries; src/nystrom.jl:117-124 is the CPU loop it
+// replaces), for the Laplace (2D/3D) and Helmholtz (3D) single-layer,
+// double-layer, adjoint-double-layer and hypersingular kernels
+// (src/kernels.jl:137-204, 347-413).
+//
+// Design (B200, sm_100a):
+//  * A pack kernel folds the density into per-source records
+//    (coordinates + w*sigma, or the dipole w*sigma*n for DL/HS), padded to
+//    whole tiles with zero charges.
+//  * The pair kernel gives each thread TPT targets held in registers.  Source
+//    tiles are streamed into shared memory by the TMA bulk-copy engine
+//    (cp.async.bulk + mbarrier, two stages, one elected thread issues) and
+//    read back as broadcasts.  Each CTA covers one target block and one chunk
+//    of the source tiles (grid.y = split), so every SM stays busy even when
+//    the target count is small; partial sums go to scratch and are reduced in
+//    a fixed order by the epilogue (deterministic, no atomics).
+//  * FP64 form: FP64 pairs and sums.  FP32C form: FP32 pairs, summed in FP32
+//    over groups of 32 sources, groups folded into a (sum, compensation)
+//    pair with Knuth's TwoSum (error-free), so the long sum over N sources
+//    carries no O(N eps) growth.
+//  * The epilogue applies the kernel constant, alpha/beta, and the CSR
+//    correction row in the same pass (the fused near-field correction).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.h"
+#include "device_common.cuh"
+
+namespace inti {
+
+constexpr int kBlock = 128;  // threads per CTA
+constexpr int kTPT = 2;      // targets per thread
+constexpr int kTile64 = 128; // sources per shared-memory stage (FP64)
+constexpr int kTile32 = 256; // sources per shared-memory stage (FP32C)
+constexpr int kGroup = 32;   // FP32C: sources summed before a compensated fold
+
+// ---------------------------------------------------------------------------
+// Source record layouts (elements of R per source):
+//   Laplace  SL/ADL : x y [z] q            (q = w*sigma)
+//   Laplace  DL/HS  : x y [z] p_x p_y [p_z] (p = w*sigma*n_y)
+//   Helmholtz SL/ADL: x y z qr qi
+//   Helmholtz DL/HS : x y z pr_x pr_y pr_z pi_x pi_y pi_z
+// each padded so that a record is a multiple of 16 bytes.
+// ---------------------------------------------------------------------------
+template <int PDE, int KIND, int DIM, class R>
+struct Rec {
+  static constexpr bool dipole = (KIND == DL || KIND == HS);
+  static constexpr bool cplx = (PDE == HELMHOLTZ);
+  static constexpr int used = DIM + (cplx ? 2 : 1) * (dipole ? DIM : 1);
+  static constexpr int align = 16 / sizeof(R);
+  static constexpr int n = (used + align - 1) / align * align;
+  static constexpr bool tnormal = (KIND == ADL || KIND == HS);
+};
+
+template <int PDE, int KIND, int DIM, class R>
+__global__ void pack_sources(int64_t n, int64_t npad, const double* __restrict__ xs,
+                             const double* __restrict__ ns, const double* __restrict__ w,
+                             const double* __restrict__ sigma, R* __restrict__ out) {
+  using RC = Rec<PDE, KIND, DIM, R>;
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= npad) return;
+  R rec[RC::n];
+#pragma unroll
+  for (int c = 0; c < RC::n; ++c) rec[c] = R(0);
+  if (j < n) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) rec[c] = R(xs[DIM * j + c]);
+    const double wj = w[j];
+    double qr, qi = 0.0;
+    if (RC::cplx) {
+      qr = wj * sigma[2 * j];
+      qi = wj * sigma[2 * j + 1];
+    } else {
+      qr = wj * sigma[j];
+    }
+    if (RC::dipole) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        rec[DIM + c] = R(qr * ns[DIM * j + c]);
+        if (RC::cplx) rec[2 * DIM + c] = R(qi * ns[DIM * j + c]);
+      }
+    } else {
+      rec[DIM] = R(qr);
+      if (RC::cplx) rec[DIM + 1] = R(qi);
+    }
+  }
+  R* o = out + j * RC::n;
+#pragma unroll
+  for (int c = 0; c < RC::n; ++c) o[c] = rec[c];
+}
+
+// ---------------------------------------------------------------------------
+// Per-pair accumulation.  Kernel constants (1/(4pi), signs) are applied once
+// in the epilogue; the self pair (|r|^2 <= tol^2) contributes exactly zero.
+// ---------------------------------------------------------------------------
+template <class R>
+struct MathOps;
+template <>
+struct MathOps<double> {
+  static __device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
+  static __device__ __forceinline__ double lg(double v) { return log(v); }
+  static __device__ __forceinline__ void scpi(double v, double* s, double* c) { sincospi(v, s, c); }
+  static __device__ __forceinline__ double tol2() { return kSamePointTol2; }
+};
+template <>
+struct MathOps<float> {
+  static __device__ __forceinline__ float rsq(float v) { return rsqrtf(v); }
+  static __device__ __forceinline__ float lg(float v) { return __logf(v); }
+  static __device__ __forceinline__ void scpi(float v, float* s, float* c) { sincospif(v, s, c); }
+  static __device__ __forceinline__ float tol2() { return 1.0e-28f; }
+};
+
+template <class R, int DIM, bool TN>
+struct Target {
+  R x[DIM];
+  R n[TN ? DIM : 1];
+};
+
+template <int PDE, int KIND, int DIM, class R>
+__device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DIM, R>::tnormal>& t,
+                                          const R* __restrict__ s, R kpi, R k, R& ar, R& ai) {
+  using M = MathOps<R>;
+  R r[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) r[c] = t.x[c] - s[c];
+  R d2 = r[0] * r[0];
+#pragma unroll
+  for (int c = 1; c < DIM; ++c) d2 = fma(r[c], r[c], d2);
+  const bool keep = d2 > M::tol2();
+  if (PDE == LAPLACE) {
+    if (KIND == SL) {
+      if (DIM == 2) {
+        // -log(d)/(2pi) = log(d^2) * (-1/(4pi)); constant in the epilogue
+        const R l = M::lg(d2);
+        ar += keep ? l * s[2] : R(0);
+      } else {
+        const R ri = keep ? M::rsq(d2) : R(0);
+        ar = fma(ri, s[3], ar);
+      }
+    } else if (KIND == DL) {
+      R rp = r[0] * s[DIM];
+#pragma unroll
+      for (int c = 1; c < DIM; ++c) rp = fma(r[c], s[DIM + c], rp);
+      if (DIM == 2) {
+        const R ri = keep ? R(1) / d2 : R(0);
+        ar = fma(rp, ri, ar);
+      } else {
+        const R ri = keep ? M::rsq(d2) : R(0);
+        ar = fma(rp, ri * ri * ri, ar);
+      }
+    } else if (KIND == ADL) {
+      R rn = r[0] * t.n[0];
+#pragma unroll
+      for (int c = 1; c < DIM; ++c) rn = fma(r[c], t.n[c], rn);
+      const R q = s[DIM];
+      if (DIM == 2) {
+        const R ri = keep ? R(1) / d2 : R(0);
+        ar = fma(rn * q, ri, ar);
+      } else {
+        const R ri = keep ? M::rsq(d2) : R(0);
+        ar = fma(rn * q, ri * ri * ri, ar);
+      }
+    } else {  // HS: (nx.p - DIM (r.nx)(r.p)/d^2) / d^DIM
+      R rn = r[0] * t.n[0], rp = r[0] * s[DIM], np = t.n[0] * s[DIM];
+#pragma unroll
+      for (int c = 1; c < DIM; ++c) {
+        rn = fma(r[c], t.n[c], rn);
+        rp = fma(r[c], s[DIM + c], rp);
+        np = fma(t.n[c], s[DIM + c], np);
+      }
+      if (DIM == 2) {
+        const R id2 = keep ? R(1) / d2 : R(0);
+        ar = fma(id2, fma(R(-2) * rn * rp, id2, np), ar);
+      } else {
+        const R ri = keep ? M::rsq(d2) : R(0);
+        const R id2 = ri * ri;
+        ar = fma(id2 * ri, fma(R(-3) * rn * rp, id2, np), ar);
+      }
+    }
+  } else {  // Helmholtz 3D
+    const R ri = keep ? M::rsq(d2) : R(0);
+    const R d = d2 * ri;  // 0 for the self pair
+    R sn, cs;
+    M::scpi(d * kpi, &sn, &cs);
+    if (KIND == SL || KIND == ADL) {
+      R g_r, g_i;  // G (without 1/4pi) or the ADL factor
+      if (KIND == SL) {
+        g_r = ri * cs;
+        g_i = ri * sn;
+      } else {
+        // e^{ikd}(1/d - ik) (r.nx) / d^2
+        const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
+        R rn = r[0] * t.n[0];
+        rn = fma(r[1], t.n[1], rn);
+        rn = fma(r[2], t.n[2], rn);
+        const R f = rn * ri * ri;
+        g_r = er * f;
+        g_i = ei * f;
+      }
+      const R qr = s[3], qi = s[4];
+      ar = fma(g_r, qr, fma(-g_i, qi, ar));
+      ai = fma(g_r, qi, fma(g_i, qr, ai));
+    } else if (KIND == DL) {
+      const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
+      const R id2 = ri * ri;
+      R A = r[0] * s[3], B = r[0] * s[6];
+      A = fma(r[1], s[4], A);
+      A = fma(r[2], s[5], A);
+      B = fma(r[1], s[7], B);
+      B = fma(r[2], s[8], B);
+      const R gr = er * id2, gi = ei * id2;
+      ar = fma(gr, A, fma(-gi, B, ar));
+      ai = fma(gr, B, fma(gi, A, ai));
+    } else {  // HS
+      const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
+      const R id2 = ri * ri;
+      R rn = r[0] * t.n[0];
+      rn = fma(r[1], t.n[1], rn);
+      rn = fma(r[2], t.n[2], rn);
+      R A = r[0] * s[3], B = r[0] * s[6], NA = t.n[0] * s[3], NB = t.n[0] * s[6];
+#pragma unroll
+      for (int c = 1; c < 3; ++c) {
+        A = fma(r[c], s[3 + c], A);
+        B = fma(r[c], s[6 + c], B);
+        NA = fma(t.n[c], s[3 + c], NA);
+        NB = fma(t.n[c], s[6 + c], NB);
+      }
+      // b = e(1/d - ik) id2 ; a = e (3(ikd-1) + k^2 d^2) id2^2 / d
+      const R br = er * id2, bi = ei * id2;
+      const R fr = fma(k * d, k * d, R(-3)), fi = R(3) * k * d;
+      const R sa = id2 * id2 * ri;
+      const R a_r = sa * fma(cs, fr, -sn * fi), a_i = sa * fma(cs, fi, sn * fr);
+      // value = a (r.nx)(r.p) + b (nx.p), p complex = A + iB (r.p), NA + iNB (nx.p)
+      const R tr = rn * A, ti = rn * B;
+      ar += fma(a_r, tr, -a_i * ti) + fma(br, NA, -bi * NB);
+      ai += fma(a_r, ti, a_i * tr) + fma(br, NB, bi * NA);
+    }
+  }
+}
+
+// Accumulator: FP64 plain; FP32 with a per-group sum and a TwoSum-folded
+// (hi, lo) pair.
+template <class R, bool CPLX>
+struct Acc;
+template <bool CPLX>
+struct Acc<double, CPLX> {
+  double r = 0, i = 0;
+  __device__ __forceinline__ double& gr() { return r; }
+  __device__ __forceinline__ double& gi() { return i; }
+  __device__ __forceinline__ void fold() {}
+};
+__device__ __forceinline__ void two_sum_fold(float& hi, float& lo, float& g) {
+  const float t = hi + g;
+  const float bp = t - hi;
+  const float e = (hi - (t - bp)) + (g - bp);
+  hi = t;
+  lo += e;
+  g = 0.f;
+}
+template <bool CPLX>
+struct Acc<float, CPLX> {
+  float gr_ = 0, gi_ = 0, hr = 0, lr = 0, hi = 0, li = 0;
+  __device__ __forceinline__ float& gr() { return gr_; }
+  __device__ __forceinline__ float& gi() { return gi_; }
+  __device__ __forceinline__ void fold() {
+    two_sum_fold(hr, lr, gr_);
+    if (CPLX) two_sum_fold(hi, li, gi_);
+  }
+};
+
+// Partial accumulator storage per (split, target).
+template <class R, bool CPLX>
+struct PartialT;
+template <>
+struct PartialT<double, false> { using T = double; };
+template <>
+struct PartialT<double, true> { using T = double2; };
+template <>
+struct PartialT<float, false> { using T = float2; };
+template <>
+struct PartialT<float, true> { using T = float4; };
+
+__device__ __forceinline__ void store_partial(double* p, const Acc<double, false>& a) { *p = a.r; }
+__device__ __forceinline__ void store_partial(double2* p, const Acc<double, true>& a) {
+  *p = make_double2(a.r, a.i);
+}
+__device__ __forceinline__ void store_partial(float2* p, const Acc<float, false>& a) {
+  *p = make_float2(a.hr, a.lr);
+}
+__device__ __forceinline__ void store_partial(float4* p, const Acc<float, true>& a) {
+  *p = make_float4(a.hr, a.lr, a.hi, a.li);
+}
+
+struct FwdArgs {
+  int64_t m;
+  int64_t n_tiles;
+  int tiles_per_split;
+  const double* tcoords;
+  const double* tnormals;
+  const void* packed;
+  void* partial;
+  double k;
+  int* err;
+};
+
+template <int PDE, int KIND, int DIM, class R, int TILE>
+__global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
+  using RC = Rec<PDE, KIND, DIM, R>;
+  constexpr bool CPLX = RC::cplx;
+  using P = typename PartialT<R, CPLX>::T;
+  constexpr uint32_t kStageBytes = TILE * RC::n * sizeof(R);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* stage0 = reinterpret_cast<R*>(smem_raw);
+  R* stage1 = reinterpret_cast<R*>(smem_raw + kStageBytes);
+  __shared__ __align__(8) uint64_t full[2];
+
+  const int tid = threadIdx.x;
+  const int64_t base = (int64_t)blockIdx.x * (kBlock * kTPT);
+  const int split = blockIdx.y;
+  const int64_t t0 = (int64_t)split * a.tiles_per_split;
+  const int64_t t1 = min(a.n_tiles, t0 + a.tiles_per_split);
+  const R* src = static_cast<const R*>(a.packed);
+
+  Target<R, DIM, RC::tnormal> tg[kTPT];
+  Acc<R, CPLX> acc[kTPT];
+#pragma unroll
+  for (int u = 0; u < kTPT; ++u) {
+    const int64_t i = min(base + u * kBlock + tid, a.m - 1);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) tg[u].x[c] = R(a.tcoords[DIM * i + c]);
+    if (RC::tnormal) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) tg[u].n[c] = R(a.tnormals[DIM * i + c]);
+    }
+  }
+  const R k = R(a.k);
+  const R kpi = R(a.k / kPi);
+
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  int64_t issued = t0;  // next tile to issue (meaningful in thread 0)
+  if (tid == 0) {
+    for (int s = 0; s < 2 && issued < t1; ++s, ++issued) {
+      mbar_arrive_expect_tx(&full[s], kStageBytes);
+      bulk_copy_g2s(s ? stage1 : stage0, src + issued * TILE * RC::n, kStageBytes, &full[s]);
+    }
+  }
+
+  for (int64_t t = t0; t < t1; ++t) {
+    const int st = (int)((t - t0) & 1);
+    const uint32_t parity = (uint32_t)(((t - t0) >> 1) & 1);
+    const bool ok = mbar_wait_bounded(&full[st], parity);
+    if (!__syncthreads_and(ok)) {
+      // A bulk copy never completed: record it, drain what is still in
+      // flight (bounded), and leave without touching the results.
+      if (tid == 0) {
+        atomicExch(a.err, kErrWaitTimeout);
+        for (int64_t q = t + 1; q < issued; ++q)
+          mbar_wait_bounded(&full[(q - t0) & 1], (uint32_t)(((q - t0) >> 1) & 1));
+      }
+      return;
+    }
+    const R* sp = st ? stage1 : stage0;
+#pragma unroll 1
+    for (int g = 0; g < TILE; g += kGroup) {
+#pragma unroll 4
+      for (int s = 0; s < kGroup; ++s) {
+        const R* rec = sp + (g + s) * RC::n;
+#pragma unroll
+        for (int u = 0; u < kTPT; ++u) pair_step<PDE, KIND, DIM, R>(tg[u], rec, kpi, k, acc[u].gr(), acc[u].gi());
+      }
+#pragma unroll
+      for (int u = 0; u < kTPT; ++u) acc[u].fold();
+    }
+    __syncthreads();  // every thread is done reading this stage
+    if (tid == 0 && issued < t1) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&full[st], kStageBytes);
+      bulk_copy_g2s(st ? stage1 : stage0, src + issued * TILE * RC::n, kStageBytes, &full[st]);
+      ++issued;
+    }
+  }
+  P* out = static_cast<P*>(a.partial) + (int64_t)split * a.m;
+#pragma unroll
+  for (int u = 0; u < kTPT; ++u) {
+    const int64_t i = base + u * kBlock + tid;
+    if (i < a.m) store_partial(out + i, acc[u]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Epilogue: y_i = alpha*(scale*sum_s partial[s][i] + sum_p C_ip x_p) + beta*y_i
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 load_partial(const double* p) { return make_double2(*p, 0.0); }
+__device__ __forceinline__ double2 load_partial(const double2* p) { return *p; }
+__device__ __forceinline__ double2 load_partial(const float2* p) {
+  const float2 v = *p;
+  return make_double2((double)v.x + (double)v.y, 0.0);
+}
+__device__ __forceinline__ double2 load_partial(const float4* p) {
+  const float4 v = *p;
+  return make_double2((double)v.x + (double)v.y, (double)v.z + (double)v.w);
+}
+
+struct EpiArgs {
+  int64_t m;
+  int split;
+  const void* partial;
+  double scale;
+  const int64_t* rowptr;  // null when no correction
+  const int32_t* col;
+  const double* val;
+  const double* x;
+  double* y;
+  double ar, ai, br, bi;
+  bool beta_zero;
+};
+
+template <class P, bool CPLX>
+__global__ void pair_epilogue_kernel(EpiArgs e) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= e.m) return;
+  const P* part = static_cast<const P*>(e.partial);
+  double sr = 0.0, si = 0.0;
+  for (int s = 0; s < e.split; ++s) {
+    const double2 v = load_partial(part + (int64_t)s * e.m + i);
+    sr += v.x;
+    si += v.y;
+  }
+  sr *= e.scale;
+  si *= e.scale;
+  if (e.rowptr) {
+    const int64_t p0 = e.rowptr[i], p1 = e.rowptr[i + 1];
+    for (int64_t p = p0; p < p1; ++p) {
+      const int32_t j = e.col[p];
+      if (CPLX) {
+        const double2 v = reinterpret_cast<const double2*>(e.val)[p];
+        const double2 xv = reinterpret_cast<const double2*>(e.x)[j];
+        sr = fma(v.x, xv.x, fma(-v.y, xv.y, sr));
+        si = fma(v.x, xv.y, fma(v.y, xv.x, si));
+      } else {
+        sr = fma(e.val[p], e.x[j], sr);
+      }
+    }
+  }
+  if (CPLX) {
+    double yr = e.ar * sr - e.ai * si, yi = e.ar * si + e.ai * sr;
+    if (!e.beta_zero) {
+      const double2 yo = reinterpret_cast<const double2*>(e.y)[i];
+      yr += e.br * yo.x - e.bi * yo.y;
+      yi += e.br * yo.y + e.bi * yo.x;
+    }
+    reinterpret_cast<double2*>(e.y)[i] = make_double2(yr, yi);
+  } else {
+    double yr = e.ar * sr;
+    if (!e.beta_zero) yr += e.br * e.y[i];
+    e.y[i] = yr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Dense assembly out[i + m*j] = K(x_i, y_j) w_j (column-major).
+// ---------------------------------------------------------------------------
+template <int PDE, int KIND, int DIM>
+__global__ void assemble_kernel(int64_t m, int64_t n, const double* tc, const double* tn,
+                                const double* sc, const double* sn, const double* w, double k,
+                                double* out) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t j = blockIdx.y;
+  if (i >= m) return;
+  const double2 v = kernel_value<PDE, KIND, DIM>(tc + DIM * i, tn ? tn + DIM * i : nullptr,
+                                                 sc + DIM * j, sn ? sn + DIM * j : nullptr, k);
+  const double wj = w[j];
+  if (PDE == HELMHOLTZ) {
+    reinterpret_cast<double2*>(out)[i + m * j] = make_double2(v.x * wj, v.y * wj);
+  } else {
+    out[i + m * j] = v.x * wj;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Transpose apply z_j = w_j * sum_i K(x_i, y_j) g_i: each thread owns source
+// nodes, target tiles are staged in shared memory (plain loads; this is the
+// adjoint's density gradient, not the forward hot loop).
+// ---------------------------------------------------------------------------
+template <int PDE, int KIND, int DIM>
+__global__ void __launch_bounds__(kBlock) transpose_kernel(int64_t m, int64_t n, const double* tc,
+                                                          const double* tn, const double* sc,
+                                                          const double* sn, const double* w,
+                                                          const double* g, double k, int tiles_per_split,
+                                                          double2* partial) {
+  constexpr int T = 64;
+  __shared__ double stc[T * DIM], stn[T * DIM], sg[T * 2];
+  const int64_t j = blockIdx.x * (int64_t)kBlock + threadIdx.x;
+  const int64_t jj = min(j, n - 1);
+  double y[DIM], ny[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) {
+    y[c] = sc[DIM * jj + c];
+    ny[c] = sn ? sn[DIM * jj + c] : 0.0;
+  }
+  const int64_t ntile = (m + T - 1) / T;
+  const int64_t i0 = (int64_t)blockIdx.y * tiles_per_split;
+  const int64_t i1 = min(ntile, i0 + tiles_per_split);
+  double ar = 0.0, ai = 0.0;
+  for (int64_t t = i0; t < i1; ++t) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < T; q += kBlock) {
+      const int64_t i = t * T + q;
+      const bool in = i < m;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        stc[q * DIM + c] = in ? tc[DIM * i + c] : 0.0;
+        stn[q * DIM + c] = (in && tn) ? tn[DIM * i + c] : 0.0;
+      }
+      if (PDE == HELMHOLTZ) {
+        sg[2 * q] = in ? g[2 * i] : 0.0;
+        sg[2 * q + 1] = in ? g[2 * i + 1] : 0.0;
+      } else {
+        sg[2 * q] = in ? g[i] : 0.0;
+        sg[2 * q + 1] = 0.0;
+      }
+    }
+    __syncthreads();
+    for (int q = 0; q < T; ++q) {
+      const double2 kv = kernel_value<PDE, KIND, DIM>(&stc[q * DIM], &stn[q * DIM], y, ny, k);
+      const double gr = sg[2 * q], gi = sg[2 * q + 1];
+      ar = fma(kv.x, gr, fma(-kv.y, gi, ar));
+      ai = fma(kv.x, gi, fma(kv.y, gr, ai));
+    }
+  }
+  if (j < n) {
+    const double wj = w[j];
+    partial[(int64_t)blockIdx.y * n + j] = make_double2(ar * wj, ai * wj);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host-side dispatch
+// ---------------------------------------------------------------------------
+int pair_tile(int precision) { return precision == INTI_FP32C ? kTile32 : kTile64; }
+
+template <class R>
+static int rec_elems(int pde, int kind, int dim) {
+  const bool dip = kind == DL || kind == HS;
+  const bool cp = pde == HELMHOLTZ;
+  const int used = dim + (cp ? 2 : 1) * (dip ? dim : 1);
+  const int al = 16 / (int)sizeof(R);
+  return (used + al - 1) / al * al;
+}
+
+int pair_record_bytes(int pde, int kind, int dim, int precision) {
+  return precision == INTI_FP32C ? rec_elems<float>(pde, kind, dim) * 4
+                                 : rec_elems<double>(pde, kind, dim) * 8;
+}
+
+int pair_partial_bytes(int pde, int precision) {
+  if (precision == INTI_FP32C) return pde == HELMHOLTZ ? 16 : 8;
+  return pde == HELMHOLTZ ? 16 : 8;
+}
+
+// Kernel constant applied in the epilogue (see pair_step).
+static double pair_scale(int pde, int kind, int dim) {
+  const double c3 = 1.0 / (4 * kPi), c2 = 1.0 / (2 * kPi);
+  if (pde == HELMHOLTZ) return kind == ADL ? -c3 : c3;
+  if (dim == 2) {
+    switch (kind) {
+      case SL: return -1.0 / (4 * kPi);  // applied to log(d^2)
+      case DL: return c2;
+      case ADL: return -c2;
+      default: return c2;
+    }
+  }
+  return kind == ADL ? -c3 : c3;
+}
+
+template <class F>
+static void dispatch(int pde, int kind, int dim, F&& f);
+
+template <int PDE, int KIND, int DIM>
+struct Tag {
+  static constexpr int pde = PDE, kind = KIND, dim = DIM;
+};
+
+template <class F>
+static void dispatch(int pde, int kind, int dim, F&& f) {
+  if (pde == LAPLACE && dim == 3) {
+    switch (kind) {
+      case SL: return f(Tag<LAPLACE, SL, 3>());
+      case DL: return f(Tag<LAPLACE, DL, 3>());
+      case ADL: return f(Tag<LAPLACE, ADL, 3>());
+      case HS: return f(Tag<LAPLACE, HS, 3>());
+    }
+  } else if (pde == LAPLACE && dim == 2) {
+    switch (kind) {
+      case SL: return f(Tag<LAPLACE, SL, 2>());
+      case DL: return f(Tag<LAPLACE, DL, 2>());
+      case ADL: return f(Tag<LAPLACE, ADL, 2>());
+      case HS: return f(Tag<LAPLACE, HS, 2>());
+    }
+  } else if (pde == HELMHOLTZ && dim == 3) {
+    switch (kind) {
+      case SL: return f(Tag<HELMHOLTZ, SL, 3>());
+      case DL: return f(Tag<HELMHOLTZ, DL, 3>());
+      case ADL: return f(Tag<HELMHOLTZ, ADL, 3>());
+      case HS: return f(Tag<HELMHOLTZ, HS, 3>());
+    }
+  }
+  throw Error(INTI_E_UNSUPPORTED, "unsupported operator: pde=" + std::to_string(pde) +
+                                      " kernel=" + std::to_string(kind) +
+                                      " dim=" + std::to_string(dim));
+}
+
+template <class T, class R>
+static const void* fwd_kernel_ptr() {
+  constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
+  return reinterpret_cast<const void*>(&pair_forward<T::pde, T::kind, T::dim, R, TILE>);
+}
+
+template <class T, class R>
+static size_t fwd_smem() {
+  constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
+  return 2 * (size_t)TILE * Rec<T::pde, T::kind, T::dim, R>::n * sizeof(R);
+}
+
+int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
+                    int64_t n) {
+  int occ = 1;
+  dispatch(pde, kind, dim, [&](auto tag) {
+    using T = decltype(tag);
+    const void* fn;
+    size_t sm;
+    if (precision == INTI_FP32C) {
+      fn = fwd_kernel_ptr<T, float>();
+      sm = fwd_smem<T, float>();
+    } else {
+      fn = fwd_kernel_ptr<T, double>();
+      sm = fwd_smem<T, double>();
+    }
+    INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    INTI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBlock, sm));
+  });
+  occ = std::max(occ, 1);
+  const int64_t tile = pair_tile(precision);
+  const int64_t n_tiles = std::max<int64_t>(1, (n + tile - 1) / tile);
+  const int64_t blocks = (m + kBlock * kTPT - 1) / (kBlock * kTPT);
+  const int64_t slots = (int64_t)ctx->num_sms * occ;
+  // Smallest split whose last wave is >= 90% full (or that reaches 8
+  // waves), never more chunks than source tiles.
+  int best = 1;
+  double best_eff = -1.0;
+  for (int s = 1; s <= 64 && s <= n_tiles; ++s) {
+    const int64_t tps = (n_tiles + s - 1) / s;
+    const int64_t eff_s = (n_tiles + tps - 1) / tps;  // chunks actually used
+    const double waves = (double)(blocks * eff_s) / (double)slots;
+    const double eff = waves / std::ceil(waves);
+    if (eff > best_eff + 1e-9) {
+      best_eff = eff;
+      best = s;
+    }
+    if ((eff >= 0.9 && waves >= 1.0) || waves >= 8.0) {
+      best = s;
+      break;
+    }
+  }
+  return best;
+}
+
+int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
+  const int tile = pair_tile(L.precision);
+  const int64_t npad = L.n_tiles * tile;
+  const int tps = (int)((L.n_tiles + L.split - 1) / L.split);
+  int launches = 0;
+  dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
+    using T = decltype(tag);
+    auto go = [&](auto rtag) {
+      using R = decltype(rtag);
+      constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
+      const int pb = 256;
+      ProfScope ps(ctx, "pack");
+      pack_sources<T::pde, T::kind, T::dim, R><<<(unsigned)((npad + pb - 1) / pb), pb, 0, ctx->stream>>>(
+          L.n, npad, L.scoords, L.snormals, L.sweights, L.x, static_cast<R*>(L.packed));
+      FwdArgs a;
+      a.m = L.m;
+      a.n_tiles = L.n_tiles;
+      a.tiles_per_split = tps;
+      a.tcoords = L.tcoords;
+      a.tnormals = L.tnormals;
+      a.packed = L.packed;
+      a.partial = L.partial;
+      a.k = L.k;
+      a.err = L.err_flag;
+      const size_t sm = fwd_smem<T, R>();
+      auto fn = &pair_forward<T::pde, T::kind, T::dim, R, TILE>;
+      INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      dim3 grid((unsigned)((L.m + kBlock * kTPT - 1) / (kBlock * kTPT)), (unsigned)L.split);
+      ProfScope pp(ctx, "pair");
+      fn<<<grid, kBlock, sm, ctx->stream>>>(a);
+      launches = 2;
+    };
+    if (L.precision == INTI_FP32C)
+      go(float());
+    else
+      go(double());
+  });
+  INTI_CUDA(cudaGetLastError());
+  ctx->launches += launches;
+  return launches;
+}
+
+int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x,
+                  double* y, const double* alpha, const double* beta) {
+  EpiArgs e;
+  e.m = L.m;
+  e.split = L.split;
+  e.partial = L.partial;
+  e.scale = pair_scale(L.pde, L.kind, L.dim);
+  e.rowptr = corr ? corr->rowptr.as<int64_t>() : nullptr;
+  e.col = corr ? corr->col.as<int32_t>() : nullptr;
+  e.val = corr ? corr->val.as<double>() : nullptr;
+  e.x = x;
+  e.y = y;
+  e.ar = alpha ? alpha[0] : 1.0;
+  e.ai = alpha ? alpha[1] : 0.0;
+  e.br = beta ? beta[0] : 0.0;
+  e.bi = beta ? beta[1] : 0.0;
+  e.beta_zero = (e.br == 0.0 && e.bi == 0.0);
+  const int tb = 256;
+  const unsigned gb = (unsigned)((L.m + tb - 1) / tb);
+  const bool cplx = L.pde == HELMHOLTZ;
+  ProfScope pe(ctx, "epilogue");
+  if (L.precision == INTI_FP32C) {
+    if (cplx)
+      pair_epilogue_kernel<float4, true><<<gb, tb, 0, ctx->stream>>>(e);
+    else
+      pair_epilogue_kernel<float2, false><<<gb, tb, 0, ctx->stream>>>(e);
+  } else {
+    if (cplx)
+      pair_epilogue_kernel<double2, true><<<gb, tb, 0, ctx->stream>>>(e);
+    else
+      pair_epilogue_kernel<double, false><<<gb, tb, 0, ctx->stream>>>(e);
+  }
+  INTI_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return 1;
+}
+
+int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {
+  if (L.n > 65535 * 1024LL) throw Error(INTI_E_ARG, "assemble: too many source columns");
+  dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
+    using T = decltype(tag);
+    dim3 grid((unsigned)((L.m + 255) / 256), (unsigned)L.n);
+    assemble_kernel<T::pde, T::kind, T::dim><<<grid, 256, 0, ctx->stream>>>(
+        L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.k, out);
+  });
+  INTI_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return 1;
+}
+
+// Transpose: the roles of the two node sets swap; partial is split x n double2.
+int pair_transpose_launch(inti_ctx* ctx, const PairLaunch& L) {
+  const int64_t ntile = (L.m + 63) / 64;
+  const int tps = (int)((ntile + L.split - 1) / L.split);
+  dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
+    using T = decltype(tag);
+    dim3 grid((unsigned)((L.n + kBlock - 1) / kBlock), (unsigned)L.split);
+    ProfScope pt(ctx, "transpose");
+    transpose_kernel<T::pde, T::kind, T::dim><<<grid, kBlock, 0, ctx->stream>>>(
+        L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.x, L.k, tps,
+        static_cast<double2*>(L.partial));
+  });
+  INTI_CUDA(cudaGetLastError());
+  ctx->launches += 1;
+  return 1;
+}
+
+}  // namespace inti

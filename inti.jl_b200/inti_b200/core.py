@@ -1,0 +1,683 @@
+"""Host-side mirror of Inti.jl's operator surface over libinti_b200.
+
+Names, argument meaning and error behaviour follow the reference:
+
+* ``Laplace(dim=)``, ``Helmholtz(k=, dim=)`` (src/kernels.jl:118-128, 310-335);
+* ``SingleLayerKernel``, ``DoubleLayerKernel``, ``AdjointDoubleLayerKernel``,
+  ``HyperSingularKernel`` (src/kernels.jl:52-112);
+* ``IntegralOperator(K, target, source=target)`` whose entries are
+  ``K(x_i, y_j)·w_j`` (src/nystrom.jl:67-96), applied on the fly on the GPU,
+  and ``assemble_matrix`` (src/nystrom.jl:103-124);
+* ``single_double_layer`` / ``adj_double_layer_hypersingular``
+  (src/api.jl:65-212) with ``compression=dict(method="b200", precision=...)``
+  and ``correction=dict(method="dim"|"none")``; the result is ``S = A + δS``,
+  a lazy map like ``LinearMap(Smat) + LinearMap(δS)`` (src/api.jl:179-184)
+  whose apply runs the pair kernel and the CSR correction in one pass;
+* ``bdim_correction`` (src/bdim.jl:50-196, target === source) built on the GPU;
+* ``single_double_layer_potential`` / ``IntegralPotential`` (src/api.jl:220-226,
+  src/nystrom.jl:20-38);
+* ``gmres`` for ``shift·I + Σ c_t·op_t`` (the IterativeSolvers call of
+  docs/src/examples/poisson.jl:166-168), plain FP64 or mixed precision.
+
+Arrays cross the boundary as numpy arrays; complex densities are
+``complex128`` (interleaved re/im, as ComplexF64).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import numbers
+import threading
+import weakref
+
+import numpy as np
+
+from . import _lib as L
+from .geometry import Quadrature
+
+__all__ = [
+    "Context",
+    "default_context",
+    "Laplace",
+    "Helmholtz",
+    "SingleLayerKernel",
+    "DoubleLayerKernel",
+    "AdjointDoubleLayerKernel",
+    "HyperSingularKernel",
+    "IntegralOperator",
+    "assemble_matrix",
+    "CorrectionMatrix",
+    "bdim_correction",
+    "single_double_layer",
+    "adj_double_layer_hypersingular",
+    "IntegralPotential",
+    "single_double_layer_potential",
+    "I",
+    "gmres",
+    "COMPRESSION_METHODS",
+    "CORRECTION_METHODS",
+]
+
+COMPRESSION_METHODS = ("none", "b200")
+CORRECTION_METHODS = ("none", "dim")
+
+
+# ----------------------------------------------------------------------------
+# context
+# ----------------------------------------------------------------------------
+class Context:
+    """One CUDA device and stream (``inti_ctx``).  All handles created through
+    a context live on its device; calls on one context are serialised."""
+
+    def __init__(self, device: int = 0, stream: int | None = None):
+        self.lib = L.load()
+        h = C.c_void_p()
+        st = self.lib.inti_ctx_create(int(device), C.c_void_p(stream) if stream else None, C.byref(h))
+        L.check(st, None)
+        self.handle = h
+        self.device = device
+        self._fin = weakref.finalize(self, self.lib.inti_ctx_destroy, h)
+
+    def check(self, status: int) -> None:
+        L.check(status, self.handle)
+
+    @property
+    def stream(self) -> int:
+        return self.lib.inti_ctx_stream(self.handle) or 0
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.lib.inti_ctx_launch_count(self.handle))
+
+    def set_profiling(self, enable: bool) -> None:
+        """Start (clearing earlier records) or stop per-kernel event timing."""
+        self.check(self.lib.inti_ctx_set_profiling(self.handle, int(bool(enable))))
+
+    def profile(self, kernel: str) -> tuple[float, int]:
+        """(total device ms, launches) recorded for a kernel class."""
+        ms, n = C.c_double(), L.I64()
+        self.check(self.lib.inti_ctx_profile(self.handle, kernel.encode(), C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def synchronize(self) -> None:
+        self.check(self.lib.inti_ctx_synchronize(self.handle))
+
+    def measure_peaks(self) -> dict:
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        self.check(self.lib.inti_measure_peaks(self.handle, C.byref(a), C.byref(b), C.byref(c)))
+        return {"fp64_flops": a.value, "fp32_flops": b.value, "mufu_ops": c.value}
+
+
+_default = None
+_default_lock = threading.Lock()
+
+
+def default_context() -> Context:
+    global _default
+    with _default_lock:
+        if _default is None:
+            _default = Context(0)
+        return _default
+
+
+# ----------------------------------------------------------------------------
+# differential operators and kernels
+# ----------------------------------------------------------------------------
+class Laplace:
+    """``-Δu`` in ``dim`` dimensions (src/kernels.jl:118-128)."""
+
+    pde = L.LAPLACE
+    k = 0.0
+
+    def __init__(self, *, dim: int):
+        if dim not in (2, 3):
+            raise L.ArgumentError(L.E_ARG, "dim must be 2 or 3")
+        self.dim = dim
+
+    def default_density_eltype(self):
+        return np.float64
+
+    def __repr__(self):
+        return f"Laplace operator in {self.dim} dimensions: -Δu"
+
+
+class Helmholtz:
+    """``-Δu - k²u`` in ``dim`` dimensions (src/kernels.jl:310-335)."""
+
+    pde = L.HELMHOLTZ
+
+    def __init__(self, *, k, dim: int):
+        if dim not in (2, 3):
+            raise L.ArgumentError(L.E_ARG, "dim must be 2 or 3")
+        if isinstance(k, complex):
+            if k.imag < 0:
+                raise L.ArgumentError(L.E_ARG, "k must have a non-negative imaginary part")
+            if k.imag == 0:
+                k = k.real
+        self.k = k
+        self.dim = dim
+
+    def default_density_eltype(self):
+        return np.complex128
+
+    def __repr__(self):
+        return f"Helmholtz operator in {self.dim} dimensions: -Δu - k²u"
+
+
+class _Kernel:
+    kind = -1
+
+    def __init__(self, op):
+        self.op = op
+
+    def __repr__(self):
+        return f"{type(self).__name__}({self.op!r})"
+
+
+class SingleLayerKernel(_Kernel):
+    kind = L.SL
+
+
+class DoubleLayerKernel(_Kernel):
+    kind = L.DL
+
+
+class AdjointDoubleLayerKernel(_Kernel):
+    kind = L.ADL
+
+
+class HyperSingularKernel(_Kernel):
+    kind = L.HS
+
+
+# ----------------------------------------------------------------------------
+# device handles
+# ----------------------------------------------------------------------------
+def _quad_handle(q: Quadrature, ctx: Context):
+    """Device copy of a quadrature, cached on the object per context."""
+    cache = q.__dict__.setdefault("_b200", {})
+    key = id(ctx)
+    if key in cache:
+        return cache[key][0]
+    h = C.c_void_p()
+    nrm = q.normals
+    ctx.check(ctx.lib.inti_quad_create(ctx.handle, q.dim, len(q), L.dptr(q.coords), L.dptr(nrm),
+                                       L.dptr(q.weights), int(q.nq), C.byref(h)))
+    fin = weakref.finalize(q, ctx.lib.inti_quad_destroy, h)
+    cache[key] = (h, fin, ctx)
+    return h
+
+
+def _as_density(x, cplx: bool, n: int, name="x") -> np.ndarray:
+    x = np.asarray(x)
+    if x.shape[0] != n:
+        raise L.DimensionMismatch(L.E_SHAPE, f"{name} has {x.shape[0]} rows, expected {n}")
+    dt = np.complex128 if cplx else np.float64
+    if not cplx and np.iscomplexobj(x):
+        raise L.ArgumentError(L.E_ARG, "complex density for a real operator")
+    return np.ascontiguousarray(x, dtype=dt)
+
+
+class CorrectionMatrix:
+    """Sparse correction δ on the device (``inti_csr``), the counterpart of
+    the ``SparseMatrixCSC`` that ``bdim_correction`` returns
+    (src/bdim.jl:193-194).  ``to_scipy()`` gives a CSR copy on the host."""
+
+    def __init__(self, handle, ctx: Context):
+        self.handle = handle
+        self.ctx = ctx
+        m, n, nnz, dt = L.I64(), L.I64(), L.I64(), C.c_int()
+        ctx.check(ctx.lib.inti_csr_info(handle, C.byref(m), C.byref(n), C.byref(nnz), C.byref(dt)))
+        self.shape = (m.value, n.value)
+        self.nnz = nnz.value
+        self.dtype = np.complex128 if dt.value == L.C128 else np.float64
+        self._fin = weakref.finalize(self, ctx.lib.inti_csr_destroy, handle)
+
+    @classmethod
+    def from_csr(cls, indptr, indices, data, shape, ctx: Context | None = None):
+        ctx = ctx or default_context()
+        indptr = np.ascontiguousarray(indptr, dtype=np.int64)
+        indices = np.ascontiguousarray(indices, dtype=np.int32)
+        cplx = np.iscomplexobj(data)
+        data = np.ascontiguousarray(data, dtype=np.complex128 if cplx else np.float64)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.inti_csr_create(ctx.handle, shape[0], shape[1], len(indices), L.dptr(indptr),
+                                          L.dptr(indices), L.dptr(data), L.C128 if cplx else L.F64,
+                                          C.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
+    def from_csc_1based(cls, colptr, rowval, nzval, shape, ctx: Context | None = None):
+        """From Julia's ``SparseMatrixCSC`` arrays (1-based colptr/rowval)."""
+        ctx = ctx or default_context()
+        colptr = np.ascontiguousarray(colptr, dtype=np.int64)
+        rowval = np.ascontiguousarray(rowval, dtype=np.int64)
+        cplx = np.iscomplexobj(nzval)
+        nzval = np.ascontiguousarray(nzval, dtype=np.complex128 if cplx else np.float64)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.inti_csr_create_from_csc(ctx.handle, shape[0], shape[1], len(rowval),
+                                                   L.dptr(colptr), L.dptr(rowval), L.dptr(nzval),
+                                                   L.C128 if cplx else L.F64, C.byref(h)))
+        return cls(h, ctx)
+
+    def arrays(self):
+        """(indptr int64, indices int32, data) copied from the device."""
+        m, _ = self.shape
+        rp = np.empty(m + 1, np.int64)
+        col = np.empty(self.nnz, np.int32)
+        val = np.empty(self.nnz, self.dtype)
+        self.ctx.check(self.ctx.lib.inti_csr_download(self.handle, L.dptr(rp), L.dptr(col), L.dptr(val)))
+        return rp, col, val
+
+    def to_scipy(self):
+        import scipy.sparse as sp
+
+        rp, col, val = self.arrays()
+        return sp.csr_matrix((val, col, rp), shape=self.shape)
+
+    def __matmul__(self, x):
+        x = _as_density(x, self.dtype == np.complex128, self.shape[1])
+        y = np.zeros(self.shape[0], self.dtype)
+        self.ctx.check(self.ctx.lib.inti_csr_apply(self.handle, L.dptr(x), L.dptr(y), None, None, 0))
+        return y
+
+
+# ----------------------------------------------------------------------------
+# lazy linear maps
+# ----------------------------------------------------------------------------
+class _UniformScaling:
+    """``I`` of LinearAlgebra: combine as ``a*I + op``."""
+
+    def __init__(self, s=1.0):
+        self.s = s
+
+    def __mul__(self, c):
+        return _UniformScaling(self.s * c)
+
+    __rmul__ = __mul__
+
+    def __truediv__(self, c):
+        return _UniformScaling(self.s / c)
+
+    def __neg__(self):
+        return _UniformScaling(-self.s)
+
+    def __add__(self, other):
+        return LinearCombination.of(other) + self
+
+    __radd__ = __add__
+
+    def __sub__(self, other):
+        return (-LinearCombination.of(other)) + self
+
+    def __rsub__(self, other):
+        return LinearCombination.of(other) + (-self)
+
+
+I = _UniformScaling(1.0)
+
+
+class _Map:
+    """Common algebra: ``a*A``, ``A + B``, ``A + s*I``, ``A @ x``."""
+
+    def __add__(self, other):
+        return LinearCombination.of(self) + other
+
+    __radd__ = __add__
+
+    def __sub__(self, other):
+        return LinearCombination.of(self) + (-LinearCombination.of(other)
+                                             if not isinstance(other, _UniformScaling) else -other)
+
+    def __rsub__(self, other):
+        return (-LinearCombination.of(self)) + other
+
+    def __mul__(self, c):
+        if isinstance(c, numbers.Number):
+            return LinearCombination(0.0, [(c, self)])
+        return NotImplemented
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return LinearCombination(0.0, [(-1.0, self)])
+
+    def __matmul__(self, x):
+        return self.matvec(x)
+
+    def __mul_vec__(self, x):
+        return self.matvec(x)
+
+
+class LinearCombination(_Map):
+    """``shift·I + Σ coef_t·op_t`` over GPU operators sharing one quadrature."""
+
+    def __init__(self, shift, terms):
+        self.shift = shift
+        self.terms = list(terms)
+
+    @staticmethod
+    def of(x):
+        if isinstance(x, LinearCombination):
+            return x
+        if isinstance(x, _UniformScaling):
+            return LinearCombination(x.s, [])
+        if isinstance(x, GpuOperator):
+            return LinearCombination(0.0, [(1.0, x)])
+        raise TypeError(f"cannot combine {type(x).__name__}")
+
+    def __add__(self, other):
+        if isinstance(other, _UniformScaling):
+            return LinearCombination(self.shift + other.s, self.terms)
+        o = LinearCombination.of(other)
+        return LinearCombination(self.shift + o.shift, self.terms + o.terms)
+
+    def __mul__(self, c):
+        if isinstance(c, numbers.Number):
+            return LinearCombination(self.shift * c, [(a * c, t) for a, t in self.terms])
+        return NotImplemented
+
+    __rmul__ = __mul__
+
+    def __neg__(self):
+        return self * -1.0
+
+    @property
+    def shape(self):
+        return self.terms[0][1].shape
+
+    @property
+    def is_complex(self):
+        return any(t.is_complex for _, t in self.terms) or any(
+            isinstance(c, complex) and c.imag != 0 for c, _ in self.terms) or (
+            isinstance(self.shift, complex) and self.shift.imag != 0)
+
+    def matvec(self, x):
+        cplx = self.is_complex
+        x = np.asarray(x)
+        x = x.astype(np.complex128 if cplx else np.float64)
+        y = complex(self.shift) * x if cplx else float(np.real(self.shift)) * x
+        for c, t in self.terms:
+            yt = t.matvec(x)
+            y = y + (c * yt)
+        return y
+
+
+class GpuOperator(_Map):
+    """A Nyström operator ``A (+ δ)`` resident on the GPU (``inti_op``).
+
+    ``matvec`` (``@``) and ``mul(y, x, alpha, beta)`` (the 5-argument mul! of
+    LinearAlgebra) run the on-the-fly pair kernel and, when present, the
+    correction SpMV fused in its epilogue.  ``rmatvec`` applies the
+    transpose.  Arrays of shape ``(n, nrhs)`` are applied column by column.
+    """
+
+    def __init__(self, kernel: _Kernel, target: Quadrature, source: Quadrature,
+                 correction: CorrectionMatrix | None = None, precision: str = "fp64",
+                 ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.kernel = kernel
+        self.target = target
+        self.source = source
+        self.correction = correction
+        self.precision = precision
+        op = kernel.op
+        if target.dim != op.dim or source.dim != op.dim:
+            raise L.DimensionMismatch(L.E_SHAPE, "quadrature dimension differs from the operator's")
+        prec = {"fp64": L.FP64, "fp32c": L.FP32C, "mixed": L.FP64}.get(precision)
+        if prec is None:
+            raise L.ArgumentError(L.E_ARG, f"unknown precision {precision!r}")
+        th = _quad_handle(target, self.ctx)
+        sh = _quad_handle(source, self.ctx)
+        h = C.c_void_p()
+        k = complex(getattr(op, "k", 0.0))
+        self.ctx.check(self.ctx.lib.inti_op_create(self.ctx.handle, op.pde, kernel.kind, k.real, k.imag, th, sh,
+                                                   correction.handle if correction else None, prec,
+                                                   C.byref(h)))
+        self.handle = h
+        self._fin = weakref.finalize(self, self.ctx.lib.inti_op_destroy, h)
+        self.shape = (len(target), len(source))
+        self.is_complex = op.pde == L.HELMHOLTZ
+        self.dtype = np.complex128 if self.is_complex else np.float64
+
+    def _apply(self, x, transpose=False, y=None, alpha=1.0, beta=0.0):
+        m, n = self.shape
+        if transpose:
+            m, n = n, m
+        x = np.asarray(x)
+        single = x.ndim == 1
+        X = _as_density(x.reshape(n, -1) if single else x, self.is_complex, n)
+        X = np.asfortranarray(X)
+        nrhs = X.shape[1]
+        if y is None:
+            Y = np.zeros((m, nrhs), self.dtype, order="F")
+            beta = 0.0
+        else:
+            Y = np.asfortranarray(np.asarray(y, dtype=self.dtype).reshape(m, -1))
+        fn = self.ctx.lib.inti_op_apply_transpose if transpose else self.ctx.lib.inti_op_apply
+        self.ctx.check(fn(self.handle, L.dptr(X), n, L.dptr(Y), m, nrhs, L.cpair(alpha), L.cpair(beta), 0))
+        out = Y[:, 0] if single else Y
+        if y is not None:
+            np.copyto(y, out.reshape(np.shape(y)))
+            return y
+        return out
+
+    def matvec(self, x):
+        return self._apply(x)
+
+    def rmatvec(self, x):
+        """``transpose(A) * x`` (not conjugated)."""
+        return self._apply(x, transpose=True)
+
+    def mul(self, y, x, alpha=1.0, beta=0.0):
+        """``y = alpha*A*x + beta*y`` in place."""
+        return self._apply(x, y=y, alpha=alpha, beta=beta)
+
+    def apply_device(self, x_ptr: int, y_ptr: int, nrhs: int = 1, alpha=1.0, beta=0.0,
+                     ldx: int | None = None, ldy: int | None = None) -> None:
+        """Stream-ordered apply on device pointers (no copies, no sync)."""
+        m, n = self.shape
+        self.ctx.check(self.ctx.lib.inti_op_apply(self.handle, C.c_void_p(x_ptr), ldx or n, C.c_void_p(y_ptr),
+                                                  ldy or m, nrhs, L.cpair(alpha), L.cpair(beta), 1))
+
+    def grad_sources(self, g, sigma):
+        """Gradients of J with dJ/du = g for u = A·sigma (Laplace SL/DL):
+        returns dict(sigma, coords, normals, weights)."""
+        m, n = self.shape
+        g = _as_density(g, False, m, "g")
+        sigma = _as_density(sigma, False, n, "sigma")
+        dim = self.source.dim
+        out = {"sigma": np.empty(n), "coords": np.empty((n, dim)), "normals": np.empty((n, dim)),
+               "weights": np.empty(n)}
+        self.ctx.check(self.ctx.lib.inti_op_grad_sources(self.handle, L.dptr(g), L.dptr(sigma),
+                                                         L.dptr(out["sigma"]), L.dptr(out["coords"]),
+                                                         L.dptr(out["normals"]), L.dptr(out["weights"]), 0))
+        return out
+
+
+class IntegralOperator(GpuOperator):
+    """``IntegralOperator(K, target, source=target)`` (src/nystrom.jl:79-89):
+    entries ``K(x_i, y_j)·w_j`` applied on the fly, never stored."""
+
+    def __init__(self, kernel: _Kernel, target: Quadrature, source: Quadrature | None = None,
+                 precision: str = "fp64", ctx: Context | None = None):
+        super().__init__(kernel, target, target if source is None else source, None, precision, ctx)
+
+    def __getitem__(self, idx):
+        i, j = idx
+        return assemble_matrix(self)[i, j]
+
+
+def assemble_matrix(iop: GpuOperator) -> np.ndarray:
+    """Dense matrix of the (uncorrected) operator, assembled on the GPU
+    (src/nystrom.jl:103-124).  Column-major like Julia's ``Matrix``."""
+    m, n = iop.shape
+    out = np.empty((m, n), iop.dtype, order="F")
+    iop.ctx.check(iop.ctx.lib.inti_op_assemble(iop.handle, L.dptr(out), 0))
+    return out
+
+
+# ----------------------------------------------------------------------------
+# correction and the high-level constructors
+# ----------------------------------------------------------------------------
+def bdim_correction(op, target: Quadrature, source: Quadrature, *, green_multiplier=None,
+                    derivative: bool = False, ctx: Context | None = None):
+    """``(δS, δD)`` of the density-interpolation method (src/bdim.jl:50-196),
+    built on the GPU.  Only ``target is source`` is supported: each element
+    corrects its own nodes (src/quadrature.jl:250-256)."""
+    ctx = ctx or default_context()
+    if target is not source:
+        raise L.UnsupportedError(L.E_UNSUPPORTED, "bdim_correction on the GPU requires target === source")
+    h = _quad_handle(source, ctx)
+    gm = None
+    if green_multiplier is not None:
+        gm = np.ascontiguousarray(np.broadcast_to(np.asarray(green_multiplier, float), (len(source),)))
+    hs, hd = C.c_void_p(), C.c_void_p()
+    k = complex(getattr(op, "k", 0.0))
+    ctx.check(ctx.lib.inti_dim_correction(ctx.handle, op.pde, k.real, k.imag, h, int(bool(derivative)),
+                                          L.dptr(gm), C.byref(hs), C.byref(hd)))
+    return CorrectionMatrix(hs, ctx), CorrectionMatrix(hd, ctx)
+
+
+def _normalize_compression(compression):
+    """src/utils.jl:189-198: validate the method, default tol 1e-8."""
+    compression = dict(compression or {"method": "b200"})
+    method = str(compression.get("method", "b200")).lstrip(":")
+    if method not in COMPRESSION_METHODS:
+        raise L.ArgumentError(
+            L.E_ARG, f"Unknown compression.method {method}. Available options: {COMPRESSION_METHODS}")
+    compression["method"] = method
+    compression.setdefault("tol", 1e-8)
+    compression.setdefault("precision", "fp64")
+    return compression
+
+
+def _normalize_correction(correction, target, source):
+    """src/utils.jl:200-228 for the methods implemented here."""
+    correction = dict(correction or {"method": "dim"})
+    method = str(correction.get("method", "dim")).lstrip(":")
+    if method not in CORRECTION_METHODS:
+        raise L.ArgumentError(
+            L.E_ARG, f"Unknown correction.method {method}. Available options: {CORRECTION_METHODS}")
+    correction["method"] = method
+    if method == "dim":
+        if "target_location" in correction and "green_multiplier" in correction:
+            raise L.ArgumentError(L.E_ARG, "conflicting target_location and green_multiplier fields in correction")
+        if target is not source and "target_location" not in correction and "green_multiplier" not in correction:
+            raise L.ArgumentError(L.E_ARG, "missing target_location field in correction")
+        correction.setdefault("maxdist", float("inf"))
+    return correction
+
+
+def _green_multiplier(s: str) -> float:
+    """src/nystrom.jl:196-207."""
+    s = str(s).lstrip(":")
+    if s == "inside":
+        return -1.0
+    if s == "outside":
+        return 0.0
+    if s == "on":
+        return -0.5
+    raise L.ArgumentError(L.E_ARG, f"Unknown target location {s}. Expected :inside, :outside, or :on")
+
+
+def single_double_layer(*, op, target: Quadrature, source: Quadrature, compression=None,
+                        correction=None, derivative: bool = False, ctx: Context | None = None):
+    """``(S, D)`` (or ``(K, H)`` when ``derivative``) as GPU operators with the
+    correction fused (src/api.jl:65-187).  ``compression["precision"]`` is
+    ``"fp64"`` or ``"fp32c"`` (FP32 pairs, compensated sums, FP64 SpMV)."""
+    ctx = ctx or default_context()
+    compression = _normalize_compression(compression)
+    correction = _normalize_correction(correction, target, source)
+    G = AdjointDoubleLayerKernel(op) if derivative else SingleLayerKernel(op)
+    dG = HyperSingularKernel(op) if derivative else DoubleLayerKernel(op)
+    prec = compression["precision"]
+    dS = dD = None
+    if correction["method"] == "dim":
+        if "green_multiplier" in correction:
+            gm = np.asarray(correction["green_multiplier"], float)
+            if gm.shape != (len(target),):
+                raise L.DimensionMismatch(L.E_SHAPE, "green_multiplier must have one entry per target")
+        else:
+            loc = "on" if target is source else correction["target_location"]
+            gm = _green_multiplier(loc)
+        dS, dD = bdim_correction(op, target, source, green_multiplier=gm, derivative=derivative, ctx=ctx)
+    S = GpuOperator(G, target, source, dS, prec, ctx)
+    D = GpuOperator(dG, target, source, dD, prec, ctx)
+    return S, D
+
+
+def adj_double_layer_hypersingular(*, op, target: Quadrature, source: Quadrature | None = None,
+                                   compression=None, correction=None, ctx: Context | None = None):
+    """src/api.jl:197-212."""
+    return single_double_layer(op=op, target=target, source=target if source is None else source,
+                               compression=compression, correction=correction, derivative=True, ctx=ctx)
+
+
+class IntegralPotential:
+    """``IntegralPotential(kernel, quadrature)``; ``pot[σ]`` returns a callable
+    that evaluates ``Σ_j K(x, y_j) σ_j w_j`` at an array of points
+    (src/nystrom.jl:20-38), batched through one GPU operator."""
+
+    def __init__(self, kernel: _Kernel, source: Quadrature, ctx: Context | None = None):
+        self.kernel = kernel
+        self.source = source
+        self.ctx = ctx or default_context()
+
+    def __getitem__(self, sigma):
+        sigma = np.asarray(sigma)
+
+        def evaluate(x):
+            from .geometry import points
+
+            pts = np.atleast_2d(np.asarray(x, float))
+            op = GpuOperator(self.kernel, points(pts), self.source, None, "fp64", self.ctx)
+            u = op.matvec(sigma)
+            return u if np.ndim(x) > 1 else u[0]
+
+        return evaluate
+
+
+def single_double_layer_potential(*, op, source: Quadrature, ctx: Context | None = None):
+    """src/api.jl:220-226."""
+    return IntegralPotential(SingleLayerKernel(op), source, ctx), IntegralPotential(DoubleLayerKernel(op), source, ctx)
+
+
+# ----------------------------------------------------------------------------
+# solver
+# ----------------------------------------------------------------------------
+def gmres(L_, b, *, x0=None, rtol: float = 1e-10, restart: int = 100, maxiter: int = 1000,
+          mode: str = "fp64", history: bool = False):
+    """Solve ``L x = b`` for ``L = shift·I + Σ c_t·op_t`` on the GPU.
+
+    ``mode="fp64"``: restarted GMRES on the FP64 operators.  ``mode="mixed"``:
+    FP64 residuals, FP32C inner GMRES, iterative refinement.  Convergence is
+    ``‖b − L x‖₂ ≤ rtol·‖b‖₂`` with the residual formed in FP64.  Returns
+    ``(x, stats)``; ``stats["history"]`` holds relative residuals when
+    requested.
+    """
+    Lc = LinearCombination.of(L_) if not isinstance(L_, LinearCombination) else L_
+    if not Lc.terms:
+        raise L.ArgumentError(L.E_ARG, "the operator has no GPU terms")
+    ops = [t for _, t in Lc.terms]
+    ctx = ops[0].ctx
+    cplx = Lc.is_complex
+    n = ops[0].shape[1]
+    b = _as_density(b, cplx, n, "b")
+    x = np.zeros(n, b.dtype) if x0 is None else _as_density(x0, cplx, n, "x0").copy()
+    handles = (C.c_void_p * len(ops))(*[o.handle.value for o in ops])
+    coefs = (C.c_double * (2 * len(ops)))()
+    for i, (c, _) in enumerate(Lc.terms):
+        c = complex(c)
+        coefs[2 * i], coefs[2 * i + 1] = c.real, c.imag
+    sh = L.cpair(Lc.shift)
+    hist = np.zeros(maxiter + 1) if history else None
+    st = L.GmresStats()
+    m = {"fp64": L.GMRES_FP64, "mixed": L.GMRES_MIXED}.get(mode)
+    if m is None:
+        raise L.ArgumentError(L.E_ARG, f"unknown mode {mode!r}")
+    ctx.check(ctx.lib.inti_gmres(ctx.handle, len(ops), handles, coefs, sh, L.dptr(b), L.dptr(x), rtol,
+                                 restart, maxiter, m, 0, L.dptr(hist), C.byref(st)))
+    stats = st.as_dict()
+    if history:
+        stats["history"] = hist[: st.iterations + 1]
+    return x, stats

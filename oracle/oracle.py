@@ -1,0 +1,231 @@
+"""TEST INFRASTRUCTURE — ctypes binding of the CPU oracle (inti_oracle.cpp).
+
+Imported only by tests/, __graft_entry__.smoke() (as the checker) and the
+cpu_baseline / reference legs of bench.py.  The oracle is the FP64 CPU
+restatement of Inti.jl's operator path; see the header of inti_oracle.cpp
+for what pins it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB = HERE / "_build" / "liboracle.so"
+
+LAPLACE, HELMHOLTZ = 0, 1
+SL, DL, ADL, HS = 0, 1, 2, 3
+
+_lib = None
+
+
+def build() -> Path:
+    """Compile the oracle with the system g++ (no OpenMP dependency)."""
+    env = dict(os.environ)
+    # the image's default CXX wrapper may lack pieces of the toolchain
+    if Path("/usr/bin/g++").exists():
+        env["CXX"] = "/usr/bin/g++"
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True, env=env)
+    return LIB
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB.exists() or LIB.stat().st_mtime < (HERE / "inti_oracle.cpp").stat().st_mtime:
+            build()
+        _lib = C.CDLL(str(LIB))
+        P, D, I64 = C.c_void_p, C.c_double, C.c_int64
+        _lib.or_kernel.argtypes = [C.c_int, C.c_int, C.c_int, D, P, P, P, P, P]
+        _lib.or_apply.argtypes = [C.c_int, C.c_int, C.c_int, D, I64, I64, P, P, I64, P, P, P, P, P, C.c_int]
+        _lib.or_assemble.argtypes = [C.c_int, C.c_int, C.c_int, D, I64, P, P, I64, P, P, P, P, C.c_int]
+        _lib.or_csr_apply.argtypes = [I64, P, P, P, C.c_int, P, P]
+        _lib.or_coo_to_csr.argtypes = [I64, I64, P, P, P, C.c_int, P, P, P]
+        _lib.or_coo_to_csr.restype = I64
+        _lib.or_dim_sources.argtypes = [C.c_int, C.c_int, D, P, P]
+        _lib.or_bdim.argtypes = [C.c_int, C.c_int, D, I64, P, P, P, C.c_int, C.c_int, P, I64, P, P, P, P,
+                                 C.c_int]
+        _lib.or_gmres.argtypes = [C.c_int, C.c_int, D, I64, P, P, P, D, D, C.c_int, P, P, P, P, P, P, P, D,
+                                  C.c_int, C.c_int, C.c_int, P, P, C.c_int]
+        _lib.or_dl_potential_jvp.argtypes = [I64, P, I64, P, P, P, P, P, P, P, P, P, P, C.c_int]
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _c(a, dt=np.float64):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+def kernel(pde, kind, k, x, nx, y, ny) -> complex:
+    x, y = _c(x), _c(y)
+    nx = _c(nx if nx is not None else np.zeros_like(x))
+    ny = _c(ny if ny is not None else np.zeros_like(y))
+    out = np.zeros(2)
+    st = lib().or_kernel(pde, kind, len(x), k, _p(x), _p(nx), _p(y), _p(ny), _p(out))
+    if st:
+        raise ValueError("unsupported kernel")
+    return complex(out[0], out[1])
+
+
+def apply(pde, kind, k, tcoords, tnormals, scoords, snormals, sweights, sigma, rows=None,
+          nthreads=0) -> np.ndarray:
+    """Rows of y = A sigma, A_ij = K(x_i, y_j) w_j (on the fly)."""
+    tc, sc = _c(tcoords), _c(scoords)
+    dim = tc.shape[1]
+    m, n = tc.shape[0], sc.shape[0]
+    tn, sn, sw = _c(tnormals), _c(snormals), _c(sweights)
+    cplx = pde == HELMHOLTZ
+    sig = _c(sigma, np.complex128 if cplx else np.float64)
+    if rows is None:
+        out = np.zeros(m, sig.dtype)
+        lib().or_apply(pde, kind, dim, k, 0, m, _p(tc), _p(tn), n, _p(sc), _p(sn), _p(sw), _p(sig), _p(out),
+                       nthreads)
+        return out
+    rows = np.asarray(rows, np.int64)
+    out = np.zeros(len(rows), sig.dtype)
+    tmp = np.zeros(1, sig.dtype)
+    for q, r in enumerate(rows):
+        lib().or_apply(pde, kind, dim, k, int(r), 1, _p(tc), _p(tn), n, _p(sc), _p(sn), _p(sw), _p(sig),
+                       _p(tmp), nthreads)
+        out[q] = tmp[0]
+    return out
+
+
+def apply_rows_block(pde, kind, k, tcoords, tnormals, scoords, snormals, sweights, sigma, row0, nrows,
+                     nthreads=0):
+    tc, sc = _c(tcoords), _c(scoords)
+    dim = tc.shape[1]
+    n = sc.shape[0]
+    cplx = pde == HELMHOLTZ
+    sig = _c(sigma, np.complex128 if cplx else np.float64)
+    out = np.zeros(nrows, sig.dtype)
+    lib().or_apply(pde, kind, dim, k, int(row0), int(nrows), _p(tc), _p(_c(tnormals)), n, _p(sc),
+                   _p(_c(snormals)), _p(_c(sweights)), _p(sig), _p(out), nthreads)
+    return out
+
+
+def assemble(pde, kind, k, tcoords, tnormals, scoords, snormals, sweights, nthreads=0) -> np.ndarray:
+    tc, sc = _c(tcoords), _c(scoords)
+    m, n, dim = tc.shape[0], sc.shape[0], tc.shape[1]
+    cplx = pde == HELMHOLTZ
+    out = np.zeros((m, n), np.complex128 if cplx else np.float64, order="F")
+    lib().or_assemble(pde, kind, dim, k, m, _p(tc), _p(_c(tnormals)), n, _p(sc), _p(_c(snormals)),
+                      _p(_c(sweights)), _p(out), nthreads)
+    return out
+
+
+def csr_apply(indptr, indices, data, x) -> np.ndarray:
+    indptr = _c(indptr, np.int64)
+    indices = _c(indices, np.int32)
+    cplx = np.iscomplexobj(data) or np.iscomplexobj(x)
+    data = _c(data, np.complex128 if cplx else np.float64)
+    x = _c(x, data.dtype)
+    y = np.zeros(len(indptr) - 1, data.dtype)
+    lib().or_csr_apply(len(indptr) - 1, _p(indptr), _p(indices), _p(data), int(cplx), _p(x), _p(y))
+    return y
+
+
+def coo_to_csr(m, I, J, V):
+    """The CSR of ``sparse(I, J, V, m, n)``: duplicates summed, rows sorted."""
+    I, J = _c(I, np.int64), _c(J, np.int64)
+    cplx = np.iscomplexobj(V)
+    V = _c(V, np.complex128 if cplx else np.float64)
+    nnz = len(I)
+    rp = np.zeros(m + 1, np.int64)
+    col = np.zeros(max(nnz, 1), np.int32)
+    val = np.zeros(max(nnz, 1), V.dtype)
+    out = lib().or_coo_to_csr(m, nnz, _p(I), _p(J), _p(V), int(cplx), _p(rp), _p(col), _p(val))
+    return rp, col[:out], val[:out]
+
+
+def dim_sources(dim, ns, R, c):
+    c = _c(c)
+    xs = np.zeros((ns, dim))
+    lib().or_dim_sources(dim, ns, R, _p(c), _p(xs))
+    return xs
+
+
+def bdim(pde, k, coords, normals, weights, nq, derivative=False, green_multiplier=None, elements=None,
+         nthreads=0, return_theta=False):
+    """Block values of (δS, δD) for the selected elements (all if None):
+    arrays (nsel*nq, nq); row q*nq+t, column a <-> target e*nq+t, source
+    e*nq+a."""
+    x, nrm, w = _c(coords), _c(normals), _c(weights)
+    n, dim = x.shape
+    cplx = pde == HELMHOLTZ
+    sel = None if elements is None else _c(elements, np.int64)
+    nsel = n // nq if sel is None else len(sel)
+    dt = np.complex128 if cplx else np.float64
+    dS = np.zeros((nsel * nq, nq), dt)
+    dD = np.zeros((nsel * nq, nq), dt)
+    ns = int(np.ceil(3 * nq))
+    theta = np.zeros((nsel * nq, ns), np.complex128) if return_theta else None
+    gm = None if green_multiplier is None else _c(np.broadcast_to(green_multiplier, (n,)))
+    st = lib().or_bdim(pde, dim, k, n, _p(x), _p(nrm), _p(w), nq, int(derivative), _p(gm),
+                       nsel if sel is not None else 0, _p(sel), _p(dS), _p(dD), _p(theta), nthreads)
+    if st:
+        raise ValueError(f"or_bdim failed ({st})")
+    return (dS, dD, theta) if return_theta else (dS, dD)
+
+
+def block_csr(values, nq, elements=None, n=None):
+    """CSR arrays of the element-block pattern for block values from bdim()."""
+    nsel = values.shape[0] // nq
+    els = np.arange(nsel) if elements is None else np.asarray(elements)
+    rows = (els[:, None] * nq + np.arange(nq)[None, :]).reshape(-1)
+    I = np.repeat(rows, nq)
+    J = np.repeat(els * nq, nq * nq) + np.tile(np.arange(nq), nsel * nq)
+    m = n if n is not None else int(rows.max()) + 1
+    return coo_to_csr(m, I, J, values.reshape(-1))
+
+
+def gmres(pde, k, coords, normals, weights, shift, terms, b, rtol=1e-10, restart=100, maxiter=200,
+          nthreads=0):
+    """terms: list of (kind, coef, csr or None) with csr = (indptr, indices, data)."""
+    x, nrm, w = _c(coords), _c(normals), _c(weights)
+    n, dim = x.shape
+    cplx = pde == HELMHOLTZ or np.iscomplexobj(b) or any(isinstance(c, complex) for _, c, _ in terms) or \
+        isinstance(shift, complex)
+    dt = np.complex128 if cplx else np.float64
+    b = _c(b, dt)
+    sol = np.zeros(n, dt)
+    nt = len(terms)
+    kinds = (C.c_int * nt)(*[t[0] for t in terms])
+    coefs = (C.c_double * (2 * nt))()
+    keep = []
+    rps = (C.c_void_p * nt)()
+    cols = (C.c_void_p * nt)()
+    vals = (C.c_void_p * nt)()
+    for i, (kind, c, csr) in enumerate(terms):
+        c = complex(c)
+        coefs[2 * i], coefs[2 * i + 1] = c.real, c.imag
+        if csr is not None:
+            rp, col, val = _c(csr[0], np.int64), _c(csr[1], np.int32), _c(csr[2], np.complex128 if cplx else np.float64)
+            keep += [rp, col, val]
+            rps[i], cols[i], vals[i] = rp.ctypes.data, col.ctypes.data, val.ctypes.data
+    hist = np.zeros(maxiter + 1)
+    fr = C.c_double()
+    shift = complex(shift)
+    if pde == HELMHOLTZ and not cplx:
+        raise ValueError
+    it = lib().or_gmres(pde, dim, k, n, _p(x), _p(nrm), _p(w), shift.real, shift.imag, nt, kinds, coefs,
+                        C.cast(rps, C.c_void_p), C.cast(cols, C.c_void_p), C.cast(vals, C.c_void_p),
+                        _p(b), _p(sol), rtol, restart, maxiter, int(cplx), _p(hist), C.byref(fr), nthreads)
+    return sol, {"iterations": it, "relres": fr.value, "history": hist[: it + 1]}
+
+
+def dl_potential_jvp(tcoords, scoords, snormals, sweights, sigma, dsx=None, dsn=None, dsw=None, dsigma=None,
+                     nthreads=0):
+    tc, sc, sn, sw, sg = map(_c, (tcoords, scoords, snormals, sweights, sigma))
+    m, n = tc.shape[0], sc.shape[0]
+    u, du = np.zeros(m), np.zeros(m)
+    lib().or_dl_potential_jvp(m, _p(tc), n, _p(sc), _p(sn), _p(sw), _p(sg), _p(_c(dsx)), _p(_c(dsn)),
+                              _p(_c(dsw)), _p(_c(dsigma)), _p(u), _p(du), nthreads)
+    return u, du

@@ -1,0 +1,106 @@
+"""GPU pair product versus the oracle, through the C ABI (ctypes).
+
+FP64: relative 2-norm error <= 1e-12 (the reference's matrix-free vs
+entry-wise test allows 1e-7, test/fmm3d_test.jl:42).  FP32C: <= 2e-5 for
+Laplace, <= 5e-5 for Helmholtz (FP32 kernel evaluation with compensated sums).
+"""
+import numpy as np
+import pytest
+
+import inti_b200 as inti
+import oracle as O
+from helpers import density, oracle_apply, relerr, small_surfaces
+
+pytestmark = pytest.mark.gpu
+
+SURF = small_surfaces()
+KINDS = [("SL", inti.SingleLayerKernel, O.SL), ("DL", inti.DoubleLayerKernel, O.DL),
+         ("ADL", inti.AdjointDoubleLayerKernel, O.ADL), ("HS", inti.HyperSingularKernel, O.HS)]
+
+
+def ops_for(q):
+    if q.dim == 2:
+        return [(inti.Laplace(dim=2), O.LAPLACE, 0.0)]
+    return [(inti.Laplace(dim=3), O.LAPLACE, 0.0), (inti.Helmholtz(k=4.0, dim=3), O.HELMHOLTZ, 4.0)]
+
+
+CASES = [(s, ki) for s in SURF for ki in range(4)]
+
+
+@pytest.mark.parametrize("surf,ki", CASES)
+def test_fp64_matches_oracle(ctx, surf, ki):
+    q = SURF[surf]
+    name, Kc, kind = KINDS[ki]
+    for op, pde, k in ops_for(q):
+        A = inti.IntegralOperator(Kc(op), q, q, ctx=ctx)
+        x = density(len(q), pde == O.HELMHOLTZ, seed=ki + 3)
+        y = A @ x
+        ref = oracle_apply(pde, kind, k, q, q, x)
+        assert relerr(y, ref) < 1e-12, (surf, name, op)
+
+
+@pytest.mark.parametrize("surf,ki", CASES)
+def test_fp32c_matches_oracle(ctx, surf, ki):
+    q = SURF[surf]
+    name, Kc, kind = KINDS[ki]
+    for op, pde, k in ops_for(q):
+        A = inti.IntegralOperator(Kc(op), q, q, precision="fp32c", ctx=ctx)
+        x = density(len(q), pde == O.HELMHOLTZ, seed=ki + 7)
+        ref = oracle_apply(pde, kind, k, q, q, x)
+        tol = 5e-5 if pde == O.HELMHOLTZ else 2e-5
+        assert relerr(A @ x, ref) < tol, (surf, name, op)
+
+
+def test_off_surface_targets_and_potential(ctx):
+    q = SURF["ellipsoid"]
+    tgt = inti.points(1.7 * SURF["ellipsoid"].coords[::5])
+    sigma = density(len(q), False, 11)
+    Spot, Dpot = inti.single_double_layer_potential(op=inti.Laplace(dim=3), source=q, ctx=ctx)
+    u = Dpot[sigma](tgt.coords)
+    ref = O.apply(O.LAPLACE, O.DL, 0.0, tgt.coords, None, q.coords, q.normals, q.weights, sigma)
+    assert relerr(u, ref) < 1e-12
+    # exterior points: the double layer of a constant vanishes (Gauss's law)
+    assert np.max(np.abs(Dpot[np.ones(len(q))](tgt.coords))) < 1e-3
+
+
+def test_alpha_beta_and_multi_rhs(ctx):
+    q = SURF["p2sphere"]
+    op = inti.Helmholtz(k=3.0, dim=3)
+    A = inti.IntegralOperator(inti.DoubleLayerKernel(op), q, ctx=ctx)
+    X = np.stack([density(len(q), True, s) for s in range(3)], 1)
+    Y0 = np.stack([density(len(q), True, 10 + s) for s in range(3)], 1)
+    alpha, beta = 0.3 - 1.1j, -0.7 + 0.2j
+    Y = Y0.copy()
+    A.mul(Y, X, alpha, beta)
+    for c in range(3):
+        ref = alpha * oracle_apply(O.HELMHOLTZ, O.DL, 3.0, q, q, X[:, c]) + beta * Y0[:, c]
+        assert relerr(Y[:, c], ref) < 1e-12
+    # beta = 0 must not read y (NaN in y is ignored, BLAS semantics)
+    Yn = np.full_like(Y0, np.nan)
+    A.mul(Yn, X, 1.0, 0.0)
+    assert np.isfinite(Yn).all()
+
+
+def test_dense_assembly_matches_oracle(ctx):
+    q = SURF["kite"]
+    for Kc, kind in ((inti.SingleLayerKernel, O.SL), (inti.HyperSingularKernel, O.HS)):
+        A = inti.assemble_matrix(inti.IntegralOperator(Kc(inti.Laplace(dim=2)), q, ctx=ctx))
+        ref = O.assemble(O.LAPLACE, kind, 0.0, q.coords, q.normals, q.coords, q.normals, q.weights)
+        assert relerr(A, ref) < 1e-13
+
+
+def test_transpose_apply(ctx):
+    q = SURF["ellipsoid"]
+    for op, pde, k in ops_for(q):
+        A = inti.IntegralOperator(inti.DoubleLayerKernel(op), q, ctx=ctx)
+        dense = O.assemble(pde, O.DL, k, q.coords, q.normals, q.coords, q.normals, q.weights)
+        g = density(len(q), pde == O.HELMHOLTZ, 21)
+        assert relerr(A.rmatvec(g), dense.T @ g) < 1e-12
+
+
+def test_launch_counter_advances(ctx):
+    q = SURF["kite"]
+    A = inti.IntegralOperator(inti.DoubleLayerKernel(inti.Laplace(dim=2)), q, ctx=ctx)
+    before = ctx.launch_count
+    A @ np.ones(len(q))
+    assert ctx.launch_count - before == 3  # pack, pair, epilogue

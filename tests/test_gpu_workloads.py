@@ -1,0 +1,87 @@
+"""Full-size workloads: sampled-row parity with the oracle (the pattern of
+test/fmm3d_test.jl:40-42, 64 seeded rows instead of 10) and size-independent
+properties (linearity, Gauss's law) where a full CPU product would take
+minutes."""
+import numpy as np
+import pytest
+
+import inti_b200 as inti
+import oracle as O
+from helpers import density, oracle_apply, relerr
+
+pytestmark = pytest.mark.gpu
+
+ROWS = np.random.default_rng(1234).choice
+
+
+@pytest.fixture(scope="module")
+def sphere_c2(ctx):
+    q = inti.p2_sphere_quadrature(36)
+    op = inti.Helmholtz(k=10.0, dim=3)
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    return q, S, D
+
+
+def _sampled(q, nrows, seed):
+    r = np.random.default_rng(seed)
+    els = np.sort(r.choice(q.nel, nrows // q.nq + 1, replace=False))
+    rows = (els[:, None] * q.nq + np.arange(q.nq)).reshape(-1)
+    return els, rows
+
+
+def test_c2_helmholtz_sl_sampled_rows(sphere_c2):
+    q, S, _ = sphere_c2
+    assert len(q) == 62208
+    sigma = density(len(q), True, 1)
+    y = S @ sigma
+    els, rows = _sampled(q, 64, 7)
+    pair = oracle_apply(O.HELMHOLTZ, O.SL, 10.0, q, q, sigma, rows=rows)
+    dS, _ = O.bdim(O.HELMHOLTZ, 10.0, q.coords, q.normals, q.weights, q.nq, elements=els)
+    corr = np.einsum("ra,ra->r", dS, sigma[(rows // q.nq)[:, None] * q.nq + np.arange(q.nq)])
+    assert relerr(y[rows], pair + corr) < 1e-10
+
+
+def test_c2_correction_pattern_and_linearity(sphere_c2):
+    q, S, _ = sphere_c2
+    rp, col, val = S.correction.arrays()
+    assert S.correction.nnz == 6 * len(q)
+    assert np.array_equal(rp, np.arange(len(q) + 1) * 6)
+    assert np.array_equal(col, np.repeat(np.arange(len(q)) // 6 * 6, 6) + np.tile(np.arange(6), len(q)))
+    a, b = 0.3 + 0.2j, -1.1
+    x, z = density(len(q), True, 2), density(len(q), True, 3)
+    lhs = S @ (a * x + b * z)
+    rhs = a * (S @ x) + b * (S @ z)
+    assert relerr(lhs, rhs) < 1e-12
+    # S[1] on the unit sphere = e^{ik} sin(k)/k up to discretisation error
+    ref = np.exp(10j) * np.sin(10.0) / 10.0
+    s1 = S @ np.ones(len(q), complex)
+    assert np.median(np.abs(s1 - ref)) < 1e-3
+
+
+@pytest.fixture(scope="module")
+def ellipsoid_c3(ctx):
+    q = inti.ellipsoid_quadrature(61, 5)
+    op = inti.Laplace(dim=3)
+    dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
+    D64 = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, "fp64", ctx)
+    D32 = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, "fp32c", ctx)
+    return q, dD, D64, D32
+
+
+def test_c3_laplace_dl_sampled_rows(ellipsoid_c3):
+    q, dD, D64, D32 = ellipsoid_c3
+    assert len(q) == 200934
+    sigma = density(len(q), False, 5)
+    els, rows = _sampled(q, 64, 9)
+    _, dDo = O.bdim(O.LAPLACE, 0.0, q.coords, q.normals, q.weights, q.nq, elements=els)
+    corr = np.einsum("ra,ra->r", dDo, sigma[(rows // q.nq)[:, None] * q.nq + np.arange(q.nq)])
+    ref = oracle_apply(O.LAPLACE, O.DL, 0.0, q, q, sigma, rows=rows) + corr
+    assert relerr((D64 @ sigma)[rows], ref) < 1e-11
+    assert relerr((D32 @ sigma)[rows], ref) < 2e-5
+
+
+def test_c3_gauss_law_full_size(ellipsoid_c3):
+    q, dD, D64, D32 = ellipsoid_c3
+    one = np.ones(len(q))
+    assert np.max(np.abs(D64 @ one + 0.5)) < 1e-6
+    assert np.max(np.abs(D32 @ one + 0.5)) < 1e-5
