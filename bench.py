@@ -39,7 +39,7 @@ sys.path.insert(0, str(ROOT / "inti.jl_b200"))
 
 import numpy as np  # noqa: E402
 
-METRIC = "G kernel-pairs/s (Helmholtz SL, FP64, N=62208, DIM-corrected matvec)"
+METRIC = "G kernel-pairs/s"
 UNIT = "Gpairs/s"
 # Algorithmic flops per pair (FMA = 2 flops; special functions counted apart)
 FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10}
@@ -65,7 +65,7 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={q}",
-                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                       "--format=csv,noheader,nounits", "-lms", "50"],
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
@@ -95,27 +95,61 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def build_c2(ctx):
+def build_workload(name: str, ctx):
+    """(quadrature, operator, density, flops key, dtype, config) of a named
+    workload.  "c2" is the headline; the others exist to time and profile
+    the other pair kernels with the same driver."""
     import inti_b200 as inti
 
-    q = inti.p2_sphere_quadrature(36)
-    op = inti.Helmholtz(k=10.0, dim=3)
-    t0 = time.perf_counter()
-    dS, _ = inti.bdim_correction(op, q, q, ctx=ctx)
-    t_dim = time.perf_counter() - t0
-    S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, "fp64", ctx)
     r = np.random.default_rng(1)
-    sigma = (r.standard_normal(len(q)) + 1j * r.standard_normal(len(q))) / np.sqrt(2)
-    return q, S, sigma, t_dim
+    if name == "c2":
+        q = inti.p2_sphere_quadrature(36)
+        op = inti.Helmholtz(k=10.0, dim=3)
+        kern, key, prec, dt = inti.SingleLayerKernel(op), "helmholtz_sl", "fp64", "c128"
+        wl = "helmholtz3d_sl_k10_p2sphere_N62208_dim"
+    elif name == "c2_dl":
+        q = inti.p2_sphere_quadrature(36)
+        op = inti.Helmholtz(k=10.0, dim=3)
+        kern, key, prec, dt = inti.DoubleLayerKernel(op), "helmholtz_dl", "fp64", "c128"
+        wl = "helmholtz3d_dl_k10_p2sphere_N62208_dim"
+    elif name in ("c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64"):
+        q = inti.ellipsoid_quadrature(61, 5)
+        op = inti.Laplace(dim=3)
+        prec = "fp32c" if name.endswith("fp32c") else "fp64"
+        sl = name.startswith("c3_sl")
+        kern = inti.SingleLayerKernel(op) if sl else inti.DoubleLayerKernel(op)
+        key, dt = ("laplace_sl" if sl else "laplace_dl"), ("f32" if prec == "fp32c" else "f64")
+        wl = f"laplace3d_{'sl' if sl else 'dl'}_ellipsoid_N200934_dim_{prec}"
+    elif name == "c1":
+        q = inti.kite_quadrature(200, 9)
+        op = inti.Laplace(dim=2)
+        kern, key, prec, dt = inti.DoubleLayerKernel(op), "laplace2d_dl", "fp64", "f64"
+        wl = "laplace2d_dl_kite_N1000_dim"
+    else:
+        raise SystemExit(f"unknown workload {name}")
+    t0 = time.perf_counter()
+    dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
+    t_dim = time.perf_counter() - t0
+    corr = dS if isinstance(kern, inti.SingleLayerKernel) else dD
+    A = inti.GpuOperator(kern, q, q, corr, prec, ctx)
+    n = len(q)
+    if A.is_complex:
+        sigma = (r.standard_normal(n) + 1j * r.standard_normal(n)) / np.sqrt(2)
+    else:
+        sigma = r.standard_normal(n)
+    cfg = {"workload": wl, "n": n, "nnz_per_row": q.nq, "precision": prec, "dim_setup_s": t_dim}
+    return q, A, sigma, key, dt, cfg
 
 
-def cpu_sample(q, sigma, seconds: float, nthreads: int) -> dict:
+def cpu_sample(q, A, sigma, seconds: float, nthreads: int) -> dict:
     """The oracle's on-the-fly FP64 row sums on a bounded sample of rows."""
     sys.path.insert(0, str(ROOT / "oracle"))
     import oracle as O
 
     n = len(q)
-    args = (O.HELMHOLTZ, O.SL, 10.0, q.coords, q.normals, q.coords, q.normals, q.weights, sigma)
+    pde = O.HELMHOLTZ if A.is_complex else O.LAPLACE
+    k = float(getattr(A.kernel.op, "k", 0.0))
+    args = (pde, A.kernel.kind, k, q.coords, q.normals, q.coords, q.normals, q.weights, sigma)
     t0 = time.perf_counter()
     rows0 = max(8 * nthreads, 32)
     O.apply_rows_block(*args, 0, rows0, nthreads=nthreads)
@@ -202,12 +236,14 @@ def gmres_c3(ctx) -> dict:
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-gmres", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="c2",
+                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -231,13 +267,14 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ctx = inti.Context(local)
     peaks = ctx.measure_peaks()
-    q, S, sigma, t_dim = build_c2(ctx)
+    q, S, sigma, fkey, dtype, cfg = build_workload(args.workload, ctx)
     n = len(q)
     pairs = float(n) * n
     stream = torch.cuda.ExternalStream(ctx.stream, device=f"cuda:{local}")
     dev = torch.device(f"cuda:{local}")
-    xs = torch.from_numpy(sigma.view(np.float64).copy()).to(dev)
-    ys = torch.zeros(2 * n, dtype=torch.float64, device=dev)
+    comps = 2 if S.is_complex else 1
+    xs = torch.from_numpy(np.ascontiguousarray(sigma).view(np.float64).copy()).to(dev)
+    ys = torch.zeros(comps * n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     torch.cuda.synchronize(dev)
     with torch.cuda.stream(stream):
@@ -277,7 +314,7 @@ def main() -> None:
 
     # e2e through the public API with pinned host buffers
     hx = torch.from_numpy(sigma.copy()).pin_memory().numpy()
-    hy = torch.zeros(n, dtype=torch.complex128).pin_memory().numpy()
+    hy = torch.zeros(n, dtype=torch.complex128 if S.is_complex else torch.float64).pin_memory().numpy()
     for _ in range(2):
         S.mul(hy, hx)
     if dist:
@@ -290,34 +327,35 @@ def main() -> None:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": world * pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 16 * n,
-           "d2h_bytes_per_step": 16 * n, "ms_per_step": e2e_s * 1e3}
+    e2e = {"value": world * pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * comps * n,
+           "d2h_bytes_per_step": 8 * comps * n, "ms_per_step": e2e_s * 1e3}
 
     # roofline of the dominant kernel (the pair kernel)
     kern_ms = pair_ms / max(pair_launches, 1)
-    achieved = pairs * FLOPS_PER_PAIR["helmholtz_sl"] / (kern_ms * 1e-3) / 1e12
-    peak = peaks["fp64_flops"] / 1e12
-    roofline = {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": PAIR_TRAFFIC_BYTES,
-                "kernel": "pair_forward<Helmholtz,SL,3,double>", "kernel_ms": kern_ms,
-                "flops_per_pair": FLOPS_PER_PAIR["helmholtz_sl"],
-                "peak_source": "FP64 FMA throughput measured in this run (inti_measure_peaks)",
+    fp32 = cfg["precision"] == "fp32c"
+    achieved = pairs * FLOPS_PER_PAIR[fkey] / (kern_ms * 1e-3) / 1e12
+    peak = peaks["fp32_flops" if fp32 else "fp64_flops"] / 1e12
+    roofline = {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak,
+                "traffic": PAIR_TRAFFIC_BYTES if args.workload == "c2" else None,
+                "kernel": f"pair_forward ({fkey}, {'float' if fp32 else 'double'})", "kernel_ms": kern_ms,
+                "flops_per_pair": FLOPS_PER_PAIR[fkey],
+                "peak_source": f"{'FP32' if fp32 else 'FP64'} FMA throughput measured in this run "
+                               "(inti_measure_peaks), of measured",
                 "share_of_step": pair_ms / max(sum(step_ms), 1e-9),
                 "other_kernels_ms": {"pack": pack_ms / args.steps, "epilogue": epi_ms / args.steps}}
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "helmholtz3d_sl_k10_p2sphere_N62208_dim", "n": n, "nnz_per_row": 6,
-                   "precision": "fp64", "parallelism": f"replicas{world}", "l2": "flushed between steps",
-                   "dim_setup_s": t_dim},
+        "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+        "config": dict(cfg, parallelism=f"replicas{world}", l2="flushed between steps"),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk,
         "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_sample(q, sigma, args.cpu_seconds, host_cores())
-    if not args.no_gmres and world == 1:
+        line["cpu_baseline"] = cpu_sample(q, S, sigma, args.cpu_seconds, host_cores())
+    if not args.no_gmres and world == 1 and args.workload == "c2":
         line["gmres"] = gmres_c3(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)

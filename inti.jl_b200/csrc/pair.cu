@@ -684,9 +684,11 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       using R = decltype(rtag);
       constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
       const int pb = 256;
-      ProfScope ps(ctx, "pack");
-      pack_sources<T::pde, T::kind, T::dim, R><<<(unsigned)((npad + pb - 1) / pb), pb, 0, ctx->stream>>>(
-          L.n, npad, L.scoords, L.snormals, L.sweights, L.x, static_cast<R*>(L.packed));
+      {
+        ProfScope ps(ctx, "pack");
+        pack_sources<T::pde, T::kind, T::dim, R><<<(unsigned)((npad + pb - 1) / pb), pb, 0, ctx->stream>>>(
+            L.n, npad, L.scoords, L.snormals, L.sweights, L.x, static_cast<R*>(L.packed));
+      }
       FwdArgs a;
       a.m = L.m;
       a.n_tiles = L.n_tiles;

@@ -43,6 +43,8 @@ __all__ = [
     "DoubleLayerKernel",
     "AdjointDoubleLayerKernel",
     "HyperSingularKernel",
+    "GpuOperator",
+    "LinearCombination",
     "IntegralOperator",
     "assemble_matrix",
     "CorrectionMatrix",
@@ -445,6 +447,8 @@ class GpuOperator(_Map):
             m, n = n, m
         x = np.asarray(x)
         single = x.ndim == 1
+        if x.shape[0] != n:
+            raise L.DimensionMismatch(L.E_SHAPE, f"x has {x.shape[0]} rows, expected {n}")
         X = _as_density(x.reshape(n, -1) if single else x, self.is_complex, n)
         X = np.asfortranarray(X)
         nrhs = X.shape[1]

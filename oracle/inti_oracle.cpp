@@ -520,6 +520,38 @@ int or_bdim(int pde, int dim, double k, int64_t n, const double* x, const double
                        reinterpret_cast<cd*>(dS), reinterpret_cast<cd*>(dD), theta_out, nthreads);
 }
 
+// Per-node monopole traces of the DIM construction (src/bdim.jl:94-103):
+// g0[j, k] = G(y_j, xs_k), g1[j, k] = ADL(y_j, xs_k), interleaved complex,
+// n x ns row-major; used by the tests to form each element's least-squares
+// matrix and its condition number.
+int or_dim_traces(int pde, int dim, double k, int64_t n, const double* x, const double* nrm,
+                  int nq, double* g0, double* g1) {
+  const int ns = (int)std::ceil(3.0 * nq);
+  double lc[3] = {INFINITY, INFINITY, INFINITY}, hc[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t j = 0; j < n; ++j)
+    for (int c = 0; c < dim; ++c) {
+      lc[c] = std::min(lc[c], x[dim * j + c]);
+      hc[c] = std::max(hc[c], x[dim * j + c]);
+    }
+  double xc[3], diag2 = 0.0;
+  for (int c = 0; c < dim; ++c) {
+    xc[c] = (lc[c] + hc[c]) / 2;
+    diag2 += (hc[c] - lc[c]) * (hc[c] - lc[c]);
+  }
+  std::vector<double> xs((size_t)ns * dim);
+  or_dim_sources(dim, ns, 1.5 * std::sqrt(diag2) / 2, xc, xs.data());
+  for (int64_t j = 0; j < n; ++j)
+    for (int kk = 0; kk < ns; ++kk) {
+      const cd a = eval_kernel(pde, OR_SL, dim, k, x + dim * j, nrm + dim * j, &xs[dim * kk], nullptr);
+      const cd b = eval_kernel(pde, OR_ADL, dim, k, x + dim * j, nrm + dim * j, &xs[dim * kk], nullptr);
+      g0[2 * (j * ns + kk)] = a.real();
+      g0[2 * (j * ns + kk) + 1] = a.imag();
+      g1[2 * (j * ns + kk)] = b.real();
+      g1[2 * (j * ns + kk) + 1] = b.imag();
+    }
+  return ns;
+}
+
 }  // extern "C"
 
 // --------------------------------------------------------------------------

@@ -51,6 +51,7 @@ def lib() -> C.CDLL:
                                  C.c_int]
         _lib.or_gmres.argtypes = [C.c_int, C.c_int, D, I64, P, P, P, D, D, C.c_int, P, P, P, P, P, P, P, D,
                                   C.c_int, C.c_int, C.c_int, P, P, C.c_int]
+        _lib.or_dim_traces.argtypes = [C.c_int, C.c_int, D, I64, P, P, C.c_int, P, P]
         _lib.or_dl_potential_jvp.argtypes = [I64, P, I64, P, P, P, P, P, P, P, P, P, P, C.c_int]
     return _lib
 
@@ -229,3 +230,19 @@ def dl_potential_jvp(tcoords, scoords, snormals, sweights, sigma, dsx=None, dsn=
     lib().or_dl_potential_jvp(m, _p(tc), n, _p(sc), _p(sn), _p(sw), _p(sg), _p(_c(dsx)), _p(_c(dsn)),
                               _p(_c(dsw)), _p(_c(dsigma)), _p(u), _p(du), nthreads)
     return u, du
+
+
+def dim_element_conds(pde, k, coords, normals, nq, elements=None):
+    """2-norm condition number of each element's least-squares matrix
+    M^T = [g0[el,:]; g1[el,:]]^T (ns x 2nq), src/bdim.jl:160-163."""
+    x, nrm = _c(coords), _c(normals)
+    n, dim = x.shape
+    ns = int(np.ceil(3 * nq))
+    g0 = np.zeros((n, ns), np.complex128)
+    g1 = np.zeros((n, ns), np.complex128)
+    lib().or_dim_traces(pde, dim, k, n, _p(x), _p(nrm), nq, _p(g0), _p(g1))
+    els = np.arange(n // nq) if elements is None else np.asarray(elements)
+    M = np.concatenate([g0.reshape(-1, nq, ns)[els], g1.reshape(-1, nq, ns)[els]], axis=1)
+    if pde == LAPLACE:
+        M = M.real
+    return np.linalg.cond(np.transpose(M, (0, 2, 1)))

@@ -39,3 +39,36 @@ def small_surfaces():
         "p2sphere": G.p2_sphere_quadrature(3),
         "star": G.star_quadrature(G.star_coefficients(np.random.default_rng(3)), 3),
     }
+
+
+EPS = np.finfo(float).eps
+
+
+def dim_values_close(pde, k, q, gpu_csr, ora_csr, elements=None, factor=1024.0):
+    """Condition-aware comparison of DIM weights: for each element block the
+    max deviation must stay below factor*eps*cond(M_e)*max|δ| (each weight is
+    the solution of a least-squares problem with matrix M_e^T, so no two
+    implementations agree beyond that).  Returns the worst ratio
+    deviation / allowance (<= 1 passes)."""
+    nq = q.nq
+    els = np.arange(q.nel) if elements is None else np.asarray(elements)
+    conds = O.dim_element_conds(pde, k, q.coords, q.normals, nq, els)
+    g_rp, g_col, g_val = gpu_csr
+    o_rp, o_col, o_val = ora_csr
+    worst = 0.0
+    for e, c in zip(els, conds):
+        rows = e * nq + np.arange(nq)
+        gv = np.concatenate([g_val[g_rp[i]:g_rp[i + 1]] for i in rows])
+        ov = np.concatenate([o_val[o_rp[i]:o_rp[i + 1]] for i in rows])
+        allow = factor * EPS * c * max(np.max(np.abs(ov)), 1e-300) + 1e-300
+        worst = max(worst, float(np.max(np.abs(gv - ov)) / allow))
+    return worst
+
+
+def harmonic_traces(pde, k, q, xs, c=0.7):
+    """γ₀u, γ₁u of u = c*G(·, xs) on the nodes of q (smooth densities)."""
+    g0 = np.array([O.kernel(pde, O.SL, k, x, n, xs, None) for x, n in zip(q.coords, q.normals)]) * c
+    g1 = np.array([O.kernel(pde, O.ADL, k, x, n, xs, None) for x, n in zip(q.coords, q.normals)]) * c
+    if pde == O.LAPLACE:
+        return g0.real.copy(), g1.real.copy()
+    return g0, g1
