@@ -145,6 +145,17 @@ int inti_csr_destroy(inti_csr* c);
 int inti_op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
                    const inti_quad* target, const inti_quad* source,
                    const inti_csr* correction, int precision, inti_op** out);
+/* A = c_dl*(D + C_dl) + c_sl*(S + C_sl) (3D) evaluated in ONE pass over the
+ * pairs: the combined-field operator the reference composes as a LinearMap
+ * sum (docs/src/examples/helmholtz_scattering.jl:485-486,
+ * L = I/2 + D - i*k*S).  c_dl, c_sl: 2 doubles each (re, im; real for
+ * Laplace).  The corrections (either may be NULL) are merged once into
+ * c_dl*C_dl + c_sl*C_sl.  inti_gmres fuses DL + SL terms into this operator
+ * by itself. */
+int inti_op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im,
+                            const inti_quad* target, const inti_quad* source,
+                            const inti_csr* corr_dl, const inti_csr* corr_sl, const double* c_dl,
+                            const double* c_sl, int precision, inti_op** out);
 int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype);
 /* Y = alpha*(A*X + C*X) + beta*Y for nrhs columns (leading dimensions ldx,
  * ldy in elements).  alpha, beta: 2 doubles each (re, im); NULL means 1, 0.
@@ -206,6 +217,13 @@ int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, doub
  * on this device, in operations per second (FMA counted as 2 flops). */
 int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops,
                        double* mufu_ops);
+
+/* Accuracy of the pair loops' fast special functions on this device, against
+ * extended-precision host values: out[0] max relative error of the FP64
+ * reciprocal square root over [1e-27, 1e27]; out[1], out[2] max absolute
+ * error of the FP64 e^{i theta} for theta <= 25 and theta <= 1000; out[3]
+ * the same for the FP32 form, theta <= 25. */
+int inti_selftest_math(inti_ctx* ctx, double* out);
 
 #ifdef __cplusplus
 }

@@ -112,6 +112,10 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
   L.split = op->split;
   L.n_tiles = op->n_tiles;
   L.err_flag = op->ctx->err_flag.as<int>();
+  L.c1[0] = op->c1[0];
+  L.c1[1] = op->c1[1];
+  L.c2[0] = op->c2[0];
+  L.c2[1] = op->c2[1];
   return L;
 }
 
@@ -499,6 +503,17 @@ int inti_op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   });
 }
 
+int inti_op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
+                            const inti_quad* source, const inti_csr* corr_dl, const inti_csr* corr_sl,
+                            const double* c_dl, const double* c_sl, int precision, inti_op** out) {
+  if (!ctx || !out) return INTI_E_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    *out = op_create_combined(ctx, pde, k_re, k_im, target, source, corr_dl, corr_sl, c_dl, c_sl,
+                              precision);
+  });
+}
+
 int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype) {
   if (!op) return INTI_E_ARG;
   if (m) *m = op->target->n;
@@ -613,6 +628,11 @@ int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, doub
   return guarded(ctx, [&] {
     grad_sources(op, g, sigma, dsigma, dcoords, dnormals, dweights, on_device);
   });
+}
+
+int inti_selftest_math(inti_ctx* ctx, double* out) {
+  if (!ctx || !out) return INTI_E_ARG;
+  return guarded(ctx, [&] { selftest_math(ctx, out); });
 }
 
 int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops, double* mufu_ops) {

@@ -76,6 +76,7 @@ struct inti_ctx {
   std::string last_error;
   int64_t launches = 0;
   inti::DevBuf err_flag;  // device int: nonzero when a bounded wait ran out
+  inti::DevBuf expi64, expi32;  // e^{i m delta} tables of the Helmholtz pair loops
   // per-kernel-class event timing (inti_ctx_set_profiling)
   bool profiling = false;
   struct Span {
@@ -129,7 +130,7 @@ struct ProfScope {
 
 // Launch plumbing implemented in the .cu files.
 enum Pde { LAPLACE = INTI_LAPLACE, HELMHOLTZ = INTI_HELMHOLTZ };
-enum Kind { SL = INTI_SL, DL = INTI_DL, ADL = INTI_ADL, HS = INTI_HS };
+enum Kind { SL = INTI_SL, DL = INTI_DL, ADL = INTI_ADL, HS = INTI_HS, CF = 4 /* c1*DL + c2*SL */ };
 
 // Per-apply description of the pair product A*x for one right-hand side.
 struct PairLaunch {
@@ -144,11 +145,15 @@ struct PairLaunch {
   const double* x;         // density, n (x2 complex)
   void* packed;            // scratch: packed source records (n padded)
   void* partial;           // scratch: split x m accumulators
+  double c1[2], c2[2];     // CF: dipole and charge coefficients (complex)
   int split;               // number of source chunks (computed by plan)
   int64_t n_tiles;         // padded source tiles
   int* err_flag;
 };
 
+// e^{i m 2pi/1024} tables (device, owned by the context).
+const double2* expi_table_f64(inti_ctx* ctx);
+const float2* expi_table_f32(inti_ctx* ctx);
 // Source records per tile (must match the kernel template parameter).
 int pair_tile(int precision);
 // Bytes of one packed source record.

@@ -141,6 +141,65 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
 // Error codes written to the context's device flag.
 constexpr int kErrWaitTimeout = 1;
 
+// ---------------------------------------------------------------------------
+// Fast special functions for the pair loops, from published methods:
+//  * rsqrt: hardware approximation (MUFU) refined by one third-order Newton
+//    step for 1/sqrt(x): with e = 1 - x*y^2, y' = y*(1 + e/2 + 3e^2/8)
+//    (Householder's method of order 3); relative error ~(5/16)e^3.
+//  * e^{i*theta} for theta = u*delta, delta = 2*pi/kExpiTable: split
+//    u = m + f (m = rint(u), |f| <= 1/2), take e^{i*m*delta} from a table
+//    built on the host in extended precision, and e^{i*f*delta} from its
+//    Taylor series (|f*delta| <= pi/1024: sin to r^5, cos to r^4 leave
+//    truncation errors below 2e-18).
+// The accuracy of both is measured on the device by inti_selftest_math.
+// ---------------------------------------------------------------------------
+constexpr int kExpiTable = 1024;
+
+__device__ __forceinline__ double rsqrt_approx_f64(double x) {
+  double r;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  return r;
+}
+__device__ __forceinline__ float rsqrt_approx_f32(float x) {
+  float r;
+  asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
+// 1/sqrt(x) to ~1 ulp for normal x > 0 (inf/NaN for x == 0, as 1/sqrt).
+__device__ __forceinline__ double rsqrt_fast(double x) {
+  const double y = rsqrt_approx_f64(x);
+  const double t = x * y;
+  const double e = fma(-t, y, 1.0);
+  const double p = fma(e, 0.375, 0.5);
+  return fma(y, e * p, y);
+}
+__device__ __forceinline__ float rsqrt_fast(float x) { return rsqrt_approx_f32(x); }
+
+template <class R, class R2>
+__device__ __forceinline__ void expi_table_eval(R u, const R2* __restrict__ tab, R delta, R& c, R& s) {
+  const R m = rint(u);
+  const R r = (u - m) * delta;
+  const R r2 = r * r;
+  R cp, sp;
+  if (sizeof(R) == 8) {
+    cp = fma(r2, fma(r2, R(1.0 / 24.0), R(-0.5)), R(1));
+    sp = fma(r2 * r, fma(r2, R(1.0 / 120.0), R(-1.0 / 6.0)), r);
+  } else {
+    // float: |r| <= pi/1024 makes r^4/24 and r^5/120 negligible
+    cp = fma(r2, R(-0.5), R(1));
+    sp = fma(r2 * r, R(-1.0 / 6.0), r);
+  }
+  int mi;
+  if (sizeof(R) == 8)
+    mi = __double2int_rn((double)m);
+  else
+    mi = __float2int_rn((float)m);
+  const R2 t = tab[mi & (kExpiTable - 1)];
+  c = fma(cp, t.x, -sp * t.y);
+  s = fma(sp, t.x, cp * t.y);
+}
+
 template <class T>
 __device__ __forceinline__ T warp_sum(T v) {
 #pragma unroll

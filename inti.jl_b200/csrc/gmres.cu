@@ -346,6 +346,28 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
     if (c.imag() != 0.0) cpx = true;
     S.coefs.push_back(c);
   }
+  // Fuse a double-layer and a single-layer term over the same nodes into one
+  // combined-field operator: one pass over the pairs per Krylov step.
+  std::vector<std::unique_ptr<inti_op>> fused;
+  for (size_t a = 0; a < S.ops64.size(); ++a) {
+    if (S.ops64[a]->kind != INTI_DL || S.ops64[a]->dim != 3) continue;
+    for (size_t b = 0; b < S.ops64.size(); ++b) {
+      inti_op *D = S.ops64[a], *Sl = S.ops64[b];
+      if (b == a || Sl->kind != INTI_SL || Sl->pde != D->pde || Sl->k != D->k || Sl->target != D->target ||
+          Sl->source != D->source)
+        continue;
+      const double cd[2] = {S.coefs[a].real(), S.coefs[a].imag()};
+      const double cs[2] = {S.coefs[b].real(), S.coefs[b].imag()};
+      if (D->pde == INTI_LAPLACE && (cd[1] != 0.0 || cs[1] != 0.0)) continue;
+      fused.emplace_back(op_create_combined(ctx, D->pde, D->k, 0.0, D->target, D->source, D->corr, Sl->corr,
+                                            cd, cs, INTI_FP64));
+      S.ops64[a] = fused.back().get();
+      S.coefs[a] = cplx(1, 0);
+      S.ops64.erase(S.ops64.begin() + b);
+      S.coefs.erase(S.coefs.begin() + b);
+      break;
+    }
+  }
   S.shift = shift ? cplx(shift[0], shift[1]) : cplx(0, 0);
   if (S.shift.imag() != 0.0) cpx = true;
   for (auto* op : S.ops64)
@@ -357,8 +379,7 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
   S.nblk = std::max(1, std::min<int>(ctx->num_sms * 2, (int)((S.n + kDotBlock - 1) / kDotBlock)));
   if (mode == INTI_GMRES_MIXED) {
     for (auto* op : S.ops64) {
-      S.owned32.emplace_back(op_create(ctx, op->pde, op->kind, op->k, 0.0, op->target, op->source,
-                                       op->corr, INTI_FP32C));
+      S.owned32.emplace_back(op_clone_precision(op, INTI_FP32C));
       S.ops32.push_back(S.owned32.back().get());
     }
   }
@@ -437,6 +458,7 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
   cudaEventDestroy(e1);
   if (!on_device) INTI_CUDA(cudaMemcpyAsync(x, xdev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
+  S.owned32.clear();  // twins refer to the fused operators' corrections
   if (stats) {
     stats->iterations = iters;
     stats->outer = outer;

@@ -13,6 +13,8 @@ struct inti_op {
   const inti_quad* source = nullptr;
   const inti_csr* corr = nullptr;
   std::unique_ptr<inti_csr> corrT;  // transposed correction, built on first A^T apply
+  std::unique_ptr<inti_csr> owned_corr;  // CF: c1*C_dl + c2*C_sl merged
+  double c1[2] = {1.0, 0.0}, c2[2] = {0.0, 0.0};  // CF coefficients
   // scratch owned by the operator
   inti::DevBuf packed;    // packed source records, n_tiles * tile
   inti::DevBuf partial;   // split x m accumulators
@@ -34,6 +36,10 @@ void op_apply_transpose_device(inti_op* op, const double* x, double* y, const do
 inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
                    const inti_quad* target, const inti_quad* source, const inti_csr* correction,
                    int precision);
+inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
+                            const inti_quad* source, const inti_csr* corr_dl, const inti_csr* corr_sl,
+                            const double* c_dl, const double* c_sl, int precision);
+inti_op* op_clone_precision(const inti_op* op, int precision);
 void op_prepare_transpose(inti_op* op);
 void transpose_epilogue(inti_ctx* ctx, int64_t n, int split, const void* partial,
                         const inti_csr* corrT, const double* x, double* y, const double* alpha,
@@ -53,5 +59,6 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
 void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsigma,
                   double* dcoords, double* dnormals, double* dweights, int on_device);
 void measure_peaks(inti_ctx* ctx, double* fp64, double* fp32, double* mufu);
+void selftest_math(inti_ctx* ctx, double* out);
 
 }  // namespace inti

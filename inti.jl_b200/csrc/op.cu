@@ -5,7 +5,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
+#include <memory>
 #include <string>
+#include <vector>
 
 #include "common.h"
 #include "device_common.cuh"
@@ -65,7 +68,140 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   return op.release();
 }
 
+// c1*C_dl + c2*C_sl with the union of the two patterns (host merge, once).
+static std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
+                                                   const inti_csr* b, const double* cb, int64_t m,
+                                                   int64_t n, bool cplx) {
+  const int comps = cplx ? 2 : 1;
+  struct Host {
+    std::vector<int64_t> rp;
+    std::vector<int32_t> col;
+    std::vector<double> val;
+  };
+  auto fetch = [&](const inti_csr* c) {
+    Host h;
+    h.rp.assign(m + 1, 0);
+    if (!c) return h;
+    h.col.resize(c->nnz);
+    h.val.resize((size_t)c->nnz * comps);
+    INTI_CUDA(cudaMemcpy(h.rp.data(), c->rowptr.p, sizeof(int64_t) * (m + 1), cudaMemcpyDeviceToHost));
+    INTI_CUDA(cudaMemcpy(h.col.data(), c->col.p, sizeof(int32_t) * c->nnz, cudaMemcpyDeviceToHost));
+    INTI_CUDA(cudaMemcpy(h.val.data(), c->val.p, sizeof(double) * comps * c->nnz, cudaMemcpyDeviceToHost));
+    return h;
+  };
+  INTI_CUDA(cudaStreamSynchronize(ctx->stream));
+  const Host A = fetch(a), B = fetch(b);
+  std::vector<int64_t> rp(m + 1, 0);
+  std::vector<int32_t> col;
+  std::vector<double> val;
+  col.reserve(A.col.size() + B.col.size());
+  val.reserve((A.col.size() + B.col.size()) * comps);
+  auto scaled = [&](const Host& H, int64_t p, const double* c, double* out) {
+    const double vr = H.val[p * comps], vi = cplx ? H.val[p * comps + 1] : 0.0;
+    out[0] = c[0] * vr - c[1] * vi;
+    out[1] = c[0] * vi + c[1] * vr;
+  };
+  for (int64_t i = 0; i < m; ++i) {
+    int64_t pa = A.rp[i], pb = B.rp[i];
+    const int64_t ea = A.rp[i + 1], eb = B.rp[i + 1];
+    while (pa < ea || pb < eb) {
+      const int32_t ja = pa < ea ? A.col[pa] : INT32_MAX, jb = pb < eb ? B.col[pb] : INT32_MAX;
+      const int32_t j = std::min(ja, jb);
+      double v[2] = {0, 0}, t[2];
+      if (ja == j) {
+        scaled(A, pa++, ca, t);
+        v[0] += t[0];
+        v[1] += t[1];
+      }
+      if (jb == j) {
+        scaled(B, pb++, cb, t);
+        v[0] += t[0];
+        v[1] += t[1];
+      }
+      col.push_back(j);
+      val.push_back(v[0]);
+      if (cplx) val.push_back(v[1]);
+    }
+    rp[i + 1] = (int64_t)col.size();
+  }
+  return std::unique_ptr<inti_csr>(csr_create_host(ctx, m, n, (int64_t)col.size(), rp.data(), col.data(),
+                                                   val.data(), cplx ? INTI_C128 : INTI_F64));
+}
+
+inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
+                            const inti_quad* source, const inti_csr* corr_dl, const inti_csr* corr_sl,
+                            const double* c_dl, const double* c_sl, int precision) {
+  req(target && source, INTI_E_ARG, "target/source quadrature is NULL");
+  req(source->dim == 3, INTI_E_UNSUPPORTED, "the combined-field operator is implemented in 3D");
+  req(c_dl && c_sl, INTI_E_ARG, "coefficients are NULL");
+  const bool cplx = pde == INTI_HELMHOLTZ;
+  if (!cplx) req(c_dl[1] == 0.0 && c_sl[1] == 0.0, INTI_E_UNSUPPORTED,
+                 "complex coefficients need a Helmholtz (complex) operator");
+  // validate both halves like two ordinary operators
+  std::unique_ptr<inti_op> probe_d(op_create(ctx, pde, INTI_DL, k_re, k_im, target, source, corr_dl, precision));
+  std::unique_ptr<inti_op> probe_s(op_create(ctx, pde, INTI_SL, k_re, k_im, target, source, corr_sl, precision));
+  probe_d.reset();
+  probe_s.reset();
+  std::unique_ptr<inti_op> op(new inti_op());
+  op->ctx = ctx;
+  op->pde = pde;
+  op->kind = CF;
+  op->dim = 3;
+  op->precision = precision;
+  op->k = k_re;
+  op->target = target;
+  op->source = source;
+  op->c1[0] = c_dl[0];
+  op->c1[1] = c_dl[1];
+  op->c2[0] = c_sl[0];
+  op->c2[1] = c_sl[1];
+  if (corr_dl || corr_sl) {
+    op->owned_corr = merge_corrections(ctx, corr_dl, c_dl, corr_sl, c_sl, target->n, source->n, cplx);
+    op->corr = op->owned_corr.get();
+  }
+  const int64_t tile = pair_tile(precision);
+  op->n_tiles = std::max<int64_t>(1, (source->n + tile - 1) / tile);
+  op->split = pair_plan_split(ctx, pde, CF, 3, precision, target->n, source->n);
+  op->packed.ensure((size_t)op->n_tiles * tile * pair_record_bytes(pde, CF, 3, precision));
+  op->partial.ensure((size_t)op->split * target->n * pair_partial_bytes(pde, precision));
+  const int comps = cplx ? 2 : 1;
+  const int64_t big = std::max(target->n, source->n);
+  op->xbuf.ensure(sizeof(double) * comps * big);
+  op->ybuf.ensure(sizeof(double) * comps * big);
+  return op.release();
+}
+
+// The same operator (kernel, coefficients, correction) in another precision.
+// The twin refers to op's correction: destroy it first.
+inti_op* op_clone_precision(const inti_op* op, int precision) {
+  std::unique_ptr<inti_op> t(new inti_op());
+  t->ctx = op->ctx;
+  t->pde = op->pde;
+  t->kind = op->kind;
+  t->dim = op->dim;
+  t->precision = precision;
+  t->k = op->k;
+  t->target = op->target;
+  t->source = op->source;
+  t->corr = op->corr;
+  for (int i = 0; i < 2; ++i) {
+    t->c1[i] = op->c1[i];
+    t->c2[i] = op->c2[i];
+  }
+  const int64_t tile = pair_tile(precision);
+  t->n_tiles = std::max<int64_t>(1, (op->source->n + tile - 1) / tile);
+  t->split = pair_plan_split(op->ctx, op->pde, op->kind, op->dim, precision, op->target->n, op->source->n);
+  t->packed.ensure((size_t)t->n_tiles * tile * pair_record_bytes(op->pde, op->kind, op->dim, precision));
+  t->partial.ensure((size_t)t->split * op->target->n * pair_partial_bytes(op->pde, precision));
+  const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
+  const int64_t big = std::max(op->target->n, op->source->n);
+  t->xbuf.ensure(sizeof(double) * comps * big);
+  t->ybuf.ensure(sizeof(double) * comps * big);
+  return t.release();
+}
+
 void op_prepare_transpose(inti_op* op) {
+  if (op->kind == CF) throw Error(INTI_E_UNSUPPORTED, "transpose of a combined-field operator");
   const int64_t ntile = (op->target->n + 63) / 64;
   const int64_t blocks = (op->source->n + 127) / 128;
   const int64_t want = (int64_t)op->ctx->num_sms * 8;

@@ -25,6 +25,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "common.h"
 #include "device_common.cuh"
@@ -32,7 +33,7 @@
 namespace inti {
 
 constexpr int kBlock = 128;  // threads per CTA
-constexpr int kTPT = 2;      // targets per thread
+constexpr int kTPT = 4;      // targets per thread
 constexpr int kTile64 = 128; // sources per shared-memory stage (FP64)
 constexpr int kTile32 = 256; // sources per shared-memory stage (FP32C)
 constexpr int kGroup = 32;   // FP32C: sources summed before a compensated fold
@@ -45,11 +46,13 @@ constexpr int kGroup = 32;   // FP32C: sources summed before a compensated fold
 //   Helmholtz DL/HS : x y z pr_x pr_y pr_z pi_x pi_y pi_z
 // each padded so that a record is a multiple of 16 bytes.
 // ---------------------------------------------------------------------------
+//   combined field (CF): x y z | dipole c1*w*sigma*n_y | charge c2*w*sigma
 template <int PDE, int KIND, int DIM, class R>
 struct Rec {
-  static constexpr bool dipole = (KIND == DL || KIND == HS);
+  static constexpr bool dipole = (KIND == DL || KIND == HS || KIND == CF);
+  static constexpr bool charge2 = (KIND == CF);
   static constexpr bool cplx = (PDE == HELMHOLTZ);
-  static constexpr int used = DIM + (cplx ? 2 : 1) * (dipole ? DIM : 1);
+  static constexpr int used = DIM + (cplx ? 2 : 1) * ((dipole ? DIM : 1) + (charge2 ? 1 : 0));
   static constexpr int align = 16 / sizeof(R);
   static constexpr int n = (used + align - 1) / align * align;
   static constexpr bool tnormal = (KIND == ADL || KIND == HS);
@@ -58,7 +61,8 @@ struct Rec {
 template <int PDE, int KIND, int DIM, class R>
 __global__ void pack_sources(int64_t n, int64_t npad, const double* __restrict__ xs,
                              const double* __restrict__ ns, const double* __restrict__ w,
-                             const double* __restrict__ sigma, R* __restrict__ out) {
+                             const double* __restrict__ sigma, double2 c1, double2 c2,
+                             R* __restrict__ out) {
   using RC = Rec<PDE, KIND, DIM, R>;
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= npad) return;
@@ -75,6 +79,15 @@ __global__ void pack_sources(int64_t n, int64_t npad, const double* __restrict__
       qi = wj * sigma[2 * j + 1];
     } else {
       qr = wj * sigma[j];
+    }
+    if (RC::charge2) {
+      // monopole charge c2*q after the dipole block
+      const double mr = c2.x * qr - c2.y * qi, mi = c2.x * qi + c2.y * qr;
+      rec[DIM + (RC::cplx ? 2 : 1) * DIM] = R(mr);
+      if (RC::cplx) rec[DIM + 2 * DIM + 1] = R(mi);
+      const double dr = c1.x * qr - c1.y * qi, di = c1.x * qi + c1.y * qr;
+      qr = dr;
+      qi = di;
     }
     if (RC::dipole) {
 #pragma unroll
@@ -100,16 +113,16 @@ template <class R>
 struct MathOps;
 template <>
 struct MathOps<double> {
-  static __device__ __forceinline__ double rsq(double v) { return rsqrt(v); }
+  using R2 = double2;
+  static __device__ __forceinline__ double rsq(double v) { return rsqrt_fast(v); }
   static __device__ __forceinline__ double lg(double v) { return log(v); }
-  static __device__ __forceinline__ void scpi(double v, double* s, double* c) { sincospi(v, s, c); }
   static __device__ __forceinline__ double tol2() { return kSamePointTol2; }
 };
 template <>
 struct MathOps<float> {
-  static __device__ __forceinline__ float rsq(float v) { return rsqrtf(v); }
+  using R2 = float2;
+  static __device__ __forceinline__ float rsq(float v) { return rsqrt_fast(v); }
   static __device__ __forceinline__ float lg(float v) { return __logf(v); }
-  static __device__ __forceinline__ void scpi(float v, float* s, float* c) { sincospif(v, s, c); }
   static __device__ __forceinline__ float tol2() { return 1.0e-28f; }
 };
 
@@ -119,9 +132,16 @@ struct Target {
   R n[TN ? DIM : 1];
 };
 
+// Helmholtz phase: e^{ikd} = expi(d * kT) with kT = k*kExpiTable/(2 pi)
+// (table + Taylor, see expi_table_eval).
+struct HelmConst {
+  double kT, delta;
+};
+
 template <int PDE, int KIND, int DIM, class R>
 __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DIM, R>::tnormal>& t,
-                                          const R* __restrict__ s, R kpi, R k, R& ar, R& ai) {
+                                          const R* __restrict__ s, R kT, R delta, R k,
+                                          const typename MathOps<R>::R2* __restrict__ tab, R& ar, R& ai) {
   using M = MathOps<R>;
   R r[DIM];
 #pragma unroll
@@ -140,7 +160,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
         const R ri = keep ? M::rsq(d2) : R(0);
         ar = fma(ri, s[3], ar);
       }
-    } else if (KIND == DL) {
+    } else if (KIND == DL || KIND == CF) {
       R rp = r[0] * s[DIM];
 #pragma unroll
       for (int c = 1; c < DIM; ++c) rp = fma(r[c], s[DIM + c], rp);
@@ -149,6 +169,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
         ar = fma(rp, ri, ar);
       } else {
         const R ri = keep ? M::rsq(d2) : R(0);
+        if (KIND == CF) ar = fma(ri, s[2 * DIM], ar);
         ar = fma(rp, ri * ri * ri, ar);
       }
     } else if (KIND == ADL) {
@@ -184,7 +205,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
     const R ri = keep ? M::rsq(d2) : R(0);
     const R d = d2 * ri;  // 0 for the self pair
     R sn, cs;
-    M::scpi(d * kpi, &sn, &cs);
+    expi_table_eval<R, typename MathOps<R>::R2>(d * kT, tab, delta, cs, sn);
     if (KIND == SL || KIND == ADL) {
       R g_r, g_i;  // G (without 1/4pi) or the ADL factor
       if (KIND == SL) {
@@ -203,7 +224,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
       const R qr = s[3], qi = s[4];
       ar = fma(g_r, qr, fma(-g_i, qi, ar));
       ai = fma(g_r, qi, fma(g_i, qr, ai));
-    } else if (KIND == DL) {
+    } else if (KIND == DL || KIND == CF) {
       const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
       const R id2 = ri * ri;
       R A = r[0] * s[3], B = r[0] * s[6];
@@ -214,6 +235,12 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
       const R gr = er * id2, gi = ei * id2;
       ar = fma(gr, A, fma(-gi, B, ar));
       ai = fma(gr, B, fma(gi, A, ai));
+      if (KIND == CF) {  // + e^{ikd}/d * (c2 w sigma)
+        const R hr = cs * ri, hi = sn * ri;
+        const R qr = s[9], qi = s[10];
+        ar = fma(hr, qr, fma(-hi, qi, ar));
+        ai = fma(hr, qi, fma(hi, qr, ai));
+      }
     } else {  // HS
       const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
       const R id2 = ri * ri;
@@ -303,6 +330,8 @@ struct FwdArgs {
   const void* packed;
   void* partial;
   double k;
+  double kT, delta;   // Helmholtz phase scaling (see HelmConst)
+  const void* expi;   // kExpiTable (cos, sin) entries in R precision
   int* err;
 };
 
@@ -311,10 +340,12 @@ __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
   using RC = Rec<PDE, KIND, DIM, R>;
   constexpr bool CPLX = RC::cplx;
   using P = typename PartialT<R, CPLX>::T;
+  using R2 = typename MathOps<R>::R2;
   constexpr uint32_t kStageBytes = TILE * RC::n * sizeof(R);
   extern __shared__ __align__(128) unsigned char smem_raw[];
   R* stage0 = reinterpret_cast<R*>(smem_raw);
   R* stage1 = reinterpret_cast<R*>(smem_raw + kStageBytes);
+  R2* tab = reinterpret_cast<R2*>(smem_raw + 2 * kStageBytes);  // Helmholtz only
   __shared__ __align__(8) uint64_t full[2];
 
   const int tid = threadIdx.x;
@@ -337,7 +368,12 @@ __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
     }
   }
   const R k = R(a.k);
-  const R kpi = R(a.k / kPi);
+  const R kT = R(a.kT);
+  const R delta = R(a.delta);
+  if (RC::cplx) {
+    const R2* g = static_cast<const R2*>(a.expi);
+    for (int q = tid; q < kExpiTable; q += kBlock) tab[q] = g[q];
+  }
 
   if (tid == 0) {
     mbar_init(&full[0], 1);
@@ -370,11 +406,12 @@ __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
     const R* sp = st ? stage1 : stage0;
 #pragma unroll 1
     for (int g = 0; g < TILE; g += kGroup) {
-#pragma unroll 4
+#pragma unroll 2
       for (int s = 0; s < kGroup; ++s) {
         const R* rec = sp + (g + s) * RC::n;
 #pragma unroll
-        for (int u = 0; u < kTPT; ++u) pair_step<PDE, KIND, DIM, R>(tg[u], rec, kpi, k, acc[u].gr(), acc[u].gi());
+        for (int u = 0; u < kTPT; ++u)
+          pair_step<PDE, KIND, DIM, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
       }
 #pragma unroll
       for (int u = 0; u < kTPT; ++u) acc[u].fold();
@@ -547,11 +584,45 @@ __global__ void __launch_bounds__(kBlock) transpose_kernel(int64_t m, int64_t n,
 // ---------------------------------------------------------------------------
 int pair_tile(int precision) { return precision == INTI_FP32C ? kTile32 : kTile64; }
 
+// e^{i m delta}, delta = fl(2 pi / kExpiTable), m = 0..kExpiTable-1, computed
+// in x87 extended precision (m*delta is exact there) and rounded once.
+static std::vector<long double> expi_host(bool sine) {
+  const double delta = 2 * kPi / kExpiTable;
+  std::vector<long double> v(kExpiTable);
+  for (int m = 0; m < kExpiTable; ++m) {
+    const long double a = (long double)m * (long double)delta;
+    v[m] = sine ? sinl(a) : cosl(a);
+  }
+  return v;
+}
+
+const double2* expi_table_f64(inti_ctx* ctx) {
+  if (!ctx->expi64.p) {
+    const auto c = expi_host(false), s = expi_host(true);
+    std::vector<double2> t(kExpiTable);
+    for (int m = 0; m < kExpiTable; ++m) t[m] = make_double2((double)c[m], (double)s[m]);
+    ctx->expi64.ensure(sizeof(double2) * kExpiTable);
+    INTI_CUDA(cudaMemcpy(ctx->expi64.p, t.data(), sizeof(double2) * kExpiTable, cudaMemcpyHostToDevice));
+  }
+  return ctx->expi64.as<double2>();
+}
+
+const float2* expi_table_f32(inti_ctx* ctx) {
+  if (!ctx->expi32.p) {
+    const auto c = expi_host(false), s = expi_host(true);
+    std::vector<float2> t(kExpiTable);
+    for (int m = 0; m < kExpiTable; ++m) t[m] = make_float2((float)c[m], (float)s[m]);
+    ctx->expi32.ensure(sizeof(float2) * kExpiTable);
+    INTI_CUDA(cudaMemcpy(ctx->expi32.p, t.data(), sizeof(float2) * kExpiTable, cudaMemcpyHostToDevice));
+  }
+  return ctx->expi32.as<float2>();
+}
+
 template <class R>
 static int rec_elems(int pde, int kind, int dim) {
-  const bool dip = kind == DL || kind == HS;
+  const bool dip = kind == DL || kind == HS || kind == CF;
   const bool cp = pde == HELMHOLTZ;
-  const int used = dim + (cp ? 2 : 1) * (dip ? dim : 1);
+  const int used = dim + (cp ? 2 : 1) * ((dip ? dim : 1) + (kind == CF ? 1 : 0));
   const int al = 16 / (int)sizeof(R);
   return (used + al - 1) / al * al;
 }
@@ -569,6 +640,7 @@ int pair_partial_bytes(int pde, int precision) {
 // Kernel constant applied in the epilogue (see pair_step).
 static double pair_scale(int pde, int kind, int dim) {
   const double c3 = 1.0 / (4 * kPi), c2 = 1.0 / (2 * kPi);
+  if (kind == CF) return c3;  // 3D only: DL and SL share 1/(4 pi)
   if (pde == HELMHOLTZ) return kind == ADL ? -c3 : c3;
   if (dim == 2) {
     switch (kind) {
@@ -597,6 +669,7 @@ static void dispatch(int pde, int kind, int dim, F&& f) {
       case DL: return f(Tag<LAPLACE, DL, 3>());
       case ADL: return f(Tag<LAPLACE, ADL, 3>());
       case HS: return f(Tag<LAPLACE, HS, 3>());
+      case CF: return f(Tag<LAPLACE, CF, 3>());
     }
   } else if (pde == LAPLACE && dim == 2) {
     switch (kind) {
@@ -611,6 +684,7 @@ static void dispatch(int pde, int kind, int dim, F&& f) {
       case DL: return f(Tag<HELMHOLTZ, DL, 3>());
       case ADL: return f(Tag<HELMHOLTZ, ADL, 3>());
       case HS: return f(Tag<HELMHOLTZ, HS, 3>());
+      case CF: return f(Tag<HELMHOLTZ, CF, 3>());
     }
   }
   throw Error(INTI_E_UNSUPPORTED, "unsupported operator: pde=" + std::to_string(pde) +
@@ -627,7 +701,8 @@ static const void* fwd_kernel_ptr() {
 template <class T, class R>
 static size_t fwd_smem() {
   constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
-  return 2 * (size_t)TILE * Rec<T::pde, T::kind, T::dim, R>::n * sizeof(R);
+  const size_t table = T::pde == HELMHOLTZ ? (size_t)kExpiTable * 2 * sizeof(R) : 0;
+  return 2 * (size_t)TILE * Rec<T::pde, T::kind, T::dim, R>::n * sizeof(R) + table;
 }
 
 int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
@@ -687,7 +762,8 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       {
         ProfScope ps(ctx, "pack");
         pack_sources<T::pde, T::kind, T::dim, R><<<(unsigned)((npad + pb - 1) / pb), pb, 0, ctx->stream>>>(
-            L.n, npad, L.scoords, L.snormals, L.sweights, L.x, static_cast<R*>(L.packed));
+            L.n, npad, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
+            make_double2(L.c2[0], L.c2[1]), static_cast<R*>(L.packed));
       }
       FwdArgs a;
       a.m = L.m;
@@ -698,6 +774,9 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       a.packed = L.packed;
       a.partial = L.partial;
       a.k = L.k;
+      a.kT = L.k * kExpiTable / (2 * kPi);
+      a.delta = 2 * kPi / kExpiTable;
+      a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
       a.err = L.err_flag;
       const size_t sm = fwd_smem<T, R>();
       auto fn = &pair_forward<T::pde, T::kind, T::dim, R, TILE>;
@@ -756,11 +835,14 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
 
 int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {
   if (L.n > 65535 * 1024LL) throw Error(INTI_E_ARG, "assemble: too many source columns");
+  if (L.kind == CF) throw Error(INTI_E_UNSUPPORTED, "assemble the DL and SL parts separately");
   dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
     using T = decltype(tag);
-    dim3 grid((unsigned)((L.m + 255) / 256), (unsigned)L.n);
-    assemble_kernel<T::pde, T::kind, T::dim><<<grid, 256, 0, ctx->stream>>>(
-        L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.k, out);
+    if constexpr (T::kind != CF) {
+      dim3 grid((unsigned)((L.m + 255) / 256), (unsigned)L.n);
+      assemble_kernel<T::pde, T::kind, T::dim><<<grid, 256, 0, ctx->stream>>>(
+          L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.k, out);
+    }
   });
   INTI_CUDA(cudaGetLastError());
   ctx->launches += 1;
@@ -771,13 +853,16 @@ int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {
 int pair_transpose_launch(inti_ctx* ctx, const PairLaunch& L) {
   const int64_t ntile = (L.m + 63) / 64;
   const int tps = (int)((ntile + L.split - 1) / L.split);
+  if (L.kind == CF) throw Error(INTI_E_UNSUPPORTED, "transpose of a combined-field operator");
   dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
     using T = decltype(tag);
-    dim3 grid((unsigned)((L.n + kBlock - 1) / kBlock), (unsigned)L.split);
-    ProfScope pt(ctx, "transpose");
-    transpose_kernel<T::pde, T::kind, T::dim><<<grid, kBlock, 0, ctx->stream>>>(
-        L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.x, L.k, tps,
-        static_cast<double2*>(L.partial));
+    if constexpr (T::kind != CF) {
+      dim3 grid((unsigned)((L.n + kBlock - 1) / kBlock), (unsigned)L.split);
+      ProfScope pt(ctx, "transpose");
+      transpose_kernel<T::pde, T::kind, T::dim><<<grid, kBlock, 0, ctx->stream>>>(
+          L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.x, L.k, tps,
+          static_cast<double2*>(L.partial));
+    }
   });
   INTI_CUDA(cudaGetLastError());
   ctx->launches += 1;

@@ -107,6 +107,7 @@ SIGNATURES = {
     "inti_csr_apply": (C.c_int, [P, P, P, D, D, C.c_int]),
     "inti_csr_destroy": (C.c_int, [P]),
     "inti_op_create": (C.c_int, [P, C.c_int, C.c_int, C.c_double, C.c_double, P, P, P, C.c_int, PP]),
+    "inti_op_create_combined": (C.c_int, [P, C.c_int, C.c_double, C.c_double, P, P, P, P, D, D, C.c_int, PP]),
     "inti_op_info": (C.c_int, [P, C.POINTER(I64), C.POINTER(I64), C.POINTER(C.c_int)]),
     "inti_op_apply": (C.c_int, [P, P, I64, P, I64, C.c_int32, D, D, C.c_int]),
     "inti_op_apply_transpose": (C.c_int, [P, P, I64, P, I64, C.c_int32, D, D, C.c_int]),
@@ -117,6 +118,7 @@ SIGNATURES = {
                              C.c_int32, C.c_int, P, C.POINTER(GmresStats)]),
     "inti_op_grad_sources": (C.c_int, [P, P, P, P, P, P, P, C.c_int]),
     "inti_measure_peaks": (C.c_int, [P, D, D, D]),
+    "inti_selftest_math": (C.c_int, [P, D]),
 }
 
 _lib = None

@@ -44,6 +44,7 @@ __all__ = [
     "AdjointDoubleLayerKernel",
     "HyperSingularKernel",
     "GpuOperator",
+    "CombinedFieldOperator",
     "LinearCombination",
     "IntegralOperator",
     "assemble_matrix",
@@ -102,6 +103,13 @@ class Context:
 
     def synchronize(self) -> None:
         self.check(self.lib.inti_ctx_synchronize(self.handle))
+
+    def selftest_math(self) -> dict:
+        """Accuracy of the device's fast rsqrt / e^{iθ} helpers (see the ABI)."""
+        out = (C.c_double * 4)()
+        self.check(self.lib.inti_selftest_math(self.handle, out))
+        return {"rsqrt_f64_maxrel": out[0], "expi_f64_maxabs_25": out[1], "expi_f64_maxabs_1000": out[2],
+                "expi_f32_maxabs_25": out[3]}
 
     def measure_peaks(self) -> dict:
         a, b, c = C.c_double(), C.c_double(), C.c_double()
@@ -496,6 +504,39 @@ class GpuOperator(_Map):
                                                          L.dptr(out["sigma"]), L.dptr(out["coords"]),
                                                          L.dptr(out["normals"]), L.dptr(out["weights"]), 0))
         return out
+
+
+class CombinedFieldOperator(GpuOperator):
+    """``c_D·D + c_S·S`` of two GPU operators (a double layer and a single
+    layer over the same nodes, corrections included), applied in one pass
+    over the node pairs.  The lazy sum ``c_D*D + c_S*S`` of the reference's
+    LinearMaps (docs/src/examples/helmholtz_scattering.jl:485-486) gives the
+    same product with two passes."""
+
+    def __init__(self, D: GpuOperator, S: GpuOperator, c_D=1.0, c_S=1.0, precision: str | None = None):
+        if not (isinstance(D.kernel, DoubleLayerKernel) and isinstance(S.kernel, SingleLayerKernel)):
+            raise L.ArgumentError(L.E_ARG, "expected a double-layer and a single-layer operator")
+        if D.target is not S.target or D.source is not S.source:
+            raise L.ArgumentError(L.E_ARG, "both operators must share target and source")
+        self.ctx = D.ctx
+        self.kernel = D.kernel
+        self.target, self.source = D.target, D.source
+        self.correction = None
+        self.precision = precision or D.precision
+        prec = {"fp64": L.FP64, "fp32c": L.FP32C}[self.precision]
+        op = D.kernel.op
+        k = complex(getattr(op, "k", 0.0))
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.inti_op_create_combined(
+            self.ctx.handle, op.pde, k.real, k.imag, _quad_handle(D.target, self.ctx),
+            _quad_handle(D.source, self.ctx), D.correction.handle if D.correction else None,
+            S.correction.handle if S.correction else None, L.cpair(c_D), L.cpair(c_S), prec, C.byref(h)))
+        self.handle = h
+        self._keep = (D, S)
+        self._fin = weakref.finalize(self, self.ctx.lib.inti_op_destroy, h)
+        self.shape = D.shape
+        self.is_complex = D.is_complex
+        self.dtype = D.dtype
 
 
 class IntegralOperator(GpuOperator):

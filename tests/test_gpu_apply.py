@@ -105,3 +105,27 @@ def test_launch_counter_advances(ctx):
     before = ctx.launch_count
     A @ np.ones(len(q))
     assert ctx.launch_count - before == 3  # pack, pair, epilogue
+
+
+def test_fast_special_functions_accuracy(ctx):
+    """The pair loops' rsqrt and e^{iθ} against extended precision."""
+    r = ctx.selftest_math()
+    assert r["rsqrt_f64_maxrel"] < 4e-16, r
+    assert r["expi_f64_maxabs_25"] < 8e-16, r
+    assert r["expi_f64_maxabs_1000"] < 2e-13, r
+    assert r["expi_f32_maxabs_25"] < 4e-6, r
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32c", 5e-5)])
+def test_combined_field_operator(ctx, prec, tol):
+    """c_D·(D + δD) + c_S·(S + δS) in one pass equals the two products."""
+    q = SURF["ellipsoid"]
+    for op, pde, k, cD, cS in ((inti.Laplace(dim=3), O.LAPLACE, 0.0, 1.0, 0.7),
+                              (inti.Helmholtz(k=3.0, dim=3), O.HELMHOLTZ, 3.0, 1.0, -3.0j)):
+        S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+        C = inti.CombinedFieldOperator(D, S, cD, cS, precision=prec)
+        x = density(len(q), pde == O.HELMHOLTZ, 31)
+        dS, dD = S.correction.arrays(), D.correction.arrays()
+        ref = cD * (oracle_apply(pde, O.DL, k, q, q, x) + O.csr_apply(*dD, x)) + \
+            cS * (oracle_apply(pde, O.SL, k, q, q, x) + O.csr_apply(*dS, x))
+        assert relerr(C @ x, ref) < tol, (op, prec)
