@@ -218,6 +218,34 @@ int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, doub
 int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops,
                        double* mufu_ops);
 
+/* ---- allocation-free apply ------------------------------------------------
+ * No counterpart in the reference: Inti.jl's operators allocate freely.
+ * For callers that cannot call cudaMalloc when they apply the operator (a
+ * framework's caching allocator owns the device memory, a solver loop that
+ * must not pay for allocation, work issued during stream capture).
+ *
+ * y = alpha*(A x + C x) + beta*y with the same kernels as inti_op_apply, but
+ * every array is a caller-owned DEVICE pointer on the current device:
+ * target coords/normals (dim x m), source coords/normals/weights (dim x n,
+ * n), the optional CSR correction (rowptr m+1, col, val; all NULL for none),
+ * x (n) and y (m) — complex data interleaved for Helmholtz.  alpha/beta are
+ * host pairs (re, im) or NULL for 1, 0.  Work goes to `stream` (NULL: the
+ * legacy default stream); synchronize != 0 waits and reports device-side
+ * timeouts.
+ *
+ * Scratch lives in a fixed 32 MiB static device array that every GPU loading
+ * the library holds until exit; problems whose packed sources plus one
+ * partial vector exceed it are rejected with INTI_E_ARG.  The first call on a
+ * device sets that array up (address lookup, phase tables): make it before
+ * any stream capture.  All calls on a device share the array, so calls that
+ * overlap on the GPU race.  Errors: inti_last_error(NULL). */
+int inti_apply_noalloc(int pde, int kernel, int dim, double k, int precision, int64_t m,
+                       const double* tcoords, const double* tnormals, int64_t n,
+                       const double* scoords, const double* snormals, const double* sweights,
+                       const int64_t* rowptr, const int32_t* col, const double* val,
+                       const double* x, double* y, const double* alpha, const double* beta,
+                       void* stream, int synchronize);
+
 /* Accuracy of the pair loops' fast special functions on this device, against
  * extended-precision host values: out[0] max relative error of the FP64
  * reciprocal square root over [1e-27, 1e27]; out[1], out[2] max absolute

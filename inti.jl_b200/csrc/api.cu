@@ -81,6 +81,8 @@ void d2h(inti_ctx* ctx, void* dst, const void* src, size_t bytes) {
 
 namespace inti {
 
+void noalloc_error_set(const char* msg) { g_thread_error = msg; }
+
 void sync_and_check(inti_ctx* ctx) {
   INTI_CUDA(cudaStreamSynchronize(ctx->stream));
   int flag = 0;

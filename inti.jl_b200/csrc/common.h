@@ -151,6 +151,8 @@ struct PairLaunch {
   int* err_flag;
 };
 
+// Message for inti_last_error(NULL) from entry points that take no context.
+void noalloc_error_set(const char* msg);
 // e^{i m 2pi/1024} tables (device, owned by the context).
 const double2* expi_table_f64(inti_ctx* ctx);
 const float2* expi_table_f32(inti_ctx* ctx);

@@ -25,6 +25,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "common.h"
@@ -869,4 +871,204 @@ int pair_transpose_launch(inti_ctx* ctx, const PairLaunch& L) {
   return 1;
 }
 
+// ===========================================================================
+// Allocation-free apply.
+//
+// Some callers cannot call cudaMalloc at the moment they need the operator:
+// code running inside a framework whose caching allocator already owns nearly
+// all device memory (so a fresh cudaMalloc fails or fragments it), code that
+// must not pay an allocation's latency or implicit synchronisation in a
+// solver loop, and code that issues work while a stream is being captured,
+// where allocation calls are not permitted.  inti_apply_noalloc serves them:
+// the caller passes every input and output as device pointers, and the
+// scratch the pair product needs (packed source records and per-chunk partial
+// sums) lives in one fixed array of kNoAllocScratchBytes declared below.  The
+// module holds that array on every GPU that loads the library, until exit.
+//
+// The first call on a device resolves the array's device address with
+// cudaGetSymbolAddress and uploads the e^{i m delta} tables into static
+// device arrays; make that first call before any stream capture.  Every call
+// on a device shares the array and leaves its contents behind: calls that
+// overlap on the GPU (different streams, or different host threads) race
+// on it.  Nothing in the array has to start at zero: the pack kernel writes
+// every record (padding included) and the pair kernel writes every partial
+// slot it owns; only the timeout flag is cleared at the start of each call.
+// ===========================================================================
+constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
+constexpr size_t kNoAllocFlagBytes = 256;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+static __device__ __align__(16) double2 g_noalloc_expi64[kExpiTable];
+static __device__ __align__(16) float2 g_noalloc_expi32[kExpiTable];
+
+namespace {
+
+struct NoAllocDevice {
+  unsigned char* scratch = nullptr;
+  const double2* expi64 = nullptr;
+  const float2* expi32 = nullptr;
+  int num_sms = 0;
+};
+
+std::mutex g_noalloc_mu;
+NoAllocDevice g_noalloc_dev[64];
+
+// Once per device, with that device current: resolve the static arrays'
+// device addresses (the host-side names are not device addresses) and fill
+// the phase tables.
+const NoAllocDevice& noalloc_setup(int dev) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (dev < 0 || dev >= 64) throw Error(INTI_E_ARG, "device index out of range for the static scratch");
+  NoAllocDevice& d = g_noalloc_dev[dev];
+  if (d.scratch) return d;
+  void* p = nullptr;
+  INTI_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+  void* t64 = nullptr;
+  INTI_CUDA(cudaGetSymbolAddress(&t64, g_noalloc_expi64));
+  void* t32 = nullptr;
+  INTI_CUDA(cudaGetSymbolAddress(&t32, g_noalloc_expi32));
+  const auto c = expi_host(false), s = expi_host(true);
+  std::vector<double2> h64(kExpiTable);
+  std::vector<float2> h32(kExpiTable);
+  for (int m = 0; m < kExpiTable; ++m) {
+    h64[m] = make_double2((double)c[m], (double)s[m]);
+    h32[m] = make_float2((float)c[m], (float)s[m]);
+  }
+  INTI_CUDA(cudaMemcpyToSymbol(g_noalloc_expi64, h64.data(), sizeof(double2) * kExpiTable));
+  INTI_CUDA(cudaMemcpyToSymbol(g_noalloc_expi32, h32.data(), sizeof(float2) * kExpiTable));
+  INTI_CUDA(cudaDeviceGetAttribute(&d.num_sms, cudaDevAttrMultiProcessorCount, dev));
+  d.expi64 = static_cast<const double2*>(t64);
+  d.expi32 = static_cast<const float2*>(t32);
+  d.scratch = static_cast<unsigned char*>(p);
+  return d;
+}
+
+}  // namespace
+
+int apply_noalloc(int pde, int kind, int dim, double k, int precision, int64_t m, const double* tc,
+                  const double* tn, int64_t n, const double* sc, const double* sn, const double* sw,
+                  const int64_t* rowptr, const int32_t* col, const double* val, const double* x, double* y,
+                  const double* alpha, const double* beta, cudaStream_t stream, int synchronize) {
+  if (pde != INTI_LAPLACE && pde != INTI_HELMHOLTZ) throw Error(INTI_E_ARG, "unknown pde");
+  if (kind < INTI_SL || kind > INTI_HS) throw Error(INTI_E_ARG, "unknown kernel");
+  if (precision != INTI_FP64 && precision != INTI_FP32C) throw Error(INTI_E_ARG, "unknown precision");
+  if (dim != 2 && dim != 3) throw Error(INTI_E_ARG, "dim must be 2 or 3");
+  if (pde == INTI_HELMHOLTZ && dim != 3) throw Error(INTI_E_UNSUPPORTED, "Helmholtz is implemented in 3D only");
+  if (m <= 0 || n <= 0) throw Error(INTI_E_ARG, "m and n must be positive");
+  if (!tc || !sc || !sw || !x || !y) throw Error(INTI_E_ARG, "a required device pointer is NULL");
+  if ((kind == DL || kind == HS) && !sn) throw Error(INTI_E_ARG, "this kernel needs source normals");
+  if ((kind == ADL || kind == HS) && !tn) throw Error(INTI_E_ARG, "this kernel needs target normals");
+  if ((rowptr || col || val) && !(rowptr && col && val))
+    throw Error(INTI_E_ARG, "the correction needs rowptr, col and val together");
+  int dev = 0;
+  INTI_CUDA(cudaGetDevice(&dev));
+  const NoAllocDevice& D = noalloc_setup(dev);
+  const int64_t tile = pair_tile(precision);
+  const int64_t n_tiles = (n + tile - 1) / tile;
+  const size_t rec_bytes = (size_t)n_tiles * tile * pair_record_bytes(pde, kind, dim, precision);
+  const size_t packed_bytes = (rec_bytes + 255) / 256 * 256;
+  const size_t pbytes = (size_t)m * pair_partial_bytes(pde, precision);
+  const size_t room = kNoAllocScratchBytes - kNoAllocFlagBytes;
+  if (packed_bytes + pbytes > room)
+    throw Error(INTI_E_ARG, "problem too large for the fixed " + std::to_string(kNoAllocScratchBytes >> 20) +
+                                " MiB scratch of inti_apply_noalloc: needs " +
+                                std::to_string(packed_bytes + pbytes) + " bytes (use inti_op_apply)");
+  // source chunks: enough CTAs for ~2 waves, bounded by the scratch and the tiles
+  const int64_t blocks = (m + kBlock * kTPT - 1) / (kBlock * kTPT);
+  int64_t split = std::max<int64_t>(1, (2LL * D.num_sms * 4 + blocks - 1) / blocks);
+  split = std::min<int64_t>({split, n_tiles, 64, (int64_t)((room - packed_bytes) / pbytes)});
+  const int64_t tps = (n_tiles + split - 1) / split;
+  split = (n_tiles + tps - 1) / tps;
+  int* flag = reinterpret_cast<int*>(D.scratch);
+  void* packed = D.scratch + kNoAllocFlagBytes;
+  void* partial = D.scratch + kNoAllocFlagBytes + packed_bytes;
+  INTI_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), stream));
+  dispatch(pde, kind, dim, [&](auto tag) {
+    using T = decltype(tag);
+    auto go = [&](auto rtag) {
+      using R = decltype(rtag);
+      constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
+      const int64_t npad = n_tiles * TILE;
+      pack_sources<T::pde, T::kind, T::dim, R><<<(unsigned)((npad + 255) / 256), 256, 0, stream>>>(
+          n, npad, sc, sn, sw, x, make_double2(1.0, 0.0), make_double2(0.0, 0.0), static_cast<R*>(packed));
+      FwdArgs a;
+      a.m = m;
+      a.n_tiles = n_tiles;
+      a.tiles_per_split = (int)tps;
+      a.tcoords = tc;
+      a.tnormals = tn;
+      a.packed = packed;
+      a.partial = partial;
+      a.k = k;
+      a.kT = k * kExpiTable / (2 * kPi);
+      a.delta = 2 * kPi / kExpiTable;
+      a.expi = std::is_same<R, float>::value ? (const void*)D.expi32 : (const void*)D.expi64;
+      a.err = flag;
+      const size_t sm = fwd_smem<T, R>();
+      auto fn = &pair_forward<T::pde, T::kind, T::dim, R, TILE>;
+      INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      fn<<<dim3((unsigned)blocks, (unsigned)split), kBlock, sm, stream>>>(a);
+    };
+    if (precision == INTI_FP32C)
+      go(float());
+    else
+      go(double());
+  });
+  EpiArgs e;
+  e.m = m;
+  e.split = (int)split;
+  e.partial = partial;
+  e.scale = pair_scale(pde, kind, dim);
+  e.rowptr = rowptr;
+  e.col = col;
+  e.val = val;
+  e.x = x;
+  e.y = y;
+  e.ar = alpha ? alpha[0] : 1.0;
+  e.ai = alpha ? alpha[1] : 0.0;
+  e.br = beta ? beta[0] : 0.0;
+  e.bi = beta ? beta[1] : 0.0;
+  e.beta_zero = (e.br == 0.0 && e.bi == 0.0);
+  const unsigned gb = (unsigned)((m + 255) / 256);
+  const bool cplx = pde == HELMHOLTZ;
+  if (precision == INTI_FP32C) {
+    if (cplx)
+      pair_epilogue_kernel<float4, true><<<gb, 256, 0, stream>>>(e);
+    else
+      pair_epilogue_kernel<float2, false><<<gb, 256, 0, stream>>>(e);
+  } else {
+    if (cplx)
+      pair_epilogue_kernel<double2, true><<<gb, 256, 0, stream>>>(e);
+    else
+      pair_epilogue_kernel<double, false><<<gb, 256, 0, stream>>>(e);
+  }
+  INTI_CUDA(cudaGetLastError());
+  if (synchronize) {
+    INTI_CUDA(cudaStreamSynchronize(stream));
+    int f = 0;
+    INTI_CUDA(cudaMemcpy(&f, flag, sizeof(int), cudaMemcpyDeviceToHost));
+    if (f) throw Error(INTI_E_TIMEOUT, "a device-side bounded wait ran out (code " + std::to_string(f) + ")");
+  }
+  return INTI_OK;
+}
+
 }  // namespace inti
+
+extern "C" int inti_apply_noalloc(int pde, int kernel, int dim, double k, int precision, int64_t m,
+                                  const double* tcoords, const double* tnormals, int64_t n,
+                                  const double* scoords, const double* snormals, const double* sweights,
+                                  const int64_t* rowptr, const int32_t* col, const double* val,
+                                  const double* x, double* y, const double* alpha, const double* beta,
+                                  void* stream, int synchronize) {
+  try {
+    return inti::apply_noalloc(pde, kernel, dim, k, precision, m, tcoords, tnormals, n, scoords, snormals,
+                               sweights, rowptr, col, val, x, y, alpha, beta,
+                               static_cast<cudaStream_t>(stream), synchronize);
+  } catch (const inti::Error& e) {
+    inti::noalloc_error_set(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    inti::noalloc_error_set(e.what());
+    return INTI_E_ARG;
+  }
+}

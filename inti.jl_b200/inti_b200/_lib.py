@@ -119,6 +119,8 @@ SIGNATURES = {
     "inti_op_grad_sources": (C.c_int, [P, P, P, P, P, P, P, C.c_int]),
     "inti_measure_peaks": (C.c_int, [P, D, D, D]),
     "inti_selftest_math": (C.c_int, [P, D]),
+    "inti_apply_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, I64, P, P, I64, P, P, P,
+                                     P, P, P, P, P, D, D, P, C.c_int]),
 }
 
 _lib = None
