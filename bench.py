@@ -45,7 +45,7 @@ UNIT = "Gpairs/s"
 FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10}
 # DRAM bytes (read + write) of one pair-kernel launch on this workload, from
 # the ncu capture summarised in profiles/pair_forward_helmholtz_sl_fp64_p2sphere62k.md
-PAIR_TRAFFIC_BYTES = None
+PAIR_TRAFFIC_BYTES = 4.516e6
 
 
 def host_cores() -> int:
