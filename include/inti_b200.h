@@ -69,8 +69,10 @@ enum { INTI_LAPLACE = 0, INTI_HELMHOLTZ = 1 };
 enum { INTI_SL = 0, INTI_DL = 1, INTI_ADL = 2, INTI_HS = 3 };
 /* arithmetic of the pair evaluation */
 enum {
-  INTI_FP64 = 0, /* FP64 pairs and accumulation */
-  INTI_FP32C = 1 /* FP32 pairs, compensated (two-sum) accumulation; FP64 correction SpMV */
+  INTI_FP64 = 0,  /* FP64 pairs and accumulation */
+  INTI_FP32C = 1, /* FP32 pairs, compensated (two-sum) accumulation; FP64 correction SpMV */
+  INTI_TF32 = 2   /* batches only: kernel tile x density block on the tensor cores (TF32 in,
+                     FP32 accumulate); FP64 correction SpMV */
 };
 /* element type of densities / correction values */
 enum { INTI_F64 = 0, INTI_C128 = 1 };
@@ -217,6 +219,28 @@ int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, doub
  * on this device, in operations per second (FMA counted as 2 flops). */
 int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops,
                        double* mufu_ops);
+
+/* ---- batches: many surfaces, many right-hand sides, one launch ----------
+ * The block-diagonal operator diag(A_1 + C_1, ..., A_S + C_S) over S
+ * quadratures of uneven size (the batching form of the workloads: plane
+ * waves on a batch of star-shaped surfaces).  kernel: INTI_SL, INTI_DL or
+ * 4 (combined field c_dl*DL + c_sl*SL, coefficients as 2 doubles each).
+ * corr_dl / corr_sl: per-surface corrections (arrays of S handles, entries
+ * or arrays may be NULL); they are merged with the coefficients.  Densities
+ * are column-major over the concatenated nodes (surface s occupies rows
+ * off_s .. off_s + n_s - 1 of every column). */
+typedef struct inti_batch inti_batch;
+int inti_batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quads, int pde, int kernel,
+                      double k_re, double k_im, const double* c_dl, const double* c_sl,
+                      const inti_csr* const* corr_dl, const inti_csr* const* corr_sl,
+                      inti_batch** out);
+/* Y = alpha*(A X + C X) + beta*Y for nrhs columns.  precision INTI_FP64
+ * (CUDA cores) or INTI_TF32 (Helmholtz: kernel tiles x density blocks on the
+ * tcgen05 tensor cores, FP32 accumulation, FP64 correction). */
+int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
+                     int32_t nrhs, const double* alpha, const double* beta, int on_device);
+int64_t inti_batch_size(const inti_batch* b);
+int inti_batch_destroy(inti_batch* b);
 
 /* ---- allocation-free apply ------------------------------------------------
  * No counterpart in the reference: Inti.jl's operators allocate freely.

@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.h"
 #include "common.h"
 #include "internal.h"
 
@@ -629,6 +630,54 @@ int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, doub
   inti_ctx* ctx = op->ctx;
   return guarded(ctx, [&] {
     grad_sources(op, g, sigma, dsigma, dcoords, dnormals, dweights, on_device);
+  });
+}
+
+int inti_batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quads, int pde, int kernel,
+                      double k_re, double k_im, const double* c_dl, const double* c_sl,
+                      const inti_csr* const* corr_dl, const inti_csr* const* corr_sl, inti_batch** out) {
+  if (!ctx || !out) return INTI_E_ARG;
+  *out = nullptr;
+  return guarded(ctx, [&] {
+    *out = batch_create(ctx, nsurf, quads, pde, kernel, k_re, k_im, c_dl, c_sl, corr_dl, corr_sl);
+  });
+}
+
+int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
+                     int32_t nrhs, const double* alpha, const double* beta, int on_device) {
+  if (!b) return INTI_E_ARG;
+  inti_ctx* ctx = b->ctx;
+  return guarded(ctx, [&] {
+    require(x && y, INTI_E_ARG, "x/y NULL");
+    require(nrhs >= 1, INTI_E_ARG, "nrhs must be >= 1");
+    const int64_t n = b->off.back();
+    require(ldx >= n && ldy >= n, INTI_E_SHAPE, "leading dimension smaller than the node count");
+    const int comps = b->pde == INTI_HELMHOLTZ ? 2 : 1;
+    if (on_device) {
+      batch_apply_device(b, precision, x, ldx, y, ldy, nrhs, alpha, beta);
+      return;
+    }
+    DevBuf xd, yd;
+    const size_t bx = sizeof(double) * comps * (size_t)ldx * nrhs, by = sizeof(double) * comps * (size_t)ldy * nrhs;
+    xd.ensure(bx);
+    yd.ensure(by);
+    h2d(ctx, xd.p, x, bx);
+    const bool bz = !beta || (beta[0] == 0.0 && beta[1] == 0.0);
+    if (!bz) h2d(ctx, yd.p, y, by);
+    batch_apply_device(b, precision, xd.as<double>(), ldx, yd.as<double>(), ldy, nrhs, alpha, beta);
+    d2h(ctx, y, yd.p, by);
+    sync_and_check(ctx);
+  });
+}
+
+int64_t inti_batch_size(const inti_batch* b) { return b ? b->off.back() : -1; }
+
+int inti_batch_destroy(inti_batch* b) {
+  if (!b) return INTI_OK;
+  inti_ctx* ctx = b->ctx;
+  return guarded(ctx, [&] {
+    INTI_CUDA(cudaStreamSynchronize(ctx->stream));
+    delete b;
   });
 }
 

@@ -1,0 +1,392 @@
+// Batched multi-right-hand-side operators: many surfaces of uneven size and
+// many densities per surface in one launch (the batching form of the
+// workloads: plane-wave right-hand sides on a batch of star surfaces).
+//
+// A batch holds S quadratures concatenated in one node array (segment s =
+// nodes off[s] .. off[s+1]-1) and one operator kind for all of them; the
+// product is block diagonal: Y_s = A_s X_s (+ corrections), each A_s the
+// on-the-fly Nystrom operator of surface s.  Densities are column-major
+// (node, rhs) over the concatenated nodes.
+//
+// Two arithmetic forms of the pair product:
+//  * FP64 on CUDA cores (mrhs_fp64): each thread owns one target and a
+//    chunk of 16 right-hand sides; source tiles and their densities are
+//    staged in shared memory; the kernel value is computed once per pair and
+//    applied to the 16 columns.
+//  * TF32 on the tensor cores (mrhs_tc.cu): the kernel tile is generated by
+//    CUDA cores into shared memory and multiplied with the staged density
+//    block by tcgen05.mma into a TMEM accumulator.
+// Work items are (surface, 128-target block) ordered by surface size,
+// largest first, so the uneven surfaces balance across the SMs.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <numeric>
+#include <vector>
+
+#include "batch.h"
+#include "common.h"
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace inti {
+
+// Complex kernel value K(x, y) without the 1/(4 pi) factor, fast math
+// (rsqrt_fast, table e^{ikd}); kind SL, DL or CF (= c1*DL + c2*SL with the
+// coefficients applied by the caller through the returned pair).
+struct KPair {
+  double2 dl, sl;
+};
+
+__device__ __forceinline__ KPair helm_kernels(const double* x, const double* y, const double* ny, double k,
+                                              double kT, double delta, const double2* tab, bool want_dl,
+                                              bool want_sl) {
+  const double r0 = x[0] - y[0], r1 = x[1] - y[1], r2 = x[2] - y[2];
+  const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
+  const bool keep = d2 > kSamePointTol2;
+  const double ri = keep ? rsqrt_fast(d2) : 0.0;
+  const double d = d2 * ri;
+  double cs, sn;
+  expi_table_eval<double, double2>(d * kT, tab, delta, cs, sn);
+  KPair o;
+  o.sl = make_double2(0.0, 0.0);
+  o.dl = make_double2(0.0, 0.0);
+  if (want_sl) o.sl = make_double2(ri * cs, ri * sn);
+  if (want_dl) {
+    const double er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
+    const double rn = fma(r2, ny[2], fma(r1, ny[1], r0 * ny[0]));
+    const double f = rn * ri * ri;
+    o.dl = make_double2(er * f, ei * f);
+  }
+  return o;
+}
+
+__device__ __forceinline__ double2 lap_kernels(const double* x, const double* y, const double* ny, double c1,
+                                               double c2, int kind) {
+  const double r0 = x[0] - y[0], r1 = x[1] - y[1], r2 = x[2] - y[2];
+  const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
+  const bool keep = d2 > kSamePointTol2;
+  const double ri = keep ? rsqrt_fast(d2) : 0.0;
+  double v = 0.0;
+  if (kind != SL) {
+    const double rn = fma(r2, ny[2], fma(r1, ny[1], r0 * ny[0]));
+    v = rn * ri * ri * ri * (kind == CF ? c1 : 1.0);
+  }
+  if (kind != DL) v = fma(ri, kind == CF ? c2 : 1.0, v);
+  return make_double2(v, 0.0);
+}
+
+constexpr int kMrhsBlock = 128;
+constexpr int kMrhsTile = 32;
+constexpr int kMrhsCols = 16;  // right-hand sides per thread
+
+// Y[c][i] = alpha * (scale * sum_j K_ij w_j X[c][j]) + beta * Y[c][i]
+// for the targets of item blockIdx.x and columns blockIdx.y*16 .. +15.
+template <int PDE, int KIND>
+__global__ void __launch_bounds__(kMrhsBlock) mrhs_fp64(BatchArgs a) {
+  constexpr bool CPLX = PDE == HELMHOLTZ;
+  __shared__ double sx[kMrhsTile * 3], sn[kMrhsTile * 3], sw[kMrhsTile];
+  __shared__ double2 sX[kMrhsTile * kMrhsCols];
+  __shared__ double2 tab[kExpiTable];
+  const int item = blockIdx.x;
+  const int s = a.item_surf[item];
+  const int64_t off = a.off[s], n = a.off[s + 1] - off;
+  const int64_t i_loc = (int64_t)a.item_block[item] * kMrhsBlock + threadIdx.x;
+  const bool active = i_loc < n;
+  const int64_t i = off + min(i_loc, n - 1);
+  const int c0 = blockIdx.y * kMrhsCols;
+  const int ncol = min(kMrhsCols, a.nrhs - c0);
+  if (CPLX)
+    for (int q = threadIdx.x; q < kExpiTable; q += kMrhsBlock) tab[q] = a.expi[q];
+  double xi[3] = {a.coords[3 * i], a.coords[3 * i + 1], a.coords[3 * i + 2]};
+  double2 acc[kMrhsCols];
+#pragma unroll
+  for (int c = 0; c < kMrhsCols; ++c) acc[c] = make_double2(0.0, 0.0);
+  const double kT = a.k * kExpiTable / (2 * kPi), delta = 2 * kPi / kExpiTable;
+  for (int64_t j0 = 0; j0 < n; j0 += kMrhsTile) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < kMrhsTile; q += kMrhsBlock) {
+      const int64_t j = j0 + q;
+      const bool in = j < n;
+      for (int c = 0; c < 3; ++c) {
+        sx[3 * q + c] = in ? a.coords[3 * (off + j) + c] : 0.0;
+        sn[3 * q + c] = (in && a.normals) ? a.normals[3 * (off + j) + c] : 0.0;
+      }
+      sw[q] = in ? a.weights[off + j] : 0.0;
+    }
+    for (int q = threadIdx.x; q < kMrhsTile * kMrhsCols; q += kMrhsBlock) {
+      const int jj = q / kMrhsCols, c = q % kMrhsCols;
+      const int64_t j = j0 + jj;
+      double2 v = make_double2(0.0, 0.0);
+      if (j < n && c < ncol) {
+        const int64_t idx = (int64_t)(c0 + c) * a.ldx + off + j;
+        v = CPLX ? reinterpret_cast<const double2*>(a.x)[idx] : make_double2(a.x[idx], 0.0);
+      }
+      sX[q] = v;
+    }
+    __syncthreads();
+    const int cnt = (int)(n - j0 < kMrhsTile ? n - j0 : kMrhsTile);
+    for (int q = 0; q < cnt; ++q) {
+      double2 kv;
+      if (CPLX) {
+        const KPair kp = helm_kernels(xi, &sx[3 * q], &sn[3 * q], a.k, kT, delta, tab, KIND != SL, KIND != DL);
+        if (KIND == SL)
+          kv = kp.sl;
+        else if (KIND == DL)
+          kv = kp.dl;
+        else  // c1*DL + c2*SL, complex coefficients
+          kv = make_double2(a.c1r * kp.dl.x - a.c1i * kp.dl.y + a.c2r * kp.sl.x - a.c2i * kp.sl.y,
+                            a.c1r * kp.dl.y + a.c1i * kp.dl.x + a.c2r * kp.sl.y + a.c2i * kp.sl.x);
+      } else {
+        kv = lap_kernels(xi, &sx[3 * q], &sn[3 * q], a.c1r, a.c2r, KIND);
+      }
+      const double w = sw[q];
+      kv.x *= w;
+      kv.y *= w;
+#pragma unroll
+      for (int c = 0; c < kMrhsCols; ++c) {
+        const double2 xv = sX[q * kMrhsCols + c];
+        acc[c].x = fma(kv.x, xv.x, fma(-kv.y, xv.y, acc[c].x));
+        acc[c].y = fma(kv.x, xv.y, fma(kv.y, xv.x, acc[c].y));
+      }
+    }
+  }
+  if (!active) return;
+  const double sc = 1.0 / (4 * kPi);
+#pragma unroll
+  for (int c = 0; c < kMrhsCols; ++c) {
+    if (c >= ncol) break;
+    const int64_t idx = (int64_t)(c0 + c) * a.ldy + i;
+    double yr = sc * acc[c].x, yi = sc * acc[c].y;
+    double orr = a.ar * yr - a.ai * yi, oi = a.ar * yi + a.ai * yr;
+    if (CPLX) {
+      double2* Y = reinterpret_cast<double2*>(a.y);
+      if (!a.beta_zero) {
+        const double2 yo = Y[idx];
+        orr += a.br * yo.x - a.bi * yo.y;
+        oi += a.br * yo.y + a.bi * yo.x;
+      }
+      Y[idx] = make_double2(orr, oi);
+    } else {
+      if (!a.beta_zero) orr += a.br * a.y[idx];
+      a.y[idx] = orr;
+    }
+  }
+}
+
+// Multi-column CSR correction: Y[c][i] += alpha * sum_p val[p] X[c][col[p]]
+template <bool CPLX>
+__global__ void csr_mrhs(int64_t m, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+                        const double* __restrict__ val, const double* __restrict__ x, int64_t ldx, double* y,
+                        int64_t ldy, int nrhs, double ar, double ai) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int c = blockIdx.y;
+  if (i >= m || c >= nrhs) return;
+  double sr = 0.0, si = 0.0;
+  for (int64_t p = rowptr[i]; p < rowptr[i + 1]; ++p) {
+    const int64_t j = (int64_t)c * ldx + col[p];
+    if (CPLX) {
+      const double2 v = reinterpret_cast<const double2*>(val)[p];
+      const double2 xv = reinterpret_cast<const double2*>(x)[j];
+      sr = fma(v.x, xv.x, fma(-v.y, xv.y, sr));
+      si = fma(v.x, xv.y, fma(v.y, xv.x, si));
+    } else {
+      sr = fma(val[p], x[j], sr);
+    }
+  }
+  const int64_t o = (int64_t)c * ldy + i;
+  if (CPLX) {
+    double2* Y = reinterpret_cast<double2*>(y);
+    double2 yo = Y[o];
+    yo.x += ar * sr - ai * si;
+    yo.y += ar * si + ai * sr;
+    Y[o] = yo;
+  } else {
+    y[o] += ar * sr;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+inti_batch* batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quads, int pde, int kind,
+                         double k_re, double k_im, const double* c_dl, const double* c_sl,
+                         const inti_csr* const* corr_dl, const inti_csr* const* corr_sl) {
+  if (nsurf < 1 || !quads) throw Error(INTI_E_ARG, "a batch needs at least one surface");
+  if (pde != INTI_LAPLACE && pde != INTI_HELMHOLTZ) throw Error(INTI_E_ARG, "unknown pde");
+  if (kind != SL && kind != DL && kind != CF) throw Error(INTI_E_ARG, "batch kernels are SL, DL or the combined field");
+  if (pde == INTI_HELMHOLTZ && k_im != 0.0) throw Error(INTI_E_UNSUPPORTED, "complex wavenumbers are not implemented");
+  const bool cplx = pde == INTI_HELMHOLTZ;
+  double c1[2] = {1.0, 0.0}, c2[2] = {1.0, 0.0};
+  if (kind == CF) {
+    if (!c_dl || !c_sl) throw Error(INTI_E_ARG, "combined-field coefficients are NULL");
+    c1[0] = c_dl[0];
+    c1[1] = c_dl[1];
+    c2[0] = c_sl[0];
+    c2[1] = c_sl[1];
+    if (!cplx && (c1[1] != 0.0 || c2[1] != 0.0))
+      throw Error(INTI_E_UNSUPPORTED, "complex coefficients need a Helmholtz operator");
+  }
+  std::unique_ptr<inti_batch> b(new inti_batch());
+  b->ctx = ctx;
+  b->pde = pde;
+  b->kind = kind;
+  b->k = k_re;
+  for (int q = 0; q < 2; ++q) {
+    b->c1[q] = c1[q];
+    b->c2[q] = c2[q];
+  }
+  b->off.assign(nsurf + 1, 0);
+  for (int s = 0; s < nsurf; ++s) {
+    const inti_quad* q = quads[s];
+    if (!q) throw Error(INTI_E_ARG, "quadrature is NULL");
+    if (q->ctx != ctx) throw Error(INTI_E_STATE, "quadrature belongs to another context");
+    if (q->dim != 3) throw Error(INTI_E_UNSUPPORTED, "batches are 3D");
+    if (kind != SL && !q->has_normals) throw Error(INTI_E_ARG, "double-layer kernels need normals");
+    b->off[s + 1] = b->off[s] + q->n;
+  }
+  const int64_t ntot = b->off[nsurf];
+  std::vector<double> X(3 * ntot), N(3 * ntot, 0.0), W(ntot);
+  for (int s = 0; s < nsurf; ++s) {
+    const inti_quad* q = quads[s];
+    std::copy(q->h_coords.begin(), q->h_coords.end(), X.begin() + 3 * b->off[s]);
+    if (q->has_normals) std::copy(q->h_normals.begin(), q->h_normals.end(), N.begin() + 3 * b->off[s]);
+    std::copy(q->h_weights.begin(), q->h_weights.end(), W.begin() + b->off[s]);
+  }
+  b->coords.ensure(sizeof(double) * 3 * ntot);
+  b->normals.ensure(sizeof(double) * 3 * ntot);
+  b->weights.ensure(sizeof(double) * ntot);
+  INTI_CUDA(cudaMemcpy(b->coords.p, X.data(), sizeof(double) * 3 * ntot, cudaMemcpyHostToDevice));
+  INTI_CUDA(cudaMemcpy(b->normals.p, N.data(), sizeof(double) * 3 * ntot, cudaMemcpyHostToDevice));
+  INTI_CUDA(cudaMemcpy(b->weights.p, W.data(), sizeof(double) * ntot, cudaMemcpyHostToDevice));
+  b->h_off = b->off;
+  b->d_off.ensure(sizeof(int64_t) * (nsurf + 1));
+  INTI_CUDA(cudaMemcpy(b->d_off.p, b->off.data(), sizeof(int64_t) * (nsurf + 1), cudaMemcpyHostToDevice));
+  // work items: (surface, 128-target block), largest surfaces first
+  std::vector<int> order(nsurf);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int c) { return quads[a]->n > quads[c]->n; });
+  std::vector<int32_t> isurf, iblk;
+  for (int s : order)
+    for (int64_t t = 0; t * kMrhsBlock < quads[s]->n; ++t) {
+      isurf.push_back(s);
+      iblk.push_back((int32_t)t);
+    }
+  b->nitems = (int)isurf.size();
+  b->item_surf.ensure(sizeof(int32_t) * b->nitems);
+  b->item_block.ensure(sizeof(int32_t) * b->nitems);
+  INTI_CUDA(cudaMemcpy(b->item_surf.p, isurf.data(), sizeof(int32_t) * b->nitems, cudaMemcpyHostToDevice));
+  INTI_CUDA(cudaMemcpy(b->item_block.p, iblk.data(), sizeof(int32_t) * b->nitems, cudaMemcpyHostToDevice));
+  // block-diagonal correction c1*C_dl + c2*C_sl (or the single kernel's)
+  std::vector<int64_t> rp(ntot + 1, 0);
+  std::vector<int32_t> col;
+  std::vector<double> val;
+  const int comps = cplx ? 2 : 1;
+  bool any = false;
+  for (int s = 0; s < nsurf; ++s) {
+    const inti_csr* a = corr_dl ? corr_dl[s] : nullptr;
+    const inti_csr* c = corr_sl ? corr_sl[s] : nullptr;
+    if (kind == SL) a = nullptr;
+    if (kind == DL) c = nullptr;
+    const int64_t ns = quads[s]->n;
+    for (const inti_csr* m : {a, c})
+      if (m && (m->m != ns || m->n != ns || m->dtype != (cplx ? INTI_C128 : INTI_F64)))
+        throw Error(INTI_E_SHAPE, "a correction does not match its surface (size or dtype)");
+    std::unique_ptr<inti_csr> merged;
+    const double one[2] = {1.0, 0.0};
+    if (a || c) {
+      merged = merge_corrections(ctx, a, kind == CF ? c1 : one, c, kind == CF ? c2 : one, ns, ns, cplx);
+      any = true;
+      std::vector<int64_t> mrp(ns + 1);
+      std::vector<int32_t> mcol(merged->nnz);
+      std::vector<double> mval((size_t)merged->nnz * comps);
+      INTI_CUDA(cudaMemcpy(mrp.data(), merged->rowptr.p, sizeof(int64_t) * (ns + 1), cudaMemcpyDeviceToHost));
+      INTI_CUDA(cudaMemcpy(mcol.data(), merged->col.p, sizeof(int32_t) * merged->nnz, cudaMemcpyDeviceToHost));
+      INTI_CUDA(cudaMemcpy(mval.data(), merged->val.p, sizeof(double) * comps * merged->nnz, cudaMemcpyDeviceToHost));
+      for (int64_t i = 0; i < ns; ++i) {
+        for (int64_t p = mrp[i]; p < mrp[i + 1]; ++p) {
+          col.push_back((int32_t)(mcol[p] + b->off[s]));
+          for (int q = 0; q < comps; ++q) val.push_back(mval[p * comps + q]);
+        }
+        rp[b->off[s] + i + 1] = (int64_t)col.size();
+      }
+    } else {
+      for (int64_t i = 0; i < ns; ++i) rp[b->off[s] + i + 1] = (int64_t)col.size();
+    }
+  }
+  if (any)
+    b->corr.reset(csr_create_host(ctx, ntot, ntot, (int64_t)col.size(), rp.data(), col.data(), val.data(),
+                                  cplx ? INTI_C128 : INTI_F64));
+  b->expi = expi_table_f64(ctx);
+  return b.release();
+}
+
+void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
+                        int32_t nrhs, const double* alpha, const double* beta) {
+  inti_ctx* ctx = b->ctx;
+  const bool cplx = b->pde == INTI_HELMHOLTZ;
+  BatchArgs a;
+  a.off = b->d_off.as<int64_t>();
+  a.item_surf = b->item_surf.as<int32_t>();
+  a.item_block = b->item_block.as<int32_t>();
+  a.coords = b->coords.as<double>();
+  a.normals = b->normals.as<double>();
+  a.weights = b->weights.as<double>();
+  a.x = x;
+  a.ldx = ldx;
+  a.y = y;
+  a.ldy = ldy;
+  a.nrhs = nrhs;
+  a.k = b->k;
+  a.c1r = b->c1[0];
+  a.c1i = b->c1[1];
+  a.c2r = b->c2[0];
+  a.c2i = b->c2[1];
+  a.ar = alpha ? alpha[0] : 1.0;
+  a.ai = alpha ? alpha[1] : 0.0;
+  a.br = beta ? beta[0] : 0.0;
+  a.bi = beta ? beta[1] : 0.0;
+  a.beta_zero = a.br == 0.0 && a.bi == 0.0;
+  a.expi = b->expi;
+  if (precision == INTI_TF32) {
+    if (!cplx) throw Error(INTI_E_UNSUPPORTED, "the tensor-core form is implemented for Helmholtz");
+    mrhs_tc_launch(b, a);
+  } else if (precision == INTI_FP64) {
+    dim3 grid((unsigned)b->nitems, (unsigned)((nrhs + kMrhsCols - 1) / kMrhsCols));
+    ProfScope ps(ctx, "batch");
+    auto go = [&](auto pc, auto kc) {
+      constexpr int P = decltype(pc)::value, K = decltype(kc)::value;
+      mrhs_fp64<P, K><<<grid, kMrhsBlock, 0, ctx->stream>>>(a);
+    };
+    if (cplx) {
+      if (b->kind == SL) go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, SL>());
+      else if (b->kind == DL) go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, DL>());
+      else go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, CF>());
+    } else {
+      if (b->kind == SL) go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, SL>());
+      else if (b->kind == DL) go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, DL>());
+      else go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, CF>());
+    }
+    ctx->launches++;
+  } else {
+    throw Error(INTI_E_ARG, "batch precision must be FP64 or TF32");
+  }
+  INTI_CUDA(cudaGetLastError());
+  if (b->corr) {
+    const int64_t m = b->off.back();
+    dim3 grid((unsigned)((m + 255) / 256), (unsigned)nrhs);
+    if (cplx)
+      csr_mrhs<true><<<grid, 256, 0, ctx->stream>>>(m, b->corr->rowptr.as<int64_t>(), b->corr->col.as<int32_t>(),
+                                                    b->corr->val.as<double>(), x, ldx, y, ldy, nrhs, a.ar, a.ai);
+    else
+      csr_mrhs<false><<<grid, 256, 0, ctx->stream>>>(m, b->corr->rowptr.as<int64_t>(), b->corr->col.as<int32_t>(),
+                                                     b->corr->val.as<double>(), x, ldx, y, ldy, nrhs, a.ar, a.ai);
+    ctx->launches++;
+    INTI_CUDA(cudaGetLastError());
+  }
+}
+
+}  // namespace inti

@@ -1,0 +1,57 @@
+// Batch handle and launch arguments shared by batch.cu (FP64 path, host)
+// and mrhs_tc.cu (tensor-core path).  Internal.
+#pragma once
+
+#include <memory>
+#include <vector>
+
+#include "common.h"
+
+struct inti_batch {
+  inti_ctx* ctx = nullptr;
+  int pde = INTI_HELMHOLTZ, kind = INTI_SL;
+  double k = 0.0;
+  double c1[2] = {1.0, 0.0}, c2[2] = {1.0, 0.0};
+  std::vector<int64_t> off, h_off;  // node offsets of the surfaces (S+1)
+  inti::DevBuf d_off, coords, normals, weights;
+  inti::DevBuf item_surf, item_block;  // work items, largest surfaces first
+  int nitems = 0;
+  std::unique_ptr<inti_csr> corr;  // block-diagonal correction (global indices)
+  const double2* expi = nullptr;
+  // tensor-core path: packed density blocks and source records, tile
+  // offsets, 256-target work items, work counter
+  inti::DevBuf tc_b, tc_src, tc_counter, tc_toff, tc_items;
+  int64_t tc_ntiles = 0;
+  int tc_nitems = 0;
+  const float2* expi32 = nullptr;
+};
+
+namespace inti {
+
+struct BatchArgs {
+  const int64_t* off;
+  const int32_t* item_surf;
+  const int32_t* item_block;
+  const double* coords;
+  const double* normals;
+  const double* weights;
+  const double* x;
+  int64_t ldx;
+  double* y;
+  int64_t ldy;
+  int nrhs;
+  double k;
+  double c1r, c1i, c2r, c2i;
+  double ar, ai, br, bi;
+  bool beta_zero;
+  const double2* expi;
+};
+
+void mrhs_tc_launch(inti_batch* b, const BatchArgs& a);
+inti_batch* batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quads, int pde, int kind,
+                         double k_re, double k_im, const double* c_dl, const double* c_sl,
+                         const inti_csr* const* corr_dl, const inti_csr* const* corr_sl);
+void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
+                        int32_t nrhs, const double* alpha, const double* beta);
+
+}  // namespace inti

@@ -40,6 +40,9 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
                             const inti_quad* source, const inti_csr* corr_dl, const inti_csr* corr_sl,
                             const double* c_dl, const double* c_sl, int precision);
 inti_op* op_clone_precision(const inti_op* op, int precision);
+std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
+                                            const inti_csr* b, const double* cb, int64_t m, int64_t n,
+                                            bool cplx);
 void op_prepare_transpose(inti_op* op);
 void transpose_epilogue(inti_ctx* ctx, int64_t n, int split, const void* partial,
                         const inti_csr* corrT, const double* x, double* y, const double* alpha,

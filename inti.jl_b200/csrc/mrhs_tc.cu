@@ -1,0 +1,522 @@
+// Tensor-core (tcgen05, TF32 in / FP32 accumulate) form of the batched
+// multi-right-hand-side Helmholtz product Y = K X over many surfaces.
+//
+// The complex product is a real GEMM: with A[i][2j] = Re K_ij,
+// A[i][2j+1] = Im K_ij (targets x 2*sources) and, for right-hand side r,
+// B[2j][r] = Re x_jr, B[2j+1][r] = -Im x_jr, B[2j][64+r] = Im x_jr,
+// B[2j+1][64+r] = Re x_jr (x already multiplied by the weight w_j), the
+// columns 0..63 of A*B are Re Y and 64..127 are Im Y.
+//
+// One persistent CTA per SM (256 threads) takes work items (surface, block
+// of 256 targets) from an atomic counter, largest surfaces first.  Per
+// stage of 32 sources:
+//   * the source records (FP32 coordinates/normals) of stage t+2 and the
+//     packed density block B of stage t+1 are copied into shared memory by
+//     the TMA bulk engine (cp.async.bulk) completing on mbarriers;
+//   * every thread evaluates K for its target row and the 32 sources on the
+//     CUDA cores (FP32, table e^{ikd}) and stores them, rounded to TF32, in
+//     the canonical K-major no-swizzle layout (8-row x 16-byte core
+//     matrices; LBO = 128 B between K chunks, SBO = 2048 B between row
+//     groups);
+//   * one thread issues 2 x 8 tcgen05.mma (M = 128, N = 128, K = 8) into two
+//     TMEM accumulators (128 lanes x 128 FP32 columns each) and commits them
+//     to an mbarrier that frees the A/B buffers.
+// At the end of an item each warp reads its lane quarter of the accumulators
+// with tcgen05.ld and writes alpha*Y/(4 pi) + beta*Y in FP64.
+//
+// Every wait is bounded.  On a timeout the CTA records the error, drains its
+// own copies and MMAs (bounded), frees its TMEM and leaves.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "batch.h"
+#include "common.h"
+#include "device_common.cuh"
+#include "internal.h"
+
+namespace inti {
+
+constexpr int TC_THREADS = 256;
+constexpr int TC_ROWS = 256;             // targets per item (2 accumulators x 128)
+constexpr int TC_R = 64;                 // complex right-hand sides per pass
+constexpr int TC_N = 2 * TC_R;           // real accumulator columns
+constexpr int TC_J = 32;                 // sources per stage
+constexpr int TC_K = 2 * TC_J;           // K elements per stage
+constexpr int TC_A_BYTES = 128 * TC_K * 4;           // one accumulator's A tile: 32 KB
+constexpr int TC_B_BYTES = TC_N * TC_K * 4;          // 32 KB
+constexpr int TC_S_FLOATS = 8;                       // x y z nx ny nz pad pad
+constexpr int TC_S_BYTES = TC_J * TC_S_FLOATS * 4;   // 1 KB
+// dynamic shared memory layout (bytes)
+constexpr int TC_OFF_A = 0;                               // 2 stages x 2 accumulators x 32 KB
+constexpr int TC_OFF_B = TC_OFF_A + 2 * 2 * TC_A_BYTES;   // 2 stages x 32 KB
+constexpr int TC_OFF_S = TC_OFF_B + 2 * TC_B_BYTES;       // 3 stages x 1 KB
+constexpr int TC_OFF_T = TC_OFF_S + 3 * TC_S_BYTES;       // e^{i m delta} table (float2)
+constexpr int TC_SMEM = TC_OFF_T + kExpiTable * 8;
+constexpr uint32_t TC_TMEM_COLS = 256;
+// instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N = 128, M = 128
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                              ((uint32_t)(128 >> 4) << 24);
+
+// K-major no-swizzle canonical offset of element (row, k) in a 128 x 64 tile
+__host__ __device__ constexpr uint32_t tc_kmajor_off(int row, int k) {
+  return (uint32_t)((row >> 3) * 2048 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ uint64_t tc_smem_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;    // leading byte offset: next K chunk
+  d |= (uint64_t)((2048 >> 4) & 0x3FFF) << 32;   // stride byte offset: next 8-row group
+  d |= (uint64_t)1 << 46;                        // descriptor version (sm_100)
+  return d;                                      // base offset 0, no swizzle
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return r;
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+#pragma unroll
+  for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+__device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+struct TcArgs {
+  const int64_t* off;        // surface node offsets
+  const int64_t* toff;       // surface offsets in source tiles
+  const int32_t* item_surf;  // items: surface, 256-target block
+  const int32_t* item_block;
+  int nitems;
+  int ncolgroups;            // passes of 64 right-hand sides
+  const float* src;          // packed source records, TC_J per tile
+  const uint32_t* bpack;     // packed density blocks, per (column group, tile)
+  int64_t ntiles;            // tiles per column group
+  const double* coords;      // FP64 targets
+  double* y;
+  int64_t ldy;
+  int nrhs;
+  float k, kT, delta;
+  float c1r, c1i, c2r, c2i;
+  int kind;
+  double ar, ai, br, bi;
+  bool beta_zero;
+  const float2* expi;
+  int* counter;
+  int* err;
+};
+
+// K(x, y) for the Helmholtz kernels (without 1/(4 pi)), FP32.
+__device__ __forceinline__ float2 tc_kernel(const float* x, const float* s, const TcArgs& a,
+                                            const float2* __restrict__ tab) {
+  const float r0 = x[0] - s[0], r1 = x[1] - s[1], r2 = x[2] - s[2];
+  const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+  const bool keep = d2 > 1.0e-28f;
+  const float ri = keep ? rsqrt_approx_f32(d2) : 0.0f;
+  const float d = d2 * ri;
+  float cs, sn;
+  expi_table_eval<float, float2>(d * a.kT, tab, a.delta, cs, sn);
+  float vr = 0.f, vi = 0.f;
+  if (a.kind != DL) {  // SL part e^{ikd}/d
+    const float sr = ri * cs, si = ri * sn;
+    if (a.kind == SL) {
+      vr = sr;
+      vi = si;
+    } else {
+      vr = a.c2r * sr - a.c2i * si;
+      vi = a.c2r * si + a.c2i * sr;
+    }
+  }
+  if (a.kind != SL) {  // DL part e^{ikd}(1/d - ik)(r.n)/d^2
+    const float er = fmaf(cs, ri, a.k * sn), ei = fmaf(sn, ri, -a.k * cs);
+    const float rn = fmaf(r2, s[5], fmaf(r1, s[4], r0 * s[3]));
+    const float f = rn * ri * ri;
+    const float dr = er * f, di = ei * f;
+    if (a.kind == DL) {
+      vr = dr;
+      vi = di;
+    } else {
+      vr += a.c1r * dr - a.c1i * di;
+      vi += a.c1r * di + a.c1i * dr;
+    }
+  }
+  return make_float2(vr, vi);
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t fullS[3], fullB[2], mmaDone[2];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int item_sh;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  float2* tab = reinterpret_cast<float2*>(sm + TC_OFF_T);
+  for (int q = tid; q < kExpiTable; q += TC_THREADS) tab[q] = a.expi[q];
+  if (tid == 0) {
+    for (int q = 0; q < 3; ++q) mbar_init(&fullS[q], 1);
+    for (int q = 0; q < 2; ++q) {
+      mbar_init(&fullB[q], 1);
+      mbar_init(&mmaDone[q], 1);
+    }
+    mbar_fence_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  const uint32_t sbase = smem_u32(sm);
+
+  // uses of each barrier so far (thread-uniform): phase = (uses / nbuf) & 1
+  uint32_t gS = 0;   // source-record stages consumed
+  uint32_t gB = 0;   // density stages consumed (= MMA groups issued)
+  uint32_t gD = 0;   // MMA groups waited for
+  uint32_t issuedS = 0, issuedB = 0;  // thread 0: copies issued
+  uint32_t consumedB = 0, committed = 0;  // thread 0: density copies landed, MMA groups committed
+  bool ok = true;
+
+  for (;;) {
+    if (tid == 0) item_sh = atomicAdd(a.counter, 1);
+    __syncthreads();
+    const int it = item_sh;
+    if (it >= a.nitems * a.ncolgroups) break;
+    const int cg = it / a.nitems;
+    const int item = it % a.nitems;
+    const int s = a.item_surf[item];
+    const int64_t off = a.off[s], n = a.off[s + 1] - off;
+    const int64_t T = (n + TC_J - 1) / TC_J;
+    const float* srcs = a.src + (size_t)a.toff[s] * TC_J * TC_S_FLOATS;
+    const uint32_t* bp = a.bpack + ((size_t)cg * a.ntiles + a.toff[s]) * (TC_B_BYTES / 4);
+    const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + tid;
+    const bool active = row_loc < n;
+    const int64_t ti = off + min(row_loc, n - 1);
+    const float xt[3] = {(float)a.coords[3 * ti], (float)a.coords[3 * ti + 1], (float)a.coords[3 * ti + 2]};
+    const int acc = tid >> 7;          // accumulator of this row
+    const int row = tid & 127;         // row inside the accumulator
+    // prologue: source records of stages 0 and 1, density of stage 0
+    if (tid == 0) {
+      for (int64_t t = 0; t < 2 && t < T; ++t) {
+        const uint32_t b = (gS + (uint32_t)t) % 3;
+        mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
+        bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)t * TC_J * TC_S_FLOATS, TC_S_BYTES, &fullS[b]);
+        ++issuedS;
+      }
+      const uint32_t b = gB & 1;
+      mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
+      bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp, TC_B_BYTES, &fullB[b]);
+      ++issuedB;
+    }
+    for (int64_t t = 0; t < T; ++t) {
+      // 1. source records of stage t
+      const uint32_t sb = gS % 3;
+      ok = mbar_wait_bounded(&fullS[sb], (gS / 3) & 1);
+      if (!__syncthreads_and(ok)) goto fail;
+      // 2. kernel values for this row and the 32 sources, TF32, into A[stage]
+      {
+        const float* S = reinterpret_cast<const float*>(sm + TC_OFF_S + sb * TC_S_BYTES);
+        const uint32_t ab = TC_OFF_A + ((gB & 1) * 2 + acc) * TC_A_BYTES;
+        const int nsrc = (int)(n - t * TC_J < TC_J ? n - t * TC_J : TC_J);
+#pragma unroll 2
+        for (int j = 0; j < TC_J; j += 2) {
+          float2 k0 = make_float2(0.f, 0.f), k1 = make_float2(0.f, 0.f);
+          if (j < nsrc) k0 = tc_kernel(xt, S + j * TC_S_FLOATS, a, tab);
+          if (j + 1 < nsrc) k1 = tc_kernel(xt, S + (j + 1) * TC_S_FLOATS, a, tab);
+          uint4 v = make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
+          *reinterpret_cast<uint4*>(sm + ab + tc_kmajor_off(row, 2 * j)) = v;
+        }
+      }
+      ++gS;
+      fence_proxy_async_smem();
+      __syncthreads();
+      // 3. MMAs of stage t (one thread), then the next copies
+      if (tid == 0) {
+        const uint32_t bb = gB & 1;
+        ok = mbar_wait_bounded(&fullB[bb], (gB >> 1) & 1);
+        if (ok) {
+          ++consumedB;
+          tc_fence_after();
+          const uint32_t bsm = sbase + TC_OFF_B + bb * TC_B_BYTES;
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const uint32_t asm_ = sbase + TC_OFF_A + (bb * 2 + q) * TC_A_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TC_K / 8; ++kk)
+              tc_mma(tmem + q * TC_N, tc_smem_desc(asm_ + kk * 256), tc_smem_desc(bsm + kk * 256),
+                     (t > 0 || kk > 0) ? 1u : 0u);
+          }
+          tc_commit(&mmaDone[bb]);
+          ++committed;
+        }
+        ++gB;
+        // MMAs of stage t-1 must be done before B(t+1) overwrites their buffer
+        if (ok && t >= 1) {
+          ok = mbar_wait_bounded(&mmaDone[gD & 1], (gD >> 1) & 1);
+          ++gD;
+        }
+        if (ok && t + 1 < T) {
+          const uint32_t b = gB & 1;
+          mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
+          bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp + (size_t)(t + 1) * (TC_B_BYTES / 4), TC_B_BYTES,
+                        &fullB[b]);
+          ++issuedB;
+        }
+        if (ok && t + 2 < T) {
+          const uint32_t b = (gS + 1) % 3;
+          mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
+          bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)(t + 2) * TC_J * TC_S_FLOATS, TC_S_BYTES,
+                        &fullS[b]);
+          ++issuedS;
+        }
+      } else {
+        ++gB;
+        if (t >= 1) ++gD;
+      }
+      if (!__syncthreads_and(ok)) goto fail;
+    }
+    // 4. the last MMA group, then read the accumulators
+    if (tid == 0) {
+      ok = mbar_wait_bounded(&mmaDone[gD & 1], (gD >> 1) & 1);
+    }
+    ++gD;
+    if (!__syncthreads_and(ok)) goto fail;
+    tc_fence_after();
+    {
+      const int q = warp & 3;  // lane quarter
+      const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16) + acc * TC_N;
+      const double sc = 1.0 / (4 * kPi);
+      const int c0 = cg * TC_R;
+      for (int m = 0; m < TC_R; m += 16) {
+        float re[16], im[16];
+        tc_ld16(lane_addr + m, re);
+        tc_ld16(lane_addr + TC_R + m, im);
+        tc_wait_ld();
+        if (active) {
+#pragma unroll
+          for (int c = 0; c < 16; ++c) {
+            const int col = c0 + m + c;
+            if (col >= a.nrhs) break;
+            const int64_t o = (int64_t)col * a.ldy + off + row_loc;
+            const double yr = sc * re[c], yi = sc * im[c];
+            double orr = a.ar * yr - a.ai * yi, oi = a.ar * yi + a.ai * yr;
+            double2* Y = reinterpret_cast<double2*>(a.y);
+            if (!a.beta_zero) {
+              const double2 yo = Y[o];
+              orr += a.br * yo.x - a.bi * yo.y;
+              oi += a.br * yo.y + a.bi * yo.x;
+            }
+            Y[o] = make_double2(orr, oi);
+          }
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();  // accumulators read before the next item overwrites them
+  }
+  goto done;
+fail:
+  if (tid == 0) {
+    atomicExch(a.err, kErrWaitTimeout);
+    // drain: every issued copy and MMA group must land before the CTA leaves
+    while (gS < issuedS) {
+      mbar_wait_bounded(&fullS[gS % 3], (gS / 3) & 1);
+      ++gS;
+    }
+    while (consumedB < issuedB) {
+      mbar_wait_bounded(&fullB[consumedB & 1], (consumedB >> 1) & 1);
+      ++consumedB;
+    }
+    while (gD < committed) {
+      mbar_wait_bounded(&mmaDone[gD & 1], (gD >> 1) & 1);
+      ++gD;
+    }
+  }
+  __syncthreads();
+done:
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+  }
+}
+
+// Source records: x y z nx ny nz (FP32) per source, tiles of TC_J per
+// surface, zero-padded.
+__global__ void tc_pack_sources(int nsurf, const int64_t* off, const int64_t* toff, const double* coords,
+                                const double* normals, float* out) {
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // padded source slot
+  // find the surface of slot g (tiles are few; linear scan over surfaces)
+  int s = 0;
+  while (s + 1 < nsurf && toff[s + 1] * TC_J <= g) ++s;
+  if (g >= toff[nsurf] * TC_J) return;
+  const int64_t j = g - toff[s] * TC_J;
+  const int64_t n = off[s + 1] - off[s];
+  float* o = out + g * TC_S_FLOATS;
+  if (j < n) {
+    const int64_t i = off[s] + j;
+    for (int c = 0; c < 3; ++c) {
+      o[c] = (float)coords[3 * i + c];
+      o[3 + c] = normals ? (float)normals[3 * i + c] : 0.f;
+    }
+  } else {
+    for (int c = 0; c < 6; ++c) o[c] = 0.f;
+  }
+  o[6] = 0.f;
+  o[7] = 0.f;
+}
+
+// Density blocks: for column group cg and tile (surface s, local tile lt),
+// B[n][k] in the canonical K-major layout (see the header), TF32.
+__global__ void tc_pack_density(int nsurf, const int64_t* off, const int64_t* toff, int64_t ntiles,
+                                const double* weights, const double* x, int64_t ldx, int nrhs, int cg,
+                                uint32_t* out) {
+  const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t tile = gid / (TC_N * TC_K / 4);  // one thread per 16-byte chunk
+  if (tile >= ntiles) return;
+  const int rem = (int)(gid % (TC_N * TC_K / 4));
+  const int nn = rem / (TC_K / 4), kc = rem % (TC_K / 4);  // column n, K chunk
+  int s = 0;
+  while (s + 1 < nsurf && toff[s + 1] <= tile) ++s;
+  const int64_t n = off[s + 1] - off[s];
+  const int64_t lt = tile - toff[s];
+  const int r = nn & (TC_R - 1);
+  const bool imag_half = nn >= TC_R;
+  const int col = cg * TC_R + r;
+  uint32_t v[4];
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    const int k = 4 * kc + e;
+    const int64_t j = lt * TC_J + (k >> 1);
+    float val = 0.f;
+    if (j < n && col < nrhs) {
+      const int64_t node = off[s] + j;
+      const double2 xv = reinterpret_cast<const double2*>(x)[(int64_t)col * ldx + node];
+      const double w = weights[node];
+      const double xr = w * xv.x, xi = w * xv.y;
+      // rows 2j: (Re x, Im x) for the (Re, Im) halves; rows 2j+1: (-Im x, Re x)
+      if ((k & 1) == 0)
+        val = (float)(imag_half ? xi : xr);
+      else
+        val = (float)(imag_half ? xr : -xi);
+    }
+    v[e] = to_tf32(val);
+  }
+  uint32_t* o = out + (((size_t)cg * ntiles + tile) * (TC_B_BYTES / 4)) + tc_kmajor_off(nn, 4 * kc) / 4;
+  *reinterpret_cast<uint4*>(o) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
+  inti_ctx* ctx = b->ctx;
+  const int nsurf = (int)b->off.size() - 1;
+  // tile offsets and 256-target items (largest surfaces first), built once
+  if (!b->tc_src.p) {
+    std::vector<int64_t> toff(nsurf + 1, 0);
+    for (int s = 0; s < nsurf; ++s) toff[s + 1] = toff[s] + (b->off[s + 1] - b->off[s] + TC_J - 1) / TC_J;
+    std::vector<int> order(nsurf);
+    for (int s = 0; s < nsurf; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
+      return b->off[p + 1] - b->off[p] > b->off[q + 1] - b->off[q];
+    });
+    std::vector<int32_t> isurf, iblk;
+    for (int s : order)
+      for (int64_t t = 0; t * TC_ROWS < b->off[s + 1] - b->off[s]; ++t) {
+        isurf.push_back(s);
+        iblk.push_back((int32_t)t);
+      }
+    b->tc_ntiles = toff[nsurf];
+    b->tc_nitems = (int)isurf.size();
+    b->tc_toff.ensure(sizeof(int64_t) * (nsurf + 1));
+    INTI_CUDA(cudaMemcpy(b->tc_toff.p, toff.data(), sizeof(int64_t) * (nsurf + 1), cudaMemcpyHostToDevice));
+    b->tc_items.ensure(sizeof(int32_t) * 2 * b->tc_nitems);
+    INTI_CUDA(cudaMemcpy(b->tc_items.p, isurf.data(), sizeof(int32_t) * b->tc_nitems, cudaMemcpyHostToDevice));
+    INTI_CUDA(cudaMemcpy(b->tc_items.as<int32_t>() + b->tc_nitems, iblk.data(), sizeof(int32_t) * b->tc_nitems,
+                         cudaMemcpyHostToDevice));
+    b->tc_src.ensure(sizeof(float) * TC_S_FLOATS * TC_J * b->tc_ntiles);
+    const int64_t slots = b->tc_ntiles * TC_J;
+    tc_pack_sources<<<(unsigned)((slots + 255) / 256), 256, 0, ctx->stream>>>(
+        nsurf, b->d_off.as<int64_t>(), b->tc_toff.as<int64_t>(), b->coords.as<double>(),
+        b->kind == SL ? nullptr : b->normals.as<double>(), b->tc_src.as<float>());
+    ctx->launches++;
+    b->tc_counter.ensure(sizeof(int));
+    b->expi32 = expi_table_f32(ctx);
+  }
+  const int ncg = (a.nrhs + TC_R - 1) / TC_R;
+  b->tc_b.ensure((size_t)ncg * b->tc_ntiles * TC_B_BYTES);
+  {
+    ProfScope pp(ctx, "batch_pack");
+    for (int cg = 0; cg < ncg; ++cg) {
+      const int64_t chunks = b->tc_ntiles * (TC_N * TC_K / 4);
+      tc_pack_density<<<(unsigned)((chunks + 255) / 256), 256, 0, ctx->stream>>>(
+          nsurf, b->d_off.as<int64_t>(), b->tc_toff.as<int64_t>(), b->tc_ntiles, b->weights.as<double>(), a.x,
+          a.ldx, a.nrhs, cg, b->tc_b.as<uint32_t>());
+      ctx->launches++;
+    }
+  }
+  TcArgs t;
+  t.off = b->d_off.as<int64_t>();
+  t.toff = b->tc_toff.as<int64_t>();
+  t.item_surf = b->tc_items.as<int32_t>();
+  t.item_block = b->tc_items.as<int32_t>() + b->tc_nitems;
+  t.nitems = b->tc_nitems;
+  t.ncolgroups = ncg;
+  t.src = b->tc_src.as<float>();
+  t.bpack = b->tc_b.as<uint32_t>();
+  t.ntiles = b->tc_ntiles;
+  t.coords = b->coords.as<double>();
+  t.y = a.y;
+  t.ldy = a.ldy;
+  t.nrhs = a.nrhs;
+  t.k = (float)b->k;
+  t.kT = (float)(b->k * kExpiTable / (2 * kPi));
+  t.delta = (float)(2 * kPi / kExpiTable);
+  t.c1r = (float)b->c1[0];
+  t.c1i = (float)b->c1[1];
+  t.c2r = (float)b->c2[0];
+  t.c2i = (float)b->c2[1];
+  t.kind = b->kind;
+  t.ar = a.ar;
+  t.ai = a.ai;
+  t.br = a.br;
+  t.bi = a.bi;
+  t.beta_zero = a.beta_zero;
+  t.expi = b->expi32;
+  t.counter = b->tc_counter.as<int>();
+  t.err = ctx->err_flag.as<int>();
+  INTI_CUDA(cudaMemsetAsync(b->tc_counter.p, 0, sizeof(int), ctx->stream));
+  INTI_CUDA(cudaFuncSetAttribute(mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+  ProfScope pk(ctx, "batch_tc");
+  mrhs_tc_kernel<<<ctx->num_sms, TC_THREADS, TC_SMEM, ctx->stream>>>(t);
+  ctx->launches++;
+  INTI_CUDA(cudaGetLastError());
+}
+
+}  // namespace inti

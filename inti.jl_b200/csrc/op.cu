@@ -69,7 +69,7 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
 }
 
 // c1*C_dl + c2*C_sl with the union of the two patterns (host merge, once).
-static std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
+std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
                                                    const inti_csr* b, const double* cb, int64_t m,
                                                    int64_t n, bool cplx) {
   const int comps = cplx ? 2 : 1;

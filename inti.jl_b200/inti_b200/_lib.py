@@ -19,7 +19,8 @@ LIB_PATH = Path(os.environ.get("INTI_B200_LIB", _HERE.parent / "_build" / "libin
 OK, E_ARG, E_SHAPE, E_CUDA, E_NONFINITE, E_TIMEOUT, E_NOMEM, E_UNSUPPORTED, E_NOCONV, E_STATE = range(10)
 LAPLACE, HELMHOLTZ = 0, 1
 SL, DL, ADL, HS = 0, 1, 2, 3
-FP64, FP32C = 0, 1
+FP64, FP32C, TF32 = 0, 1, 2
+CF = 4
 F64, C128 = 0, 1
 H2D, D2H, D2D = 0, 1, 2
 GMRES_FP64, GMRES_MIXED = 0, 1
@@ -119,6 +120,10 @@ SIGNATURES = {
     "inti_op_grad_sources": (C.c_int, [P, P, P, P, P, P, P, C.c_int]),
     "inti_measure_peaks": (C.c_int, [P, D, D, D]),
     "inti_selftest_math": (C.c_int, [P, D]),
+    "inti_batch_create": (C.c_int, [P, C.c_int32, PP, C.c_int, C.c_int, C.c_double, C.c_double, D, D, PP, PP, PP]),
+    "inti_batch_apply": (C.c_int, [P, C.c_int, P, I64, P, I64, C.c_int32, D, D, C.c_int]),
+    "inti_batch_size": (I64, [P]),
+    "inti_batch_destroy": (C.c_int, [P]),
     "inti_apply_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_double, C.c_int, I64, P, P, I64, P, P, P,
                                      P, P, P, P, P, D, D, P, C.c_int]),
 }

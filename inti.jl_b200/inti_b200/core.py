@@ -45,6 +45,7 @@ __all__ = [
     "HyperSingularKernel",
     "GpuOperator",
     "CombinedFieldOperator",
+    "BatchOperator",
     "LinearCombination",
     "IntegralOperator",
     "assemble_matrix",
@@ -537,6 +538,64 @@ class CombinedFieldOperator(GpuOperator):
         self.shape = D.shape
         self.is_complex = D.is_complex
         self.dtype = D.dtype
+
+
+class BatchOperator:
+    """Block-diagonal ``diag(A_1 + C_1, …, A_S + C_S)`` over many surfaces,
+    applied to many right-hand sides in one launch (``inti_batch``).
+
+    ``kind`` is ``"SL"``, ``"DL"`` or ``"CF"`` (``c_dl·DL + c_sl·SL``).
+    ``corrections`` is a list of ``(δS, δD)`` pairs (``bdim_correction``
+    output) or None.  Densities are ``(N_total, nrhs)`` arrays over the
+    concatenated nodes, surface order as given.
+    """
+
+    def __init__(self, op, quads, kind="SL", corrections=None, c_dl=1.0, c_sl=1.0, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.op = op
+        self.quads = list(quads)
+        kinds = {"SL": L.SL, "DL": L.DL, "CF": L.CF}
+        if kind not in kinds:
+            raise L.ArgumentError(L.E_ARG, f"unknown batch kernel {kind!r}")
+        qh = (C.c_void_p * len(self.quads))(*[_quad_handle(q, self.ctx).value for q in self.quads])
+        dS = dD = None
+        if corrections is not None:
+            dS = (C.c_void_p * len(self.quads))(*[(c[0].handle.value if c and c[0] else None) for c in corrections])
+            dD = (C.c_void_p * len(self.quads))(*[(c[1].handle.value if c and c[1] else None) for c in corrections])
+        k = complex(getattr(op, "k", 0.0))
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.inti_batch_create(self.ctx.handle, len(self.quads), qh, op.pde, kinds[kind],
+                                                      k.real, k.imag, L.cpair(c_dl), L.cpair(c_sl), dD, dS,
+                                                      C.byref(h)))
+        self.handle = h
+        self._keep = (corrections,)
+        self._fin = weakref.finalize(self, self.ctx.lib.inti_batch_destroy, h)
+        self.n = int(self.ctx.lib.inti_batch_size(h))
+        self.offsets = np.cumsum([0] + [len(q) for q in self.quads])
+        self.is_complex = op.pde == L.HELMHOLTZ
+        self.dtype = np.complex128 if self.is_complex else np.float64
+
+    def apply(self, X, precision: str = "fp64", Y=None, alpha=1.0, beta=0.0):
+        prec = {"fp64": L.FP64, "tf32": L.TF32}.get(precision)
+        if prec is None:
+            raise L.ArgumentError(L.E_ARG, f"unknown batch precision {precision!r}")
+        X = np.asarray(X)
+        single = X.ndim == 1
+        X = np.asfortranarray(_as_density(X.reshape(self.n, -1) if single else X, self.is_complex, self.n))
+        nrhs = X.shape[1]
+        if Y is None:
+            Yo = np.zeros((self.n, nrhs), self.dtype, order="F")
+            beta = 0.0
+        else:
+            Yo = np.asfortranarray(np.asarray(Y, dtype=self.dtype).reshape(self.n, -1)).copy(order="F")
+        self.ctx.check(self.ctx.lib.inti_batch_apply(self.handle, prec, L.dptr(X), self.n, L.dptr(Yo), self.n, nrhs,
+                                                     L.cpair(alpha), L.cpair(beta), 0))
+        return Yo[:, 0] if single else Yo
+
+    def apply_device(self, x_ptr: int, y_ptr: int, nrhs: int, precision: str = "fp64", alpha=1.0, beta=0.0):
+        prec = {"fp64": L.FP64, "tf32": L.TF32}[precision]
+        self.ctx.check(self.ctx.lib.inti_batch_apply(self.handle, prec, C.c_void_p(x_ptr), self.n, C.c_void_p(y_ptr),
+                                                     self.n, nrhs, L.cpair(alpha), L.cpair(beta), 1))
 
 
 class IntegralOperator(GpuOperator):

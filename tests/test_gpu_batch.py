@@ -1,0 +1,87 @@
+"""Batched multi-surface, multi-RHS operators (one launch over uneven star
+surfaces).  FP64 batch against the single-surface operators (themselves
+checked against the oracle); the TF32 tensor-core batch (tcgen05) against the
+FP64 batch at TF32 accuracy."""
+import numpy as np
+import pytest
+
+import inti_b200 as inti
+from helpers import relerr
+
+pytestmark = pytest.mark.gpu
+
+
+def stars(ns=(3, 2, 4), seed=0):
+    r = np.random.default_rng(seed)
+    return [inti.star_quadrature(inti.star_coefficients(r), n) for n in ns]
+
+
+def rhs(n, nrhs, cplx, seed=1):
+    r = np.random.default_rng(seed)
+    X = r.standard_normal((n, nrhs))
+    if cplx:
+        X = X + 1j * r.standard_normal((n, nrhs))
+    return X
+
+
+def per_surface(op, quads, kind, corrs, X, cD=1.0, cS=1.0, ctx=None):
+    out = []
+    off = 0
+    for q, (dS, dD) in zip(quads, corrs):
+        n = len(q)
+        Xs = X[off:off + n]
+        if kind == "SL":
+            A = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, ctx=ctx)
+        elif kind == "DL":
+            A = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, ctx=ctx)
+        else:
+            D = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, ctx=ctx)
+            S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, ctx=ctx)
+            A = inti.CombinedFieldOperator(D, S, cD, cS)
+        out.append(A @ Xs)
+        off += n
+    return np.concatenate(out, axis=0)
+
+
+@pytest.mark.parametrize("kind", ["SL", "DL", "CF"])
+@pytest.mark.parametrize("pde", ["helmholtz", "laplace"])
+def test_batch_fp64_matches_single_surface_operators(ctx, kind, pde):
+    quads = stars()
+    op = inti.Helmholtz(k=5.0, dim=3) if pde == "helmholtz" else inti.Laplace(dim=3)
+    corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
+    cD, cS = (1.0, -5.0j) if pde == "helmholtz" else (1.0, 0.5)
+    B = inti.BatchOperator(op, quads, kind, corrs, cD, cS, ctx=ctx)
+    X = rhs(B.n, 5, pde == "helmholtz")
+    ref = per_surface(op, quads, kind, corrs, X, cD, cS, ctx)
+    assert relerr(B.apply(X), ref) < 1e-12
+    # alpha / beta
+    Y0 = rhs(B.n, 5, pde == "helmholtz", 9)
+    got = B.apply(X, Y=Y0, alpha=0.5, beta=2.0)
+    assert relerr(got, 0.5 * ref + 2.0 * Y0) < 1e-12
+
+
+@pytest.mark.parametrize("kind", ["SL", "DL", "CF"])
+@pytest.mark.parametrize("nrhs", [5, 64, 70])
+def test_batch_tf32_tensor_cores_match_fp64(ctx, kind, nrhs):
+    quads = stars((4, 3, 6, 2), seed=3)
+    op = inti.Helmholtz(k=5.0, dim=3)
+    corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
+    B = inti.BatchOperator(op, quads, kind, corrs, 1.0, -5.0j, ctx=ctx)
+    X = rhs(B.n, nrhs, True, 4)
+    y64 = B.apply(X, "fp64")
+    y32 = B.apply(X, "tf32")
+    # TF32 inputs (11-bit significands), FP32 accumulation
+    for c in range(nrhs):
+        assert relerr(y32[:, c], y64[:, c]) < 5e-3, c
+
+
+def test_batch_tf32_second_call_and_beta(ctx):
+    quads = stars((3, 5), seed=5)
+    op = inti.Helmholtz(k=5.0, dim=3)
+    B = inti.BatchOperator(op, quads, "SL", None, ctx=ctx)
+    X1, X2 = rhs(B.n, 8, True, 1), rhs(B.n, 8, True, 2)
+    Y0 = rhs(B.n, 8, True, 3)
+    a = B.apply(X1, "tf32")
+    b = B.apply(X2, "tf32", Y=Y0, alpha=1.5, beta=-1.0)
+    assert relerr(a, B.apply(X1)) < 5e-3
+    assert relerr(b, 1.5 * B.apply(X2) - Y0) < 5e-3
