@@ -233,6 +233,106 @@ def gmres_c3(ctx) -> dict:
     return out
 
 
+def build_c4(ctx, nsurf: int = 32, nrhs: int = 64, seed: int = 4):
+    """32 seeded star surfaces r = 1 + 0.2*sum a_lm Y_lm (l <= 3), n x n cells
+    per cube-sphere patch with n in [6, 27] (N_s = 54 n^2: 1,944 .. 39,366
+    nodes), GL3x3; Helmholtz k = 5 combined field D - i k S with per-surface
+    DIM corrections; 64 plane waves exp(i k d.x), d uniform on the sphere."""
+    import inti_b200 as inti
+
+    r = np.random.default_rng(seed)
+    ns = r.integers(6, 28, nsurf)
+    quads = [inti.star_quadrature(inti.star_coefficients(r), int(n)) for n in ns]
+    k = 5.0
+    op = inti.Helmholtz(k=k, dim=3)
+    t0 = time.perf_counter()
+    corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
+    t_dim = time.perf_counter() - t0
+    B = inti.BatchOperator(op, quads, "CF", corrs, 1.0, -1j * k, ctx=ctx)
+    d = r.standard_normal((nrhs, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    X = np.concatenate([np.exp(1j * k * (q.coords @ d.T)) for q in quads], axis=0)
+    pairs = float(sum(len(q) ** 2 for q in quads))
+    cfg = {"workload": "helmholtz3d_cfie_k5_32stars_64rhs_dim", "surfaces": nsurf, "n_total": B.n,
+           "n_min": int(min(len(q) for q in quads)), "n_max": int(max(len(q) for q in quads)), "nrhs": nrhs,
+           "sum_n2": pairs, "dim_setup_s": t_dim}
+    return B, X, pairs, cfg, quads
+
+
+def bench_batch(args, ctx, peaks, torch) -> dict:
+    """Batched multi-RHS apply (config 4): value = kernel pairs x right-hand
+    sides per second through the TF32 tensor-core path."""
+    B, X, pairs, cfg, quads = build_c4(ctx)
+    nrhs = X.shape[1]
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    xs = torch.from_numpy(np.asfortranarray(X).T.copy().view(np.float64)).to(dev)  # column-major: col c at c*n
+    ys = torch.zeros_like(xs)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    out = {}
+    for prec in ("tf32", "fp64"):
+        steps = args.steps if prec == "tf32" else max(3, args.steps // 10)
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                B.apply_device(xs.data_ptr(), ys.data_ptr(), nrhs, prec)
+            stream.synchronize()
+            clocks = Clocks(0) if prec == "tf32" else None
+            launches0 = ctx.launch_count
+            ctx.set_profiling(True)
+            evs = []
+            for _ in range(steps):
+                flush.zero_()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                B.apply_device(xs.data_ptr(), ys.data_ptr(), nrhs, prec)
+                e1.record(stream)
+                evs.append((e0, e1))
+            stream.synchronize()
+            ms = sum(a.elapsed_time(b) for a, b in evs) / steps
+            kern = ctx.profile("batch_tc" if prec == "tf32" else "batch")
+            pack = ctx.profile("batch_pack")
+            ctx.set_profiling(False)
+            out[prec] = {"ms": ms, "value": pairs * nrhs / (ms * 1e-3) / 1e9, "kernel_ms": kern[0] / max(kern[1], 1),
+                         "pack_ms": pack[0] / max(pack[1], 1) if pack[1] else 0.0,
+                         "launches": ctx.launch_count - launches0}
+            if clocks:
+                out[prec]["clocks"] = clocks.stop()
+    # e2e: host (pinned) densities through BatchOperator.apply
+    hx = torch.from_numpy(np.asfortranarray(X)).pin_memory().numpy()
+    for _ in range(2):
+        B.apply(hx, "tf32")
+    t0 = time.perf_counter()
+    e2steps = max(3, args.steps // 3)
+    for _ in range(e2steps):
+        B.apply(hx, "tf32")
+    e2e_s = (time.perf_counter() - t0) / e2steps
+    tf = out["tf32"]
+    # tensor work actually issued: per surface M x K x N = (targets padded to 256) x
+    # (2 x sources padded to 32) x 128, two flops per multiply-add
+    flops = sum(2.0 * (-(-len(q) // 256) * 256) * (2 * (-(-len(q) // 32) * 32)) * 128 for q in quads)
+    tc_peak = 1656.8 / 2  # dense TF32 = half the measured dense BF16 rate (MEASURED_PEAKS.json)
+    achieved = flops / (tf["kernel_ms"] * 1e-3) / 1e12
+    line = {
+        "metric": METRIC, "value": tf["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tf["ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "tf32", "data": "synthetic",
+        "config": dict(cfg, precision="tf32 tensor cores, fp32 accumulate, fp64 correction", l2="flushed between steps",
+                       unit_note="pairs x right-hand sides"),
+        "e2e": {"value": pairs * nrhs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 16 * B.n * nrhs,
+                "d2h_bytes_per_step": 16 * B.n * nrhs, "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": tf["launches"],
+        "roofline": {"bound": "tensor", "achieved": achieved, "peak": tc_peak, "unit": "TFLOP/s",
+                     "frac": achieved / tc_peak, "traffic": None, "kernel": "mrhs_tc_kernel (tcgen05.mma kind::tf32)",
+                     "kernel_ms": tf["kernel_ms"],
+                     "peak_source": "half the measured dense BF16 cuBLAS rate in MEASURED_PEAKS.json, of measured"},
+        "clocks": tf.get("clocks"),
+        "fp64_batch": {"value": out["fp64"]["value"], "ms": out["fp64"]["ms"]},
+        "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
+    }
+    return line
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -243,7 +343,7 @@ def main() -> None:
     ap.add_argument("--no-gmres", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1"])
+                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -267,6 +367,14 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ctx = inti.Context(local)
     peaks = ctx.measure_peaks()
+    if args.workload == "c4":
+        line = bench_batch(args, ctx, peaks, torch)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     q, S, sigma, fkey, dtype, cfg = build_workload(args.workload, ctx)
     n = len(q)
     pairs = float(n) * n

@@ -38,7 +38,7 @@
 
 namespace inti {
 
-constexpr int TC_THREADS = 256;
+constexpr int TC_THREADS = 512;           // two threads per target row
 constexpr int TC_ROWS = 256;             // targets per item (2 accumulators x 128)
 constexpr int TC_R = 64;                 // complex right-hand sides per pass
 constexpr int TC_N = 2 * TC_R;           // real accumulator columns
@@ -132,49 +132,49 @@ struct TcArgs {
   int* err;
 };
 
-// K(x, y) for the Helmholtz kernels (without 1/(4 pi)), FP32.
-__device__ __forceinline__ float2 tc_kernel(const float* x, const float* s, const TcArgs& a,
+// Per-launch constants of the kernel values.
+struct TcConst {
+  float k, kT, delta, c1r, c1i, c2r, c2i;
+};
+
+// K(x, y) for the Helmholtz kernels (without 1/(4 pi)), FP32:
+//   SL: e^{ikd}/d
+//   DL: e^{ikd}/d * (1/d - ik) g,  g = (r.n)/d
+//   CF: e^{ikd}/d * (c2 + c1 (1/d - ik) g)
+template <int KIND>
+__device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, const float2 s1, const TcConst& c,
                                             const float2* __restrict__ tab) {
-  const float r0 = x[0] - s[0], r1 = x[1] - s[1], r2 = x[2] - s[2];
+  const float r0 = x[0] - s0.x, r1 = x[1] - s0.y, r2 = x[2] - s0.z;
   const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
   const bool keep = d2 > 1.0e-28f;
   const float ri = keep ? rsqrt_approx_f32(d2) : 0.0f;
   const float d = d2 * ri;
   float cs, sn;
-  expi_table_eval<float, float2>(d * a.kT, tab, a.delta, cs, sn);
-  float vr = 0.f, vi = 0.f;
-  if (a.kind != DL) {  // SL part e^{ikd}/d
-    const float sr = ri * cs, si = ri * sn;
-    if (a.kind == SL) {
-      vr = sr;
-      vi = si;
-    } else {
-      vr = a.c2r * sr - a.c2i * si;
-      vi = a.c2r * si + a.c2i * sr;
-    }
+  expi_table_eval<float, float2>(d * c.kT, tab, c.delta, cs, sn);
+  const float hr = cs * ri, hi = sn * ri;  // e^{ikd}/d
+  if (KIND == SL) return make_float2(hr, hi);
+  const float rn = fmaf(r2, s1.y, fmaf(r1, s1.x, r0 * s0.w));
+  const float g = rn * ri;
+  float br, bi;
+  if (KIND == DL) {  // (1/d - ik) g
+    br = g * ri;
+    bi = -c.k * g;
+  } else {  // c2 + c1 (g/d - i k g)
+    const float gr = g * ri, gk = c.k * g;
+    br = fmaf(c.c1r, gr, fmaf(c.c1i, gk, c.c2r));
+    bi = fmaf(c.c1i, gr, fmaf(-c.c1r, gk, c.c2i));
   }
-  if (a.kind != SL) {  // DL part e^{ikd}(1/d - ik)(r.n)/d^2
-    const float er = fmaf(cs, ri, a.k * sn), ei = fmaf(sn, ri, -a.k * cs);
-    const float rn = fmaf(r2, s[5], fmaf(r1, s[4], r0 * s[3]));
-    const float f = rn * ri * ri;
-    const float dr = er * f, di = ei * f;
-    if (a.kind == DL) {
-      vr = dr;
-      vi = di;
-    } else {
-      vr += a.c1r * dr - a.c1i * di;
-      vi += a.c1r * di + a.c1i * dr;
-    }
-  }
-  return make_float2(vr, vi);
+  return make_float2(fmaf(hr, br, -hi * bi), fmaf(hr, bi, hi * br));
 }
 
+template <int KIND>
 __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
   __shared__ __align__(8) uint64_t fullS[3], fullB[2], mmaDone[2];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int item_sh;
   const int tid = threadIdx.x, warp = tid >> 5;
+  const TcConst kc{a.k, a.kT, a.delta, a.c1r, a.c1i, a.c2r, a.c2i};
   float2* tab = reinterpret_cast<float2*>(sm + TC_OFF_T);
   for (int q = tid; q < kExpiTable; q += TC_THREADS) tab[q] = a.expi[q];
   if (tid == 0) {
@@ -216,12 +216,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
     const int64_t T = (n + TC_J - 1) / TC_J;
     const float* srcs = a.src + (size_t)a.toff[s] * TC_J * TC_S_FLOATS;
     const uint32_t* bp = a.bpack + ((size_t)cg * a.ntiles + a.toff[s]) * (TC_B_BYTES / 4);
-    const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + tid;
+    const int trow = tid & (TC_ROWS - 1);  // target row of this thread (two threads per row)
+    const int half = tid >> 8;             // which 16 sources of a stage
+    const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + trow;
     const bool active = row_loc < n;
     const int64_t ti = off + min(row_loc, n - 1);
     const float xt[3] = {(float)a.coords[3 * ti], (float)a.coords[3 * ti + 1], (float)a.coords[3 * ti + 2]};
-    const int acc = tid >> 7;          // accumulator of this row
-    const int row = tid & 127;         // row inside the accumulator
+    const int acc = trow >> 7;             // accumulator of this row
+    const int row = trow & 127;            // row inside the accumulator
     // prologue: source records of stages 0 and 1, density of stage 0
     if (tid == 0) {
       for (int64_t t = 0; t < 2 && t < T; ++t) {
@@ -245,11 +247,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
         const float* S = reinterpret_cast<const float*>(sm + TC_OFF_S + sb * TC_S_BYTES);
         const uint32_t ab = TC_OFF_A + ((gB & 1) * 2 + acc) * TC_A_BYTES;
         const int nsrc = (int)(n - t * TC_J < TC_J ? n - t * TC_J : TC_J);
-#pragma unroll 2
-        for (int j = 0; j < TC_J; j += 2) {
-          float2 k0 = make_float2(0.f, 0.f), k1 = make_float2(0.f, 0.f);
-          if (j < nsrc) k0 = tc_kernel(xt, S + j * TC_S_FLOATS, a, tab);
-          if (j + 1 < nsrc) k1 = tc_kernel(xt, S + (j + 1) * TC_S_FLOATS, a, tab);
+        const int j0 = half * (TC_J / 2);
+#pragma unroll 4
+        for (int j = j0; j < j0 + TC_J / 2; j += 2) {
+          const float4 a0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
+          const float2 b0 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
+          const float4 a1 = *reinterpret_cast<const float4*>(S + (j + 1) * TC_S_FLOATS);
+          const float2 b1 = *reinterpret_cast<const float2*>(S + (j + 1) * TC_S_FLOATS + 4);
+          float2 k0 = tc_kernel<KIND>(xt, a0, b0, kc, tab);
+          float2 k1 = tc_kernel<KIND>(xt, a1, b1, kc, tab);
+          if (j >= nsrc) k0 = make_float2(0.f, 0.f);
+          if (j + 1 >= nsrc) k1 = make_float2(0.f, 0.f);
           uint4 v = make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
           *reinterpret_cast<uint4*>(sm + ab + tc_kmajor_off(row, 2 * j)) = v;
         }
@@ -310,11 +318,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
     if (!__syncthreads_and(ok)) goto fail;
     tc_fence_after();
     {
-      const int q = warp & 3;  // lane quarter
+      // warp w: accumulator (w>>2)&1, lane quarter w&3 (its TMEM lanes),
+      // column half w>>3
+      const int q = warp & 3;
       const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16) + acc * TC_N;
       const double sc = 1.0 / (4 * kPi);
       const int c0 = cg * TC_R;
-      for (int m = 0; m < TC_R; m += 16) {
+      for (int m = half * (TC_R / 2); m < (half + 1) * (TC_R / 2); m += 16) {
         float re[16], im[16];
         tc_ld16(lane_addr + m, re);
         tc_ld16(lane_addr + TC_R + m, im);
@@ -512,9 +522,17 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
   t.counter = b->tc_counter.as<int>();
   t.err = ctx->err_flag.as<int>();
   INTI_CUDA(cudaMemsetAsync(b->tc_counter.p, 0, sizeof(int), ctx->stream));
-  INTI_CUDA(cudaFuncSetAttribute(mrhs_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-  ProfScope pk(ctx, "batch_tc");
-  mrhs_tc_kernel<<<ctx->num_sms, TC_THREADS, TC_SMEM, ctx->stream>>>(t);
+  auto launch = [&](auto kern) {
+    INTI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+    ProfScope pk(ctx, "batch_tc");
+    kern<<<ctx->num_sms, TC_THREADS, TC_SMEM, ctx->stream>>>(t);
+  };
+  if (b->kind == SL)
+    launch(mrhs_tc_kernel<SL>);
+  else if (b->kind == DL)
+    launch(mrhs_tc_kernel<DL>);
+  else
+    launch(mrhs_tc_kernel<CF>);
   ctx->launches++;
   INTI_CUDA(cudaGetLastError());
 }
