@@ -239,6 +239,16 @@ int inti_batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quad
  * tcgen05 tensor cores, FP32 accumulation, FP64 correction). */
 int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
                      int32_t nrhs, const double* alpha, const double* beta, int on_device);
+/* GMRES on every (surface, column) system shift*I + A_s + C_s at once, in
+ * lockstep: one batched operator launch per Krylov step (Helmholtz).
+ * mode INTI_GMRES_FP64, or INTI_GMRES_MIXED: inner solves on the TF32
+ * tensor-core operator, FP64 residuals.  B/X: ld x nrhs complex, X is the
+ * initial guess on input.  relres (nullable, S*nrhs doubles, index
+ * s*nrhs + r) receives each system's final FP64 relative residual; stats
+ * report the worst. */
+int inti_batch_gmres(inti_batch* b, const double* shift, const double* B, double* X, int64_t ld,
+                     int32_t nrhs, double rtol, int32_t restart, int32_t maxiter, int32_t mode,
+                     int on_device, double* relres, inti_gmres_stats* stats);
 int64_t inti_batch_size(const inti_batch* b);
 int inti_batch_destroy(inti_batch* b);
 

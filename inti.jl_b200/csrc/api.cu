@@ -670,6 +670,16 @@ int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx,
   });
 }
 
+int inti_batch_gmres(inti_batch* b, const double* shift, const double* B, double* X, int64_t ld, int32_t nrhs,
+                     double rtol, int32_t restart, int32_t maxiter, int32_t mode, int on_device, double* relres,
+                     inti_gmres_stats* stats) {
+  if (!b) return INTI_E_ARG;
+  inti_ctx* ctx = b->ctx;
+  return guarded(ctx, [&] {
+    batch_gmres(b, shift, B, X, ld, nrhs, rtol, restart, maxiter, mode, on_device, relres, stats);
+  });
+}
+
 int64_t inti_batch_size(const inti_batch* b) { return b ? b->off.back() : -1; }
 
 int inti_batch_destroy(inti_batch* b) {

@@ -51,6 +51,9 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a);
 inti_batch* batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quads, int pde, int kind,
                          double k_re, double k_im, const double* c_dl, const double* c_sl,
                          const inti_csr* const* corr_dl, const inti_csr* const* corr_sl);
+void batch_gmres(inti_batch* b, const double* shift, const double* B, double* X, int64_t ldb, int32_t nrhs,
+                 double rtol, int32_t restart, int32_t maxiter, int32_t mode, int on_device, double* relres_out,
+                 inti_gmres_stats* stats);
 void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
                         int32_t nrhs, const double* alpha, const double* beta);
 

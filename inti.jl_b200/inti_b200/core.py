@@ -581,16 +581,43 @@ class BatchOperator:
             raise L.ArgumentError(L.E_ARG, f"unknown batch precision {precision!r}")
         X = np.asarray(X)
         single = X.ndim == 1
-        X = np.asfortranarray(_as_density(X.reshape(self.n, -1) if single else X, self.is_complex, self.n))
+        X = X.reshape(self.n, -1) if single else X
+        if X.shape[0] != self.n:
+            raise L.DimensionMismatch(L.E_SHAPE, f"X has {X.shape[0]} rows, expected {self.n}")
+        if not self.is_complex and np.iscomplexobj(X):
+            raise L.ArgumentError(L.E_ARG, "complex density for a real operator")
+        X = np.asfortranarray(X, dtype=self.dtype)  # no copy when already column-major of this dtype
         nrhs = X.shape[1]
         if Y is None:
             Yo = np.zeros((self.n, nrhs), self.dtype, order="F")
             beta = 0.0
         else:
-            Yo = np.asfortranarray(np.asarray(Y, dtype=self.dtype).reshape(self.n, -1)).copy(order="F")
+            Yin = np.asarray(Y)
+            Yo = Yin if (Yin.dtype == self.dtype and Yin.flags.f_contiguous and Yin.shape == (self.n, nrhs)) else \
+                np.asfortranarray(Yin.reshape(self.n, -1), dtype=self.dtype).copy(order="F")
         self.ctx.check(self.ctx.lib.inti_batch_apply(self.handle, prec, L.dptr(X), self.n, L.dptr(Yo), self.n, nrhs,
                                                      L.cpair(alpha), L.cpair(beta), 0))
         return Yo[:, 0] if single else Yo
+
+    def gmres(self, B, *, shift=0.0, X0=None, rtol: float = 1e-10, restart: int = 30, maxiter: int = 300,
+              mode: str = "fp64"):
+        """Solve ``(shift·I + A_s + C_s) x = b`` for every surface and column
+        in lockstep; returns ``(X, stats)`` with ``stats["relres"]`` the
+        per-system FP64 relative residuals ``(S, nrhs)``."""
+        B = np.asarray(B)
+        single = B.ndim == 1
+        Bm = np.asfortranarray(_as_density(B.reshape(self.n, -1) if single else B, True, self.n))
+        nrhs = Bm.shape[1]
+        X = np.zeros_like(Bm, order="F") if X0 is None else np.asfortranarray(
+            _as_density(np.asarray(X0).reshape(self.n, -1), True, self.n)).copy(order="F")
+        rel = np.zeros(len(self.quads) * nrhs)
+        st = L.GmresStats()
+        m = {"fp64": L.GMRES_FP64, "mixed": L.GMRES_MIXED}[mode]
+        self.ctx.check(self.ctx.lib.inti_batch_gmres(self.handle, L.cpair(shift), L.dptr(Bm), L.dptr(X), self.n, nrhs,
+                                                     rtol, restart, maxiter, m, 0, L.dptr(rel), C.byref(st)))
+        stats = st.as_dict()
+        stats["relres_all"] = rel.reshape(len(self.quads), nrhs)
+        return (X[:, 0] if single else X), stats
 
     def apply_device(self, x_ptr: int, y_ptr: int, nrhs: int, precision: str = "fp64", alpha=1.0, beta=0.0):
         prec = {"fp64": L.FP64, "tf32": L.TF32}[precision]

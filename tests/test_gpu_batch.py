@@ -85,3 +85,34 @@ def test_batch_tf32_second_call_and_beta(ctx):
     b = B.apply(X2, "tf32", Y=Y0, alpha=1.5, beta=-1.0)
     assert relerr(a, B.apply(X1)) < 5e-3
     assert relerr(b, 1.5 * B.apply(X2) - Y0) < 5e-3
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_batch_gmres_cfie(ctx, mode):
+    """I/2 + D - i k S on each surface, every column, one lockstep solve;
+    each system's FP64 residual <= 1e-10, and the solutions agree with
+    one-surface solves."""
+    quads = stars((3, 2, 4), seed=7)
+    k = 3.0
+    op = inti.Helmholtz(k=k, dim=3)
+    corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
+    B = inti.BatchOperator(op, quads, "CF", corrs, 1.0, -1j * k, ctx=ctx)
+    R = 4
+    rhs_ = rhs(B.n, R, True, 11)
+    X, st = B.gmres(rhs_, shift=0.5, rtol=1e-10, restart=30, maxiter=300, mode=mode)
+    assert st["converged"] == 1, st
+    assert np.max(st["relres_all"]) <= 1e-10
+    # independent FP64 check of the residual with the FP64 batch operator
+    res = rhs_ - (0.5 * X + B.apply(X, "fp64"))
+    off = B.offsets
+    for s in range(len(quads)):
+        for c in range(R):
+            seg = slice(off[s], off[s + 1])
+            assert np.linalg.norm(res[seg, c]) <= 2e-10 * np.linalg.norm(rhs_[seg, c])
+    # against the single-surface solver
+    q = quads[1]
+    dS, dD = corrs[1]
+    S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, ctx=ctx)
+    D = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, ctx=ctx)
+    x1, _ = inti.gmres(0.5 * inti.I + D - 1j * k * S, rhs_[off[1]:off[2], 2], rtol=1e-12)
+    assert relerr(X[off[1]:off[2], 2], x1) < 1e-8
