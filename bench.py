@@ -299,13 +299,15 @@ def bench_batch(args, ctx, peaks, torch) -> dict:
             if clocks:
                 out[prec]["clocks"] = clocks.stop()
     # e2e: host (pinned) densities through BatchOperator.apply
-    hx = torch.from_numpy(np.asfortranarray(X)).pin_memory().numpy()
+    # pinned host buffers in column-major order (torch stores row-major: use the transpose view)
+    hx = torch.from_numpy(np.ascontiguousarray(X.T)).pin_memory().numpy().T
+    hy = torch.zeros((nrhs, B.n), dtype=torch.complex128).pin_memory().numpy().T
     for _ in range(2):
-        B.apply(hx, "tf32")
+        B.apply(hx, "tf32", Y=hy)
     t0 = time.perf_counter()
     e2steps = max(3, args.steps // 3)
     for _ in range(e2steps):
-        B.apply(hx, "tf32")
+        B.apply(hx, "tf32", Y=hy)
     e2e_s = (time.perf_counter() - t0) / e2steps
     tf = out["tf32"]
     # tensor work actually issued: per surface M x K x N = (targets padded to 256) x
@@ -330,6 +332,17 @@ def bench_batch(args, ctx, peaks, torch) -> dict:
         "fp64_batch": {"value": out["fp64"]["value"], "ms": out["fp64"]["ms"]},
         "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
     }
+    if not args.no_gmres:
+        # scattering solves (I/2 + D - i k S) sigma = -u_inc for all 32 x 64 systems
+        g = {"rtol": 1e-10, "restart": 30, "systems": len(quads) * nrhs}
+        for mode in ("mixed", "fp64"):
+            _, st = B.gmres(-X, shift=0.5, rtol=1e-10, restart=30, maxiter=300, mode=mode)
+            g[mode] = {"seconds": st["seconds"], "iterations": st["iterations"], "outer": st["outer"],
+                       "fp64_applies": st["fp64_applies"], "tf32_applies": st["fp32_applies"],
+                       "worst_relres_fp64": st["relres"], "converged": bool(st["converged"])}
+        if g["fp64"]["converged"] and g["mixed"]["converged"]:
+            g["mixed_speedup_vs_fp64"] = g["fp64"]["seconds"] / g["mixed"]["seconds"]
+        line["gmres"] = g
     return line
 
 
