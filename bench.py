@@ -46,6 +46,8 @@ FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "lap
 # DRAM bytes (read + write) of one pair-kernel launch on this workload, from
 # the ncu capture summarised in profiles/pair_forward_helmholtz_sl_fp64_p2sphere62k.md
 PAIR_TRAFFIC_BYTES = 4.516e6
+# Algorithmic flops per pair of the source-gradient (adjoint) pass
+ADJ_FLOPS_PER_PAIR = {"laplace_dl": 40, "laplace_sl": 19}
 
 
 def host_cores() -> int:
@@ -346,6 +348,196 @@ def bench_batch(args, ctx, peaks, torch) -> dict:
     return line
 
 
+def build_c5(ctx, ntargets: int = 4096, seed: int = 5):
+    """Ellipsoid (1, 0.7, 0.5), n = 31 cells per patch, GL 3x3: N = 51,894
+    nodes.  The density comes from a GPU solve of the Laplace combined field
+    (½I + D + S) sigma = g, g from 8 seeded interior point sources; 4096
+    seeded targets lie on the 1.5x scaled ellipsoid; u* = D[sigma + noise]."""
+    import inti_b200 as inti
+
+    q = inti.ellipsoid_quadrature(31, 5)
+    op = inti.Laplace(dim=3)
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    r = np.random.default_rng(seed)
+    src = r.uniform(-1, 1, (64, 3))
+    src = src[np.sum((src / np.array([0.5, 0.35, 0.25])) ** 2, 1) < 1][:8]
+    c = r.standard_normal(len(src))
+    b = (c[None, :] / (4 * np.pi * np.linalg.norm(q.coords[:, None, :] - src[None], axis=2))).sum(1)
+    sigma, st = inti.gmres(0.5 * inti.I + D + S, b, rtol=1e-10, restart=100, maxiter=500, mode="mixed")
+    dirs = r.standard_normal((ntargets, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    tgt = inti.points(1.5 * dirs * np.array([1.0, 0.7, 0.5]))
+    P = inti.GpuOperator(inti.DoubleLayerKernel(op), tgt, q, ctx=ctx)
+    ustar = P @ (sigma + 0.05 * np.abs(sigma).mean() * r.standard_normal(len(q)))
+    cfg = {"workload": "laplace3d_dl_potential_value_and_gradient_ellipsoid_N51894_4096targets", "n": len(q),
+           "targets": ntargets, "density_solve": {"converged": bool(st["converged"]), "relres": st["relres"]},
+           "gradients": "dJ/dsigma, dJ/dcoords, dJ/dnormals, dJ/dweights for J = 0.5 |D[sigma] - u*|^2"}
+    return q, tgt, P, sigma, ustar, cfg
+
+
+def bench_adjoint(args, ctx, peaks, torch) -> dict:
+    """Value and full source gradient of J = ½‖D[σ] − u*‖² (config 5): one
+    step = the forward DL potential (u − u* in its epilogue) plus the adjoint
+    pass; value = (forward + adjoint) kernel pairs per second."""
+    q, tgt, P, sigma, ustar, cfg = build_c5(ctx)
+    n, m = len(q), len(tgt)
+    pairs = 2.0 * m * n
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    f64 = dict(dtype=torch.float64, device=dev)
+    sig = torch.from_numpy(sigma).to(dev)
+    ust = torch.from_numpy(ustar).to(dev)
+    u = torch.zeros(m, **f64)
+    ds, dw = torch.zeros(n, **f64), torch.zeros(n, **f64)
+    dc, dn = torch.zeros(3 * n, **f64), torch.zeros(3 * n, **f64)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+
+    def step():
+        u.copy_(ust)
+        P.apply_device(sig.data_ptr(), u.data_ptr(), 1, 1.0, -1.0)  # u = D sigma - u*
+        P.grad_sources_device(u.data_ptr(), sig.data_ptr(), ds.data_ptr(), dc.data_ptr(), dn.data_ptr(),
+                              dw.data_ptr())
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+        stream.synchronize()
+        clocks = Clocks(0)
+        launches0 = ctx.launch_count
+        ctx.set_profiling(True)
+        evs = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            evs.append((e0, e1))
+        stream.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        adj_ms, adj_n = ctx.profile("adjoint")
+        fwd_ms, fwd_n = ctx.profile("pair")
+        ctx.set_profiling(False)
+        launches = ctx.launch_count - launches0
+        clk = clocks.stop()
+    # e2e: the user's calls with host arrays
+    for _ in range(2):
+        g = P @ sigma - ustar
+        P.grad_sources(g, sigma)
+    e2steps = max(3, args.steps)
+    t0 = time.perf_counter()
+    for _ in range(e2steps):
+        g = P @ sigma - ustar
+        grad = P.grad_sources(g, sigma)
+        J = 0.5 * float(g @ g)
+    e2e_s = (time.perf_counter() - t0) / e2steps
+    adj_kern = adj_ms / max(adj_n, 1)
+    achieved = m * n * ADJ_FLOPS_PER_PAIR["laplace_dl"] / (adj_kern * 1e-3) / 1e12
+    peak = peaks["fp64_flops"] / 1e12
+    line = {
+        "metric": METRIC, "value": pairs / (ms * 1e-3) / 1e9, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": dict(cfg, l2="flushed between steps", unit_note="forward + adjoint pairs (2 M N per step)"),
+        "e2e": {"value": pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * (2 * n + m),
+                "d2h_bytes_per_step": 8 * (m + 8 * n), "ms_per_step": e2e_s * 1e3, "J": J},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "adjoint_sources (laplace_dl, double)", "kernel_ms": adj_kern,
+                     "flops_per_pair": ADJ_FLOPS_PER_PAIR["laplace_dl"],
+                     "forward_kernel_ms": fwd_ms / max(fwd_n, 1),
+                     "peak_source": "FP64 FMA throughput measured in this run (inti_measure_peaks), of measured"},
+        "clocks": clk,
+    }
+    if not args.no_cpu:
+        # The reference has no adjoint; its route to these gradients is forward-mode
+        # dual numbers (ForwardDiff), one pass over all pairs per input direction.
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        nthreads = host_cores()
+        t0 = time.perf_counter()
+        reps = 0
+        dsx = np.random.default_rng(1).standard_normal(q.coords.shape)
+        while True:
+            O.dl_potential_jvp(tgt.coords, q.coords, q.normals, q.weights, sigma, dsx, None, None, None, nthreads)
+            reps += 1
+            if time.perf_counter() - t0 > min(args.cpu_seconds, 10.0):
+                break
+        t_jvp = (time.perf_counter() - t0) / reps
+        line["cpu_baseline"] = {
+            "value": m * n / t_jvp / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{reps} dual-number (value + one directional derivative) passes over all {m} x {n} pairs",
+            "full_gradient_forward_mode_s_estimate": t_jvp * 8 * n,
+        }
+    return line
+
+
+def bench_csr(args, ctx, torch) -> dict:
+    """Correction SpMV bandwidth (the standalone `inti_csr_apply`) on C3's DIM
+    pattern replicated 20 times: 20 x 22,326 elements of 9 nodes, 4,018,680
+    rows with their own element's 9 columns (nnz = 36.2M), real (δD) and
+    complex (δS) values.  At C3's own size the SpMV is ~25 MB and
+    latency-bound; this scaled pattern exceeds L2 several times over."""
+    import inti_b200 as inti
+
+    nq, m = 9, 20 * 200_934
+    r = np.random.default_rng(3)
+    indptr = np.arange(0, m * nq + 1, nq, dtype=np.int64)
+    indices = ((np.arange(m, dtype=np.int64) // nq * nq)[:, None] + np.arange(nq)).astype(np.int32).ravel()
+    dev = torch.device("cuda:0")
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    out = {}
+    for dt in ("f64", "c128"):
+        cplx = dt == "c128"
+        vals = r.standard_normal(m * nq) + (1j * r.standard_normal(m * nq) if cplx else 0)
+        Cm = inti.CorrectionMatrix.from_csr(indptr, indices, vals, (m, m), ctx=ctx)
+        del vals
+        comps = 2 if cplx else 1
+        x = torch.randn(comps * m, dtype=torch.float64, device=dev)
+        y = torch.zeros(comps * m, dtype=torch.float64, device=dev)
+        torch.cuda.synchronize(dev)
+        vb = 16 if cplx else 8
+        algo = m * nq * (vb + 4) + (m + 1) * 8 + m * vb + m * vb  # beta = 0: y written once
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                Cm.apply_device(x.data_ptr(), y.data_ptr())
+            stream.synchronize()
+            launches0 = ctx.launch_count
+            evs = []
+            for _ in range(args.steps):
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                Cm.apply_device(x.data_ptr(), y.data_ptr())
+                e1.record(stream)
+                evs.append((e0, e1))
+            stream.synchronize()
+            ms = sum(a.elapsed_time(b) for a, b in evs) / args.steps
+        out[dt] = {"ms": ms, "gbs": algo / (ms * 1e-3) / 1e9, "algorithmic_bytes": algo,
+                   "launches": ctx.launch_count - launches0}
+        # parity on sampled rows against the host product of the same arrays
+        rows = r.integers(0, m, 64)
+        xh = x.cpu().numpy().view(np.complex128) if cplx else x.cpu().numpy()
+        ia, ja, va = Cm.arrays()
+        yh = y.cpu().numpy().view(np.complex128) if cplx else y.cpu().numpy()
+        ref = np.array([va[ia[i]:ia[i + 1]] @ xh[ja[ia[i]:ia[i + 1]]] for i in rows])
+        out[dt]["sampled_rows_max_relerr"] = float(np.max(np.abs(yh[rows] - ref) / np.maximum(np.abs(ref), 1e-300)))
+        del Cm
+    peak = 6557.1  # MEASURED_PEAKS.json hbm_gbs
+    return {"metric": "correction SpMV bandwidth", "value": out["f64"]["gbs"], "unit": "GB/s", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["f64"]["ms"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "dim_pattern_c3x20_rows4018680_nq9", "nnz": m * nq,
+                       "l2": "inputs larger than L2 (>= 470 MB per step)"},
+            "roofline": {"bound": "hbm", "achieved": out["f64"]["gbs"], "peak": peak, "unit": "GB/s",
+                         "frac": out["f64"]["gbs"] / peak, "traffic": None, "kernel": "csr_kernel<8, real>",
+                         "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured"},
+            "complex": out["c128"], "real": out["f64"], "gpu_launches": out["f64"]["launches"]}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -356,7 +548,7 @@ def main() -> None:
     ap.add_argument("--no-gmres", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4"])
+                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -380,8 +572,11 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ctx = inti.Context(local)
     peaks = ctx.measure_peaks()
-    if args.workload == "c4":
-        line = bench_batch(args, ctx, peaks, torch)
+    if args.workload in ("c4", "c5", "csr"):
+        if args.workload == "csr":
+            line = bench_csr(args, ctx, torch)
+        else:
+            line = (bench_batch if args.workload == "c4" else bench_adjoint)(args, ctx, peaks, torch)
         if rank == 0:
             print(json.dumps(line), flush=True)
         if dist:

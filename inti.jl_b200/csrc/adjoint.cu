@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
       if (!(d2 > kSamePointTol2)) continue;
       const double gi = sg[q];
       if (DIM == 3) {
-        const double ri = rsqrt(d2);
+        const double ri = rsqrt_fast(d2);
         const double ri3 = ri * ri * ri;
         if (KIND == SL) {
           s = fma(gi, ri, s);
@@ -164,7 +164,7 @@ void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsi
   if (!g || !sigma) throw Error(INTI_E_ARG, "g/sigma NULL");
   const int64_t m = op->target->n, n = op->source->n;
   const int dim = op->dim;
-  DevBuf gd, sd, o_s, o_c, o_n, o_w, part;
+  DevBuf gd, sd, o_s, o_c, o_n, o_w;
   const double* G = g;
   const double* SG = sigma;
   double *DS = dsigma, *DC = dcoords, *DN = dnormals, *DW = dweights;
@@ -187,7 +187,8 @@ void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsi
   const int tps = (int)((ntile + split - 1) / split);
   split = (int)((ntile + tps - 1) / tps);
   const int W = 2 * dim + 2;
-  part.ensure(sizeof(double) * (size_t)split * n * W);
+  op->gpartial.ensure(sizeof(double) * (size_t)split * n * W);
+  double* part = op->gpartial.as<double>();
   const double* TX = op->target->coords.as<double>();
   const double* SX = op->source->coords.as<double>();
   const double* SN = op->source->has_normals ? op->source->normals.as<double>() : nullptr;
@@ -195,10 +196,13 @@ void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsi
   auto go = [&](auto kind_c, auto dim_c) {
     constexpr int K = decltype(kind_c)::value;
     constexpr int D = decltype(dim_c)::value;
-    adjoint_sources<K, D><<<dim3((unsigned)blocks, (unsigned)split), kAdjBlock, 0, ctx->stream>>>(
-        m, n, TX, G, SX, SN, tps, part.as<double>());
+    {
+      ProfScope pa(ctx, "adjoint");
+      adjoint_sources<K, D><<<dim3((unsigned)blocks, (unsigned)split), kAdjBlock, 0, ctx->stream>>>(
+          m, n, TX, G, SX, SN, tps, part);
+    }
     adjoint_reduce<K, D><<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
-        n, split, part.as<double>(), SW, SG, DS, DC, DN, DW);
+        n, split, part, SW, SG, DS, DC, DN, DW);
     ctx->launches += 2;
   };
   if (dim == 3 && op->kind == INTI_SL) go(std::integral_constant<int, SL>(), std::integral_constant<int, 3>());

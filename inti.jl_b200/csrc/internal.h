@@ -20,6 +20,7 @@ struct inti_op {
   inti::DevBuf partial;   // split x m accumulators
   inti::DevBuf xbuf, ybuf;  // staging for host-pointer applies
   inti::DevBuf tpartial;  // transpose: tsplit x n double2
+  inti::DevBuf gpartial;  // source gradients: split x n x (2 dim + 2)
   int split = 1;
   int tsplit = 1;
   int64_t n_tiles = 1;

@@ -291,6 +291,11 @@ class CorrectionMatrix:
         self.ctx.check(self.ctx.lib.inti_csr_apply(self.handle, L.dptr(x), L.dptr(y), None, None, 0))
         return y
 
+    def apply_device(self, x_ptr: int, y_ptr: int, alpha=1.0, beta=0.0) -> None:
+        """Stream-ordered ``y = alpha*C*x + beta*y`` on device pointers."""
+        self.ctx.check(self.ctx.lib.inti_csr_apply(self.handle, C.c_void_p(x_ptr), C.c_void_p(y_ptr),
+                                                   L.cpair(alpha), L.cpair(beta), 1))
+
 
 # ----------------------------------------------------------------------------
 # lazy linear maps
@@ -505,6 +510,14 @@ class GpuOperator(_Map):
                                                          L.dptr(out["sigma"]), L.dptr(out["coords"]),
                                                          L.dptr(out["normals"]), L.dptr(out["weights"]), 0))
         return out
+
+    def grad_sources_device(self, g_ptr: int, sigma_ptr: int, dsigma_ptr: int, dcoords_ptr: int,
+                            dnormals_ptr: int, dweights_ptr: int) -> None:
+        """Stream-ordered ``grad_sources`` on device pointers (no copies, no
+        sync); an output pointer of 0 skips that gradient."""
+        v = lambda p: C.c_void_p(p or None)  # noqa: E731
+        self.ctx.check(self.ctx.lib.inti_op_grad_sources(self.handle, v(g_ptr), v(sigma_ptr), v(dsigma_ptr),
+                                                         v(dcoords_ptr), v(dnormals_ptr), v(dweights_ptr), 1))
 
 
 class CombinedFieldOperator(GpuOperator):

@@ -68,3 +68,28 @@ def test_density_gradient_is_transpose_apply(ctx):
     q, tgt, op, sigma, ustar = setup(ctx)
     g = density(len(tgt), False, 9)
     assert relerr(op.grad_sources(g, sigma)["sigma"], op.rmatvec(g)) < 1e-13
+
+
+def test_device_gradients_match_host(ctx):
+    import torch
+
+    q, tgt, op, sigma, ustar = setup(ctx)
+    g = density(len(tgt), False, 9)
+    ref = op.grad_sources(g, sigma)
+    dev = torch.device("cuda:0")
+    n = len(q)
+    gd, sd = torch.from_numpy(g).to(dev), torch.from_numpy(sigma).to(dev)
+    outs = {k: torch.full((s,), np.nan, dtype=torch.float64, device=dev)
+            for k, s in (("sigma", n), ("coords", 3 * n), ("normals", 3 * n), ("weights", n))}
+    torch.cuda.synchronize()
+    op.grad_sources_device(gd.data_ptr(), sd.data_ptr(), outs["sigma"].data_ptr(), outs["coords"].data_ptr(),
+                           outs["normals"].data_ptr(), outs["weights"].data_ptr())
+    ctx.synchronize()
+    for k, v in outs.items():
+        assert np.array_equal(v.cpu().numpy().reshape(ref[k].shape), ref[k]), k
+    # a zero output pointer skips that gradient
+    outs["weights"].fill_(np.nan)
+    torch.cuda.synchronize()
+    op.grad_sources_device(gd.data_ptr(), sd.data_ptr(), outs["sigma"].data_ptr(), 0, 0, 0)
+    ctx.synchronize()
+    assert torch.isnan(outs["weights"]).all()
