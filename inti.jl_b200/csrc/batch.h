@@ -23,7 +23,6 @@ struct inti_batch {
   inti::DevBuf tc_b, tc_src, tc_counter, tc_toff, tc_items;
   int64_t tc_ntiles = 0;
   int tc_nitems = 0;
-  const float2* expi32 = nullptr;
 };
 
 namespace inti {

@@ -2,10 +2,14 @@
 // SparseMatrixCSC * Vector inside LinearMap(Smat) + LinearMap(δS)
 // (src/api.jl:179-184) and of axpy!(true, δS, Smat) (src/api.jl:171-173).
 //
-// HBM-bound: each row is owned by a group of G lanes (G a power of two chosen
-// from the mean row length) that read the row's values and column indices
-// with coalesced, vectorised loads and reduce with shuffles in a fixed order
-// (deterministic).
+// HBM-bound.  Short rows (the DIM patterns: nq = 5..9 per row) use a
+// row-block ("CSR-stream", Greathouse & Daga, SC'14) kernel: a CTA owns R
+// consecutive rows, whose nonzeros are one contiguous range; all threads
+// stream that range with coalesced loads, multiply by the gathered x and
+// park the products in shared memory, then one thread per row sums its
+// segment in order.  A block whose range overflows shared memory falls back
+// to one warp per row.  Long rows use G lanes per row (G a power of two)
+// with a shuffle reduction.  Every sum has a fixed order (deterministic).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -60,6 +64,91 @@ __global__ void csr_kernel(int64_t m, const int64_t* __restrict__ rowptr,
   }
 }
 
+constexpr int kStreamThreads = 256;
+constexpr int kStreamBytes = 32768;  // products parked per CTA
+
+template <bool CPLX>
+__device__ __forceinline__ void csr_finish(int64_t row, double sr, double si, double* __restrict__ y,
+                                           double ar, double ai, double br, double bi, bool beta_zero) {
+  if (CPLX) {
+    double yr = ar * sr - ai * si, yi = ar * si + ai * sr;
+    if (!beta_zero) {
+      const double2 yo = reinterpret_cast<const double2*>(y)[row];
+      yr += br * yo.x - bi * yo.y;
+      yi += br * yo.y + bi * yo.x;
+    }
+    reinterpret_cast<double2*>(y)[row] = make_double2(yr, yi);
+  } else {
+    double yr = ar * sr;
+    if (!beta_zero) yr += br * y[row];
+    y[row] = yr;
+  }
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(kStreamThreads) csr_stream_kernel(
+    int64_t m, int rows_per_block, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+    const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y, double ar,
+    double ai, double br, double bi, bool beta_zero) {
+  constexpr int CAP = kStreamBytes / (CPLX ? 16 : 8);
+  __shared__ __align__(16) double prod[kStreamBytes / 8];
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+  const int64_t r1 = r0 + rows_per_block < m ? r0 + rows_per_block : m;
+  const int64_t p0 = rowptr[r0], p1 = rowptr[r1];
+  const int tid = threadIdx.x;
+  if (p1 - p0 <= CAP) {
+    for (int64_t p = p0 + tid; p < p1; p += kStreamThreads) {
+      const int32_t j = __ldg(col + p);
+      if (CPLX) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(val) + p);
+        const double2 xv = __ldg(reinterpret_cast<const double2*>(x) + j);
+        reinterpret_cast<double2*>(prod)[p - p0] =
+            make_double2(fma(v.x, xv.x, -v.y * xv.y), fma(v.x, xv.y, v.y * xv.x));
+      } else {
+        prod[p - p0] = __ldg(val + p) * __ldg(x + j);
+      }
+    }
+    __syncthreads();
+    for (int64_t row = r0 + tid; row < r1; row += kStreamThreads) {
+      const int a = (int)(rowptr[row] - p0), b = (int)(rowptr[row + 1] - p0);
+      double sr = 0.0, si = 0.0;
+      for (int q = a; q < b; ++q) {
+        if (CPLX) {
+          const double2 v = reinterpret_cast<const double2*>(prod)[q];
+          sr += v.x;
+          si += v.y;
+        } else {
+          sr += prod[q];
+        }
+      }
+      csr_finish<CPLX>(row, sr, si, y, ar, ai, br, bi, beta_zero);
+    }
+    return;
+  }
+  // overflow: one warp per row, lanes striding the row, shuffle reduction
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int64_t row = r0 + warp; row < r1; row += kStreamThreads / 32) {
+    double sr = 0.0, si = 0.0;
+    for (int64_t p = rowptr[row] + lane; p < rowptr[row + 1]; p += 32) {
+      const int32_t j = __ldg(col + p);
+      if (CPLX) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(val) + p);
+        const double2 xv = __ldg(reinterpret_cast<const double2*>(x) + j);
+        sr = fma(v.x, xv.x, fma(-v.y, xv.y, sr));
+        si = fma(v.x, xv.y, fma(v.y, xv.x, si));
+      } else {
+        sr = fma(__ldg(val + p), __ldg(x + j), sr);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      if (CPLX) si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) csr_finish<CPLX>(row, sr, si, y, ar, ai, br, bi, beta_zero);
+  }
+}
+
 template <int G>
 static void csr_go(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, double ar,
                    double ai, double br, double bi, bool bz) {
@@ -84,16 +173,21 @@ int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, cons
   const bool bz = br == 0.0 && bi == 0.0;
   const double mean = (double)c->nnz / (double)c->m;
   ProfScope pc(ctx, "csr");
-  if (mean <= 2)
-    csr_go<2>(ctx, c, x, y, ar, ai, br, bi, bz);
-  else if (mean <= 6)
-    csr_go<4>(ctx, c, x, y, ar, ai, br, bi, bz);
-  else if (mean <= 12)
-    csr_go<8>(ctx, c, x, y, ar, ai, br, bi, bz);
-  else if (mean <= 24)
-    csr_go<16>(ctx, c, x, y, ar, ai, br, bi, bz);
-  else
+  const bool cplx = c->dtype == INTI_C128;
+  if (mean <= 64) {
+    // rows per CTA: fill ~80% of the product buffer at the mean row length
+    const int cap = kStreamBytes / (cplx ? 16 : 8);
+    const int rpb = (int)std::max<double>(1.0, std::min<double>(kStreamThreads, 0.8 * cap / std::max(mean, 1.0)));
+    const unsigned grid = (unsigned)((c->m + rpb - 1) / rpb);
+    if (cplx)
+      csr_stream_kernel<true><<<grid, kStreamThreads, 0, ctx->stream>>>(
+          c->m, rpb, c->rowptr.as<int64_t>(), c->col.as<int32_t>(), c->val.as<double>(), x, y, ar, ai, br, bi, bz);
+    else
+      csr_stream_kernel<false><<<grid, kStreamThreads, 0, ctx->stream>>>(
+          c->m, rpb, c->rowptr.as<int64_t>(), c->col.as<int32_t>(), c->val.as<double>(), x, y, ar, ai, br, bi, bz);
+  } else {
     csr_go<32>(ctx, c, x, y, ar, ai, br, bi, bz);
+  }
   INTI_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return 1;

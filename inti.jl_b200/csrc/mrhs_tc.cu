@@ -7,22 +7,23 @@
 // B[2j+1][64+r] = Re x_jr (x already multiplied by the weight w_j), the
 // columns 0..63 of A*B are Re Y and 64..127 are Im Y.
 //
-// One persistent CTA per SM (256 threads) takes work items (surface, block
-// of 256 targets) from an atomic counter, largest surfaces first.  Per
-// stage of 32 sources:
-//   * the source records (FP32 coordinates/normals) of stage t+2 and the
-//     packed density block B of stage t+1 are copied into shared memory by
-//     the TMA bulk engine (cp.async.bulk) completing on mbarriers;
-//   * every thread evaluates K for its target row and the 32 sources on the
-//     CUDA cores (FP32, table e^{ikd}) and stores them, rounded to TF32, in
-//     the canonical K-major no-swizzle layout (8-row x 16-byte core
-//     matrices; LBO = 128 B between K chunks, SBO = 2048 B between row
-//     groups);
-//   * one thread issues 2 x 8 tcgen05.mma (M = 128, N = 128, K = 8) into two
-//     TMEM accumulators (128 lanes x 128 FP32 columns each) and commits them
-//     to an mbarrier that frees the A/B buffers.
-// At the end of an item each warp reads its lane quarter of the accumulators
-// with tcgen05.ld and writes alpha*Y/(4 pi) + beta*Y in FP64.
+// One persistent CTA per SM takes work items (surface, block of 256 targets)
+// from an atomic counter, largest surfaces first.  Per stage of 32 sources:
+//   * one control lane copies the source records (FP32 coordinates/normals)
+//     of stage t+2 and the packed density block B of stage t+1 into shared
+//     memory with the TMA bulk engine (cp.async.bulk) completing on mbarriers;
+//   * 16 generator warps evaluate K for their target rows and the 32 sources
+//     on the CUDA cores (FP32; e^{ikd} from the MUFU sine/cosine) and store
+//     them, rounded to TF32, in the canonical K-major no-swizzle layout
+//     (8-row x 16-byte core matrices; LBO = 128 B between K chunks,
+//     SBO = 2048 B between row groups);
+//   * the control lane issues 2 x 8 tcgen05.mma (M = 128, N = 128, K = 8)
+//     into two TMEM accumulators (128 lanes x 128 FP32 columns each) and
+//     commits them to the mbarrier that frees the A and B buffers.
+// Generation of stage t+1 overlaps the MMAs of stage t; the roles meet only
+// at mbarriers, with one CTA barrier per item.  At the end of an item each
+// generator warp reads its lane quarter of the accumulators with tcgen05.ld
+// and writes alpha*Y/(4 pi) + beta*Y in FP64.
 //
 // Every wait is bounded.  On a timeout the CTA records the error, drains its
 // own copies and MMAs (bounded), frees its TMEM and leaves.
@@ -38,7 +39,8 @@
 
 namespace inti {
 
-constexpr int TC_THREADS = 512;           // two threads per target row
+constexpr int TC_GEN_WARPS = 16;                    // two generator threads per target row
+constexpr int TC_THREADS = 32 * (TC_GEN_WARPS + 1);  // + one copy/MMA warp
 constexpr int TC_ROWS = 256;             // targets per item (2 accumulators x 128)
 constexpr int TC_R = 64;                 // complex right-hand sides per pass
 constexpr int TC_N = 2 * TC_R;           // real accumulator columns
@@ -52,8 +54,7 @@ constexpr int TC_S_BYTES = TC_J * TC_S_FLOATS * 4;   // 1 KB
 constexpr int TC_OFF_A = 0;                               // 2 stages x 2 accumulators x 32 KB
 constexpr int TC_OFF_B = TC_OFF_A + 2 * 2 * TC_A_BYTES;   // 2 stages x 32 KB
 constexpr int TC_OFF_S = TC_OFF_B + 2 * TC_B_BYTES;       // 3 stages x 1 KB
-constexpr int TC_OFF_T = TC_OFF_S + 3 * TC_S_BYTES;       // e^{i m delta} table (float2)
-constexpr int TC_SMEM = TC_OFF_T + kExpiTable * 8;
+constexpr int TC_SMEM = TC_OFF_S + 3 * TC_S_BYTES;
 constexpr uint32_t TC_TMEM_COLS = 256;
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N = 128, M = 128
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
@@ -122,67 +123,83 @@ struct TcArgs {
   double* y;
   int64_t ldy;
   int nrhs;
-  float k, kT, delta;
+  float k;
   float c1r, c1i, c2r, c2i;
   int kind;
   double ar, ai, br, bi;
   bool beta_zero;
-  const float2* expi;
   int* counter;
   int* err;
 };
 
 // Per-launch constants of the kernel values.
 struct TcConst {
-  float k, kT, delta, c1r, c1i, c2r, c2i;
+  float k, c1r, c1i, c2r, c2i, kc1r, kc1i;
 };
 
-// K(x, y) for the Helmholtz kernels (without 1/(4 pi)), FP32:
-//   SL: e^{ikd}/d
-//   DL: e^{ikd}/d * (1/d - ik) g,  g = (r.n)/d
-//   CF: e^{ikd}/d * (c2 + c1 (1/d - ik) g)
-template <int KIND>
-__device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, const float2 s1, const TcConst& c,
-                                            const float2* __restrict__ tab) {
-  const float r0 = x[0] - s0.x, r1 = x[1] - s0.y, r2 = x[2] - s0.z;
-  const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
-  const bool keep = d2 > 1.0e-28f;
-  const float ri = keep ? rsqrt_approx_f32(d2) : 0.0f;
-  const float d = d2 * ri;
-  float cs, sn;
-  expi_table_eval<float, float2>(d * c.kT, tab, c.delta, cs, sn);
-  const float hr = cs * ri, hi = sn * ri;  // e^{ikd}/d
-  if (KIND == SL) return make_float2(hr, hi);
-  const float rn = fmaf(r2, s1.y, fmaf(r1, s1.x, r0 * s0.w));
-  const float g = rn * ri;
-  float br, bi;
-  if (KIND == DL) {  // (1/d - ik) g
-    br = g * ri;
-    bi = -c.k * g;
-  } else {  // c2 + c1 (g/d - i k g)
-    const float gr = g * ri, gk = c.k * g;
-    br = fmaf(c.c1r, gr, fmaf(c.c1i, gk, c.c2r));
-    bi = fmaf(c.c1i, gr, fmaf(-c.c1r, gk, c.c2i));
-  }
-  return make_float2(fmaf(hr, br, -hi * bi), fmaf(hr, bi, hi * br));
+// e^{i x} from the hardware sine/cosine approximations (MUFU).  Their
+// absolute error (~1e-6 for the |k d| of a surface) is three orders below the
+// TF32 rounding (2^-11) the values get next.
+__device__ __forceinline__ void sincos_mufu(float x, float& s, float& c) {
+  asm("sin.approx.ftz.f32 %0, %1;" : "=f"(s) : "f"(x));
+  asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
 }
 
+// K(x, y) for the Helmholtz kernels (without 1/(4 pi)), FP32, with
+// P = (r.n)/d^2 and Q = (r.n)/d^3:
+//   SL: e^{ikd}/d
+//   DL: e^{ikd} (1/d - ik) (r.n)/d^2          = e^{ikd} (Q - i k P)
+//   CF: e^{ikd} (c2/d + c1 (Q - i k P))
+template <int KIND>
+__device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, const float2 s1, const TcConst& c) {
+  const float r0 = x[0] - s0.x, r1 = x[1] - s0.y, r2 = x[2] - s0.z;
+  const float d2 = fmaf(r2, r2, fmaf(r1, r1, r0 * r0));
+  const float ri = d2 > 1.0e-28f ? rsqrt_approx_f32(d2) : 0.0f;
+  float sn, cs;
+  sincos_mufu(c.k * (d2 * ri), sn, cs);
+  if (KIND == SL) return make_float2(cs * ri, sn * ri);
+  const float rn = fmaf(r2, s1.y, fmaf(r1, s1.x, r0 * s0.w));
+  const float P = rn * ri * ri;
+  const float Q = P * ri;
+  float br, bi;
+  if (KIND == DL) {
+    br = Q;
+    bi = -c.k * P;
+  } else {
+    br = fmaf(c.c2r, ri, fmaf(c.c1r, Q, c.kc1i * P));
+    bi = fmaf(c.c2i, ri, fmaf(c.c1i, Q, -c.kc1r * P));
+  }
+  return make_float2(fmaf(cs, br, -sn * bi), fmaf(cs, bi, sn * br));
+}
+
+// Roles: warps 0..15 generate the A tiles (two threads per target row, 16
+// sources each per stage) and run the epilogue; warp 16 (one elected lane)
+// issues the bulk copies and the MMAs.  Hand-offs go through mbarriers:
+//   fullS[3]   source records of a stage landed        (copy engine)
+//   fullB[2]   density block of a stage landed         (copy engine)
+//   aFull[2]   A tiles of a stage written              (16 generator warps)
+//   mmaDone[2] MMA group of a stage complete           (tcgen05.commit)
+// Stage g of the CTA (counted over all its items) uses fullS[g % 3] and
+// buffer g & 1 of the others; every wait names the phase of exactly one
+// pending completion (the previous one on that barrier is known complete and
+// the next cannot start before the waiter acts), so the parity test is exact.
 template <int KIND>
 __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ __align__(8) uint64_t fullS[3], fullB[2], mmaDone[2];
+  __shared__ __align__(8) uint64_t fullS[3], fullB[2], aFull[2], mmaDone[2], drainBar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int item_sh;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const TcConst kc{a.k, a.kT, a.delta, a.c1r, a.c1i, a.c2r, a.c2i};
-  float2* tab = reinterpret_cast<float2*>(sm + TC_OFF_T);
-  for (int q = tid; q < kExpiTable; q += TC_THREADS) tab[q] = a.expi[q];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const bool control = warp == TC_GEN_WARPS;
+  const TcConst kc{a.k, a.c1r, a.c1i, a.c2r, a.c2i, a.k * a.c1r, a.k * a.c1i};
   if (tid == 0) {
     for (int q = 0; q < 3; ++q) mbar_init(&fullS[q], 1);
     for (int q = 0; q < 2; ++q) {
       mbar_init(&fullB[q], 1);
+      mbar_init(&aFull[q], TC_GEN_WARPS);
       mbar_init(&mmaDone[q], 1);
     }
+    mbar_init(&drainBar, 1);
     mbar_fence_init();
   }
   if (warp == 0) {
@@ -196,12 +213,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   const uint32_t tmem = tmem_base_sh;
   const uint32_t sbase = smem_u32(sm);
 
-  // uses of each barrier so far (thread-uniform): phase = (uses / nbuf) & 1
-  uint32_t gS = 0;   // source-record stages consumed
-  uint32_t gB = 0;   // density stages consumed (= MMA groups issued)
-  uint32_t gD = 0;   // MMA groups waited for
-  uint32_t issuedS = 0, issuedB = 0;  // thread 0: copies issued
-  uint32_t consumedB = 0, committed = 0;  // thread 0: density copies landed, MMA groups committed
+  uint32_t g = 0;                   // first stage of the current item (same in every thread)
+  uint32_t nS = 0, nB = 0, nC = 0;  // control lane: source copies, density copies, MMA groups issued
   bool ok = true;
 
   for (;;) {
@@ -213,64 +226,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
     const int item = it % a.nitems;
     const int s = a.item_surf[item];
     const int64_t off = a.off[s], n = a.off[s + 1] - off;
-    const int64_t T = (n + TC_J - 1) / TC_J;
+    const uint32_t T = (uint32_t)((n + TC_J - 1) / TC_J);
     const float* srcs = a.src + (size_t)a.toff[s] * TC_J * TC_S_FLOATS;
     const uint32_t* bp = a.bpack + ((size_t)cg * a.ntiles + a.toff[s]) * (TC_B_BYTES / 4);
-    const int trow = tid & (TC_ROWS - 1);  // target row of this thread (two threads per row)
-    const int half = tid >> 8;             // which 16 sources of a stage
-    const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + trow;
-    const bool active = row_loc < n;
-    const int64_t ti = off + min(row_loc, n - 1);
-    const float xt[3] = {(float)a.coords[3 * ti], (float)a.coords[3 * ti + 1], (float)a.coords[3 * ti + 2]};
-    const int acc = trow >> 7;             // accumulator of this row
-    const int row = trow & 127;            // row inside the accumulator
-    // prologue: source records of stages 0 and 1, density of stage 0
-    if (tid == 0) {
-      for (int64_t t = 0; t < 2 && t < T; ++t) {
-        const uint32_t b = (gS + (uint32_t)t) % 3;
-        mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
-        bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)t * TC_J * TC_S_FLOATS, TC_S_BYTES, &fullS[b]);
-        ++issuedS;
-      }
-      const uint32_t b = gB & 1;
-      mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
-      bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp, TC_B_BYTES, &fullB[b]);
-      ++issuedB;
-    }
-    for (int64_t t = 0; t < T; ++t) {
-      // 1. source records of stage t
-      const uint32_t sb = gS % 3;
-      ok = mbar_wait_bounded(&fullS[sb], (gS / 3) & 1);
-      if (!__syncthreads_and(ok)) goto fail;
-      // 2. kernel values for this row and the 32 sources, TF32, into A[stage]
-      {
-        const float* S = reinterpret_cast<const float*>(sm + TC_OFF_S + sb * TC_S_BYTES);
-        const uint32_t ab = TC_OFF_A + ((gB & 1) * 2 + acc) * TC_A_BYTES;
-        const int nsrc = (int)(n - t * TC_J < TC_J ? n - t * TC_J : TC_J);
-        const int j0 = half * (TC_J / 2);
-#pragma unroll 4
-        for (int j = j0; j < j0 + TC_J / 2; j += 2) {
-          const float4 a0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
-          const float2 b0 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
-          const float4 a1 = *reinterpret_cast<const float4*>(S + (j + 1) * TC_S_FLOATS);
-          const float2 b1 = *reinterpret_cast<const float2*>(S + (j + 1) * TC_S_FLOATS + 4);
-          float2 k0 = tc_kernel<KIND>(xt, a0, b0, kc, tab);
-          float2 k1 = tc_kernel<KIND>(xt, a1, b1, kc, tab);
-          if (j >= nsrc) k0 = make_float2(0.f, 0.f);
-          if (j + 1 >= nsrc) k1 = make_float2(0.f, 0.f);
-          uint4 v = make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
-          *reinterpret_cast<uint4*>(sm + ab + tc_kmajor_off(row, 2 * j)) = v;
+    if (control) {
+      if (lane == 0) {
+        for (uint32_t t = 0; t < 2 && t < T; ++t) {
+          const uint32_t b = (g + t) % 3;
+          mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
+          bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)t * TC_J * TC_S_FLOATS, TC_S_BYTES, &fullS[b]);
+          ++nS;
         }
-      }
-      ++gS;
-      fence_proxy_async_smem();
-      __syncthreads();
-      // 3. MMAs of stage t (one thread), then the next copies
-      if (tid == 0) {
-        const uint32_t bb = gB & 1;
-        ok = mbar_wait_bounded(&fullB[bb], (gB >> 1) & 1);
-        if (ok) {
-          ++consumedB;
+        mbar_arrive_expect_tx(&fullB[g & 1], TC_B_BYTES);
+        bulk_copy_g2s(sm + TC_OFF_B + (g & 1) * TC_B_BYTES, bp, TC_B_BYTES, &fullB[g & 1]);
+        ++nB;
+        for (uint32_t t = 0; t < T; ++t) {
+          const uint32_t gg = g + t, bb = gg & 1;
+          ok = mbar_wait_bounded(&aFull[bb], (gg >> 1) & 1) && mbar_wait_bounded(&fullB[bb], (gg >> 1) & 1);
+          if (!ok) break;
           tc_fence_after();
           const uint32_t bsm = sbase + TC_OFF_B + bb * TC_B_BYTES;
 #pragma unroll
@@ -282,91 +255,118 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
                      (t > 0 || kk > 0) ? 1u : 0u);
           }
           tc_commit(&mmaDone[bb]);
-          ++committed;
+          ++nC;
+          if (t + 1 < T) {
+            // density buffer (gg+1)&1 was last read by MMA group gg-1
+            if (gg >= 1) ok = mbar_wait_bounded(&mmaDone[(gg - 1) & 1], ((gg - 1) >> 1) & 1);
+            if (!ok) break;
+            const uint32_t b = (gg + 1) & 1;
+            mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
+            bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp + (size_t)(t + 1) * (TC_B_BYTES / 4), TC_B_BYTES,
+                          &fullB[b]);
+            ++nB;
+          }
+          if (t + 2 < T) {
+            // source buffer (gg+2)%3 held stage gg-1, read before aFull(gg-1)
+            const uint32_t b = (gg + 2) % 3;
+            mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
+            bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)(t + 2) * TC_J * TC_S_FLOATS, TC_S_BYTES,
+                          &fullS[b]);
+            ++nS;
+          }
         }
-        ++gB;
-        // MMAs of stage t-1 must be done before B(t+1) overwrites their buffer
-        if (ok && t >= 1) {
-          ok = mbar_wait_bounded(&mmaDone[gD & 1], (gD >> 1) & 1);
-          ++gD;
-        }
-        if (ok && t + 1 < T) {
-          const uint32_t b = gB & 1;
-          mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
-          bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp + (size_t)(t + 1) * (TC_B_BYTES / 4), TC_B_BYTES,
-                        &fullB[b]);
-          ++issuedB;
-        }
-        if (ok && t + 2 < T) {
-          const uint32_t b = (gS + 1) % 3;
-          mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
-          bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)(t + 2) * TC_J * TC_S_FLOATS, TC_S_BYTES,
-                        &fullS[b]);
-          ++issuedS;
-        }
-      } else {
-        ++gB;
-        if (t >= 1) ++gD;
       }
-      if (!__syncthreads_and(ok)) goto fail;
-    }
-    // 4. the last MMA group, then read the accumulators
-    if (tid == 0) {
-      ok = mbar_wait_bounded(&mmaDone[gD & 1], (gD >> 1) & 1);
-    }
-    ++gD;
-    if (!__syncthreads_and(ok)) goto fail;
-    tc_fence_after();
-    {
-      // warp w: accumulator (w>>2)&1, lane quarter w&3 (its TMEM lanes),
-      // column half w>>3
-      const int q = warp & 3;
-      const uint32_t lane_addr = tmem + ((uint32_t)(32 * q) << 16) + acc * TC_N;
-      const double sc = 1.0 / (4 * kPi);
-      const int c0 = cg * TC_R;
-      for (int m = half * (TC_R / 2); m < (half + 1) * (TC_R / 2); m += 16) {
-        float re[16], im[16];
-        tc_ld16(lane_addr + m, re);
-        tc_ld16(lane_addr + TC_R + m, im);
-        tc_wait_ld();
-        if (active) {
+      __syncwarp();
+    } else {
+      const int trow = tid & (TC_ROWS - 1);  // target row of this thread (two threads per row)
+      const int half = tid >> 8;             // which 16 sources of a stage
+      const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + trow;
+      const bool active = row_loc < n;
+      const int64_t ti = off + min(row_loc, n - 1);
+      const float xt[3] = {(float)a.coords[3 * ti], (float)a.coords[3 * ti + 1], (float)a.coords[3 * ti + 2]};
+      const int acc = trow >> 7;  // accumulator of this row
+      const int row = trow & 127;
+      const int j0 = half * (TC_J / 2);
+      for (uint32_t t = 0; t < T; ++t) {
+        const uint32_t gg = g + t, sb = gg % 3;
+        bool w = mbar_wait_bounded(&fullS[sb], (gg / 3) & 1);
+        // A buffer gg&1 was last read by MMA group gg-2
+        if (w && gg >= 2) w = mbar_wait_bounded(&mmaDone[gg & 1], ((gg - 2) >> 1) & 1);
+        if (!__all_sync(0xffffffffu, w)) {
+          ok = false;
+          break;
+        }
+        // padded sources (past n) have zero density rows: their finite values add nothing
+        const float* S = reinterpret_cast<const float*>(sm + TC_OFF_S + sb * TC_S_BYTES);
+        const uint32_t ab = TC_OFF_A + ((gg & 1) * 2 + acc) * TC_A_BYTES;
+#pragma unroll 4
+        for (int j = j0; j < j0 + TC_J / 2; j += 2) {
+          const float4 a0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
+          const float2 b0 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
+          const float4 a1 = *reinterpret_cast<const float4*>(S + (j + 1) * TC_S_FLOATS);
+          const float2 b1 = *reinterpret_cast<const float2*>(S + (j + 1) * TC_S_FLOATS + 4);
+          const float2 k0 = tc_kernel<KIND>(xt, a0, b0, kc);
+          const float2 k1 = tc_kernel<KIND>(xt, a1, b1, kc);
+          *reinterpret_cast<uint4*>(sm + ab + tc_kmajor_off(row, 2 * j)) =
+              make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
+        }
+        fence_proxy_async_smem();
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&aFull[gg & 1]);
+      }
+      if (ok) {
+        const uint32_t gl = g + T - 1;
+        ok = __all_sync(0xffffffffu, mbar_wait_bounded(&mmaDone[gl & 1], (gl >> 1) & 1));
+      }
+      if (ok) {
+        tc_fence_after();
+        // warp w: accumulator (w>>2)&1, TMEM lane quarter w&3, column half w>>3
+        const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + acc * TC_N;
+        const double sc = 1.0 / (4 * kPi);
+        const int c0 = cg * TC_R;
+        double2* Y = reinterpret_cast<double2*>(a.y);
+        for (int m = half * (TC_R / 2); m < (half + 1) * (TC_R / 2); m += 16) {
+          float re[16], im[16];
+          tc_ld16(lane_addr + m, re);
+          tc_ld16(lane_addr + TC_R + m, im);
+          tc_wait_ld();
+          if (active) {
 #pragma unroll
-          for (int c = 0; c < 16; ++c) {
-            const int col = c0 + m + c;
-            if (col >= a.nrhs) break;
-            const int64_t o = (int64_t)col * a.ldy + off + row_loc;
-            const double yr = sc * re[c], yi = sc * im[c];
-            double orr = a.ar * yr - a.ai * yi, oi = a.ar * yi + a.ai * yr;
-            double2* Y = reinterpret_cast<double2*>(a.y);
-            if (!a.beta_zero) {
-              const double2 yo = Y[o];
-              orr += a.br * yo.x - a.bi * yo.y;
-              oi += a.br * yo.y + a.bi * yo.x;
+            for (int c = 0; c < 16; ++c) {
+              const int col = c0 + m + c;
+              if (col >= a.nrhs) break;
+              const int64_t o = (int64_t)col * a.ldy + off + row_loc;
+              const double yr = sc * re[c], yi = sc * im[c];
+              double orr = a.ar * yr - a.ai * yi, oi = a.ar * yi + a.ai * yr;
+              if (!a.beta_zero) {
+                const double2 yo = Y[o];
+                orr += a.br * yo.x - a.bi * yo.y;
+                oi += a.br * yo.y + a.bi * yo.x;
+              }
+              Y[o] = make_double2(orr, oi);
             }
-            Y[o] = make_double2(orr, oi);
           }
         }
       }
     }
+    g += T;
     tc_fence_before();
-    __syncthreads();  // accumulators read before the next item overwrites them
+    // accumulators read (or the item abandoned) before the next item's MMAs
+    if (__syncthreads_or(!ok)) goto fail;
   }
   goto done;
 fail:
-  if (tid == 0) {
+  if (control && lane == 0) {
     atomicExch(a.err, kErrWaitTimeout);
-    // drain: every issued copy and MMA group must land before the CTA leaves
-    while (gS < issuedS) {
-      mbar_wait_bounded(&fullS[gS % 3], (gS / 3) & 1);
-      ++gS;
-    }
-    while (consumedB < issuedB) {
-      mbar_wait_bounded(&fullB[consumedB & 1], (consumedB >> 1) & 1);
-      ++consumedB;
-    }
-    while (gD < committed) {
-      mbar_wait_bounded(&mmaDone[gD & 1], (gD >> 1) & 1);
-      ++gD;
+    // Everything this CTA put in flight must land before it leaves: at most
+    // the last three source copies and the last two density copies are
+    // pending (each alone on its barrier), and one more commit tracks every
+    // MMA issued so far.
+    for (uint32_t q = nS > 3 ? nS - 3 : 0; q < nS; ++q) mbar_wait_bounded(&fullS[q % 3], (q / 3) & 1);
+    for (uint32_t q = nB > 2 ? nB - 2 : 0; q < nB; ++q) mbar_wait_bounded(&fullB[q & 1], (q >> 1) & 1);
+    if (nC > 0) {
+      tc_commit(&drainBar);
+      mbar_wait_bounded(&drainBar, 0);
     }
   }
   __syncthreads();
@@ -477,7 +477,6 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
         b->kind == SL ? nullptr : b->normals.as<double>(), b->tc_src.as<float>());
     ctx->launches++;
     b->tc_counter.ensure(sizeof(int));
-    b->expi32 = expi_table_f32(ctx);
   }
   const int ncg = (a.nrhs + TC_R - 1) / TC_R;
   b->tc_b.ensure((size_t)ncg * b->tc_ntiles * TC_B_BYTES);
@@ -506,8 +505,6 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
   t.ldy = a.ldy;
   t.nrhs = a.nrhs;
   t.k = (float)b->k;
-  t.kT = (float)(b->k * kExpiTable / (2 * kPi));
-  t.delta = (float)(2 * kPi / kExpiTable);
   t.c1r = (float)b->c1[0];
   t.c1i = (float)b->c1[1];
   t.c2r = (float)b->c2[0];
@@ -518,7 +515,6 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
   t.br = a.br;
   t.bi = a.bi;
   t.beta_zero = a.beta_zero;
-  t.expi = b->expi32;
   t.counter = b->tc_counter.as<int>();
   t.err = ctx->err_flag.as<int>();
   INTI_CUDA(cudaMemsetAsync(b->tc_counter.p, 0, sizeof(int), ctx->stream));
