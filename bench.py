@@ -71,6 +71,13 @@ class Clocks:
                                       stdout=self.f, stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
+        # nvidia-smi takes a while to start: wait (bounded) for its first
+        # sample so that short timed regions are covered
+        t0 = time.perf_counter()
+        while self.p is not None and time.perf_counter() - t0 < 10.0:
+            if Path(self.f.name).stat().st_size > 0:
+                break
+            time.sleep(0.05)
 
     def stop(self) -> dict:
         if self.p is None:

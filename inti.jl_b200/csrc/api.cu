@@ -657,7 +657,8 @@ int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx,
       batch_apply_device(b, precision, x, ldx, y, ldy, nrhs, alpha, beta);
       return;
     }
-    DevBuf xd, yd;
+    // staging buffers are kept on the handle: no allocation per call once they fit
+    DevBuf &xd = b->xstage, &yd = b->ystage;
     const size_t bx = sizeof(double) * comps * (size_t)ldx * nrhs, by = sizeof(double) * comps * (size_t)ldy * nrhs;
     xd.ensure(bx);
     yd.ensure(by);

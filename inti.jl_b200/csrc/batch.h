@@ -21,6 +21,7 @@ struct inti_batch {
   // tensor-core path: packed density blocks and source records, tile
   // offsets, 256-target work items, work counter
   inti::DevBuf tc_b, tc_src, tc_counter, tc_toff, tc_items;
+  inti::DevBuf xstage, ystage;  // staging for host-pointer applies
   int64_t tc_ntiles = 0;
   int tc_nitems = 0;
 };

@@ -145,11 +145,16 @@ __device__ __forceinline__ void sincos_mufu(float x, float& s, float& c) {
   asm("cos.approx.ftz.f32 %0, %1;" : "=f"(c) : "f"(x));
 }
 
+// Kernel variant of the combined field with c1 = 1 and c2 = i*eta (the
+// Brakhage-Werner form D - i eta S), chosen on the host.
+constexpr int CFI = 5;
+
 // K(x, y) for the Helmholtz kernels (without 1/(4 pi)), FP32, with
-// P = (r.n)/d^2 and Q = (r.n)/d^3:
-//   SL: e^{ikd}/d
-//   DL: e^{ikd} (1/d - ik) (r.n)/d^2          = e^{ikd} (Q - i k P)
-//   CF: e^{ikd} (c2/d + c1 (Q - i k P))
+// u = (r.n)/d, P = (r.n)/d^2 and Q = (r.n)/d^3:
+//   SL:  e^{ikd}/d
+//   DL:  e^{ikd} (1/d - ik) (r.n)/d^2          = e^{ikd} (Q - i k P)
+//   CF:  e^{ikd} (c2/d + c1 (Q - i k P))
+//   CFI: e^{ikd} (Q + i (eta - k u)/d)         (c1 = 1, c2 = i eta)
 template <int KIND>
 __device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, const float2 s1, const TcConst& c) {
   const float r0 = x[0] - s0.x, r1 = x[1] - s0.y, r2 = x[2] - s0.z;
@@ -159,22 +164,29 @@ __device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, con
   sincos_mufu(c.k * (d2 * ri), sn, cs);
   if (KIND == SL) return make_float2(cs * ri, sn * ri);
   const float rn = fmaf(r2, s1.y, fmaf(r1, s1.x, r0 * s0.w));
-  const float P = rn * ri * ri;
-  const float Q = P * ri;
+  const float u = rn * ri;
   float br, bi;
-  if (KIND == DL) {
-    br = Q;
-    bi = -c.k * P;
+  if (KIND == CFI) {
+    br = u * (ri * ri);
+    bi = ri * fmaf(-c.k, u, c.c2i);
   } else {
-    br = fmaf(c.c2r, ri, fmaf(c.c1r, Q, c.kc1i * P));
-    bi = fmaf(c.c2i, ri, fmaf(c.c1i, Q, -c.kc1r * P));
+    const float P = u * ri;
+    const float Q = P * ri;
+    if (KIND == DL) {
+      br = Q;
+      bi = -c.k * P;
+    } else {
+      br = fmaf(c.c2r, ri, fmaf(c.c1r, Q, c.kc1i * P));
+      bi = fmaf(c.c2i, ri, fmaf(c.c1i, Q, -c.kc1r * P));
+    }
   }
   return make_float2(fmaf(cs, br, -sn * bi), fmaf(cs, bi, sn * br));
 }
 
-// Roles: warps 0..15 generate the A tiles (two threads per target row, 16
-// sources each per stage) and run the epilogue; warp 16 (one elected lane)
-// issues the bulk copies and the MMAs.  Hand-offs go through mbarriers:
+// Roles: warps 0..15 generate the A tiles (each thread two target rows, one
+// per accumulator, and 8 sources of a stage) and run the epilogue; warp 16
+// (one elected lane) issues the bulk copies and the MMAs.  Hand-offs go
+// through mbarriers:
 //   fullS[3]   source records of a stage landed        (copy engine)
 //   fullB[2]   density block of a stage landed         (copy engine)
 //   aFull[2]   A tiles of a stage written              (16 generator warps)
@@ -183,6 +195,9 @@ __device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, con
 // buffer g & 1 of the others; every wait names the phase of exactly one
 // pending completion (the previous one on that barrier is known complete and
 // the next cannot start before the waiter acts), so the parity test is exact.
+// (Splitting aFull/mmaDone per K quarter, so that warp groups drift apart
+// without waiting for one another, measured slower: four commits per stage
+// cost more than the skew they hide.)
 template <int KIND>
 __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
@@ -278,15 +293,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
       }
       __syncwarp();
     } else {
-      const int trow = tid & (TC_ROWS - 1);  // target row of this thread (two threads per row)
-      const int half = tid >> 8;             // which 16 sources of a stage
-      const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + trow;
-      const bool active = row_loc < n;
-      const int64_t ti = off + min(row_loc, n - 1);
-      const float xt[3] = {(float)a.coords[3 * ti], (float)a.coords[3 * ti + 1], (float)a.coords[3 * ti + 2]};
-      const int acc = trow >> 7;  // accumulator of this row
-      const int row = trow & 127;
-      const int j0 = half * (TC_J / 2);
+      // generation: rows ra (accumulator 0) and ra + 128 (accumulator 1),
+      // sources 8*quarter .. 8*quarter+7 of each stage
+      const int ra = tid & 127;
+      const int j0 = (tid >> 7) * (TC_J / 4);
+      const int64_t blk0 = (int64_t)a.item_block[item] * TC_ROWS;
+      float xt[2][3];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int64_t ti = off + min(blk0 + ra + 128 * h, n - 1);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) xt[h][c] = (float)a.coords[3 * ti + c];
+      }
       for (uint32_t t = 0; t < T; ++t) {
         const uint32_t gg = g + t, sb = gg % 3;
         bool w = mbar_wait_bounded(&fullS[sb], (gg / 3) & 1);
@@ -298,17 +316,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
         }
         // padded sources (past n) have zero density rows: their finite values add nothing
         const float* S = reinterpret_cast<const float*>(sm + TC_OFF_S + sb * TC_S_BYTES);
-        const uint32_t ab = TC_OFF_A + ((gg & 1) * 2 + acc) * TC_A_BYTES;
-#pragma unroll 4
-        for (int j = j0; j < j0 + TC_J / 2; j += 2) {
+        unsigned char* A0 = sm + TC_OFF_A + (gg & 1) * 2 * TC_A_BYTES;
+#pragma unroll 2
+        for (int j = j0; j < j0 + TC_J / 4; j += 2) {
           const float4 a0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
           const float2 b0 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
           const float4 a1 = *reinterpret_cast<const float4*>(S + (j + 1) * TC_S_FLOATS);
           const float2 b1 = *reinterpret_cast<const float2*>(S + (j + 1) * TC_S_FLOATS + 4);
-          const float2 k0 = tc_kernel<KIND>(xt, a0, b0, kc);
-          const float2 k1 = tc_kernel<KIND>(xt, a1, b1, kc);
-          *reinterpret_cast<uint4*>(sm + ab + tc_kmajor_off(row, 2 * j)) =
-              make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
+          const uint32_t o = tc_kmajor_off(ra, 2 * j);
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const float2 k0 = tc_kernel<KIND>(xt[h], a0, b0, kc);
+            const float2 k1 = tc_kernel<KIND>(xt[h], a1, b1, kc);
+            *reinterpret_cast<uint4*>(A0 + h * TC_A_BYTES + o) =
+                make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
+          }
         }
         fence_proxy_async_smem();
         __syncwarp();
@@ -321,6 +343,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
       if (ok) {
         tc_fence_after();
         // warp w: accumulator (w>>2)&1, TMEM lane quarter w&3, column half w>>3
+        const int acc = (warp >> 2) & 1, half = warp >> 3;
+        const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + acc * 128 + (warp & 3) * 32 + lane;
+        const bool active = row_loc < n;
         const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + acc * TC_N;
         const double sc = 1.0 / (4 * kPi);
         const int c0 = cg * TC_R;
@@ -527,6 +552,8 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
     launch(mrhs_tc_kernel<SL>);
   else if (b->kind == DL)
     launch(mrhs_tc_kernel<DL>);
+  else if (b->c1[0] == 1.0 && b->c1[1] == 0.0 && b->c2[0] == 0.0)
+    launch(mrhs_tc_kernel<CFI>);
   else
     launch(mrhs_tc_kernel<CF>);
   ctx->launches++;

@@ -60,13 +60,15 @@ def test_batch_fp64_matches_single_surface_operators(ctx, kind, pde):
     assert relerr(got, 0.5 * ref + 2.0 * Y0) < 1e-12
 
 
-@pytest.mark.parametrize("kind", ["SL", "DL", "CF"])
+@pytest.mark.parametrize("kind", ["SL", "DL", "CF", "CF_general"])
 @pytest.mark.parametrize("nrhs", [5, 64, 70])
 def test_batch_tf32_tensor_cores_match_fp64(ctx, kind, nrhs):
     quads = stars((4, 3, 6, 2), seed=3)
     op = inti.Helmholtz(k=5.0, dim=3)
     corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
-    B = inti.BatchOperator(op, quads, kind, corrs, 1.0, -5.0j, ctx=ctx)
+    # D - 5i S takes the Brakhage-Werner kernel variant; other couplings the general one
+    cD, cS = (0.7 + 0.2j, 0.3 - 2.0j) if kind == "CF_general" else (1.0, -5.0j)
+    B = inti.BatchOperator(op, quads, kind[:2], corrs, cD, cS, ctx=ctx)
     X = rhs(B.n, nrhs, True, 4)
     y64 = B.apply(X, "fp64")
     y32 = B.apply(X, "tf32")
