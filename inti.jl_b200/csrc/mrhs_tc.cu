@@ -40,27 +40,37 @@
 namespace inti {
 
 constexpr int TC_GEN_WARPS = 16;                    // two generator threads per target row
-constexpr int TC_THREADS = 32 * (TC_GEN_WARPS + 1);  // + one copy/MMA warp
+constexpr int TC_THREADS = 32 * (TC_GEN_WARPS + 2);  // + MMA-issue and copy warps
 constexpr int TC_ROWS = 256;             // targets per item (2 accumulators x 128)
 constexpr int TC_R = 64;                 // complex right-hand sides per pass
 constexpr int TC_N = 2 * TC_R;           // real accumulator columns
 constexpr int TC_J = 32;                 // sources per stage
 constexpr int TC_K = 2 * TC_J;           // K elements per stage
-constexpr int TC_A_BYTES = 128 * TC_K * 4;           // one accumulator's A tile: 32 KB
 constexpr int TC_B_BYTES = TC_N * TC_K * 4;          // 32 KB
 constexpr int TC_S_FLOATS = 8;                       // x y z nx ny nz pad pad
 constexpr int TC_S_BYTES = TC_J * TC_S_FLOATS * 4;   // 1 KB
 // dynamic shared memory layout (bytes)
-constexpr int TC_OFF_A = 0;                               // 2 stages x 2 accumulators x 32 KB
-constexpr int TC_OFF_B = TC_OFF_A + 2 * 2 * TC_A_BYTES;   // 2 stages x 32 KB
-constexpr int TC_OFF_S = TC_OFF_B + 2 * TC_B_BYTES;       // 3 stages x 1 KB
-constexpr int TC_SMEM = TC_OFF_S + 3 * TC_S_BYTES;
-constexpr uint32_t TC_TMEM_COLS = 256;
+// Ring depths: a bulk copy from L2 takes ~1500 cycles to land, longer than
+// a stage's MMAs, so densities are fetched TC_NB - 1 stages and source
+// records TC_NS - 1 stages ahead of use.
+constexpr int TC_NB = 4;
+constexpr int TC_NS = 8;
+constexpr int TC_OFF_B = 0;                                   // TC_NB stages x 32 KB
+constexpr int TC_OFF_S = TC_OFF_B + TC_NB * TC_B_BYTES;       // TC_NS stages x 1 KB
+constexpr int TC_SMEM = TC_OFF_S + TC_NS * TC_S_BYTES;
+// tensor memory (512 columns x 128 lanes x 32 bit): accumulators in columns
+// 0..255 (128 each), then the A tiles, TC_K columns per accumulator and stage
+constexpr uint32_t TC_TMEM_COLS = 512;
+constexpr uint32_t TC_TMEM_A = 2 * TC_N;
+__host__ __device__ constexpr uint32_t tc_a_col(uint32_t stage_buf, int acc) {
+  return TC_TMEM_A + (2 * stage_buf + (uint32_t)acc) * TC_K;
+}
+static_assert(TC_TMEM_A + 4 * TC_K <= TC_TMEM_COLS, "A tiles exceed tensor memory");
 // instruction descriptor: F32 accumulate, TF32 A and B, both K-major, N = 128, M = 128
 constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
                               ((uint32_t)(128 >> 4) << 24);
 
-// K-major no-swizzle canonical offset of element (row, k) in a 128 x 64 tile
+// K-major no-swizzle canonical offset of element (row, k) in a 128 x 64 shared-memory tile
 __host__ __device__ constexpr uint32_t tc_kmajor_off(int row, int k) {
   return (uint32_t)((row >> 3) * 2048 + (k >> 2) * 128 + (row & 7) * 16 + (k & 3) * 4);
 }
@@ -79,13 +89,53 @@ __device__ __forceinline__ uint32_t to_tf32(float v) {
   return r;
 }
 
-__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// Round-half-away to TF32 for the tensor core's own reads: adding half a TF32
+// unit in the last place (bit 12) to the FP32 pattern makes the 19 bits the
+// MMA reads the rounded value (one integer add; cvt.rna costs several
+// instructions).  Finite inputs only.
+__device__ __forceinline__ uint32_t tf32_bits(float v) { return __float_as_uint(v) + 0x1000u; }
+
+// D (tensor memory) += A (tensor memory: lanes = rows, 8 columns = K) x B (shared memory descriptor)
+__device__ __forceinline__ void tc_mma_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
 }
+
+// The 8 MMAs (K = 8 each) of one accumulator and stage in one block: A
+// columns advance by 8, the B descriptor's start address by 256 bytes (16 in
+// its address field).  Only the first MMA of an item overwrites D.
+__device__ __forceinline__ void tc_mma8_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t accumulate) {
+#define TC_MMA_NEXT                                     \
+  "add.u32 a, a, 8;\n\tadd.s64 b, b, 16;\n\t"          \
+  "tcgen05.mma.cta_group::1.kind::tf32 [%0], [a], b, %3, q;\n\t"
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t.reg .b64 b;\n\t.reg .b32 a;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\tsetp.eq.b32 q, 0, 0;\n\t"
+      "mov.b32 a, %1;\n\tmov.b64 b, %2;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], [a], b, %3, p;\n\t" TC_MMA_NEXT TC_MMA_NEXT TC_MMA_NEXT TC_MMA_NEXT
+          TC_MMA_NEXT TC_MMA_NEXT TC_MMA_NEXT "}\n" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(TC_IDESC), "r"(accumulate));
+#undef TC_MMA_NEXT
+}
+static_assert(TC_K == 64, "tc_mma8_ts issues exactly 8 K-steps of 8");
+
+// True in exactly one lane of a converged warp.
+__device__ __forceinline__ bool elect_one() {
+  uint32_t e;
+  asm volatile("{\n\t.reg .pred P;\n\telect.sync _|P, 0xffffffff;\n\tselp.b32 %0, 1, 0, P;\n\t}" : "=r"(e));
+  return e != 0;
+}
+
+// 8 consecutive 32-bit columns of this thread's tensor-memory lane
+__device__ __forceinline__ void tc_st8(uint32_t taddr, const uint32_t* v) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
+               "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+               : "memory");
+}
+__device__ __forceinline__ void tc_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
@@ -183,37 +233,46 @@ __device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, con
   return make_float2(fmaf(cs, br, -sn * bi), fmaf(cs, bi, sn * br));
 }
 
-// Roles: warps 0..15 generate the A tiles (each thread two target rows, one
-// per accumulator, and 8 sources of a stage) and run the epilogue; warp 16
-// (one elected lane) issues the bulk copies and the MMAs.  Hand-offs go
-// through mbarriers:
-//   fullS[3]   source records of a stage landed        (copy engine)
-//   fullB[2]   density block of a stage landed         (copy engine)
-//   aFull[2]   A tiles of a stage written              (16 generator warps)
-//   mmaDone[2] MMA group of a stage complete           (tcgen05.commit)
-// Stage g of the CTA (counted over all its items) uses fullS[g % 3] and
-// buffer g & 1 of the others; every wait names the phase of exactly one
-// pending completion (the previous one on that barrier is known complete and
-// the next cannot start before the waiter acts), so the parity test is exact.
+// Roles (warp w, one elected lane for the first two):
+//   w = 0       MMA issuer: waits for a stage's A tiles and density block,
+//               issues its 16 MMAs and commits them;
+//   w = 1       copy producer: refills the density and source-record rings
+//               (TMA bulk copies) as soon as the MMAs of a stage have freed
+//               its buffers;
+//   w = 2..17   generators (each thread two target rows, one per
+//               accumulator, and 8 sources of a stage) and the epilogue.
+// Splitting issue and production keeps each lane's serial path short: the
+// barrier and copy operations of one lane queue behind the generators' own
+// shared/tensor-memory traffic, so a lane doing both fell behind.
+// Hand-offs go through mbarriers:
+//   fullS[NS]    source records of a stage landed    (copy engine)
+//   fullB[NB]    density block of a stage landed     (copy engine)
+//   aFull[2]     A tiles of a stage written          (16 generator warps)
+//   mmaDone[NB]  MMA group of a stage complete       (tcgen05.commit)
+// Stage g of the CTA (counted over all its items) uses fullS[g % NS],
+// fullB[g % NB], mmaDone[g % NB] and A buffer g & 1.  Every wait names the
+// phase of exactly one pending completion (the previous one on that barrier
+// is known complete and the next cannot start before the waiter acts), so
+// the parity test is exact.
 // (Splitting aFull/mmaDone per K quarter, so that warp groups drift apart
 // without waiting for one another, measured slower: four commits per stage
 // cost more than the skew they hide.)
 template <int KIND>
 __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   extern __shared__ __align__(1024) unsigned char sm[];
-  __shared__ __align__(8) uint64_t fullS[3], fullB[2], aFull[2], mmaDone[2], drainBar;
+  __shared__ __align__(8) uint64_t fullS[TC_NS], fullB[TC_NB], aFull[2], mmaDone[TC_NB], drainBar;
   __shared__ uint32_t tmem_base_sh;
   __shared__ int item_sh;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const bool control = warp == TC_GEN_WARPS;
+  const int gw = warp - 2;  // generator index 0..15
   const TcConst kc{a.k, a.c1r, a.c1i, a.c2r, a.c2i, a.k * a.c1r, a.k * a.c1i};
   if (tid == 0) {
-    for (int q = 0; q < 3; ++q) mbar_init(&fullS[q], 1);
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < TC_NS; ++q) mbar_init(&fullS[q], 1);
+    for (int q = 0; q < TC_NB; ++q) {
       mbar_init(&fullB[q], 1);
-      mbar_init(&aFull[q], TC_GEN_WARPS);
       mbar_init(&mmaDone[q], 1);
     }
+    for (int q = 0; q < 2; ++q) mbar_init(&aFull[q], TC_GEN_WARPS);
     mbar_init(&drainBar, 1);
     mbar_fence_init();
   }
@@ -228,8 +287,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   const uint32_t tmem = tmem_base_sh;
   const uint32_t sbase = smem_u32(sm);
 
-  uint32_t g = 0;                   // first stage of the current item (same in every thread)
-  uint32_t nS = 0, nB = 0, nC = 0;  // control lane: source copies, density copies, MMA groups issued
+  uint32_t g = 0;          // first stage of the current item (same in every thread)
+  uint32_t nS = 0, nB = 0;  // producer lane: source and density copies issued
+  uint32_t nC = 0;          // issuer lane: MMA groups committed
   bool ok = true;
 
   for (;;) {
@@ -244,59 +304,71 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
     const uint32_t T = (uint32_t)((n + TC_J - 1) / TC_J);
     const float* srcs = a.src + (size_t)a.toff[s] * TC_J * TC_S_FLOATS;
     const uint32_t* bp = a.bpack + ((size_t)cg * a.ntiles + a.toff[s]) * (TC_B_BYTES / 4);
-    if (control) {
-      if (lane == 0) {
-        for (uint32_t t = 0; t < 2 && t < T; ++t) {
-          const uint32_t b = (g + t) % 3;
+    if (warp == 0) {
+      // The whole warp runs the loop on warp-uniform operands and one elected
+      // lane issues: measured ~2x faster MMA issue than a lone lane when the
+      // generator warps compete for the scheduler.
+      for (uint32_t t = 0; t < T; ++t) {
+        const uint32_t gg = g + t, bb = gg & 1, nb = gg % TC_NB;
+        ok = mbar_wait_bounded(&aFull[bb], (gg >> 1) & 1) && mbar_wait_bounded(&fullB[nb], (gg / TC_NB) & 1);
+        if (!__all_sync(0xffffffffu, ok)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint64_t bdesc = tc_smem_desc(sbase + TC_OFF_B + nb * TC_B_BYTES);
+        if (elect_one()) {
+          tc_mma8_ts(tmem, tmem + tc_a_col(bb, 0), bdesc, t > 0 ? 1u : 0u);
+          tc_mma8_ts(tmem + TC_N, tmem + tc_a_col(bb, 1), bdesc, t > 0 ? 1u : 0u);
+          tc_commit(&mmaDone[nb]);
+        }
+        __syncwarp();
+        ++nC;
+      }
+    } else if (warp == 1) {
+      // Stage x's copies go to the buffers of stage x - NB (densities) and
+      // x - NS (sources); both are free once MMA group x - NB, respectively
+      // x - NS, is complete, which (MMAs completing in order) the wait for
+      // the MMA group one stage earlier than x's first use guarantees.
+      auto copyS = [&](uint32_t t) {
+        const uint32_t b = (g + t) % TC_NS;
+        if (elect_one()) {
           mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
           bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)t * TC_J * TC_S_FLOATS, TC_S_BYTES, &fullS[b]);
-          ++nS;
         }
-        mbar_arrive_expect_tx(&fullB[g & 1], TC_B_BYTES);
-        bulk_copy_g2s(sm + TC_OFF_B + (g & 1) * TC_B_BYTES, bp, TC_B_BYTES, &fullB[g & 1]);
+        __syncwarp();
+        ++nS;
+      };
+      auto copyB = [&](uint32_t t) {
+        const uint32_t b = (g + t) % TC_NB;
+        if (elect_one()) {
+          mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
+          bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp + (size_t)t * (TC_B_BYTES / 4), TC_B_BYTES, &fullB[b]);
+        }
+        __syncwarp();
         ++nB;
-        for (uint32_t t = 0; t < T; ++t) {
-          const uint32_t gg = g + t, bb = gg & 1;
-          ok = mbar_wait_bounded(&aFull[bb], (gg >> 1) & 1) && mbar_wait_bounded(&fullB[bb], (gg >> 1) & 1);
-          if (!ok) break;
-          tc_fence_after();
-          const uint32_t bsm = sbase + TC_OFF_B + bb * TC_B_BYTES;
-#pragma unroll
-          for (int q = 0; q < 2; ++q) {
-            const uint32_t asm_ = sbase + TC_OFF_A + (bb * 2 + q) * TC_A_BYTES;
-#pragma unroll
-            for (int kk = 0; kk < TC_K / 8; ++kk)
-              tc_mma(tmem + q * TC_N, tc_smem_desc(asm_ + kk * 256), tc_smem_desc(bsm + kk * 256),
-                     (t > 0 || kk > 0) ? 1u : 0u);
-          }
-          tc_commit(&mmaDone[bb]);
-          ++nC;
-          if (t + 1 < T) {
-            // density buffer (gg+1)&1 was last read by MMA group gg-1
-            if (gg >= 1) ok = mbar_wait_bounded(&mmaDone[(gg - 1) & 1], ((gg - 1) >> 1) & 1);
-            if (!ok) break;
-            const uint32_t b = (gg + 1) & 1;
-            mbar_arrive_expect_tx(&fullB[b], TC_B_BYTES);
-            bulk_copy_g2s(sm + TC_OFF_B + b * TC_B_BYTES, bp + (size_t)(t + 1) * (TC_B_BYTES / 4), TC_B_BYTES,
-                          &fullB[b]);
-            ++nB;
-          }
-          if (t + 2 < T) {
-            // source buffer (gg+2)%3 held stage gg-1, read before aFull(gg-1)
-            const uint32_t b = (gg + 2) % 3;
-            mbar_arrive_expect_tx(&fullS[b], TC_S_BYTES);
-            bulk_copy_g2s(sm + TC_OFF_S + b * TC_S_BYTES, srcs + (size_t)(t + 2) * TC_J * TC_S_FLOATS, TC_S_BYTES,
-                          &fullS[b]);
-            ++nS;
-          }
+      };
+      // prologue: buffers released by the previous item
+      for (uint32_t t = 0; t < TC_NS - 1 && t < T; ++t) copyS(t);
+      for (uint32_t t = 0; t < TC_NB - 1 && t < T; ++t) copyB(t);
+      for (uint32_t t = 0; t + TC_NB - 1 < T || t + TC_NS - 1 < T; ++t) {
+        const uint32_t gg = g + t;
+        // MMA group gg-1 read density buffer (gg-1)%NB and, through its A
+        // tiles, the source records of stage gg-1
+        if (gg >= 1) ok = mbar_wait_bounded(&mmaDone[(gg - 1) % TC_NB], ((gg - 1) / TC_NB) & 1);
+        if (!__all_sync(0xffffffffu, ok)) {
+          ok = false;
+          break;
         }
+        if (t + TC_NB - 1 < T) copyB(t + TC_NB - 1);
+        if (t + TC_NS - 1 < T) copyS(t + TC_NS - 1);
       }
-      __syncwarp();
     } else {
       // generation: rows ra (accumulator 0) and ra + 128 (accumulator 1),
-      // sources 8*quarter .. 8*quarter+7 of each stage
-      const int ra = tid & 127;
-      const int j0 = (tid >> 7) * (TC_J / 4);
+      // sources 8*(gw>>2) .. +7 of each stage; ra lies in the tensor-memory
+      // lane quarter warp % 4 that this warp may access
+      const int ra = 32 * (warp & 3) + lane;
+      const int j0 = (gw >> 2) * (TC_J / 4);
       const int64_t blk0 = (int64_t)a.item_block[item] * TC_ROWS;
       float xt[2][3];
 #pragma unroll
@@ -305,48 +377,53 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) xt[h][c] = (float)a.coords[3 * ti + c];
       }
+      const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
       for (uint32_t t = 0; t < T; ++t) {
-        const uint32_t gg = g + t, sb = gg % 3;
-        bool w = mbar_wait_bounded(&fullS[sb], (gg / 3) & 1);
+        const uint32_t gg = g + t, sb = gg % TC_NS;
+        bool w = mbar_wait_bounded(&fullS[sb], (gg / TC_NS) & 1);
         // A buffer gg&1 was last read by MMA group gg-2
-        if (w && gg >= 2) w = mbar_wait_bounded(&mmaDone[gg & 1], ((gg - 2) >> 1) & 1);
+        if (w && gg >= 2) w = mbar_wait_bounded(&mmaDone[(gg - 2) % TC_NB], ((gg - 2) / TC_NB) & 1);
         if (!__all_sync(0xffffffffu, w)) {
           ok = false;
           break;
         }
+        tc_fence_after();
         // padded sources (past n) have zero density rows: their finite values add nothing
         const float* S = reinterpret_cast<const float*>(sm + TC_OFF_S + sb * TC_S_BYTES);
-        unsigned char* A0 = sm + TC_OFF_A + (gg & 1) * 2 * TC_A_BYTES;
-#pragma unroll 2
-        for (int j = j0; j < j0 + TC_J / 4; j += 2) {
-          const float4 a0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
-          const float2 b0 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
-          const float4 a1 = *reinterpret_cast<const float4*>(S + (j + 1) * TC_S_FLOATS);
-          const float2 b1 = *reinterpret_cast<const float2*>(S + (j + 1) * TC_S_FLOATS + 4);
-          const uint32_t o = tc_kmajor_off(ra, 2 * j);
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const float2 k0 = tc_kernel<KIND>(xt[h], a0, b0, kc);
-            const float2 k1 = tc_kernel<KIND>(xt[h], a1, b1, kc);
-            *reinterpret_cast<uint4*>(A0 + h * TC_A_BYTES + o) =
-                make_uint4(to_tf32(k0.x), to_tf32(k0.y), to_tf32(k1.x), to_tf32(k1.y));
+        for (int jq = 0; jq < TC_J / 4; jq += 4) {
+          uint32_t v[2][8];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int j = j0 + jq + e;
+            const float4 s0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
+            const float2 s1 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const float2 kv = tc_kernel<KIND>(xt[h], s0, s1, kc);
+              v[h][2 * e] = tf32_bits(kv.x);
+              v[h][2 * e + 1] = tf32_bits(kv.y);
+            }
           }
+#pragma unroll
+          for (int h = 0; h < 2; ++h) tc_st8(lane_base + tc_a_col(gg & 1, h) + 2 * (j0 + jq), v[h]);
         }
-        fence_proxy_async_smem();
+        tc_wait_st();
+        tc_fence_before();
         __syncwarp();
         if (lane == 0) mbar_arrive(&aFull[gg & 1]);
       }
       if (ok) {
         const uint32_t gl = g + T - 1;
-        ok = __all_sync(0xffffffffu, mbar_wait_bounded(&mmaDone[gl & 1], (gl >> 1) & 1));
+        ok = __all_sync(0xffffffffu, mbar_wait_bounded(&mmaDone[gl % TC_NB], (gl / TC_NB) & 1));
       }
       if (ok) {
         tc_fence_after();
-        // warp w: accumulator (w>>2)&1, TMEM lane quarter w&3, column half w>>3
-        const int acc = (warp >> 2) & 1, half = warp >> 3;
-        const int64_t row_loc = (int64_t)a.item_block[item] * TC_ROWS + acc * 128 + (warp & 3) * 32 + lane;
+        // generator gw: accumulator (gw>>2)&1, TMEM lane quarter warp&3, column half gw>>3
+        const int acc = (gw >> 2) & 1, half = gw >> 3;
+        const int64_t row_loc = blk0 + acc * 128 + ra;
         const bool active = row_loc < n;
-        const uint32_t lane_addr = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + acc * TC_N;
+        const uint32_t lane_addr = lane_base + acc * TC_N;
         const double sc = 1.0 / (4 * kPi);
         const int c0 = cg * TC_R;
         double2* Y = reinterpret_cast<double2*>(a.y);
@@ -381,18 +458,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
   }
   goto done;
 fail:
-  if (control && lane == 0) {
-    atomicExch(a.err, kErrWaitTimeout);
-    // Everything this CTA put in flight must land before it leaves: at most
-    // the last three source copies and the last two density copies are
-    // pending (each alone on its barrier), and one more commit tracks every
-    // MMA issued so far.
-    for (uint32_t q = nS > 3 ? nS - 3 : 0; q < nS; ++q) mbar_wait_bounded(&fullS[q % 3], (q / 3) & 1);
-    for (uint32_t q = nB > 2 ? nB - 2 : 0; q < nB; ++q) mbar_wait_bounded(&fullB[q & 1], (q >> 1) & 1);
-    if (nC > 0) {
+  if (tid == 0) atomicExch(a.err, kErrWaitTimeout);
+  // Everything this CTA put in flight must land before it leaves: at most the
+  // last NS source copies and the last NB density copies are pending (each
+  // alone on its barrier), and one more commit tracks every MMA issued.
+  if (warp == 1 && lane == 0) {
+    for (uint32_t q = nS > TC_NS ? nS - TC_NS : 0; q < nS; ++q) mbar_wait_bounded(&fullS[q % TC_NS], (q / TC_NS) & 1);
+    for (uint32_t q = nB > TC_NB ? nB - TC_NB : 0; q < nB; ++q) mbar_wait_bounded(&fullB[q % TC_NB], (q / TC_NB) & 1);
+  }
+  if (warp == 0) {
+    // the MMAs were issued by the elected lane: the same lane commits
+    if (nC > 0 && elect_one()) {
       tc_commit(&drainBar);
       mbar_wait_bounded(&drainBar, 0);
     }
+    __syncwarp();
   }
   __syncthreads();
 done:
