@@ -219,6 +219,10 @@ int inti_op_grad_sources(inti_op* op, const double* g, const double* sigma, doub
  * on this device, in operations per second (FMA counted as 2 flops). */
 int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops,
                        double* mufu_ops);
+/* Tensor-core throughput (flop/s) of back-to-back tcgen05.mma kind::tf32,
+ * M = N = 128, K = 8, on every SM: the shape the batched kernel issues.
+ * No counterpart in the reference (measurement support for the roofline). */
+int inti_measure_peak_tf32(inti_ctx* ctx, double* tf32_flops);
 
 /* ---- batches: many surfaces, many right-hand sides, one launch ----------
  * The block-diagonal operator diag(A_1 + C_1, ..., A_S + C_S) over S

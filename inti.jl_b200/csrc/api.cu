@@ -702,4 +702,9 @@ int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops, do
   return guarded(ctx, [&] { measure_peaks(ctx, fp64_flops, fp32_flops, mufu_ops); });
 }
 
+int inti_measure_peak_tf32(inti_ctx* ctx, double* tf32_flops) {
+  if (!ctx || !tf32_flops) return INTI_E_ARG;
+  return guarded(ctx, [&] { measure_peak_tf32(ctx, tf32_flops); });
+}
+
 }  // extern "C"

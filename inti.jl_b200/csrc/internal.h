@@ -63,6 +63,7 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
 void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsigma,
                   double* dcoords, double* dnormals, double* dweights, int on_device);
 void measure_peaks(inti_ctx* ctx, double* fp64, double* fp32, double* mufu);
+void measure_peak_tf32(inti_ctx* ctx, double* tf32_flops);
 void selftest_math(inti_ctx* ctx, double* out);
 
 }  // namespace inti

@@ -7,19 +7,22 @@
 // B[2j+1][64+r] = Re x_jr (x already multiplied by the weight w_j), the
 // columns 0..63 of A*B are Re Y and 64..127 are Im Y.
 //
-// One persistent CTA per SM takes work items (surface, block of 256 targets)
-// from an atomic counter, largest surfaces first.  Per stage of 32 sources:
-//   * one control lane copies the source records (FP32 coordinates/normals)
-//     of stage t+2 and the packed density block B of stage t+1 into shared
-//     memory with the TMA bulk engine (cp.async.bulk) completing on mbarriers;
+// One persistent CTA per SM (18 warps) takes work items (surface, block of
+// 256 targets) from an atomic counter, largest surfaces first.  Per stage of
+// 32 sources:
+//   * a producer warp copies the source records (FP32 coordinates/normals)
+//     and the packed density block B of later stages into shared-memory
+//     rings with the TMA bulk engine (cp.async.bulk) completing on mbarriers;
 //   * 16 generator warps evaluate K for their target rows and the 32 sources
-//     on the CUDA cores (FP32; e^{ikd} from the MUFU sine/cosine) and store
-//     them, rounded to TF32, in the canonical K-major no-swizzle layout
-//     (8-row x 16-byte core matrices; LBO = 128 B between K chunks,
-//     SBO = 2048 B between row groups);
-//   * the control lane issues 2 x 8 tcgen05.mma (M = 128, N = 128, K = 8)
-//     into two TMEM accumulators (128 lanes x 128 FP32 columns each) and
-//     commits them to the mbarrier that frees the A and B buffers.
+//     on the CUDA cores (FP32; e^{ikd} from the MUFU sine/cosine), round to
+//     TF32 and store them with tcgen05.st straight into tensor memory, the A
+//     operand of the MMAs (lanes = rows, one 32-bit column per K element);
+//   * an MMA warp issues 2 x 8 tcgen05.mma (M = 128, N = 128, K = 8; A from
+//     tensor memory, B from shared memory in the canonical K-major
+//     no-swizzle layout: 8-row x 16-byte core matrices, LBO = 128 B between
+//     K chunks, SBO = 2048 B between row groups) into two TMEM accumulators
+//     (128 lanes x 128 FP32 columns each) and commits them to the mbarrier
+//     that frees the A and B buffers.
 // Generation of stage t+1 overlaps the MMAs of stage t; the roles meet only
 // at mbarriers, with one CTA barrier per item.  At the end of an item each
 // generator warp reads its lane quarter of the accumulators with tcgen05.ld
@@ -547,6 +550,66 @@ __global__ void tc_pack_density(int nsurf, const int64_t* off, const int64_t* to
   }
   uint32_t* o = out + (((size_t)cg * ntiles + tile) * (TC_B_BYTES / 4)) + tc_kmajor_off(nn, 4 * kc) / 4;
   *reinterpret_cast<uint4*>(o) = make_uint4(v[0], v[1], v[2], v[3]);
+}
+
+// Throughput of the tensor cores for the MMA shape the batch kernel issues
+// (kind::tf32, M = N = 128, K = 8, A in tensor memory, B in shared memory):
+// one CTA per SM issues `rounds` x 8 back-to-back MMAs on zeroed operands.
+__global__ void __launch_bounds__(128, 1) tc_peak_probe(int rounds, int* err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base_sh;
+  for (int i = threadIdx.x; i < TC_B_BYTES / 4; i += blockDim.x) reinterpret_cast<uint32_t*>(sm)[i] = 0;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_sh)),
+                 "r"(TC_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  fence_proxy_async_smem();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  if (threadIdx.x < 32) {
+    const uint64_t bdesc = tc_smem_desc(smem_u32(sm));
+    if (elect_one()) {
+      for (int r = 0; r < rounds; ++r) tc_mma8_ts(tmem, tmem + TC_TMEM_A, bdesc, r > 0 ? 1u : 0u);
+      tc_commit(&bar);
+      if (!mbar_wait_bounded(&bar, 0)) atomicExch(err, kErrWaitTimeout);
+    }
+    __syncwarp();
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_TMEM_COLS));
+  }
+}
+
+void measure_peak_tf32(inti_ctx* ctx, double* tf32_flops) {
+  const int rounds = 8192;  // ~4 ms of MMAs: launch and TMEM allocation costs drop below 1%
+  INTI_CUDA(cudaFuncSetAttribute(tc_peak_probe, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_B_BYTES));
+  cudaEvent_t e0, e1;
+  INTI_CUDA(cudaEventCreate(&e0));
+  INTI_CUDA(cudaEventCreate(&e1));
+  tc_peak_probe<<<ctx->num_sms, 128, TC_B_BYTES, ctx->stream>>>(rounds, ctx->err_flag.as<int>());  // warm-up
+  INTI_CUDA(cudaEventRecord(e0, ctx->stream));
+  tc_peak_probe<<<ctx->num_sms, 128, TC_B_BYTES, ctx->stream>>>(rounds, ctx->err_flag.as<int>());
+  INTI_CUDA(cudaEventRecord(e1, ctx->stream));
+  ctx->launches += 2;
+  INTI_CUDA(cudaEventSynchronize(e1));
+  float ms = 0;
+  INTI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  INTI_CUDA(cudaGetLastError());
+  sync_and_check(ctx);
+  *tf32_flops = 2.0 * 128 * TC_N * 8 * (TC_K / 8) * (double)rounds * ctx->num_sms / (ms * 1e-3);
 }
 
 void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {

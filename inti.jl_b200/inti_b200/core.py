@@ -113,9 +113,10 @@ class Context:
                 "expi_f32_maxabs_25": out[3]}
 
     def measure_peaks(self) -> dict:
-        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        a, b, c, t = C.c_double(), C.c_double(), C.c_double(), C.c_double()
         self.check(self.lib.inti_measure_peaks(self.handle, C.byref(a), C.byref(b), C.byref(c)))
-        return {"fp64_flops": a.value, "fp32_flops": b.value, "mufu_ops": c.value}
+        self.check(self.lib.inti_measure_peak_tf32(self.handle, C.byref(t)))
+        return {"fp64_flops": a.value, "fp32_flops": b.value, "mufu_ops": c.value, "tf32_flops": t.value}
 
 
 _default = None
