@@ -174,7 +174,7 @@ int inti_op_apply_transpose(inti_op* op, const double* x, int64_t ldx, double* y
 int inti_op_assemble(inti_op* op, double* out, int on_device);
 int inti_op_destroy(inti_op* op);
 
-/* ---- BDIM correction on the GPU (src/bdim.jl:50-196, target === source) -- */
+/* ---- BDIM correction on the GPU (src/bdim.jl:50-196) ------------------- */
 /* green_multiplier: n values or NULL for -1/2 (on the surface,
  * src/nystrom.jl:196-207).  derivative = 1 builds the ADL/HS corrections.
  * Outputs two CSR handles (δS, δD) with the element-block pattern of
@@ -182,6 +182,18 @@ int inti_op_destroy(inti_op* op);
 int inti_dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im,
                         const inti_quad* q, int derivative, const double* green_multiplier,
                         inti_csr** dS, inti_csr** dD);
+/* The same for targets other than the source nodes (src/api.jl:105-148 and
+ * bdim.jl:50-196 with etype_to_nearest_points, src/quadrature.jl:264-286):
+ * each target is assigned to the element of its nearest source node (ties to
+ * the lowest node index) when that distance is <= maxdist (INFINITY: every
+ * target); green_multiplier (m values, required) is -1 inside, 0 outside,
+ * -1/2 on the surface (src/nystrom.jl:196-207).  Outputs m x n CSR handles
+ * whose row i holds the nq nodes of target i's element, or nothing.
+ * derivative = 1 needs target normals. */
+int inti_dim_correction_targets(inti_ctx* ctx, int pde, double k_re, double k_im,
+                                const inti_quad* target, const inti_quad* source, int derivative,
+                                const double* green_multiplier, double maxdist, inti_csr** dS,
+                                inti_csr** dD);
 
 /* ---- GMRES on L = shift*I + sum_t coef_t * op_t ------------------------- */
 typedef struct {

@@ -611,6 +611,16 @@ int inti_dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const 
   });
 }
 
+int inti_dim_correction_targets(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
+                                const inti_quad* source, int derivative, const double* green_multiplier,
+                                double maxdist, inti_csr** dS, inti_csr** dD) {
+  if (!ctx || !dS || !dD) return INTI_E_ARG;
+  *dS = *dD = nullptr;
+  return guarded(ctx, [&] {
+    dim_correction_targets(ctx, pde, k_re, k_im, target, source, derivative, green_multiplier, maxdist, dS, dD);
+  });
+}
+
 // ---------------------------------------------------------------- GMRES
 int inti_gmres(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const double* coefs,
                const double* shift, const double* b, double* x, double rtol, int32_t restart,

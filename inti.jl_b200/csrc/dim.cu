@@ -104,9 +104,10 @@ constexpr int kThetaTile = 32;
 
 template <int PDE, int DIM, bool DERIV, int NS>
 __global__ void __launch_bounds__(kThetaBlock) dim_theta(
-    int64_t n, int ns, const double* __restrict__ x, const double* __restrict__ nrm,
-    const double* __restrict__ w, const double2* __restrict__ g0, const double2* __restrict__ g1,
-    double k, int tiles_per_split, double2* __restrict__ partial) {
+    int64_t m, int64_t n, int ns, const double* __restrict__ tx, const double* __restrict__ tn,
+    const double* __restrict__ x, const double* __restrict__ nrm, const double* __restrict__ w,
+    const double2* __restrict__ g0, const double2* __restrict__ g1, double k, int tiles_per_split,
+    double2* __restrict__ partial) {
   constexpr bool CPLX = PDE == HELMHOLTZ;
   using Sc = S<CPLX>;
   using T = typename Sc::T;
@@ -115,12 +116,12 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
   __shared__ double sx[kThetaTile * DIM], sn[kThetaTile * DIM], sw[kThetaTile];
   __shared__ T s0[kThetaTile * NS], s1[kThetaTile * NS];
   const int64_t i = blockIdx.x * (int64_t)kThetaBlock + threadIdx.x;
-  const int64_t ii = min(i, n - 1);
+  const int64_t ii = min(i, m - 1);
   double xi[DIM], ni[DIM];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) {
-    xi[c] = x[DIM * ii + c];
-    ni[c] = nrm[DIM * ii + c];
+    xi[c] = tx[DIM * ii + c];
+    ni[c] = tn ? tn[DIM * ii + c] : 0.0;  // target normals enter ADL/HS only
   }
   T acc[NS];
 #pragma unroll
@@ -158,8 +159,8 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
         acc[q] = Sc::sub(Sc::add(acc[q], Sc::mul(sv, s1[a * NS + q])), Sc::mul(dv, s0[a * NS + q]));
     }
   }
-  if (i < n) {
-    double2* out = partial + ((int64_t)blockIdx.y * n + i) * ns;
+  if (i < m) {
+    double2* out = partial + ((int64_t)blockIdx.y * m + i) * ns;
 #pragma unroll
     for (int q = 0; q < NS; ++q)
       if (q < ns) out[q] = make_double2(Sc::re(acc[q]), Sc::im(acc[q]));
@@ -168,20 +169,21 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
 
 // theta[i,k] = mu_i * B(x_i, xs_k) + sum_s partial[s][i][k]
 template <int PDE, int DIM, bool DERIV>
-__global__ void dim_theta_reduce(int64_t n, int ns, int split, const double* __restrict__ x,
-                                 const double* __restrict__ nrm, const double* __restrict__ xs,
+__global__ void dim_theta_reduce(int64_t m, int ns, int split, const double* __restrict__ tx,
+                                 const double* __restrict__ tn, const double* __restrict__ xs,
                                  const double* __restrict__ mu, double k,
                                  const double2* __restrict__ partial, double2* __restrict__ theta) {
   const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (t >= n * ns) return;
+  if (t >= m * ns) return;
   const int64_t i = t / ns;
   const int kk = (int)(t % ns);
-  const double2 b = kernel_value<PDE, DERIV ? ADL : SL, DIM>(x + DIM * i, nrm + DIM * i,
+  // tn is only read by the ADL value kernel (derivative corrections)
+  const double2 b = kernel_value<PDE, DERIV ? ADL : SL, DIM>(tx + DIM * i, tn ? tn + DIM * i : tx + DIM * i,
                                                              xs + DIM * kk, nullptr, k);
-  const double m = mu ? mu[i] : -0.5;
-  double sr = m * b.x, si = m * b.y;
+  const double mi = mu ? mu[i] : -0.5;
+  double sr = mi * b.x, si = mi * b.y;
   for (int s = 0; s < split; ++s) {
-    const double2 v = partial[(int64_t)s * n * ns + t];
+    const double2 v = partial[(int64_t)s * m * ns + t];
     sr += v.x;
     si += v.y;
   }
@@ -194,59 +196,61 @@ __global__ void dim_theta_reduce(int64_t n, int ns, int split, const double* __r
 // follow the LAPACK xLARFG convention (H = I - tau v v^H, v_k = 1, real beta).
 // ---------------------------------------------------------------------------
 template <bool CPLX, int NQ>
-__global__ void dim_lsq(int64_t nel, int ns, const double2* __restrict__ g0,
-                        const double2* __restrict__ g1, const double2* __restrict__ theta,
-                        double* __restrict__ dS, double* __restrict__ dD) {
+struct ElementLsq {
   using Sc = S<CPLX>;
   using T = typename Sc::T;
-  constexpr int NC = 2 * NQ;
-  const int lane = threadIdx.x & 31;
-  const int64_t e = blockIdx.x * (int64_t)(blockDim.x / 32) + threadIdx.x / 32;
-  if (e >= nel) return;  // whole warp leaves together
-  const bool row = lane < ns;
+  static constexpr int NC = 2 * NQ;
   T A[NC];
-#pragma unroll
-  for (int a = 0; a < NQ; ++a) {
-    const int64_t j = e * NQ + a;
-    A[a] = row ? Sc::from(g0[j * ns + lane]) : Sc::zero();
-    A[NQ + a] = row ? Sc::from(g1[j * ns + lane]) : Sc::zero();
-  }
   T tau[NC];
+  int lane;
+  bool row;
+
+  __device__ __forceinline__ void factor(int64_t e, int ns, const double2* __restrict__ g0,
+                                         const double2* __restrict__ g1) {
+    lane = threadIdx.x & 31;
+    row = lane < ns;
 #pragma unroll
-  for (int kc = 0; kc < NC; ++kc) {
-    // x = A[kc:, kc]; alpha = A[kc][kc]
-    const T alpha = Sc::shfl(A[kc], kc);
-    const double xn2 = warp_sum((row && lane > kc) ? Sc::abs2(A[kc]) : 0.0);
-    if (xn2 == 0.0 && Sc::im(alpha) == 0.0) {
-      tau[kc] = Sc::zero();
-      continue;
+    for (int a = 0; a < NQ; ++a) {
+      const int64_t j = e * NQ + a;
+      A[a] = row ? Sc::from(g0[j * ns + lane]) : Sc::zero();
+      A[NQ + a] = row ? Sc::from(g1[j * ns + lane]) : Sc::zero();
     }
-    const double nrm = sqrt(Sc::abs2(alpha) + xn2);
-    const double beta = Sc::re(alpha) >= 0 ? -nrm : nrm;
-    T tk;
-    if (CPLX) {
-      tk = Sc::from(make_double2((beta - Sc::re(alpha)) / beta, -Sc::im(alpha) / beta));
-    } else {
-      tk = Sc::from(make_double2((beta - Sc::re(alpha)) / beta, 0.0));
-    }
-    tau[kc] = tk;
-    const T ab = Sc::sub(alpha, Sc::from(make_double2(beta, 0.0)));
-    if (lane > kc) A[kc] = Sc::div(A[kc], ab);
-    if (lane == kc) A[kc] = Sc::from(make_double2(beta, 0.0));
-    // trailing columns: s = conj(tau) * (A[kc][j] + sum_{l>kc} conj(v_l) A[l][j])
 #pragma unroll
-    for (int j = kc + 1; j < NC; ++j) {
-      T contrib = (row && lane > kc) ? Sc::cmul(A[kc], A[j]) : Sc::zero();
-      if (lane == kc) contrib = A[j];
-      const T s = Sc::cmul(tk, Sc::wsum(contrib));
-      if (lane == kc) A[j] = Sc::sub(A[j], s);
-      if (row && lane > kc) A[j] = Sc::sub(A[j], Sc::mul(s, A[kc]));
+    for (int kc = 0; kc < NC; ++kc) {
+      // x = A[kc:, kc]; alpha = A[kc][kc]
+      const T alpha = Sc::shfl(A[kc], kc);
+      const double xn2 = warp_sum((row && lane > kc) ? Sc::abs2(A[kc]) : 0.0);
+      if (xn2 == 0.0 && Sc::im(alpha) == 0.0) {
+        tau[kc] = Sc::zero();
+        continue;
+      }
+      const double nrm = sqrt(Sc::abs2(alpha) + xn2);
+      const double beta = Sc::re(alpha) >= 0 ? -nrm : nrm;
+      T tk;
+      if (CPLX) {
+        tk = Sc::from(make_double2((beta - Sc::re(alpha)) / beta, -Sc::im(alpha) / beta));
+      } else {
+        tk = Sc::from(make_double2((beta - Sc::re(alpha)) / beta, 0.0));
+      }
+      tau[kc] = tk;
+      const T ab = Sc::sub(alpha, Sc::from(make_double2(beta, 0.0)));
+      if (lane > kc) A[kc] = Sc::div(A[kc], ab);
+      if (lane == kc) A[kc] = Sc::from(make_double2(beta, 0.0));
+      // trailing columns: s = conj(tau) * (A[kc][j] + sum_{l>kc} conj(v_l) A[l][j])
+#pragma unroll
+      for (int j = kc + 1; j < NC; ++j) {
+        T contrib = (row && lane > kc) ? Sc::cmul(A[kc], A[j]) : Sc::zero();
+        if (lane == kc) contrib = A[j];
+        const T s = Sc::cmul(tk, Sc::wsum(contrib));
+        if (lane == kc) A[j] = Sc::sub(A[j], s);
+        if (row && lane > kc) A[j] = Sc::sub(A[j], Sc::mul(s, A[kc]));
+      }
     }
   }
-  // solve for each of the element's own nodes (targets)
-  for (int t = 0; t < NQ; ++t) {
-    const int64_t i = e * NQ + t;
-    T b = row ? Sc::from(theta[i * ns + lane]) : Sc::zero();
+
+  // Least-squares solution for one Theta row; W is the same in every lane.
+  __device__ __forceinline__ void solve(const double2* __restrict__ theta_row, T* W) const {
+    T b = row ? Sc::from(theta_row[lane]) : Sc::zero();
 #pragma unroll
     for (int kc = 0; kc < NC; ++kc) {
       T contrib = (row && lane > kc) ? Sc::cmul(A[kc], b) : Sc::zero();
@@ -256,7 +260,6 @@ __global__ void dim_lsq(int64_t nel, int ns, const double2* __restrict__ g0,
       if (row && lane > kc) b = Sc::sub(b, Sc::mul(s, A[kc]));
     }
     // back substitution R W = (Q^H b)[0:NC]; lane c holds row c of R
-    T W[NC];
 #pragma unroll
     for (int c = NC - 1; c >= 0; --c) {
       T s = b;
@@ -265,26 +268,69 @@ __global__ void dim_lsq(int64_t nel, int ns, const double2* __restrict__ g0,
       const T wc = Sc::div(s, A[c]);
       W[c] = Sc::shfl(wc, c);
     }
-    if (lane < NQ) {
-      // row i of the CSR holds columns e*NQ .. e*NQ+NQ-1 in order
-      T vS = Sc::zero(), vD = Sc::zero();
+  }
+
+  // dS = -W[NQ + a], dD = W[a] (bdim.jl:176-179) at CSR positions p0 + a
+  __device__ __forceinline__ void store(const T* W, int64_t p0, double* __restrict__ dS,
+                                        double* __restrict__ dD) const {
+    if (lane >= NQ) return;
+    T vS = Sc::zero(), vD = Sc::zero();
 #pragma unroll
-      for (int a = 0; a < NQ; ++a)
-        if (a == lane) {
-          vS = Sc::neg(W[NQ + a]);
-          vD = W[a];
-        }
-      const int64_t p = i * NQ + lane;
-      if (CPLX) {
-        dS[2 * p] = Sc::re(vS);
-        dS[2 * p + 1] = Sc::im(vS);
-        dD[2 * p] = Sc::re(vD);
-        dD[2 * p + 1] = Sc::im(vD);
-      } else {
-        dS[p] = Sc::re(vS);
-        dD[p] = Sc::re(vD);
+    for (int a = 0; a < NQ; ++a)
+      if (a == lane) {
+        vS = Sc::neg(W[NQ + a]);
+        vD = W[a];
       }
+    const int64_t p = p0 + lane;
+    if (CPLX) {
+      dS[2 * p] = Sc::re(vS);
+      dS[2 * p + 1] = Sc::im(vS);
+      dD[2 * p] = Sc::re(vD);
+      dD[2 * p + 1] = Sc::im(vD);
+    } else {
+      dS[p] = Sc::re(vS);
+      dD[p] = Sc::re(vD);
     }
+  }
+};
+
+// target === source: each element solves for its own nq nodes; row i of the
+// CSR holds columns e*NQ .. e*NQ+NQ-1 in order.
+template <bool CPLX, int NQ>
+__global__ void dim_lsq(int64_t nel, int ns, const double2* __restrict__ g0,
+                        const double2* __restrict__ g1, const double2* __restrict__ theta,
+                        double* __restrict__ dS, double* __restrict__ dD) {
+  const int64_t e = blockIdx.x * (int64_t)(blockDim.x / 32) + threadIdx.x / 32;
+  if (e >= nel) return;  // whole warp leaves together
+  ElementLsq<CPLX, NQ> L;
+  L.factor(e, ns, g0, g1);
+  typename ElementLsq<CPLX, NQ>::T W[2 * NQ];
+  for (int t = 0; t < NQ; ++t) {
+    const int64_t i = e * NQ + t;
+    L.solve(theta + i * ns, W);
+    L.store(W, i * NQ, dS, dD);
+  }
+}
+
+// target !== source: element e solves for its near targets etgt[etptr[e] ..
+// etptr[e+1]) (rows of Theta), writing row tgt[j] of the CSR at rowptr.
+template <bool CPLX, int NQ>
+__global__ void dim_lsq_targets(int64_t nel, int ns, const double2* __restrict__ g0,
+                                const double2* __restrict__ g1, const double2* __restrict__ theta,
+                                const int64_t* __restrict__ etptr, const int64_t* __restrict__ etgt,
+                                const int64_t* __restrict__ tgt, const int64_t* __restrict__ rowptr,
+                                double* __restrict__ dS, double* __restrict__ dD) {
+  const int64_t e = blockIdx.x * (int64_t)(blockDim.x / 32) + threadIdx.x / 32;
+  if (e >= nel) return;
+  const int64_t b0 = etptr[e], b1 = etptr[e + 1];
+  if (b0 == b1) return;  // nothing near this element
+  ElementLsq<CPLX, NQ> L;
+  L.factor(e, ns, g0, g1);
+  typename ElementLsq<CPLX, NQ>::T W[2 * NQ];
+  for (int64_t b = b0; b < b1; ++b) {
+    const int64_t j = etgt[b];
+    L.solve(theta + j * ns, W);
+    L.store(W, rowptr[tgt[j]], dS, dD);
   }
 }
 
@@ -295,6 +341,50 @@ __global__ void block_pattern(int64_t n, int nq, int64_t* rowptr, int32_t* col) 
   if (i == n) return;
   const int64_t e = i / nq;
   for (int a = 0; a < nq; ++a) col[i * nq + a] = (int32_t)(e * nq + a);
+}
+
+// Nearest source node of each target (the KDTree nn of
+// src/quadrature.jl:266-270, here exhaustive): squared distances are formed
+// as ((dx*dx + dy*dy) + dz*dz) without contraction, ties go to the lowest
+// index, so the choice is reproducible bit for bit on the host.
+constexpr int kNearBlock = 256;
+template <int DIM>
+__global__ void __launch_bounds__(kNearBlock) nearest_node(int64_t m, const double* __restrict__ tx, int64_t n,
+                                                          const double* __restrict__ x, int64_t* __restrict__ best_j,
+                                                          double* __restrict__ best_d2) {
+  __shared__ double sx[kNearBlock * DIM];
+  const int64_t i = blockIdx.x * (int64_t)kNearBlock + threadIdx.x;
+  const int64_t ii = min(i, m - 1);
+  double xi[DIM];
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) xi[c] = tx[DIM * ii + c];
+  double bd = INFINITY;
+  int64_t bj = -1;
+  for (int64_t t0 = 0; t0 < n; t0 += kNearBlock) {
+    __syncthreads();
+    for (int q = threadIdx.x; q < kNearBlock * DIM; q += kNearBlock) {
+      const int64_t j = t0 + q / DIM;
+      sx[q] = j < n ? x[DIM * t0 + q] : 0.0;
+    }
+    __syncthreads();
+    const int cnt = n - t0 < kNearBlock ? (int)(n - t0) : kNearBlock;
+    for (int a = 0; a < cnt; ++a) {
+      double d2 = 0.0;
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        const double dc = __dsub_rn(xi[c], sx[a * DIM + c]);
+        d2 = c == 0 ? __dmul_rn(dc, dc) : __dadd_rn(d2, __dmul_rn(dc, dc));
+      }
+      if (d2 < bd) {
+        bd = d2;
+        bj = t0 + a;
+      }
+    }
+  }
+  if (i < m) {
+    best_j[i] = bj;
+    best_d2[i] = bd;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -326,12 +416,19 @@ static void nq_dispatch(int nq, F&& f) {
   throw Error(INTI_E_UNSUPPORTED, "DIM correction supports 1..10 nodes per element");
 }
 
-void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
-                    int derivative, const double* green_multiplier, inti_csr** dS,
-                    inti_csr** dD) {
+// Steps 1-3 shared by both forms: monopole centres and traces on the source
+// nodes, then Theta for m targets (coordinates tx, normals tn or NULL, green
+// multipliers mu or NULL for -1/2, all on the device).
+struct DimWork {
+  int ns = 0;
+  DevBuf d_xs, g0, g1, theta, part;
+};
+
+static void dim_source_setup(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
+                             DimWork& wk) {
   if (!q) throw Error(INTI_E_ARG, "quadrature is NULL");
   if (q->ctx != ctx) throw Error(INTI_E_STATE, "quadrature belongs to another context");
-  if (!q->has_normals) throw Error(INTI_E_ARG, "DIM needs a quadrature with normals");
+  if (!q->has_normals) throw Error(INTI_E_ARG, "DIM needs a source quadrature with normals");
   if (q->nq <= 0) throw Error(INTI_E_ARG, "DIM needs the element structure (nq > 0)");
   if (pde != INTI_LAPLACE && pde != INTI_HELMHOLTZ) throw Error(INTI_E_ARG, "unknown pde");
   if (pde == INTI_HELMHOLTZ && q->dim != 3) throw Error(INTI_E_UNSUPPORTED, "Helmholtz is 3D only");
@@ -339,14 +436,9 @@ void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti
   const int dim = q->dim;
   const int64_t n = q->n;
   const int nq = q->nq;
-  const int64_t nel = n / nq;
-  const int ns = (int)std::ceil(3.0 * nq);  // bdim.jl:79-80
+  wk.ns = (int)std::ceil(3.0 * nq);  // bdim.jl:79-80
+  const int ns = wk.ns;
   if (ns > 32) throw Error(INTI_E_UNSUPPORTED, "ns > 32");
-  const bool cplx = pde == INTI_HELMHOLTZ;
-  if (green_multiplier)
-    for (int64_t i = 0; i < n; ++i)
-      if (!std::isfinite(green_multiplier[i])) throw Error(INTI_E_NONFINITE, "green_multiplier contains NaN/Inf");
-
   // 1. monopole centres (bdim.jl:82-92; utils.jl:142-171)
   double lc[3] = {INFINITY, INFINITY, INFINITY}, hc[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (int64_t j = 0; j < n; ++j)
@@ -377,46 +469,62 @@ void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti
       xs[3 * (i - 1) + 2] = std::sin(theta) * radius * R + xc[2];
     }
   }
-  DevBuf d_xs, d_mu, g0, g1, theta, part;
-  d_xs.ensure(sizeof(double) * xs.size());
-  INTI_CUDA(cudaMemcpyAsync(d_xs.p, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice, ctx->stream));
-  if (green_multiplier) {
-    d_mu.ensure(sizeof(double) * n);
-    INTI_CUDA(cudaMemcpyAsync(d_mu.p, green_multiplier, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
-  }
-  g0.ensure(sizeof(double2) * n * ns);
-  g1.ensure(sizeof(double2) * n * ns);
-  theta.ensure(sizeof(double2) * n * ns);
+  wk.d_xs.ensure(sizeof(double) * xs.size());
+  INTI_CUDA(cudaMemcpyAsync(wk.d_xs.p, xs.data(), sizeof(double) * xs.size(), cudaMemcpyHostToDevice, ctx->stream));
+  // 2. traces (bdim.jl:94-103)
+  wk.g0.ensure(sizeof(double2) * n * ns);
+  wk.g1.ensure(sizeof(double2) * n * ns);
+  const int64_t tot = n * ns;
+  auto go = [&](auto pde_c, auto dim_c) {
+    constexpr int P = decltype(pde_c)::value;
+    constexpr int D = decltype(dim_c)::value;
+    dim_traces<P, D><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
+        n, ns, q->coords.as<double>(), q->normals.as<double>(), wk.d_xs.as<double>(), k_re, wk.g0.as<double2>(),
+        wk.g1.as<double2>());
+    ctx->launches++;
+  };
+  if (pde == INTI_LAPLACE && dim == 2)
+    go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, 2>());
+  else if (pde == INTI_LAPLACE)
+    go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, 3>());
+  else
+    go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, 3>());
+  INTI_CUDA(cudaGetLastError());
+}
+
+// 3. Theta = mu*B(x) + S*g1 - D*g0 over all source nodes (bdim.jl:104-118)
+static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* q, int derivative, int64_t m,
+                          const double* tx, const double* tn, const double* mu, DimWork& wk) {
+  const int dim = q->dim;
+  const int64_t n = q->n;
+  const int ns = wk.ns;
+  wk.theta.ensure(sizeof(double2) * std::max<int64_t>(m, 1) * ns);
+  if (m == 0) return;
   const double* X = q->coords.as<double>();
   const double* NR = q->normals.as<double>();
   const double* W = q->weights.as<double>();
-
   auto run = [&](auto pde_c, auto dim_c) {
     constexpr int P = decltype(pde_c)::value;
     constexpr int D = decltype(dim_c)::value;
-    const int64_t tot = n * ns;
-    dim_traces<P, D><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
-        n, ns, X, NR, d_xs.as<double>(), k_re, g0.as<double2>(), g1.as<double2>());
-    ctx->launches++;
-    // Theta split over sources so the grid covers the device
-    const int64_t blocks = (n + kThetaBlock - 1) / kThetaBlock;
+    // split over sources so the grid covers the device
+    const int64_t blocks = (m + kThetaBlock - 1) / kThetaBlock;
     const int64_t ntile = (n + kThetaTile - 1) / kThetaTile;
     const int64_t want = (int64_t)ctx->num_sms * 6;
     int split = (int)std::max<int64_t>(1, std::min<int64_t>({ntile, (want + blocks - 1) / blocks, 64}));
     const int tps = (int)((ntile + split - 1) / split);
     split = (int)((ntile + tps - 1) / tps);
-    part.ensure(sizeof(double2) * (size_t)split * n * ns);
+    wk.part.ensure(sizeof(double2) * (size_t)split * m * ns);
+    const int64_t tot = m * ns;
     auto theta_go = [&](auto nsb, auto deriv_c) {
       constexpr int NSB = decltype(nsb)::value;
       constexpr bool DV = decltype(deriv_c)::value;
       dim3 grid((unsigned)blocks, (unsigned)split);
       ProfScope pd(ctx, "dim");
       dim_theta<P, D, DV, NSB><<<grid, kThetaBlock, 0, ctx->stream>>>(
-          n, ns, X, NR, W, g0.as<double2>(), g1.as<double2>(), k_re, tps, part.as<double2>());
+          m, n, ns, tx, tn, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re, tps, wk.part.as<double2>());
       ctx->launches++;
       dim_theta_reduce<P, D, DV><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
-          n, ns, split, X, NR, d_xs.as<double>(), green_multiplier ? d_mu.as<double>() : nullptr,
-          k_re, part.as<double2>(), theta.as<double2>());
+          m, ns, split, tx, tn, wk.d_xs.as<double>(), mu, k_re, wk.part.as<double2>(), wk.theta.as<double2>());
       ctx->launches++;
     };
     auto by_ns = [&](auto deriv_c) {
@@ -437,21 +545,43 @@ void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti
   else
     run(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, 3>());
   INTI_CUDA(cudaGetLastError());
+}
 
-  // output CSR handles with the element-block pattern
-  const int comps = cplx ? 2 : 1;
-  const int64_t nnz = n * nq;
-  std::unique_ptr<inti_csr> cS(new inti_csr()), cD(new inti_csr());
-  for (auto* c : {cS.get(), cD.get()}) {
-    c->ctx = ctx;
-    c->m = n;
-    c->n = n;
-    c->nnz = nnz;
-    c->dtype = cplx ? INTI_C128 : INTI_F64;
-    c->rowptr.ensure(sizeof(int64_t) * (n + 1));
-    c->col.ensure(sizeof(int32_t) * nnz);
-    c->val.ensure(sizeof(double) * comps * nnz);
+static std::unique_ptr<inti_csr> new_csr(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz, bool cplx) {
+  std::unique_ptr<inti_csr> c(new inti_csr());
+  c->ctx = ctx;
+  c->m = m;
+  c->n = n;
+  c->nnz = nnz;
+  c->dtype = cplx ? INTI_C128 : INTI_F64;
+  c->rowptr.ensure(sizeof(int64_t) * (m + 1));
+  c->col.ensure(sizeof(int32_t) * std::max<int64_t>(nnz, 1));
+  c->val.ensure(sizeof(double) * (cplx ? 2 : 1) * std::max<int64_t>(nnz, 1));
+  return c;
+}
+
+void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
+                    int derivative, const double* green_multiplier, inti_csr** dS,
+                    inti_csr** dD) {
+  DimWork wk;
+  dim_source_setup(ctx, pde, k_re, k_im, q, wk);
+  const int64_t n = q->n;
+  const int nq = q->nq;
+  const int64_t nel = n / nq;
+  const int ns = wk.ns;
+  const bool cplx = pde == INTI_HELMHOLTZ;
+  DevBuf d_mu;
+  if (green_multiplier) {
+    for (int64_t i = 0; i < n; ++i)
+      if (!std::isfinite(green_multiplier[i])) throw Error(INTI_E_NONFINITE, "green_multiplier contains NaN/Inf");
+    d_mu.ensure(sizeof(double) * n);
+    INTI_CUDA(cudaMemcpyAsync(d_mu.p, green_multiplier, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream));
   }
+  dim_theta_run(ctx, pde, k_re, q, derivative, n, q->coords.as<double>(), q->normals.as<double>(),
+                green_multiplier ? d_mu.as<double>() : nullptr, wk);
+  // output CSR handles with the element-block pattern
+  const int64_t nnz = n * nq;
+  auto cS = new_csr(ctx, n, n, nnz, cplx), cD = new_csr(ctx, n, n, nnz, cplx);
   block_pattern<<<(unsigned)((n + 1 + 255) / 256), 256, 0, ctx->stream>>>(n, nq, cS->rowptr.as<int64_t>(), cS->col.as<int32_t>());
   ctx->launches++;
   INTI_CUDA(cudaMemcpyAsync(cD->rowptr.p, cS->rowptr.p, sizeof(int64_t) * (n + 1), cudaMemcpyDeviceToDevice, ctx->stream));
@@ -461,13 +591,128 @@ void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti
     const int warps = 4;
     const unsigned grid = (unsigned)((nel + warps - 1) / warps);
     if (cplx)
-      dim_lsq<true, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(nel, ns, g0.as<double2>(), g1.as<double2>(),
-                                                              theta.as<double2>(), cS->val.as<double>(), cD->val.as<double>());
+      dim_lsq<true, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(nel, ns, wk.g0.as<double2>(), wk.g1.as<double2>(),
+                                                              wk.theta.as<double2>(), cS->val.as<double>(), cD->val.as<double>());
     else
-      dim_lsq<false, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(nel, ns, g0.as<double2>(), g1.as<double2>(),
-                                                               theta.as<double2>(), cS->val.as<double>(), cD->val.as<double>());
+      dim_lsq<false, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(nel, ns, wk.g0.as<double2>(), wk.g1.as<double2>(),
+                                                               wk.theta.as<double2>(), cS->val.as<double>(), cD->val.as<double>());
     ctx->launches++;
   });
+  INTI_CUDA(cudaGetLastError());
+  sync_and_check(ctx);
+  *dS = cS.release();
+  *dD = cD.release();
+}
+
+void dim_correction_targets(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
+                            const inti_quad* q, int derivative, const double* green_multiplier, double maxdist,
+                            inti_csr** dS, inti_csr** dD) {
+  if (!target) throw Error(INTI_E_ARG, "target is NULL");
+  if (target->ctx != ctx) throw Error(INTI_E_STATE, "target belongs to another context");
+  if (!green_multiplier) throw Error(INTI_E_ARG, "off-surface targets need a green multiplier per target");
+  if (std::isnan(maxdist) || maxdist < 0) throw Error(INTI_E_ARG, "maxdist must be >= 0");
+  DimWork wk;
+  dim_source_setup(ctx, pde, k_re, k_im, q, wk);
+  if (target->dim != q->dim) throw Error(INTI_E_SHAPE, "target and source dimensions differ");
+  if (derivative && !target->has_normals) throw Error(INTI_E_ARG, "derivative corrections need target normals");
+  const int dim = q->dim;
+  const int64_t m = target->n, n = q->n;
+  const int nq = q->nq;
+  const int64_t nel = n / nq;
+  const int ns = wk.ns;
+  const bool cplx = pde == INTI_HELMHOLTZ;
+  for (int64_t i = 0; i < m; ++i)
+    if (!std::isfinite(green_multiplier[i])) throw Error(INTI_E_NONFINITE, "green_multiplier contains NaN/Inf");
+
+  // near lists (quadrature.jl:264-286): nearest source node of each target
+  std::vector<int64_t> best(m);
+  std::vector<double> bd2(m);
+  if (m > 0) {
+    DevBuf d_best, d_bd2;
+    d_best.ensure(sizeof(int64_t) * m);
+    d_bd2.ensure(sizeof(double) * m);
+    auto go = [&](auto dim_c) {
+      constexpr int D = decltype(dim_c)::value;
+      nearest_node<D><<<(unsigned)((m + kNearBlock - 1) / kNearBlock), kNearBlock, 0, ctx->stream>>>(
+          m, target->coords.as<double>(), n, q->coords.as<double>(), d_best.as<int64_t>(), d_bd2.as<double>());
+    };
+    if (dim == 2)
+      go(std::integral_constant<int, 2>());
+    else
+      go(std::integral_constant<int, 3>());
+    ctx->launches++;
+    INTI_CUDA(cudaGetLastError());
+    INTI_CUDA(cudaMemcpyAsync(best.data(), d_best.p, sizeof(int64_t) * m, cudaMemcpyDeviceToHost, ctx->stream));
+    INTI_CUDA(cudaMemcpyAsync(bd2.data(), d_bd2.p, sizeof(double) * m, cudaMemcpyDeviceToHost, ctx->stream));
+    sync_and_check(ctx);
+  }
+  // near targets (compact order j), element lists, output row pointers
+  std::vector<int64_t> tgt, elem_of, etptr(nel + 1, 0), rowptr(m + 1, 0);
+  for (int64_t i = 0; i < m; ++i) {
+    const bool near = best[i] >= 0 && !(std::sqrt(bd2[i]) > maxdist);
+    rowptr[i + 1] = rowptr[i] + (near ? nq : 0);
+    if (near) {
+      tgt.push_back(i);
+      elem_of.push_back(best[i] / nq);
+      ++etptr[best[i] / nq + 1];
+    }
+  }
+  const int64_t mn = (int64_t)tgt.size();
+  for (int64_t e = 0; e < nel; ++e) etptr[e + 1] += etptr[e];
+  std::vector<int64_t> etgt(std::max<int64_t>(mn, 1)), fill(etptr.begin(), etptr.end() - 1);
+  for (int64_t j = 0; j < mn; ++j) etgt[fill[elem_of[j]]++] = j;
+  // gathered near-target data for Theta
+  std::vector<double> htx((size_t)std::max<int64_t>(mn, 1) * dim), htn, hmu(std::max<int64_t>(mn, 1));
+  if (derivative) htn.resize(htx.size());
+  for (int64_t j = 0; j < mn; ++j) {
+    const int64_t i = tgt[j];
+    for (int c = 0; c < dim; ++c) {
+      htx[dim * j + c] = target->h_coords[dim * i + c];
+      if (derivative) htn[dim * j + c] = target->h_normals[dim * i + c];
+    }
+    hmu[j] = green_multiplier[i];
+  }
+  DevBuf d_tx, d_tn, d_mu, d_etptr, d_etgt, d_tgt, d_rowptr;
+  auto up = [&](DevBuf& b, const void* h, size_t bytes) {
+    b.ensure(std::max<size_t>(bytes, 16));
+    if (bytes) INTI_CUDA(cudaMemcpyAsync(b.p, h, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  };
+  up(d_tx, htx.data(), sizeof(double) * dim * mn);
+  if (derivative) up(d_tn, htn.data(), sizeof(double) * dim * mn);
+  up(d_mu, hmu.data(), sizeof(double) * mn);
+  up(d_etptr, etptr.data(), sizeof(int64_t) * (nel + 1));
+  up(d_etgt, etgt.data(), sizeof(int64_t) * mn);
+  up(d_tgt, tgt.data(), sizeof(int64_t) * mn);
+  dim_theta_run(ctx, pde, k_re, q, derivative, mn, d_tx.as<double>(), derivative ? d_tn.as<double>() : nullptr,
+                d_mu.as<double>(), wk);
+  // output CSR: row i holds the nq nodes of its element (sorted), or nothing
+  const int64_t nnz = mn * nq;
+  std::vector<int32_t> col((size_t)std::max<int64_t>(nnz, 1));
+  for (int64_t j = 0; j < mn; ++j)
+    for (int a = 0; a < nq; ++a) col[(size_t)j * nq + a] = (int32_t)(elem_of[j] * nq + a);
+  auto cS = new_csr(ctx, m, n, nnz, cplx), cD = new_csr(ctx, m, n, nnz, cplx);
+  for (auto* c : {cS.get(), cD.get()}) {
+    INTI_CUDA(cudaMemcpyAsync(c->rowptr.p, rowptr.data(), sizeof(int64_t) * (m + 1), cudaMemcpyHostToDevice, ctx->stream));
+    if (nnz) INTI_CUDA(cudaMemcpyAsync(c->col.p, col.data(), sizeof(int32_t) * nnz, cudaMemcpyHostToDevice, ctx->stream));
+  }
+  if (mn > 0)
+    nq_dispatch(nq, [&](auto nqc) {
+      constexpr int NQ = decltype(nqc)::value;
+      const int warps = 4;
+      const unsigned grid = (unsigned)((nel + warps - 1) / warps);
+      auto go = [&](auto cplx_c) {
+        constexpr bool CP = decltype(cplx_c)::value;
+        dim_lsq_targets<CP, NQ><<<grid, 32 * warps, 0, ctx->stream>>>(
+            nel, ns, wk.g0.as<double2>(), wk.g1.as<double2>(), wk.theta.as<double2>(), d_etptr.as<int64_t>(),
+            d_etgt.as<int64_t>(), d_tgt.as<int64_t>(), cS->rowptr.as<int64_t>(), cS->val.as<double>(),
+            cD->val.as<double>());
+      };
+      if (cplx)
+        go(std::true_type());
+      else
+        go(std::false_type());
+      ctx->launches++;
+    });
   INTI_CUDA(cudaGetLastError());
   sync_and_check(ctx);
   *dS = cS.release();

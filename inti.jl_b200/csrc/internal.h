@@ -53,6 +53,9 @@ inti_csr* csr_create_host(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz,
                           int dtype);
 std::unique_ptr<inti_csr> csr_transpose(inti_ctx* ctx, const inti_csr* c);
 
+void dim_correction_targets(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
+                            const inti_quad* q, int derivative, const double* green_multiplier, double maxdist,
+                            inti_csr** dS, inti_csr** dD);
 void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
                     int derivative, const double* green_multiplier, inti_csr** dS,
                     inti_csr** dD);

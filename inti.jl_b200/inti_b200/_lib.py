@@ -115,6 +115,8 @@ SIGNATURES = {
     "inti_op_assemble": (C.c_int, [P, P, C.c_int]),
     "inti_op_destroy": (C.c_int, [P]),
     "inti_dim_correction": (C.c_int, [P, C.c_int, C.c_double, C.c_double, P, C.c_int, P, PP, PP]),
+    "inti_dim_correction_targets": (C.c_int, [P, C.c_int, C.c_double, C.c_double, P, P, C.c_int, P, C.c_double,
+                                              PP, PP]),
     "inti_gmres": (C.c_int, [P, C.c_int32, PP, D, D, P, P, C.c_double, C.c_int32, C.c_int32,
                              C.c_int32, C.c_int, P, C.POINTER(GmresStats)]),
     "inti_op_grad_sources": (C.c_int, [P, P, P, P, P, P, P, C.c_int]),

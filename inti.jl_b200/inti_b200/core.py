@@ -13,7 +13,8 @@ Names, argument meaning and error behaviour follow the reference:
   and ``correction=dict(method="dim"|"none")``; the result is ``S = A + δS``,
   a lazy map like ``LinearMap(Smat) + LinearMap(δS)`` (src/api.jl:179-184)
   whose apply runs the pair kernel and the CSR correction in one pass;
-* ``bdim_correction`` (src/bdim.jl:50-196, target === source) built on the GPU;
+* ``bdim_correction`` (src/bdim.jl:50-196) built on the GPU, on the surface
+  (target === source) or for other targets near it (src/api.jl:105-148);
 * ``single_double_layer_potential`` / ``IntegralPotential`` (src/api.jl:220-226,
   src/nystrom.jl:20-38);
 * ``gmres`` for ``shift·I + Σ c_t·op_t`` (the IterativeSolvers call of
@@ -27,6 +28,7 @@ from __future__ import annotations
 import ctypes as C
 import numbers
 import threading
+import warnings
 import weakref
 
 import numpy as np
@@ -665,21 +667,31 @@ def assemble_matrix(iop: GpuOperator) -> np.ndarray:
 # correction and the high-level constructors
 # ----------------------------------------------------------------------------
 def bdim_correction(op, target: Quadrature, source: Quadrature, *, green_multiplier=None,
-                    derivative: bool = False, ctx: Context | None = None):
+                    derivative: bool = False, maxdist: float = float("inf"), ctx: Context | None = None):
     """``(δS, δD)`` of the density-interpolation method (src/bdim.jl:50-196),
-    built on the GPU.  Only ``target is source`` is supported: each element
-    corrects its own nodes (src/quadrature.jl:250-256)."""
+    built on the GPU.  With ``target is source`` each element corrects its own
+    nodes (src/quadrature.jl:250-256) and the multiplier defaults to -1/2.
+    Otherwise every target within ``maxdist`` of its nearest source node is
+    corrected through that node's element (src/quadrature.jl:264-286), and
+    ``green_multiplier`` (a scalar or one value per target) is required."""
     ctx = ctx or default_context()
-    if target is not source:
-        raise L.UnsupportedError(L.E_UNSUPPORTED, "bdim_correction on the GPU requires target === source")
-    h = _quad_handle(source, ctx)
-    gm = None
-    if green_multiplier is not None:
-        gm = np.ascontiguousarray(np.broadcast_to(np.asarray(green_multiplier, float), (len(source),)))
+    hsrc = _quad_handle(source, ctx)
     hs, hd = C.c_void_p(), C.c_void_p()
     k = complex(getattr(op, "k", 0.0))
-    ctx.check(ctx.lib.inti_dim_correction(ctx.handle, op.pde, k.real, k.imag, h, int(bool(derivative)),
-                                          L.dptr(gm), C.byref(hs), C.byref(hd)))
+    if target is source:
+        gm = None
+        if green_multiplier is not None:
+            gm = np.ascontiguousarray(np.broadcast_to(np.asarray(green_multiplier, float), (len(source),)))
+        ctx.check(ctx.lib.inti_dim_correction(ctx.handle, op.pde, k.real, k.imag, hsrc, int(bool(derivative)),
+                                              L.dptr(gm), C.byref(hs), C.byref(hd)))
+    else:
+        if green_multiplier is None:
+            raise L.ArgumentError(L.E_ARG, "off-surface targets need a green multiplier")
+        gm = np.ascontiguousarray(np.broadcast_to(np.asarray(green_multiplier, float), (len(target),)))
+        htgt = _quad_handle(target, ctx)
+        ctx.check(ctx.lib.inti_dim_correction_targets(ctx.handle, op.pde, k.real, k.imag, htgt, hsrc,
+                                                      int(bool(derivative)), L.dptr(gm), float(maxdist),
+                                                      C.byref(hs), C.byref(hd)))
     return CorrectionMatrix(hs, ctx), CorrectionMatrix(hd, ctx)
 
 
@@ -705,10 +717,15 @@ def _normalize_correction(correction, target, source):
             L.E_ARG, f"Unknown correction.method {method}. Available options: {CORRECTION_METHODS}")
     correction["method"] = method
     if method == "dim":
-        if "target_location" in correction and "green_multiplier" in correction:
-            raise L.ArgumentError(L.E_ARG, "conflicting target_location and green_multiplier fields in correction")
+        if "target_location" in correction and target is source and \
+                str(correction["target_location"]).lstrip(":") != "on":
+            warnings.warn("ignoring target_location field in correction since target === source")
         if target is not source and "target_location" not in correction and "green_multiplier" not in correction:
             raise L.ArgumentError(L.E_ARG, "missing target_location field in correction")
+        if "target_location" in correction and "green_multiplier" in correction:
+            raise L.ArgumentError(L.E_ARG, "conflicting target_location and green_multiplier fields in correction")
+        if "maxdist" not in correction and target is not source:
+            warnings.warn("missing maxdist field in correction: setting to Inf")
         correction.setdefault("maxdist", float("inf"))
     return correction
 
@@ -745,7 +762,8 @@ def single_double_layer(*, op, target: Quadrature, source: Quadrature, compressi
         else:
             loc = "on" if target is source else correction["target_location"]
             gm = _green_multiplier(loc)
-        dS, dD = bdim_correction(op, target, source, green_multiplier=gm, derivative=derivative, ctx=ctx)
+        dS, dD = bdim_correction(op, target, source, green_multiplier=gm, derivative=derivative,
+                                 maxdist=correction["maxdist"], ctx=ctx)
     S = GpuOperator(G, target, source, dS, prec, ctx)
     D = GpuOperator(dG, target, source, dD, prec, ctx)
     return S, D

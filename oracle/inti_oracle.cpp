@@ -501,6 +501,144 @@ static int bdim_impl(int pde, int dim, double k, int64_t n, const double* x, con
   return 0;
 }
 
+// --------------------------------------------------------------------------
+// BDIM correction with targets other than the source nodes (src/api.jl:105-148
+// with bdim.jl:50-196; the near list of etype_to_nearest_points,
+// src/quadrature.jl:264-286).  Each target goes to the element of its nearest
+// source node (KDTree nn in the reference; here an exhaustive search with
+// squared distances ((dx*dx + dy*dy) + dz*dz), ties to the lowest index) when
+// that distance is <= maxdist.  Theta uses the uncorrected operators from the
+// near targets to all source nodes; each element with near targets is
+// factored once and solved for every one of them.
+// --------------------------------------------------------------------------
+template <class T>
+static int bdim_targets_impl(int pde, int dim, double k, int64_t m, const double* tx, const double* tn,
+                             int64_t n, const double* x, const double* nrm, const double* w, int nq,
+                             int derivative, const double* green_mult, double maxdist,
+                             int64_t* near_elem, T* dS, T* dD, double* theta_out, int nt) {
+  const int ns = (int)std::ceil(3.0 * nq);
+  double lc[3] = {INFINITY, INFINITY, INFINITY}, hc[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (int64_t j = 0; j < n; ++j)
+    for (int c = 0; c < dim; ++c) {
+      lc[c] = std::min(lc[c], x[dim * j + c]);
+      hc[c] = std::max(hc[c], x[dim * j + c]);
+    }
+  double xc[3], diag2 = 0.0;
+  for (int c = 0; c < dim; ++c) {
+    xc[c] = (lc[c] + hc[c]) / 2;
+    diag2 += (hc[c] - lc[c]) * (hc[c] - lc[c]);
+  }
+  const double R = 1.5 * std::sqrt(diag2) / 2;
+  std::vector<double> xs((size_t)ns * dim);
+  or_dim_sources(dim, ns, R, xc, xs.data());
+  const int kG = derivative ? OR_ADL : OR_SL;
+  const int kS = derivative ? OR_ADL : OR_SL;
+  const int kD = derivative ? OR_HS : OR_DL;
+  std::vector<T> g0((size_t)n * ns), g1((size_t)n * ns);
+  parallel_for(n, nt, 64, [&](int64_t j) {
+    for (int kk = 0; kk < ns; ++kk) {
+      g0[(size_t)j * ns + kk] = kval<T>(pde, OR_SL, dim, k, x + dim * j, nrm + dim * j, &xs[dim * kk], nullptr);
+      g1[(size_t)j * ns + kk] = kval<T>(pde, OR_ADL, dim, k, x + dim * j, nrm + dim * j, &xs[dim * kk], nullptr);
+    }
+  });
+  // near lists (quadrature.jl:264-286)
+  parallel_for(m, nt, 16, [&](int64_t i) {
+    double best = INFINITY;
+    int64_t bj = -1;
+    for (int64_t j = 0; j < n; ++j) {
+      double d2 = 0.0;
+      for (int c = 0; c < dim; ++c) {
+        const double dc = tx[dim * i + c] - x[dim * j + c];
+        d2 = c == 0 ? dc * dc : d2 + dc * dc;
+      }
+      if (d2 < best) {
+        best = d2;
+        bj = j;
+      }
+    }
+    near_elem[i] = (bj >= 0 && !(std::sqrt(best) > maxdist)) ? bj / nq : -1;
+  });
+  std::vector<std::vector<int64_t>> elem_targets((size_t)(n / nq));
+  for (int64_t i = 0; i < m; ++i)
+    if (near_elem[i] >= 0) elem_targets[(size_t)near_elem[i]].push_back(i);
+  // Theta rows of the near targets (bdim.jl:104-118)
+  std::vector<T> theta((size_t)m * ns, T(0));
+  parallel_for(m, nt, 2, [&](int64_t i) {
+    if (near_elem[i] < 0) return;
+    const double* xi = tx + dim * i;
+    const double* ni = tn ? tn + dim * i : nullptr;
+    const double mu = green_mult[i];
+    std::vector<T> acc(ns), accS(ns, T(0)), accD(ns, T(0));
+    for (int kk = 0; kk < ns; ++kk) acc[kk] = mu * kval<T>(pde, kG, dim, k, xi, ni, &xs[dim * kk], nullptr);
+    for (int64_t j = 0; j < n; ++j) {
+      const T sv = kval<T>(pde, kS, dim, k, xi, ni, x + dim * j, nrm + dim * j) * w[j];
+      const T dv = kval<T>(pde, kD, dim, k, xi, ni, x + dim * j, nrm + dim * j) * w[j];
+      const T* g1j = &g1[(size_t)j * ns];
+      const T* g0j = &g0[(size_t)j * ns];
+      for (int kk = 0; kk < ns; ++kk) {
+        accS[kk] += sv * g1j[kk];
+        accD[kk] += dv * g0j[kk];
+      }
+    }
+    for (int kk = 0; kk < ns; ++kk) theta[(size_t)i * ns + kk] = (acc[kk] + accS[kk]) - accD[kk];
+  });
+  if (theta_out)
+    for (size_t q = 0; q < theta.size(); ++q) {
+      theta_out[2 * q] = realv(theta[q]);
+      theta_out[2 * q + 1] = imagv(theta[q]);
+    }
+  // per element: factor once, solve for each near target (bdim.jl:154-185)
+  parallel_for(n / nq, nt, 4, [&](int64_t e) {
+    const auto& targets = elem_targets[(size_t)e];
+    if (targets.empty()) return;
+    HouseholderQR<T> F;
+    F.rows = ns;
+    F.cols = 2 * nq;
+    F.a.assign((size_t)ns * 2 * nq, T(0));
+    for (int a = 0; a < nq; ++a) {
+      const int64_t j = e * nq + a;
+      for (int kk = 0; kk < ns; ++kk) {
+        F.a[(size_t)a * ns + kk] = g0[(size_t)j * ns + kk];
+        F.a[(size_t)(nq + a) * ns + kk] = g1[(size_t)j * ns + kk];
+      }
+    }
+    F.factor();
+    std::vector<T> b(ns), W(2 * nq);
+    for (int64_t i : targets) {
+      for (int kk = 0; kk < ns; ++kk) b[kk] = theta[(size_t)i * ns + kk];
+      F.solve(b.data(), W.data());
+      for (int a = 0; a < nq; ++a) {
+        dS[(size_t)i * nq + a] = -W[nq + a];
+        dD[(size_t)i * nq + a] = W[a];
+      }
+    }
+  });
+  return 0;
+}
+
+extern "C" {
+
+// Off-surface DIM: near_elem[i] = element of target i's nearest source node
+// (-1 if beyond maxdist); row i of dS/dD (m x nq, interleaved complex for
+// Helmholtz) holds the corrections to source nodes near_elem*nq + a.
+// tn (target normals) is needed when derivative != 0.
+int or_bdim_targets(int pde, int dim, double k, int64_t m, const double* tx, const double* tn, int64_t n,
+                    const double* x, const double* nrm, const double* w, int nq, int derivative,
+                    const double* green_mult, double maxdist, int64_t* near_elem, double* dS, double* dD,
+                    double* theta_out, int nthreads) {
+  if (n % nq) return 2;
+  if (derivative && !tn) return 3;
+  if (pde == OR_LAPLACE)
+    return bdim_targets_impl<double>(pde, dim, k, m, tx, tn, n, x, nrm, w, nq, derivative, green_mult, maxdist,
+                                     near_elem, dS, dD, theta_out, nthreads);
+  if (dim != 3) return 1;
+  return bdim_targets_impl<cd>(pde, dim, k, m, tx, tn, n, x, nrm, w, nq, derivative, green_mult, maxdist,
+                               near_elem, reinterpret_cast<cd*>(dS), reinterpret_cast<cd*>(dD), theta_out,
+                               nthreads);
+}
+
+}  // extern "C"
+
 extern "C" {
 
 // Block values of the DIM correction for the selected elements (all when

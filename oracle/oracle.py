@@ -52,6 +52,8 @@ def lib() -> C.CDLL:
         _lib.or_gmres.argtypes = [C.c_int, C.c_int, D, I64, P, P, P, D, D, C.c_int, P, P, P, P, P, P, P, D,
                                   C.c_int, C.c_int, C.c_int, P, P, C.c_int]
         _lib.or_dim_traces.argtypes = [C.c_int, C.c_int, D, I64, P, P, C.c_int, P, P]
+        _lib.or_bdim_targets.argtypes = [C.c_int, C.c_int, D, I64, P, P, I64, P, P, P, C.c_int, C.c_int, P, D,
+                                         P, P, P, P, C.c_int]
         _lib.or_dl_potential_jvp.argtypes = [I64, P, I64, P, P, P, P, P, P, P, P, P, P, C.c_int]
     return _lib
 
@@ -174,6 +176,41 @@ def bdim(pde, k, coords, normals, weights, nq, derivative=False, green_multiplie
     if st:
         raise ValueError(f"or_bdim failed ({st})")
     return (dS, dD, theta) if return_theta else (dS, dD)
+
+
+def bdim_targets(pde, k, tcoords, scoords, snormals, sweights, nq, green_multiplier, maxdist=np.inf,
+                 derivative=False, tnormals=None, nthreads=0, return_theta=False):
+    """Off-surface DIM (target !== source): (near_elem, dS, dD[, theta]) with
+    near_elem[i] the element of target i's nearest source node (-1 beyond
+    maxdist) and rows (m, nq) of corrections to that element's nodes."""
+    tx, x, nrm, w = _c(tcoords), _c(scoords), _c(snormals), _c(sweights)
+    tn = _c(tnormals)
+    m, dim = tx.shape
+    n = x.shape[0]
+    cplx = pde == HELMHOLTZ
+    dt = np.complex128 if cplx else np.float64
+    near = np.full(m, -1, np.int64)
+    dS = np.zeros((m, nq), dt)
+    dD = np.zeros((m, nq), dt)
+    ns = int(np.ceil(3 * nq))
+    theta = np.zeros((m, ns), np.complex128) if return_theta else None
+    gm = _c(np.broadcast_to(np.asarray(green_multiplier, dtype=np.float64), (m,)))
+    st = lib().or_bdim_targets(pde, dim, k, m, _p(tx), _p(tn), n, _p(x), _p(nrm), _p(w), nq, int(derivative),
+                               _p(gm), float(maxdist), _p(near), _p(dS), _p(dD), _p(theta), nthreads)
+    if st:
+        raise ValueError(f"or_bdim_targets failed ({st})")
+    return (near, dS, dD, theta) if return_theta else (near, dS, dD)
+
+
+def targets_csr(near, values, nq, n):
+    """CSR (indptr, indices, data) of off-surface DIM rows from bdim_targets."""
+    m = len(near)
+    counts = np.where(near >= 0, nq, 0)
+    indptr = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    rows = np.nonzero(near >= 0)[0]
+    indices = (near[rows][:, None] * nq + np.arange(nq)[None, :]).reshape(-1).astype(np.int32)
+    data = values[rows].reshape(-1)
+    return indptr, indices, data
 
 
 def block_csr(values, nq, elements=None, n=None):

@@ -25,7 +25,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from helpers import density, oracle_dim_csr, relerr
+from helpers import density, harmonic_traces, oracle_dim_csr, relerr
 from inti_b200 import geometry as G
 
 
@@ -227,3 +227,70 @@ def test_dual_number_jvp_matches_finite_differences():
     um = O.apply(O.LAPLACE, O.DL, 0.0, tgt, None, q.coords - h * dsx, q.normals, q.weights, sigma)
     assert relerr(du, (up - um) / (2 * h)) < 1e-7
     assert relerr(u, O.apply(O.LAPLACE, O.DL, 0.0, tgt, None, q.coords, q.normals, q.weights, sigma)) < 1e-14
+
+
+# ----------------------------------------------------------------------------
+# Off-surface DIM (target !== source), the reference's "Issue 136 - mixed
+# targets" test (test/dim_test.jl:42-91): unit circle, meshsize 0.2 (32 panels),
+# qorder 3; targets on the 31 x 31 grid of [-1.5, 1.5]^2.
+# ----------------------------------------------------------------------------
+def _targets_apply(pde, kind, k, T, q, corr, x):
+    near, vals = corr
+    ip, ix, dv = O.targets_csr(near, vals, q.nq, len(q))
+    import scipy.sparse as sp
+
+    return O.apply(pde, kind, k, T, None, q.coords, q.normals, q.weights, x) + \
+        sp.csr_matrix((dv, ix, ip), shape=(len(T), len(q))) @ x
+
+
+def test_dim_mixed_targets_known_answers():
+    q = G.circle_quadrature(32, 3)
+    g = np.arange(-1.5, 1.5 + 1e-9, 0.1)
+    T = np.array([(a, b) for a in g for b in g])
+    inn = np.linalg.norm(T, axis=1) < 1.0
+    u = np.ones(len(q))
+    # mixed green multipliers, maxdist = Inf
+    near, dS, dD = O.bdim_targets(O.LAPLACE, 0.0, T, q.coords, q.normals, q.weights, q.nq, np.where(inn, -1.0, 0.0))
+    # separately for the outside (0) and inside (-1) targets
+    To, Ti = T[~inn], T[inn]
+    no, dSo, dDo = O.bdim_targets(O.LAPLACE, 0.0, To, q.coords, q.normals, q.weights, q.nq, 0.0)
+    ni, dSi, dDi = O.bdim_targets(O.LAPLACE, 0.0, Ti, q.coords, q.normals, q.weights, q.nq, -1.0)
+    Dout = _targets_apply(O.LAPLACE, O.DL, 0.0, To, q, (no, dDo), u)
+    Din = _targets_apply(O.LAPLACE, O.DL, 0.0, Ti, q, (ni, dDi), u)
+    assert np.max(np.abs(Dout)) < 1e-3          # test/dim_test.jl:79
+    assert np.max(np.abs(Din + 1)) < 1e-3       # test/dim_test.jl:80
+    S = _targets_apply(O.LAPLACE, O.SL, 0.0, T, q, (near, dS), u)
+    So = _targets_apply(O.LAPLACE, O.SL, 0.0, To, q, (no, dSo), u)
+    Si = _targets_apply(O.LAPLACE, O.SL, 0.0, Ti, q, (ni, dSi), u)
+    assert np.max(np.abs(S[inn] - Si)) < 1e-3   # test/dim_test.jl:89
+    assert np.max(np.abs(S[~inn] - So)) < 1e-3  # test/dim_test.jl:90
+    # every target is near something when maxdist = Inf
+    assert np.all(near >= 0)
+
+
+def _sphere_targets(m=200, seed=0):
+    r = np.random.default_rng(seed)
+    d = r.standard_normal((m, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rad = np.where(np.arange(m) % 2 == 0, 0.9, 1.1)
+    return d * rad[:, None], rad < 1
+
+
+@pytest.mark.parametrize("pde,k", [(O.LAPLACE, 0.0), (O.HELMHOLTZ, 3.0)])
+def test_dim_off_surface_green_identity_3d(pde, k):
+    """Green's representation S[γ₁u] − D[γ₀u] = u inside, 0 outside for u
+    radiating from x0 outside, at targets 0.1 off the unit sphere, where the
+    plain quadrature is off by ~2.5e-3."""
+    q = G.ellipsoid_quadrature(6, 5, scaling=(1.0, 1.0, 1.0))
+    T, inn = _sphere_targets()
+    x0 = np.array([1.8, 0.3, -0.2])
+    g0, g1 = harmonic_traces(pde, k, q, x0, c=1.0)
+    uT = np.array([O.kernel(pde, O.SL, k, t, None, x0, None) for t in T])
+    uT = uT.real if pde == O.LAPLACE else uT
+    near, dS, dD = O.bdim_targets(pde, k, T, q.coords, q.normals, q.weights, q.nq, np.where(inn, -1.0, 0.0))
+    lhs0 = O.apply(pde, O.SL, k, T, None, q.coords, q.normals, q.weights, g1) - \
+        O.apply(pde, O.DL, k, T, None, q.coords, q.normals, q.weights, g0)
+    lhs = _targets_apply(pde, O.SL, k, T, q, (near, dS), g1) - _targets_apply(pde, O.DL, k, T, q, (near, dD), g0)
+    ref = np.where(inn, uT, 0)
+    err0, err = np.max(np.abs(lhs0 - ref)), np.max(np.abs(lhs - ref))
+    assert err < 1e-4 and err < err0 / 50, (err, err0)
