@@ -238,11 +238,39 @@ function bdim_correction_b200(op, Q::QuadHandle; green_multiplier = nothing, der
 end
 
 """
+    bdim_correction_b200(op, target::QuadHandle, Q::QuadHandle; green_multiplier, maxdist = Inf,
+                         derivative = false)
+
+The same for targets other than the source nodes (src/api.jl:105-148): every
+target within `maxdist` of its nearest source node is corrected through that
+node's element (src/quadrature.jl:264-286).  `green_multiplier` holds one
+value per target (`_green_multiplier` of src/nystrom.jl:196-207).
+"""
+function bdim_correction_b200(op, target::QuadHandle, Q::QuadHandle; green_multiplier, maxdist = Inf,
+                              derivative = false)
+    k = wavenumber(op)
+    dS = Ref{Ptr{Cvoid}}(C_NULL)
+    dD = Ref{Ptr{Cvoid}}(C_NULL)
+    gm = Vector{Float64}(green_multiplier)
+    GC.@preserve gm check(ccall((:inti_dim_correction_targets, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Float64, Float64, Ptr{Cvoid}, Ptr{Cvoid}, Cint, Ptr{Cvoid}, Float64,
+         Ref{Ptr{Cvoid}}, Ref{Ptr{Cvoid}}),
+        Q.ctx.ptr, pde_code(op), real(k), imag(k), target.ptr, Q.ptr, derivative, gm, Float64(maxdist), dS, dD),
+        Q.ctx.ptr)
+    hS, hD = CsrHandle(dS[], Q.ctx), CsrHandle(dD[], Q.ctx)
+    for h in (hS, hD)
+        finalizer(h -> ccall((:inti_csr_destroy, LIB), Cint, (Ptr{Cvoid},), h.ptr), h)
+    end
+    return hS, hD
+end
+
+"""
     single_double_layer(; op, target, source, compression, correction, derivative = false)
 
 Mirror of `Inti.single_double_layer` (src/api.jl:65-187) for
 `compression = (method = :b200, precision = :fp64 | :fp32c)` and
-`correction = (method = :dim,)` or `(method = :none,)`.  Returns
+`correction = (method = :dim, [target_location | green_multiplier], [maxdist])`
+or `(method = :none,)`.  Returns
 `S = A_S + δS`, `D = A_D + δD` as LinearMaps (the correction applied in the
 same device pass).
 """
@@ -256,10 +284,20 @@ function single_double_layer(; op, target, source, compression = (method = :b200
     tgt = upload(target; ctx)
     src = target === source ? tgt : upload(source; ctx)
     cS = cD = nothing
-    if correction.method == :dim
-        target === source || throw(ArgumentError("the GPU DIM correction requires target === source"))
+    if correction.method == :dim && target === source
         μ = haskey(correction, :green_multiplier) ? correction.green_multiplier : nothing
         cS, cD = bdim_correction_b200(op, src; green_multiplier = μ, derivative)
+    elseif correction.method == :dim
+        # src/utils.jl:200-228: target_location or green_multiplier, not both
+        haskey(correction, :target_location) || haskey(correction, :green_multiplier) ||
+            throw(ArgumentError("missing target_location field in correction"))
+        (haskey(correction, :target_location) && haskey(correction, :green_multiplier)) &&
+            throw(ArgumentError("conflicting target_location and green_multiplier fields in correction"))
+        haskey(correction, :maxdist) || @warn("missing maxdist field in correction: setting to Inf")
+        μ = haskey(correction, :green_multiplier) ? correction.green_multiplier :
+            fill(Inti._green_multiplier(correction.target_location), length(target))
+        cS, cD = bdim_correction_b200(op, tgt, src; green_multiplier = μ,
+                                      maxdist = get(correction, :maxdist, Inf), derivative)
     elseif correction.method != :none
         throw(ArgumentError("Unknown correction.method $(correction.method). Available options: (:dim, :none)"))
     end
