@@ -10,7 +10,10 @@ seed 1.  One step = one y = (A + δS) σ over all N² node pairs.
 
 value   kernel-pairs/s (G) with σ and y resident in HBM; L2 flushed between
         steps (a 256 MiB write, untimed), each step timed with CUDA events on
-        the library's stream.
+        the library's stream.  With N > 1 ranks (torchrun) the target rows of
+        the one operator are split over the ranks and y is all-gathered over
+        NCCL inside every step (--shard rows, strong scaling; --shard replicas
+        runs independent copies instead); time = max over ranks.
 e2e     the same metric through the public API (GpuOperator.mul with pinned
         host buffers): host->device copy of σ, the apply, device->host copy
         of y, every step.
@@ -557,6 +560,9 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-gmres", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shard", default="rows", choices=["rows", "replicas"],
+                    help="N > 1: split the target rows of one operator over the ranks (strong scaling, y "
+                         "all-gathered every step) or run independent replicas (weak scaling)")
     ap.add_argument("--workload", default="c2",
                     choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr"])
     args = ap.parse_args()
@@ -600,12 +606,36 @@ def main() -> None:
     dev = torch.device(f"cuda:{local}")
     comps = 2 if S.is_complex else 1
     xs = torch.from_numpy(np.ascontiguousarray(sigma).view(np.float64).copy()).to(dev)
-    ys = torch.zeros(comps * n, dtype=torch.float64, device=dev)
+    shard = args.shard if world > 1 else "none"
+    A, m_loc, yfull = S, n, None
+    if shard == "rows":
+        # rank r computes target rows [r0, r1) of the one operator (all sources
+        # on every rank, correction rows sliced); y is all-gathered each step
+        from inti_b200 import shard as SH
+
+        r0, r1 = SH.row_blocks(n, world)[rank]
+        prow = SH.padded_rows(n, world)
+        corr = None
+        if S.correction is not None:
+            ip, ix, dv = S.correction.arrays()
+            corr = inti.CorrectionMatrix.from_csr(*SH.slice_csr_rows(ip, ix, dv, r0, r1), (r1 - r0, n), ctx=ctx)
+        A = inti.GpuOperator(S.kernel, SH.target_block(q, r0, r1), q, corr, cfg["precision"], ctx)
+        m_loc = r1 - r0
+        ys = torch.zeros(comps * prow, dtype=torch.float64, device=dev)
+        yfull = torch.zeros(comps * prow * world, dtype=torch.float64, device=dev)
+    else:
+        ys = torch.zeros(comps * n, dtype=torch.float64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     torch.cuda.synchronize(dev)
+
+    def step():
+        A.apply_device(xs.data_ptr(), ys.data_ptr())
+        if yfull is not None:
+            dist.all_gather_into_tensor(yfull, ys)
+
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
-            S.apply_device(xs.data_ptr(), ys.data_ptr())
+            step()
         stream.synchronize()
         if dist:
             dist.barrier()
@@ -619,7 +649,7 @@ def main() -> None:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            S.apply_device(xs.data_ptr(), ys.data_ptr())
+            step()
             e1.record(stream)
             evs.append((e0, e1))
         stream.synchronize()
@@ -636,30 +666,32 @@ def main() -> None:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * pairs / (ms * 1e-3) / 1e9
+    job_pairs = pairs if shard == "rows" else world * pairs  # whole-job pairs per step
+    value = job_pairs / (ms * 1e-3) / 1e9
 
-    # e2e through the public API with pinned host buffers
+    # e2e through the public API with pinned host buffers (sharded: each rank
+    # uploads sigma and reads back its own row block)
     hx = torch.from_numpy(sigma.copy()).pin_memory().numpy()
-    hy = torch.zeros(n, dtype=torch.complex128 if S.is_complex else torch.float64).pin_memory().numpy()
+    hy = torch.zeros(m_loc, dtype=torch.complex128 if S.is_complex else torch.float64).pin_memory().numpy()
     for _ in range(2):
-        S.mul(hy, hx)
+        A.mul(hy, hx)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        S.mul(hy, hx)
+        A.mul(hy, hx)
     e2e_s = (time.perf_counter() - t0) / args.steps
     if dist:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = {"value": world * pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * comps * n,
-           "d2h_bytes_per_step": 8 * comps * n, "ms_per_step": e2e_s * 1e3}
+    e2e = {"value": job_pairs / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": 8 * comps * n * world,
+           "d2h_bytes_per_step": 8 * comps * (n if shard == "rows" else n * world), "ms_per_step": e2e_s * 1e3}
 
     # roofline of the dominant kernel (the pair kernel)
     kern_ms = pair_ms / max(pair_launches, 1)
     fp32 = cfg["precision"] == "fp32c"
-    achieved = pairs * FLOPS_PER_PAIR[fkey] / (kern_ms * 1e-3) / 1e12
+    achieved = float(m_loc) * n * FLOPS_PER_PAIR[fkey] / (kern_ms * 1e-3) / 1e12
     peak = peaks["fp32_flops" if fp32 else "fp64_flops"] / 1e12
     roofline = {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak,
@@ -673,9 +705,13 @@ def main() -> None:
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "strong" if args.shard == "rows" else "weak",
         "vs_baseline": None, "dtype": dtype, "data": "synthetic",
-        "config": dict(cfg, parallelism=f"replicas{world}", l2="flushed between steps"),
+        "config": dict(cfg, parallelism=(f"rows{world}" if args.shard == "rows" else f"replicas{world}"),
+                       l2="flushed between steps",
+                       **({"exchange": "NCCL all_gather of y every step (inside the timed region)"}
+                          if shard == "rows" else {})),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk,
         "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
     }
