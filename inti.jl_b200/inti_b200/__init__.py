@@ -16,10 +16,12 @@ from ._lib import (
 )
 from .core import *  # noqa: F401,F403
 from .core import __all__ as _core_all
+from .vdim import polynomial_solutions_vdim, vdim_correction
 from .geometry import (
     Quadrature,
     circle_quadrature,
     curve_quadrature,
+    disk_triangle_quadrature,
     ellipsoid_quadrature,
     gauss_legendre,
     kite_quadrature,
@@ -35,11 +37,14 @@ __all__ = list(_core_all) + [
     "kite_quadrature",
     "circle_quadrature",
     "curve_quadrature",
+    "disk_triangle_quadrature",
     "ellipsoid_quadrature",
     "p2_sphere_quadrature",
     "star_quadrature",
     "star_coefficients",
     "gauss_legendre",
+    "polynomial_solutions_vdim",
+    "vdim_correction",
     "ArgumentError",
     "DimensionMismatch",
     "NonFiniteError",

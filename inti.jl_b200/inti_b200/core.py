@@ -17,6 +17,8 @@ Names, argument meaning and error behaviour follow the reference:
   (target === source) or for other targets near it (src/api.jl:105-148);
 * ``single_double_layer_potential`` / ``IntegralPotential`` (src/api.jl:220-226,
   src/nystrom.jl:20-38);
+* ``volume_potential`` with the VDIM correction (src/api.jl:282-378,
+  src/vdim.jl:30-130; 2D Laplace);
 * ``gmres`` for ``shift·I + Σ c_t·op_t`` (the IterativeSolvers call of
   docs/src/examples/poisson.jl:166-168), plain FP64 or mixed precision.
 
@@ -57,6 +59,7 @@ __all__ = [
     "adj_double_layer_hypersingular",
     "IntegralPotential",
     "single_double_layer_potential",
+    "volume_potential",
     "I",
     "gmres",
     "COMPRESSION_METHODS",
@@ -774,6 +777,51 @@ def adj_double_layer_hypersingular(*, op, target: Quadrature, source: Quadrature
     """src/api.jl:197-212."""
     return single_double_layer(op=op, target=target, source=target if source is None else source,
                                compression=compression, correction=correction, derivative=True, ctx=ctx)
+
+
+def volume_potential(*, op, target: Quadrature, source: Quadrature, compression=None, correction=None,
+                     ctx: Context | None = None):
+    """``V`` (+ ``δV``) of src/api.jl:282-378: the volume potential of the
+    single-layer kernel from a volume quadrature, with the VDIM correction
+    (``correction=dict(method="dim", boundary=Q_boundary, [target_location |
+    green_multiplier], [maxdist], [interpolation_order])``).  The boundary
+    layer operators it needs are built with their own DIM correction (off the
+    surface for volume targets); the result is one GPU operator with δV fused
+    into its epilogue."""
+    from .vdim import vdim_correction
+
+    ctx = ctx or default_context()
+    correction = _normalize_correction(correction, target, source)
+    compression = _normalize_compression(compression)
+    G = SingleLayerKernel(op)
+    prec = compression["precision"]
+    V = GpuOperator(G, target, source, None, prec, ctx)
+    if correction["method"] == "none":
+        return V
+    if "green_multiplier" in correction:
+        gm = np.asarray(correction["green_multiplier"], float)
+        loc = None
+    else:
+        loc = "inside" if target is source else correction["target_location"]
+        gm = np.full(len(target), _green_multiplier(loc))
+    if "boundary" not in correction:
+        raise L.ArgumentError(L.E_ARG, "Missing correction.boundary field for :dim method on a volume potential")
+    boundary = correction["boundary"]
+    bc = {k: v for k, v in correction.items() if k not in ("boundary", "interpolation_order", "center")}
+    if loc is not None:
+        bc = dict(bc, target_location=loc)
+    bc.setdefault("maxdist", correction.get("maxdist", float("inf")))
+    if "S_b2d" in correction and "D_b2d" in correction:
+        S, D = correction["S_b2d"], correction["D_b2d"]
+    else:
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            S, D = single_double_layer(op=op, target=target, source=boundary, compression=compression,
+                                       correction=bc, ctx=ctx)
+    dV = vdim_correction(op, target, source, boundary, S, D, V, green_multiplier=gm,
+                         interpolation_order=correction.get("interpolation_order"),
+                         maxdist=correction.get("maxdist", float("inf")), center=correction.get("center"), ctx=ctx)
+    return GpuOperator(G, target, source, dV, prec, ctx)
 
 
 class IntegralPotential:

@@ -32,6 +32,7 @@ __all__ = [
     "gauss_legendre",
     "gauss_legendre_for_order",
     "VR4N6",
+    "disk_triangle_quadrature",
     "curve_quadrature",
     "kite_quadrature",
     "circle_quadrature",
@@ -462,4 +463,65 @@ def p2_sphere_quadrature(nsub: int = 36, radius: float = 1.0) -> Quadrature:
     nrm = cr / mu[..., None]
     q = Quadrature(x.reshape(-1, 3), nrm.reshape(-1, 3), w.reshape(-1), 6,
                    {"kind": "surface", "shape": "p2sphere", "nsub": nsub})
+    return q
+
+
+# ----------------------------------------------------------------------------
+# volumes (2D): the unit disk in curved triangles
+# ----------------------------------------------------------------------------
+def _disk_patches(radius: float, a: float):
+    """Five maps [0,1]^2 -> disk: the central square [-a, a]^2 and four
+    transfinite patches blending a square edge into a quarter of the circle
+    (P(s,t) = (1-t) L(s) + t C(s)).  Each returns (points, Jacobian det)."""
+
+    def centre(s, t):
+        x = np.stack([-a + 2 * a * s, -a + 2 * a * t], axis=-1)
+        return x, np.full(s.shape, 4 * a * a)
+
+    def outer(k):
+        c, sn = np.cos(k * np.pi / 2), np.sin(k * np.pi / 2)
+        rot = np.array([[c, -sn], [sn, c]])
+
+        def f(s, t):
+            L = np.stack([np.full(s.shape, a), -a + 2 * a * s], axis=-1)
+            dL = np.stack([np.zeros(s.shape), np.full(s.shape, 2 * a)], axis=-1)
+            phi = -np.pi / 4 + np.pi / 2 * s
+            C = radius * np.stack([np.cos(phi), np.sin(phi)], axis=-1)
+            dC = radius * np.pi / 2 * np.stack([-np.sin(phi), np.cos(phi)], axis=-1)
+            x = (1 - t)[..., None] * L + t[..., None] * C
+            xs = (1 - t)[..., None] * dL + t[..., None] * dC
+            xt = C - L
+            det = np.abs(xs[..., 0] * xt[..., 1] - xs[..., 1] * xt[..., 0])
+            return x @ rot.T, det
+
+        return f
+
+    return [centre] + [outer(k) for k in range(4)]
+
+
+def disk_triangle_quadrature(m: int, radius: float = 1.0, a: float | None = None) -> Quadrature:
+    """The disk of the given radius as 5 patches x m x m cells x 2 curved
+    triangles (10 m^2 elements), each with the 6-point Vioreanu-Rokhlin rule
+    (nq = 6) mapped through its patch: x = P(A x^), w = w^ |det A| |det DP|.
+    A volume quadrature for the volume potential (no normals)."""
+    a = 0.5 * radius if a is None else a
+    xh, wh = VR4N6
+    h = 1.0 / m
+    tri = []
+    for i in range(m):
+        for j in range(m):
+            s0, s1, t0, t1 = i * h, (i + 1) * h, j * h, (j + 1) * h
+            tri.append(((s0, t0), (s1, t0), (s0, t1)))
+            tri.append(((s1, t1), (s0, t1), (s1, t0)))
+    tri = np.array(tri)  # (2m^2, 3, 2) in patch coordinates
+    V0, E1, E2 = tri[:, 0], tri[:, 1] - tri[:, 0], tri[:, 2] - tri[:, 0]
+    detA = np.abs(E1[:, 0] * E2[:, 1] - E1[:, 1] * E2[:, 0])
+    st = V0[:, None, :] + xh[None, :, 0:1] * E1[:, None, :] + xh[None, :, 1:2] * E2[:, None, :]
+    coords, weights = [], []
+    for patch in _disk_patches(radius, a):
+        x, det = patch(st[..., 0], st[..., 1])
+        coords.append(x.reshape(-1, 2))
+        weights.append((wh[None, :] * detA[:, None] * det).reshape(-1))
+    q = Quadrature(np.concatenate(coords), None, np.concatenate(weights), len(wh))
+    q.meta.update(shape="disk", radius=radius, order=4)
     return q

@@ -12,6 +12,8 @@ import os
 import subprocess
 from pathlib import Path
 
+import math
+
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
@@ -283,3 +285,95 @@ def dim_element_conds(pde, k, coords, normals, nq, elements=None):
     if pde == LAPLACE:
         M = M.real
     return np.linalg.cond(np.transpose(M, (0, 2, 1)))
+
+
+# ----------------------------------------------------------------------------
+# VDIM (src/vdim.jl:30-130, 261-285), 2D Laplace, restated with dense
+# coefficient arrays C[i, j] <-> x^i y^j; particular solutions of ΔP = p by
+# the Almansi expansion P = Σ_j a_j r^(2j+2) Δ^j p.
+# ----------------------------------------------------------------------------
+def _pl_lap(C):
+    out = np.zeros_like(C)
+    out[:-2, :] += C[2:, :] * (np.arange(2, C.shape[0])[:, None] * np.arange(1, C.shape[0] - 1)[:, None])
+    out[:, :-2] += C[:, 2:] * (np.arange(2, C.shape[1])[None, :] * np.arange(1, C.shape[1] - 1)[None, :])
+    return out
+
+
+def _pl_r2(C):
+    out = np.zeros_like(C)
+    out[2:, :] += C[:-2, :]
+    out[:, 2:] += C[:, :-2]
+    return out
+
+
+def _pl_eval(C, X):
+    i, j = np.nonzero(C)
+    return (C[i, j][None, :] * X[:, 0:1] ** i[None, :] * X[:, 1:2] ** j[None, :]).sum(axis=1)
+
+
+def _pl_dx(C, d):
+    out = np.zeros_like(C)
+    if d == 0:
+        out[:-1, :] = C[1:, :] * np.arange(1, C.shape[0])[:, None]
+    else:
+        out[:, :-1] = C[:, 1:] * np.arange(1, C.shape[1])[None, :]
+    return out
+
+
+def vdim_basis(order, size=None):
+    """[(p, P)] for x^a y^b/(a! b!), a + b <= order (first index fastest)."""
+    size = size or order + 2 * (order // 2 + 1) + 3
+    out = []
+    for b in range(order + 1):
+        for a in range(order + 1):
+            if a + b > order:
+                continue
+            p = np.zeros((size, size))
+            p[a, b] = 1.0 / (math.factorial(a) * math.factorial(b))
+            m, P, term, j, c = a + b, np.zeros((size, size)), p.copy(), 0, 0.0
+            while np.any(term):
+                c = 1.0 / (2 * (2 * m + 2)) if j == 0 else -c / ((2 * j + 2) * (2 * m - 2 * j + 2))
+                T = term
+                for _ in range(j + 1):
+                    T = _pl_r2(T)
+                P = P + c * T
+                term = _pl_lap(term)
+                j += 1
+            out.append((p, P))
+    return out
+
+
+def vdim(tcoords, vcoords, vweights, nq, bcoords, bnormals, bweights, bnq, green_multiplier, order,
+         maxdist=np.inf, same=False):
+    """(near_elem, values (m, nq)) of δV; `same` when the targets are the volume nodes."""
+    import scipy.sparse as sp
+    from scipy.spatial import cKDTree
+
+    T, Y = _c(tcoords), _c(vcoords)
+    m = T.shape[0]
+    mu = np.broadcast_to(np.asarray(green_multiplier, dtype=np.float64), (m,))
+    basis = vdim_basis(order)
+    b = np.stack([_pl_eval(p, Y) for p, _ in basis], axis=1)
+    g0 = np.stack([_pl_eval(P, bcoords) for _, P in basis], axis=1)
+    g1 = np.stack([_pl_eval(_pl_dx(P, 0), bcoords) * bnormals[:, 0] + _pl_eval(_pl_dx(P, 1), bcoords) * bnormals[:, 1]
+                   for _, P in basis], axis=1)
+    near_b, bS, bD = bdim_targets(LAPLACE, 0.0, T, bcoords, bnormals, bweights, bnq, mu, maxdist=maxdist)
+    ipS, ixS, dvS = targets_csr(near_b, bS, bnq, len(bcoords))
+    ipD, ixD, dvD = targets_csr(near_b, bD, bnq, len(bcoords))
+    theta = np.zeros((m, len(basis)))
+    for n in range(len(basis)):
+        sg = apply(LAPLACE, SL, 0.0, T, None, bcoords, bnormals, bweights, g1[:, n]) + csr_apply(ipS, ixS, dvS, g1[:, n])
+        dg = apply(LAPLACE, DL, 0.0, T, None, bcoords, bnormals, bweights, g0[:, n]) + csr_apply(ipD, ixD, dvD, g0[:, n])
+        vb = apply(LAPLACE, SL, 0.0, T, None, Y, None, vweights, b[:, n])
+        theta[:, n] = sg - dg - vb + mu * _pl_eval(basis[n][1], T)
+    if same:
+        near = np.arange(m) // nq
+    else:
+        d, j = cKDTree(Y).query(T)
+        near = np.where(d <= maxdist, j // nq, -1)
+    vals = np.zeros((m, nq))
+    for i in np.nonzero(near >= 0)[0]:
+        e = near[i]
+        Le = b[e * nq:(e + 1) * nq].T
+        vals[i] = np.linalg.lstsq(Le, theta[i], rcond=None)[0]
+    return near, vals

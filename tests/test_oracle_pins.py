@@ -294,3 +294,23 @@ def test_dim_off_surface_green_identity_3d(pde, k):
     ref = np.where(inn, uT, 0)
     err0, err = np.max(np.abs(lhs0 - ref)), np.max(np.abs(lhs - ref))
     assert err < 1e-4 and err < err0 / 50, (err, err0)
+
+
+# ----------------------------------------------------------------------------
+# VDIM on the unit disk (src/vdim.jl:30-130): the volume potential of radial
+# densities is known in closed form, V[1] = (1 - r^2)/4, V[r^2] = (1 - r^4)/16
+# (−ΔV = f inside, V = 0 on the unit circle for radial f).
+# ----------------------------------------------------------------------------
+@pytest.mark.parametrize("order", [2, 4])
+def test_vdim_disk_known_answers(order):
+    Y = G.disk_triangle_quadrature(4)
+    B = G.circle_quadrature(64, 8)
+    near, vals = O.vdim(Y.coords, Y.coords, Y.weights, Y.nq, B.coords, B.normals, B.weights, B.nq, -1.0, order,
+                        same=True)
+    ip, ix, dv = O.targets_csr(near, vals, Y.nq, len(Y))
+    r2 = (Y.coords ** 2).sum(1)
+    for f, exact in ((np.ones(len(Y)), (1 - r2) / 4), (r2, (1 - r2 ** 2) / 16)):
+        V0 = O.apply(O.LAPLACE, O.SL, 0.0, Y.coords, None, Y.coords, None, Y.weights, f)
+        Vc = V0 + O.csr_apply(ip, ix, dv, f)
+        err0, err = np.max(np.abs(V0 - exact)), np.max(np.abs(Vc - exact))
+        assert err < 1e-6 and err < err0 / 1e3, (err, err0)
