@@ -347,6 +347,32 @@ def bench_batch(args, ctx, peaks, torch) -> dict:
         "fp64_batch": {"value": out["fp64"]["value"], "ms": out["fp64"]["ms"]},
         "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
     }
+    if not args.no_cpu:
+        # the reference applies its operator one right-hand side at a time: the
+        # oracle's D and S row sums (the combined field needs both passes) on a
+        # bounded sample of rows of the largest surface, one RHS, all host cores
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        big = int(np.argmax([len(q) for q in quads]))
+        qb, nb = quads[big], len(quads[big])
+        off = int(sum(len(q) for q in quads[:big]))
+        xcol = np.ascontiguousarray(X[off:off + nb, 0])
+        nthreads = host_cores()
+        rows = max(8 * nthreads, 64)
+        while True:
+            t0 = time.perf_counter()
+            for kind in (O.DL, O.SL):
+                O.apply_rows_block(O.HELMHOLTZ, kind, 5.0, qb.coords, qb.normals, qb.coords, qb.normals, qb.weights,
+                                   xcol, 0, rows, nthreads=nthreads)
+            dt = time.perf_counter() - t0
+            if dt > min(args.cpu_seconds, 10.0) / 2 or rows >= nb:
+                break
+            rows = min(nb, rows * 2)
+        line["cpu_baseline"] = {
+            "value": rows * nb / dt / 1e9, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{rows} of {nb} rows of the largest surface x 1 right-hand side, D and S row sums "
+                      f"(C++ FP64 restatement of the reference's per-RHS matvec), {dt:.1f} s"}
     if not args.no_gmres:
         # scattering solves (I/2 + D - i k S) sigma = -u_inc for all 32 x 64 systems
         g = {"rtol": 1e-10, "restart": 30, "systems": len(quads) * nrhs}
