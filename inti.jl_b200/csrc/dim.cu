@@ -48,6 +48,9 @@ struct S<false> {
   static __device__ __forceinline__ T shfl(T v, int src) { return __shfl_sync(0xffffffffu, v, src); }
   static __device__ __forceinline__ T wsum(T v) { return warp_sum(v); }
   static __device__ __forceinline__ T neg(T a) { return -a; }
+  // acc + a*b and acc - a*b as fused multiply-adds
+  static __device__ __forceinline__ T fmadd(T acc, T a, T b) { return fma(a, b, acc); }
+  static __device__ __forceinline__ T fmsub(T acc, T a, T b) { return fma(-a, b, acc); }
 };
 template <>
 struct S<true> {
@@ -77,7 +80,47 @@ struct S<true> {
   }
   static __device__ __forceinline__ T wsum(T v) { return make_double2(warp_sum(v.x), warp_sum(v.y)); }
   static __device__ __forceinline__ T neg(T a) { return make_double2(-a.x, -a.y); }
+  static __device__ __forceinline__ T fmadd(T acc, T a, T b) {
+    return make_double2(fma(a.x, b.x, fma(-a.y, b.y, acc.x)), fma(a.x, b.y, fma(a.y, b.x, acc.y)));
+  }
+  static __device__ __forceinline__ T fmsub(T acc, T a, T b) {
+    return make_double2(fma(-a.x, b.x, fma(a.y, b.y, acc.x)), fma(-a.x, b.y, fma(-a.y, b.x, acc.y)));
+  }
 };
+
+// S and D kernel values of one pair (without the weight), sharing r, 1/d and
+// e^{ikd}: the 3D single/double layer from the refined hardware rsqrt and the
+// tabulated e^{ikd} of the pair kernels (tab: the device table, read-only);
+// other kinds and 2D through kernel_value.
+template <int PDE, int DIM, bool DERIV>
+__device__ __forceinline__ void theta_sd(const double* xi, const double* ni, const double* yj,
+                                         const double* nj, double k, double kT, double delta,
+                                         const double2* __restrict__ tab, double2& sv, double2& dv) {
+  if (DIM == 3 && !DERIV) {
+    const double r0 = xi[0] - yj[0], r1 = xi[1] - yj[1], r2 = xi[2] - yj[2];
+    const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
+    const double ri = d2 > kSamePointTol2 ? rsqrt_fast(d2) : 0.0;  // self pair: every value 0
+    const double rn = fma(r2, nj[2], fma(r1, nj[1], r0 * nj[0]));
+    constexpr double c4 = 1.0 / (4 * kPi);
+    if (PDE == LAPLACE) {
+      sv = make_double2(c4 * ri, 0.0);
+      dv = make_double2(c4 * rn * (ri * ri * ri), 0.0);
+    } else {
+      double c, s;  // e^{ikd}
+      expi_table_eval<double, double2>(d2 * ri * kT, tab, delta, c, s);
+      const double g = c4 * ri;
+      sv = make_double2(g * c, g * s);
+      // e^{ikd} (1/d - ik) (r.n_y) / (4 pi d^2)
+      const double h = c4 * rn * ri * ri;
+      dv = make_double2(h * fma(c, ri, k * s), h * fma(s, ri, -k * c));
+    }
+  } else {
+    constexpr int KS = DERIV ? ADL : SL;
+    constexpr int KD = DERIV ? HS : DL;
+    sv = kernel_value<PDE, KS, DIM>(xi, ni, yj, nj, k);
+    dv = kernel_value<PDE, KD, DIM>(xi, ni, yj, nj, k);
+  }
+}
 
 // ---------------------------------------------------------------------------
 // 2. traces: g0/g1 are n x ns, row-major (ns contiguous per node).
@@ -106,13 +149,11 @@ template <int PDE, int DIM, bool DERIV, int NS>
 __global__ void __launch_bounds__(kThetaBlock) dim_theta(
     int64_t m, int64_t n, int ns, const double* __restrict__ tx, const double* __restrict__ tn,
     const double* __restrict__ x, const double* __restrict__ nrm, const double* __restrict__ w,
-    const double2* __restrict__ g0, const double2* __restrict__ g1, double k, int tiles_per_split,
-    double2* __restrict__ partial) {
+    const double2* __restrict__ g0, const double2* __restrict__ g1, double k, double kT, double delta,
+    const double2* __restrict__ tab, int tiles_per_split, double2* __restrict__ partial) {
   constexpr bool CPLX = PDE == HELMHOLTZ;
   using Sc = S<CPLX>;
   using T = typename Sc::T;
-  constexpr int KS = DERIV ? ADL : SL;
-  constexpr int KD = DERIV ? HS : DL;
   __shared__ double sx[kThetaTile * DIM], sn[kThetaTile * DIM], sw[kThetaTile];
   __shared__ T s0[kThetaTile * NS], s1[kThetaTile * NS];
   const int64_t i = blockIdx.x * (int64_t)kThetaBlock + threadIdx.x;
@@ -152,11 +193,12 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
 #pragma unroll 1
     for (int a = 0; a < kThetaTile; ++a) {
       const double wj = sw[a];
-      const T sv = Sc::scale(Sc::from(kernel_value<PDE, KS, DIM>(xi, ni, &sx[a * DIM], &sn[a * DIM], k)), wj);
-      const T dv = Sc::scale(Sc::from(kernel_value<PDE, KD, DIM>(xi, ni, &sx[a * DIM], &sn[a * DIM], k)), wj);
+      double2 sv2, dv2;
+      theta_sd<PDE, DIM, DERIV>(xi, ni, &sx[a * DIM], &sn[a * DIM], k, kT, delta, tab, sv2, dv2);
+      const T sv = Sc::scale(Sc::from(sv2), wj);
+      const T dv = Sc::scale(Sc::from(dv2), wj);
 #pragma unroll
-      for (int q = 0; q < NS; ++q)
-        acc[q] = Sc::sub(Sc::add(acc[q], Sc::mul(sv, s1[a * NS + q])), Sc::mul(dv, s0[a * NS + q]));
+      for (int q = 0; q < NS; ++q) acc[q] = Sc::fmsub(Sc::fmadd(acc[q], sv, s1[a * NS + q]), dv, s0[a * NS + q]);
     }
   }
   if (i < m) {
@@ -521,7 +563,9 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
       dim3 grid((unsigned)blocks, (unsigned)split);
       ProfScope pd(ctx, "dim");
       dim_theta<P, D, DV, NSB><<<grid, kThetaBlock, 0, ctx->stream>>>(
-          m, n, ns, tx, tn, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re, tps, wk.part.as<double2>());
+          m, n, ns, tx, tn, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re,
+          k_re * kExpiTable / (2 * kPi), 2 * kPi / kExpiTable, P == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, tps,
+          wk.part.as<double2>());
       ctx->launches++;
       dim_theta_reduce<P, D, DV><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
           m, ns, split, tx, tn, wk.d_xs.as<double>(), mu, k_re, wk.part.as<double2>(), wk.theta.as<double2>());
