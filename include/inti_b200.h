@@ -252,7 +252,10 @@ int inti_batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quad
                       inti_batch** out);
 /* Y = alpha*(A X + C X) + beta*Y for nrhs columns.  precision INTI_FP64
  * (CUDA cores) or INTI_TF32 (Helmholtz: kernel tiles x density blocks on the
- * tcgen05 tensor cores, FP32 accumulation, FP64 correction). */
+ * tcgen05 tensor cores, FP32 accumulation, FP64 correction).  With
+ * on_device = 1, a TF32 apply after a first one with the same nrhs only
+ * enqueues work on the context's stream (no allocation, no synchronisation),
+ * so it can be captured into a CUDA graph and replayed. */
 int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
                      int32_t nrhs, const double* alpha, const double* beta, int on_device);
 /* GMRES on every (surface, column) system shift*I + A_s + C_s at once, in

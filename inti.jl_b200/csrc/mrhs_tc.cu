@@ -645,6 +645,11 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
         b->kind == SL ? nullptr : b->normals.as<double>(), b->tc_src.as<float>());
     ctx->launches++;
     b->tc_counter.ensure(sizeof(int));
+    // once per batch (not per launch): an apply after the first only enqueues
+    // work, so it can be captured into a CUDA graph
+    for (const void* kern : {(const void*)mrhs_tc_kernel<SL>, (const void*)mrhs_tc_kernel<DL>,
+                             (const void*)mrhs_tc_kernel<CF>, (const void*)mrhs_tc_kernel<CFI>})
+      INTI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
   }
   const int ncg = (a.nrhs + TC_R - 1) / TC_R;
   b->tc_b.ensure((size_t)ncg * b->tc_ntiles * TC_B_BYTES);
@@ -687,7 +692,6 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
   t.err = ctx->err_flag.as<int>();
   INTI_CUDA(cudaMemsetAsync(b->tc_counter.p, 0, sizeof(int), ctx->stream));
   auto launch = [&](auto kern) {
-    INTI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
     ProfScope pk(ctx, "batch_tc");
     kern<<<ctx->num_sms, TC_THREADS, TC_SMEM, ctx->stream>>>(t);
   };
