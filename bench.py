@@ -729,6 +729,7 @@ def main() -> None:
                 "share_of_step": pair_ms / max(sum(step_ms), 1e-9),
                 "other_kernels_ms": {"pack": pack_ms / args.steps, "epilogue": epi_ms / args.steps}}
 
+    roofline["launch_shape"] = dict(A.tuning, picked_by="timing at operator creation (inti_op_tuning)")
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,

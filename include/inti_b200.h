@@ -173,6 +173,16 @@ int inti_op_apply_transpose(inti_op* op, const double* x, int64_t ldx, double* y
  * counterpart of assemble_matrix (src/nystrom.jl:103-124). */
 int inti_op_assemble(inti_op* op, double* out, int on_device);
 int inti_op_destroy(inti_op* op);
+/* Launch shape of the operator's pair kernel: targets per thread (2 or 4)
+ * and the number of source chunks (split).  Operators created through
+ * inti_op_create / inti_op_create_combined with more than 2^26 pairs pick
+ * them by timing the candidates once, on a zero density, at creation (the
+ * choice is cached per context and problem shape, and reused by operators
+ * the library derives internally); smaller ones, or a context with
+ * autotuning off, keep the occupancy heuristic.  No counterpart in the
+ * reference (launch configuration). */
+int inti_op_tuning(const inti_op* op, int32_t* targets_per_thread, int32_t* split);
+int inti_ctx_set_autotune(inti_ctx* ctx, int enable);  /* default on */
 
 /* ---- BDIM correction on the GPU (src/bdim.jl:50-196) ------------------- */
 /* green_multiplier: n values or NULL for -1/2 (on the surface,

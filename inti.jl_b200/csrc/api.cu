@@ -113,6 +113,7 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
   L.packed = op->packed.p;
   L.partial = op->partial.p;
   L.split = op->split;
+  L.tpt = op->tpt;
   L.n_tiles = op->n_tiles;
   L.err_flag = op->ctx->err_flag.as<int>();
   L.c1[0] = op->c1[0];
@@ -502,7 +503,9 @@ int inti_op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   if (!ctx || !out) return INTI_E_ARG;
   *out = nullptr;
   return guarded(ctx, [&] {
-    *out = op_create(ctx, pde, kernel, k_re, k_im, target, source, correction, precision);
+    std::unique_ptr<inti_op> op(op_create(ctx, pde, kernel, k_re, k_im, target, source, correction, precision));
+    op_autotune(op.get(), true);
+    *out = op.release();
   });
 }
 
@@ -512,9 +515,23 @@ int inti_op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   if (!ctx || !out) return INTI_E_ARG;
   *out = nullptr;
   return guarded(ctx, [&] {
-    *out = op_create_combined(ctx, pde, k_re, k_im, target, source, corr_dl, corr_sl, c_dl, c_sl,
-                              precision);
+    std::unique_ptr<inti_op> op(op_create_combined(ctx, pde, k_re, k_im, target, source, corr_dl, corr_sl,
+                                                   c_dl, c_sl, precision));
+    op_autotune(op.get(), true);
+    *out = op.release();
   });
+}
+
+int inti_op_tuning(const inti_op* op, int32_t* targets_per_thread, int32_t* split) {
+  if (!op) return INTI_E_ARG;
+  if (targets_per_thread) *targets_per_thread = op->tpt;
+  if (split) *split = op->split;
+  return INTI_OK;
+}
+
+int inti_ctx_set_autotune(inti_ctx* ctx, int enable) {
+  if (!ctx) return INTI_E_ARG;
+  return guarded(ctx, [&] { ctx->autotune = enable != 0; });
 }
 
 int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype) {

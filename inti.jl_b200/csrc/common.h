@@ -85,6 +85,10 @@ struct inti_ctx {
   };
   std::vector<Span> spans;
   std::map<std::string, std::pair<double, int64_t>> prof_totals;
+  // pair-kernel launch shapes picked by measurement (inti_ctx_set_autotune):
+  // key "pde/kind/dim/precision/m/n" -> (targets per thread, split)
+  bool autotune = true;
+  std::map<std::string, std::pair<int, int>> tuned;
 };
 
 struct inti_quad {
@@ -147,6 +151,7 @@ struct PairLaunch {
   void* partial;           // scratch: split x m accumulators
   double c1[2], c2[2];     // CF: dipole and charge coefficients (complex)
   int split;               // number of source chunks (computed by plan)
+  int tpt = 4;             // targets per thread of the pair kernel (2 or 4)
   int64_t n_tiles;         // padded source tiles
   int* err_flag;
 };
@@ -164,7 +169,7 @@ int pair_record_bytes(int pde, int kind, int dim, int precision);
 int pair_partial_bytes(int pde, int precision);
 // Choose the split for a problem on this device.
 int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
-                    int64_t n);
+                    int64_t n, int tpt = 4);
 // Enqueue pack + pair kernels (results in L.partial); returns launches.
 int pair_launch(inti_ctx* ctx, const PairLaunch& L);
 // y = alpha*(scale*sum_s partial + C x) + beta*y; complex when cplx.

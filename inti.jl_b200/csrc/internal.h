@@ -22,6 +22,7 @@ struct inti_op {
   inti::DevBuf tpartial;  // transpose: tsplit x n double2
   inti::DevBuf gpartial;  // source gradients: split x n x (2 dim + 2)
   int split = 1;
+  int tpt = 4;  // targets per thread of the pair kernel (autotuned with split)
   int tsplit = 1;
   int64_t n_tiles = 1;
 };
@@ -41,6 +42,10 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
                             const inti_quad* source, const inti_csr* corr_dl, const inti_csr* corr_sl,
                             const double* c_dl, const double* c_sl, int precision);
 inti_op* op_clone_precision(const inti_op* op, int precision);
+// Launch shape of the pair kernel: the context's cached choice for this
+// problem, else (measure = true, autotuning on, problem large enough) the
+// fastest candidate timed now, else the occupancy heuristic.
+void op_autotune(inti_op* op, bool measure);
 std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
                                             const inti_csr* b, const double* cb, int64_t m, int64_t n,
                                             bool cplx);

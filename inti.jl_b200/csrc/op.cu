@@ -65,6 +65,7 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   const int64_t big = std::max(target->n, source->n);
   op->xbuf.ensure(sizeof(double) * comps * big);
   op->ybuf.ensure(sizeof(double) * comps * big);
+  op_autotune(op.get(), false);
   return op.release();
 }
 
@@ -168,6 +169,7 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   const int64_t big = std::max(target->n, source->n);
   op->xbuf.ensure(sizeof(double) * comps * big);
   op->ybuf.ensure(sizeof(double) * comps * big);
+  op_autotune(op.get(), false);
   return op.release();
 }
 
@@ -197,7 +199,73 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
   const int64_t big = std::max(op->target->n, op->source->n);
   t->xbuf.ensure(sizeof(double) * comps * big);
   t->ybuf.ensure(sizeof(double) * comps * big);
+  op_autotune(t.get(), false);
   return t.release();
+}
+
+// Problems below this many pairs keep the heuristic shape (a timing pass
+// would cost more than it could save).
+constexpr double kTuneMinPairs = 67108864.0;
+
+void op_autotune(inti_op* op, bool measure) {
+  inti_ctx* ctx = op->ctx;
+  const int64_t m = op->target->n, n = op->source->n;
+  const std::string key = std::to_string(op->pde) + "/" + std::to_string(op->kind) + "/" +
+                          std::to_string(op->dim) + "/" + std::to_string(op->precision) + "/" +
+                          std::to_string(m) + "/" + std::to_string(n);
+  const size_t pbytes = (size_t)pair_partial_bytes(op->pde, op->precision);
+  auto set = [&](int tpt, int split) {
+    op->tpt = tpt;
+    op->split = split;
+    op->partial.ensure((size_t)split * m * pbytes);
+  };
+  auto it = ctx->tuned.find(key);
+  if (it != ctx->tuned.end()) {
+    set(it->second.first, it->second.second);
+    return;
+  }
+  if (!measure || !ctx->autotune || (double)m * (double)n < kTuneMinPairs) return;
+  // candidates: 4 or 2 targets per thread, each with the heuristic split,
+  // half of it and twice it (at most one chunk per source tile, 64 chunks)
+  std::vector<std::pair<int, int>> cand;
+  for (int tpt : {4, 2}) {
+    const int s0 = pair_plan_split(ctx, op->pde, op->kind, op->dim, op->precision, m, n, tpt);
+    const int hi = (int)std::min<int64_t>({(int64_t)2 * s0, op->n_tiles, 64});
+    for (int sp : {s0, std::max(1, s0 / 2), hi})
+      if (std::find(cand.begin(), cand.end(), std::make_pair(tpt, sp)) == cand.end()) cand.emplace_back(tpt, sp);
+  }
+  int smax = 1;
+  for (auto& c : cand) smax = std::max(smax, c.second);
+  op->partial.ensure((size_t)smax * m * pbytes);
+  // the pair kernel's cost does not depend on the density: time it on zeros
+  const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
+  INTI_CUDA(cudaMemsetAsync(op->xbuf.p, 0, sizeof(double) * comps * n, ctx->stream));
+  PairLaunch L = make_launch(op, op->xbuf.as<double>());
+  cudaEvent_t e0, e1;
+  INTI_CUDA(cudaEventCreate(&e0));
+  INTI_CUDA(cudaEventCreate(&e1));
+  pair_launch(ctx, L);  // warm-up with the heuristic shape
+  float best = -1.0f;
+  std::pair<int, int> pick(op->tpt, op->split);
+  for (auto& c : cand) {
+    L.tpt = c.first;
+    L.split = c.second;
+    INTI_CUDA(cudaEventRecord(e0, ctx->stream));
+    pair_launch(ctx, L);
+    INTI_CUDA(cudaEventRecord(e1, ctx->stream));
+    INTI_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    INTI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (best < 0.0f || ms < best) {
+      best = ms;
+      pick = c;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  sync_and_check(ctx);
+  ctx->tuned[key] = pick;
+  set(pick.first, pick.second);
 }
 
 void op_prepare_transpose(inti_op* op) {

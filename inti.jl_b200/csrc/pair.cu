@@ -337,7 +337,7 @@ struct FwdArgs {
   int* err;
 };
 
-template <int PDE, int KIND, int DIM, class R, int TILE>
+template <int PDE, int KIND, int DIM, class R, int TILE, int TPT = kTPT>
 __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
   using RC = Rec<PDE, KIND, DIM, R>;
   constexpr bool CPLX = RC::cplx;
@@ -351,16 +351,16 @@ __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
   __shared__ __align__(8) uint64_t full[2];
 
   const int tid = threadIdx.x;
-  const int64_t base = (int64_t)blockIdx.x * (kBlock * kTPT);
+  const int64_t base = (int64_t)blockIdx.x * (kBlock * TPT);
   const int split = blockIdx.y;
   const int64_t t0 = (int64_t)split * a.tiles_per_split;
   const int64_t t1 = min(a.n_tiles, t0 + a.tiles_per_split);
   const R* src = static_cast<const R*>(a.packed);
 
-  Target<R, DIM, RC::tnormal> tg[kTPT];
-  Acc<R, CPLX> acc[kTPT];
+  Target<R, DIM, RC::tnormal> tg[TPT];
+  Acc<R, CPLX> acc[TPT];
 #pragma unroll
-  for (int u = 0; u < kTPT; ++u) {
+  for (int u = 0; u < TPT; ++u) {
     const int64_t i = min(base + u * kBlock + tid, a.m - 1);
 #pragma unroll
     for (int c = 0; c < DIM; ++c) tg[u].x[c] = R(a.tcoords[DIM * i + c]);
@@ -412,11 +412,11 @@ __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
       for (int s = 0; s < kGroup; ++s) {
         const R* rec = sp + (g + s) * RC::n;
 #pragma unroll
-        for (int u = 0; u < kTPT; ++u)
+        for (int u = 0; u < TPT; ++u)
           pair_step<PDE, KIND, DIM, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
       }
 #pragma unroll
-      for (int u = 0; u < kTPT; ++u) acc[u].fold();
+      for (int u = 0; u < TPT; ++u) acc[u].fold();
     }
     __syncthreads();  // every thread is done reading this stage
     if (tid == 0 && issued < t1) {
@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(kBlock) pair_forward(FwdArgs a) {
   }
   P* out = static_cast<P*>(a.partial) + (int64_t)split * a.m;
 #pragma unroll
-  for (int u = 0; u < kTPT; ++u) {
+  for (int u = 0; u < TPT; ++u) {
     const int64_t i = base + u * kBlock + tid;
     if (i < a.m) store_partial(out + i, acc[u]);
   }
@@ -694,10 +694,10 @@ static void dispatch(int pde, int kind, int dim, F&& f) {
                                       " dim=" + std::to_string(dim));
 }
 
-template <class T, class R>
+template <class T, class R, int TPT = kTPT>
 static const void* fwd_kernel_ptr() {
   constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
-  return reinterpret_cast<const void*>(&pair_forward<T::pde, T::kind, T::dim, R, TILE>);
+  return reinterpret_cast<const void*>(&pair_forward<T::pde, T::kind, T::dim, R, TILE, TPT>);
 }
 
 template <class T, class R>
@@ -708,17 +708,18 @@ static size_t fwd_smem() {
 }
 
 int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
-                    int64_t n) {
+                    int64_t n, int tpt) {
+  if (tpt != 2 && tpt != 4) throw Error(INTI_E_ARG, "targets per thread must be 2 or 4");
   int occ = 1;
   dispatch(pde, kind, dim, [&](auto tag) {
     using T = decltype(tag);
     const void* fn;
     size_t sm;
     if (precision == INTI_FP32C) {
-      fn = fwd_kernel_ptr<T, float>();
+      fn = tpt == 2 ? fwd_kernel_ptr<T, float, 2>() : fwd_kernel_ptr<T, float, 4>();
       sm = fwd_smem<T, float>();
     } else {
-      fn = fwd_kernel_ptr<T, double>();
+      fn = tpt == 2 ? fwd_kernel_ptr<T, double, 2>() : fwd_kernel_ptr<T, double, 4>();
       sm = fwd_smem<T, double>();
     }
     INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -727,7 +728,7 @@ int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precisi
   occ = std::max(occ, 1);
   const int64_t tile = pair_tile(precision);
   const int64_t n_tiles = std::max<int64_t>(1, (n + tile - 1) / tile);
-  const int64_t blocks = (m + kBlock * kTPT - 1) / (kBlock * kTPT);
+  const int64_t blocks = (m + kBlock * tpt - 1) / (kBlock * tpt);
   const int64_t slots = (int64_t)ctx->num_sms * occ;
   // Smallest split whose last wave is >= 90% full (or that reaches 8
   // waves), never more chunks than source tiles.
@@ -781,9 +782,10 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
       a.err = L.err_flag;
       const size_t sm = fwd_smem<T, R>();
-      auto fn = &pair_forward<T::pde, T::kind, T::dim, R, TILE>;
+      auto fn = L.tpt == 2 ? &pair_forward<T::pde, T::kind, T::dim, R, TILE, 2>
+                           : &pair_forward<T::pde, T::kind, T::dim, R, TILE, 4>;
       INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-      dim3 grid((unsigned)((L.m + kBlock * kTPT - 1) / (kBlock * kTPT)), (unsigned)L.split);
+      dim3 grid((unsigned)((L.m + kBlock * L.tpt - 1) / (kBlock * L.tpt)), (unsigned)L.split);
       ProfScope pp(ctx, "pair");
       fn<<<grid, kBlock, sm, ctx->stream>>>(a);
       launches = 2;

@@ -122,6 +122,8 @@ SIGNATURES = {
     "inti_op_grad_sources": (C.c_int, [P, P, P, P, P, P, P, C.c_int]),
     "inti_measure_peaks": (C.c_int, [P, D, D, D]),
     "inti_measure_peak_tf32": (C.c_int, [P, D]),
+    "inti_op_tuning": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "inti_ctx_set_autotune": (C.c_int, [P, C.c_int]),
     "inti_selftest_math": (C.c_int, [P, D]),
     "inti_batch_create": (C.c_int, [P, C.c_int32, PP, C.c_int, C.c_int, C.c_double, C.c_double, D, D, PP, PP, PP]),
     "inti_batch_apply": (C.c_int, [P, C.c_int, P, I64, P, I64, C.c_int32, D, D, C.c_int]),

@@ -110,6 +110,11 @@ class Context:
     def synchronize(self) -> None:
         self.check(self.lib.inti_ctx_synchronize(self.handle))
 
+    def set_autotune(self, enable: bool) -> None:
+        """Pick pair-kernel launch shapes of large operators by timing (on by
+        default; see ``GpuOperator.tuning``)."""
+        self.check(self.lib.inti_ctx_set_autotune(self.handle, int(bool(enable))))
+
     def selftest_math(self) -> dict:
         """Accuracy of the device's fast rsqrt / e^{iθ} helpers (see the ABI)."""
         out = (C.c_double * 4)()
@@ -516,6 +521,13 @@ class GpuOperator(_Map):
                                                          L.dptr(out["sigma"]), L.dptr(out["coords"]),
                                                          L.dptr(out["normals"]), L.dptr(out["weights"]), 0))
         return out
+
+    @property
+    def tuning(self) -> dict:
+        """Launch shape of the pair kernel: targets per thread and split."""
+        t, s = C.c_int32(), C.c_int32()
+        self.ctx.check(self.ctx.lib.inti_op_tuning(self.handle, C.byref(t), C.byref(s)))
+        return {"targets_per_thread": t.value, "split": s.value}
 
     def grad_sources_device(self, g_ptr: int, sigma_ptr: int, dsigma_ptr: int, dcoords_ptr: int,
                             dnormals_ptr: int, dweights_ptr: int) -> None:
