@@ -268,6 +268,10 @@ int inti_ctx_destroy(inti_ctx* ctx) {
     }
     ctx->spans.clear();
     ctx->err_flag.release();
+    for (inti::DevBuf* d : {&ctx->krylov.V, &ctx->krylov.w, &ctx->krylov.r, &ctx->krylov.e, &ctx->krylov.w_outer,
+                            &ctx->krylov.partial, &ctx->krylov.h, &ctx->krylov.y, &ctx->krylov.nrm, &ctx->krylov.b,
+                            &ctx->krylov.x, &ctx->expi64, &ctx->expi32})
+      d->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   }
   delete ctx;

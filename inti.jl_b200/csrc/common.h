@@ -89,6 +89,11 @@ struct inti_ctx {
   // key "pde/kind/dim/precision/m/n" -> (targets per thread, split)
   bool autotune = true;
   std::map<std::string, std::pair<int, int>> tuned;
+  // GMRES workspace kept between solves: Krylov basis, work vectors, the
+  // reduction scratch and the staged right-hand side / solution.
+  struct {
+    inti::DevBuf V, w, r, e, w_outer, partial, h, y, nrm, b, x;
+  } krylov;
 };
 
 struct inti_quad {

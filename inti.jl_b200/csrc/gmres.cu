@@ -152,9 +152,7 @@ struct Solver {
   bool C;  // complex arithmetic
   int comps;
   int nblk;
-  DevBuf partial, hbuf, ybuf, nbuf;
   std::vector<inti_op*> ops64, ops32;
-  std::vector<std::unique_ptr<inti_op>> owned32;
   std::vector<cplx> coefs;
   cplx shift;
   int fp64_applies = 0, fp32_applies = 0;
@@ -185,6 +183,7 @@ struct Solver {
   }
   // h[0:kcount] (=|+=) V^H w  (device)
   void dots(const double* V, int64_t ldv, int kcount, const double* w, double2* h, bool acc) {
+    DevBuf& partial = ctx->krylov.partial;
     partial.ensure(sizeof(double2) * (size_t)nblk * std::max(kcount, 1));
     if (C)
       multi_dot<true><<<nblk, kDotBlock, 0, ctx->stream>>>(n, kcount, V, ldv, w, partial.as<double2>());
@@ -202,7 +201,7 @@ struct Solver {
     ctx->launches++;
   }
   double norm(const double* w) {
-    DevBuf& h = nbuf;
+    DevBuf& h = ctx->krylov.nrm;
     h.ensure(sizeof(double2));
     dots(w, 0, 1, w, h.as<double2>(), false);
     double2 v;
@@ -218,9 +217,10 @@ struct Solver {
   int gmres(bool fp32, const double* rhs, double* x, double tol_abs, int restart, int maxit,
             double bnorm_for_history, double* history, int hist_offset, double* est,
             bool x_is_zero, bool final_true_residual) {
-    DevBuf Vb, wb;
-    double* V = vec(Vb, restart + 1);
-    double* w = vec(wb);
+    double* V = vec(ctx->krylov.V, restart + 1);
+    double* w = vec(ctx->krylov.w);
+    DevBuf& hbuf = ctx->krylov.h;
+    DevBuf& ybuf = ctx->krylov.y;
     hbuf.ensure(sizeof(double2) * (restart + 2) * 2);
     double2* h1 = hbuf.as<double2>();
     double2* h2 = h1 + (restart + 2);
@@ -347,8 +347,9 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
     S.coefs.push_back(c);
   }
   // Fuse a double-layer and a single-layer term over the same nodes into one
-  // combined-field operator: one pass over the pairs per Krylov step.
-  std::vector<std::unique_ptr<inti_op>> fused;
+  // combined-field operator: one pass over the pairs per Krylov step.  The
+  // fused operator is kept on the double layer for later solves with the
+  // same single layer and coefficients.
   for (size_t a = 0; a < S.ops64.size(); ++a) {
     if (S.ops64[a]->kind != INTI_DL || S.ops64[a]->dim != 3) continue;
     for (size_t b = 0; b < S.ops64.size(); ++b) {
@@ -359,9 +360,15 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
       const double cd[2] = {S.coefs[a].real(), S.coefs[a].imag()};
       const double cs[2] = {S.coefs[b].real(), S.coefs[b].imag()};
       if (D->pde == INTI_LAPLACE && (cd[1] != 0.0 || cs[1] != 0.0)) continue;
-      fused.emplace_back(op_create_combined(ctx, D->pde, D->k, 0.0, D->target, D->source, D->corr, Sl->corr,
-                                            cd, cs, INTI_FP64));
-      S.ops64[a] = fused.back().get();
+      const double key[4] = {cd[0], cd[1], cs[0], cs[1]};
+      if (!D->fused || D->fused_sl != Sl->id || !std::equal(key, key + 4, D->fused_c)) {
+        D->fused.reset();
+        D->fused.reset(op_create_combined(ctx, D->pde, D->k, 0.0, D->target, D->source, D->corr, Sl->corr,
+                                          cd, cs, INTI_FP64));
+        D->fused_sl = Sl->id;
+        std::copy(key, key + 4, D->fused_c);
+      }
+      S.ops64[a] = D->fused.get();
       S.coefs[a] = cplx(1, 0);
       S.ops64.erase(S.ops64.begin() + b);
       S.coefs.erase(S.coefs.begin() + b);
@@ -378,13 +385,21 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
   S.n = q->n;
   S.nblk = std::max(1, std::min<int>(ctx->num_sms * 2, (int)((S.n + kDotBlock - 1) / kDotBlock)));
   if (mode == INTI_GMRES_MIXED) {
+    // FP32C twins, made once per operator; their launch shape is timed like
+    // an operator created at FP32C
     for (auto* op : S.ops64) {
-      S.owned32.emplace_back(op_clone_precision(op, INTI_FP32C));
-      S.ops32.push_back(S.owned32.back().get());
+      if (!op->twin32) {
+        op->twin32.reset(op_clone_precision(op, INTI_FP32C));
+        op_autotune(op->twin32.get(), true);
+      }
+      S.ops32.push_back(op->twin32.get());
     }
   }
   const size_t bytes = sizeof(double) * S.comps * S.n;
-  DevBuf bd, xd, rd, ed;
+  DevBuf& bd = ctx->krylov.b;
+  DevBuf& xd = ctx->krylov.x;
+  DevBuf& rd = ctx->krylov.r;
+  DevBuf& ed = ctx->krylov.e;
   const double* bdev = b;
   double* xdev = x;
   if (!on_device) {
@@ -416,8 +431,7 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
     // refinement: r = b - L64 x, solve L32 e = r, x += e
     double* r = S.vec(rd);
     double* e = S.vec(ed);
-    DevBuf wb;
-    double* w = S.vec(wb);
+    double* w = S.vec(ctx->krylov.w_outer);
     constexpr double kInnerRtol = 1.0e-5;  // FP32C operator resolves ~1e-6..1e-7
     const int max_outer = 20;
     if (S.norm(xdev) == 0.0) {
@@ -458,7 +472,6 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
   cudaEventDestroy(e1);
   if (!on_device) INTI_CUDA(cudaMemcpyAsync(x, xdev, bytes, cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
-  S.owned32.clear();  // twins refer to the fused operators' corrections
   if (stats) {
     stats->iterations = iters;
     stats->outer = outer;

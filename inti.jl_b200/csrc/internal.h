@@ -1,11 +1,22 @@
 // Operator handle and the functions the C ABI layer calls into.  Internal.
 #pragma once
 
+#include <atomic>
 #include <memory>
 
 #include "common.h"
 
+namespace inti {
+// Identity of an operator handle, never reused within the process (a freed
+// handle's address can be).
+inline uint64_t next_op_id() {
+  static std::atomic<uint64_t> counter{0};
+  return ++counter;
+}
+}  // namespace inti
+
 struct inti_op {
+  const uint64_t id = inti::next_op_id();
   inti_ctx* ctx = nullptr;
   int pde = INTI_LAPLACE, kind = INTI_SL, dim = 3, precision = INTI_FP64;
   double k = 0.0;
@@ -25,6 +36,13 @@ struct inti_op {
   int tpt = 4;  // targets per thread of the pair kernel (autotuned with split)
   int tsplit = 1;
   int64_t n_tiles = 1;
+  // Derived operators kept for repeated solves: the FP32C twin used by the
+  // mixed-precision GMRES, and (on a double layer) the combined-field operator
+  // fused with the single layer `fused_sl` under coefficients fused_c.
+  std::unique_ptr<inti_op> twin32;
+  std::unique_ptr<inti_op> fused;
+  uint64_t fused_sl = 0;
+  double fused_c[4] = {0.0, 0.0, 0.0, 0.0};
 };
 
 namespace inti {

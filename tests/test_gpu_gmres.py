@@ -70,3 +70,29 @@ def test_gmres_reports_nonconvergence(ctx):
     b = density(len(q), False, 9)
     x, st = inti.gmres(L, b, rtol=1e-14, restart=5, maxiter=4)
     assert st["converged"] == 0 and st["iterations"] == 4
+
+
+def test_gmres_repeated_solves_reuse_derived_operators(ctx):
+    """The fused combined-field operator and the FP32C twins are kept on the
+    operators: a second solve repeats the first bit for bit, and a solve with
+    another single layer or other coefficients rebuilds the fused operator."""
+    q = inti.p2_sphere_quadrature(3)
+    k = 2.0
+    op = inti.Helmholtz(k=k, dim=3)
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    b = density(len(q), True, 5)
+    for mode in ("fp64", "mixed"):
+        x1, st1 = inti.gmres(0.5 * inti.I + D - 1j * k * S, b, rtol=1e-10, restart=60, maxiter=400, mode=mode)
+        x2, st2 = inti.gmres(0.5 * inti.I + D - 1j * k * S, b, rtol=1e-10, restart=60, maxiter=400, mode=mode)
+        assert st1["converged"] == 1 and np.array_equal(x1, x2), mode
+        assert st1["iterations"] == st2["iterations"]
+    # other coefficients on the same pair of operators
+    x3, st3 = inti.gmres(0.5 * inti.I + D - 2j * k * S, b, rtol=1e-10, restart=60, maxiter=400, mode="mixed")
+    Lx = 0.5 * x3 + D @ x3 - 2j * k * (S @ x3)
+    assert st3["converged"] == 1 and np.linalg.norm(b - Lx) / np.linalg.norm(b) < 2e-10
+    # another single layer (no correction) with the same double layer
+    S2 = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp64", ctx)
+    x4, st4 = inti.gmres(0.5 * inti.I + D - 1j * k * S2, b, rtol=1e-10, restart=60, maxiter=400, mode="mixed")
+    Lx = 0.5 * x4 + D @ x4 - 1j * k * (S2 @ x4)
+    assert st4["converged"] == 1 and np.linalg.norm(b - Lx) / np.linalg.norm(b) < 2e-10
+    assert not np.allclose(x3, x4)
