@@ -49,7 +49,7 @@ __device__ __forceinline__ KPair helm_kernels(const double* x, const double* y, 
   const double ri = keep ? rsqrt_fast(d2) : 0.0;
   const double d = d2 * ri;
   double cs, sn;
-  expi_table_eval<double, double2>(d * kT, tab, delta, cs, sn);
+  expi_table_eval(d, kT, tab, delta, cs, sn);
   KPair o;
   o.sl = make_double2(0.0, 0.0);
   o.dl = make_double2(0.0, 0.0);

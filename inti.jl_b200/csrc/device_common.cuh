@@ -150,11 +150,18 @@ constexpr int kErrWaitTimeout = 1;
 //  * rsqrt: hardware approximation (MUFU) refined by one third-order Newton
 //    step for 1/sqrt(x): with e = 1 - x*y^2, y' = y*(1 + e/2 + 3e^2/8)
 //    (Householder's method of order 3); relative error ~(5/16)e^3.
-//  * e^{i*theta} for theta = u*delta, delta = 2*pi/kExpiTable: split
-//    u = m + f (m = rint(u), |f| <= 1/2), take e^{i*m*delta} from a table
-//    built on the host in extended precision, and e^{i*f*delta} from its
-//    Taylor series (|f*delta| <= pi/1024: sin to r^5, cos to r^4 leave
-//    truncation errors below 2e-18).
+//  * x^{-3/2} from the same seed: x^{-3/2} = y^3 (1 - e)^{-3/2}
+//    = y^3 (1 + 3e/2 + 15e^2/8 + O(e^3)), the binomial series cut after the
+//    quadratic term (relative error ~(35/16)e^3), one step instead of the
+//    refined 1/sqrt(x) and two products.
+//  * e^{i*theta} for theta = u*delta, u = d*kT, delta = 2*pi/kExpiTable:
+//    split u = m + f (m = rint(u), |f| <= 1/2), take e^{i*m*delta} from a
+//    table built on the host in extended precision, and e^{i*f*delta} from
+//    its Taylor series (|f*delta| <= pi/1024: sin to r^5, cos to r^4 leave
+//    truncation errors below 2e-18).  In FP64, m comes from adding and
+//    subtracting 1.5*2^52 (for |u| < 2^51 the rounded sum's low word is m in
+//    two's complement, the table index without a conversion instruction) and
+//    delta's powers are folded into the series' coefficients.
 // The accuracy of both is measured on the device by inti_selftest_math.
 // ---------------------------------------------------------------------------
 constexpr int kExpiTable = 1024;
@@ -170,6 +177,12 @@ __device__ __forceinline__ float rsqrt_approx_f32(float x) {
   return r;
 }
 
+// d^2 > (1e-14)^2 for d^2 >= +0 as a compare of the bit patterns (IEEE
+// order of non-negative doubles), on the integer pipe.
+__device__ __forceinline__ bool pair_keep(double d2) {
+  return __double_as_longlong(d2) > __double_as_longlong(1.0e-28);
+}
+
 // 1/sqrt(x) to ~1 ulp for normal x > 0 (inf/NaN for x == 0, as 1/sqrt).
 __device__ __forceinline__ double rsqrt_fast(double x) {
   const double y = rsqrt_approx_f64(x);
@@ -180,28 +193,51 @@ __device__ __forceinline__ double rsqrt_fast(double x) {
 }
 __device__ __forceinline__ float rsqrt_fast(float x) { return rsqrt_approx_f32(x); }
 
-template <class R, class R2>
-__device__ __forceinline__ void expi_table_eval(R u, const R2* __restrict__ tab, R delta, R& c, R& s) {
-  const R m = rint(u);
-  const R r = (u - m) * delta;
-  const R r2 = r * r;
-  R cp, sp;
-  if (sizeof(R) == 8) {
-    cp = fma(r2, fma(r2, R(1.0 / 24.0), R(-0.5)), R(1));
-    sp = fma(r2 * r, fma(r2, R(1.0 / 120.0), R(-1.0 / 6.0)), r);
-  } else {
-    // float: |r| <= pi/1024 makes r^4/24 and r^5/120 negligible
-    cp = fma(r2, R(-0.5), R(1));
-    sp = fma(r2 * r, R(-1.0 / 6.0), r);
-  }
-  int mi;
-  if (sizeof(R) == 8)
-    mi = __double2int_rn((double)m);
-  else
-    mi = __float2int_rn((float)m);
-  const R2 t = tab[mi & (kExpiTable - 1)];
-  c = fma(cp, t.x, -sp * t.y);
-  s = fma(sp, t.x, cp * t.y);
+// x^{-3/2} to a few ulp for normal x > 0 (NaN for x == 0).
+__device__ __forceinline__ double rsqrt_cube_fast(double x) {
+  const double y = rsqrt_approx_f64(x);
+  const double y2 = y * y;
+  const double e = fma(-x, y2, 1.0);
+  const double y3 = y2 * y;
+  const double p = fma(e, 1.875, 1.5);
+  return fma(y3, e * p, y3);
+}
+__device__ __forceinline__ float rsqrt_cube_fast(float x) {
+  const float y = rsqrt_approx_f32(x);
+  return y * y * y;
+}
+
+constexpr double kRoundShift = 6755399441055744.0;  // 1.5 * 2^52
+constexpr double kExpiDelta = 2.0 * 3.14159265358979323846 / 1024.0;
+// (c, s) = e^{i d kT delta}; delta = 2 pi / kExpiTable (FP32: passed in).
+__device__ __forceinline__ void expi_table_eval(double d, double kT, const double2* __restrict__ tab,
+                                                double /*delta*/, double& c, double& s) {
+  constexpr double D = kExpiDelta;
+  constexpr double C2 = -D * D / 2.0, C4 = D * D * D * D / 24.0;
+  constexpr double S3 = -D * D * D / 6.0, S5 = D * D * D * D * D / 120.0;
+  const double t = fma(d, kT, kRoundShift);
+  const double m = t - kRoundShift;
+  const double f = fma(d, kT, -m);
+  const double f2 = f * f;
+  const double cp = fma(f2, fma(f2, C4, C2), 1.0);
+  const double sp = f * fma(f2, fma(f2, S5, S3), D);
+  const double2 e = tab[__double2loint(t) & (kExpiTable - 1)];
+  c = fma(cp, e.x, -sp * e.y);
+  s = fma(sp, e.x, cp * e.y);
+}
+
+__device__ __forceinline__ void expi_table_eval(float d, float kT, const float2* __restrict__ tab, float delta,
+                                                float& c, float& s) {
+  const float u = d * kT;
+  const float m = rintf(u);
+  const float r = (u - m) * delta;
+  const float r2 = r * r;
+  // |r| <= pi/1024 makes r^4/24 and r^5/120 negligible in FP32
+  const float cp = fmaf(r2, -0.5f, 1.0f);
+  const float sp = fmaf(r2 * r, -1.0f / 6.0f, r);
+  const float2 t = tab[__float2int_rn(m) & (kExpiTable - 1)];
+  c = fmaf(cp, t.x, -sp * t.y);
+  s = fmaf(sp, t.x, cp * t.y);
 }
 
 template <class T>

@@ -107,7 +107,7 @@ __device__ __forceinline__ void theta_sd(const double* xi, const double* ni, con
       dv = make_double2(c4 * rn * (ri * ri * ri), 0.0);
     } else {
       double c, s;  // e^{ikd}
-      expi_table_eval<double, double2>(d2 * ri * kT, tab, delta, c, s);
+      expi_table_eval(d2 * ri, kT, tab, delta, c, s);
       const double g = c4 * ri;
       sv = make_double2(g * c, g * s);
       // e^{ikd} (1/d - ik) (r.n_y) / (4 pi d^2)

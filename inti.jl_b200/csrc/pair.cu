@@ -117,15 +117,17 @@ template <>
 struct MathOps<double> {
   using R2 = double2;
   static __device__ __forceinline__ double rsq(double v) { return rsqrt_fast(v); }
+  static __device__ __forceinline__ double rsq3(double v) { return rsqrt_cube_fast(v); }
   static __device__ __forceinline__ double lg(double v) { return log(v); }
-  static __device__ __forceinline__ double tol2() { return kSamePointTol2; }
+  static __device__ __forceinline__ bool keep(double d2) { return pair_keep(d2); }
 };
 template <>
 struct MathOps<float> {
   using R2 = float2;
   static __device__ __forceinline__ float rsq(float v) { return rsqrt_fast(v); }
+  static __device__ __forceinline__ float rsq3(float v) { return rsqrt_cube_fast(v); }
   static __device__ __forceinline__ float lg(float v) { return __logf(v); }
-  static __device__ __forceinline__ float tol2() { return 1.0e-28f; }
+  static __device__ __forceinline__ bool keep(float d2) { return d2 > 1.0e-28f; }
 };
 
 template <class R, int DIM, bool TN>
@@ -151,7 +153,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
   R d2 = r[0] * r[0];
 #pragma unroll
   for (int c = 1; c < DIM; ++c) d2 = fma(r[c], r[c], d2);
-  const bool keep = d2 > M::tol2();
+  const bool keep = M::keep(d2);
   if (PDE == LAPLACE) {
     if (KIND == SL) {
       if (DIM == 2) {
@@ -169,10 +171,12 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
       if (DIM == 2) {
         const R ri = keep ? R(1) / d2 : R(0);
         ar = fma(rp, ri, ar);
-      } else {
+      } else if (KIND == CF) {
         const R ri = keep ? M::rsq(d2) : R(0);
-        if (KIND == CF) ar = fma(ri, s[2 * DIM], ar);
+        ar = fma(ri, s[2 * DIM], ar);
         ar = fma(rp, ri * ri * ri, ar);
+      } else {
+        ar = fma(rp, keep ? M::rsq3(d2) : R(0), ar);
       }
     } else if (KIND == ADL) {
       R rn = r[0] * t.n[0];
@@ -183,8 +187,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
         const R ri = keep ? R(1) / d2 : R(0);
         ar = fma(rn * q, ri, ar);
       } else {
-        const R ri = keep ? M::rsq(d2) : R(0);
-        ar = fma(rn * q, ri * ri * ri, ar);
+        ar = fma(rn * q, keep ? M::rsq3(d2) : R(0), ar);
       }
     } else {  // HS: (nx.p - DIM (r.nx)(r.p)/d^2) / d^DIM
       R rn = r[0] * t.n[0], rp = r[0] * s[DIM], np = t.n[0] * s[DIM];
@@ -207,7 +210,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
     const R ri = keep ? M::rsq(d2) : R(0);
     const R d = d2 * ri;  // 0 for the self pair
     R sn, cs;
-    expi_table_eval<R, typename MathOps<R>::R2>(d * kT, tab, delta, cs, sn);
+    expi_table_eval(d, kT, tab, delta, cs, sn);
     if (KIND == SL || KIND == ADL) {
       R g_r, g_i;  // G (without 1/4pi) or the ADL factor
       if (KIND == SL) {

@@ -117,10 +117,10 @@ class Context:
 
     def selftest_math(self) -> dict:
         """Accuracy of the device's fast rsqrt / e^{iθ} helpers (see the ABI)."""
-        out = (C.c_double * 4)()
+        out = (C.c_double * 5)()
         self.check(self.lib.inti_selftest_math(self.handle, out))
         return {"rsqrt_f64_maxrel": out[0], "expi_f64_maxabs_25": out[1], "expi_f64_maxabs_1000": out[2],
-                "expi_f32_maxabs_25": out[3]}
+                "expi_f32_maxabs_25": out[3], "rsqrt_cube_f64_maxrel": out[4]}
 
     def measure_peaks(self) -> dict:
         a, b, c, t = C.c_double(), C.c_double(), C.c_double(), C.c_double()

@@ -108,9 +108,10 @@ def test_launch_counter_advances(ctx):
 
 
 def test_fast_special_functions_accuracy(ctx):
-    """The pair loops' rsqrt and e^{iθ} against extended precision."""
+    """The pair loops' rsqrt, x^{-3/2} and e^{iθ} against extended precision."""
     r = ctx.selftest_math()
     assert r["rsqrt_f64_maxrel"] < 4e-16, r
+    assert r["rsqrt_cube_f64_maxrel"] < 8e-16, r
     assert r["expi_f64_maxabs_25"] < 8e-16, r
     assert r["expi_f64_maxabs_1000"] < 2e-13, r
     assert r["expi_f32_maxabs_25"] < 4e-6, r
