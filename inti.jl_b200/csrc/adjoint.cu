@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
       double d2 = r[0] * r[0];
 #pragma unroll
       for (int c = 1; c < DIM; ++c) d2 = fma(r[c], r[c], d2);
-      if (!(d2 > kSamePointTol2)) continue;
+      if (!pair_keep(d2)) continue;
       const double gi = sg[q];
       if (DIM == 3) {
         const double ri = rsqrt_fast(d2);

@@ -45,7 +45,7 @@ __device__ __forceinline__ KPair helm_kernels(const double* x, const double* y, 
                                               bool want_sl) {
   const double r0 = x[0] - y[0], r1 = x[1] - y[1], r2 = x[2] - y[2];
   const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
-  const bool keep = d2 > kSamePointTol2;
+  const bool keep = pair_keep(d2);
   const double ri = keep ? rsqrt_fast(d2) : 0.0;
   const double d = d2 * ri;
   double cs, sn;
@@ -67,7 +67,7 @@ __device__ __forceinline__ double2 lap_kernels(const double* x, const double* y,
                                                double c2, int kind) {
   const double r0 = x[0] - y[0], r1 = x[1] - y[1], r2 = x[2] - y[2];
   const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
-  const bool keep = d2 > kSamePointTol2;
+  const bool keep = pair_keep(d2);
   const double ri = keep ? rsqrt_fast(d2) : 0.0;
   double v = 0.0;
   if (kind != SL) {

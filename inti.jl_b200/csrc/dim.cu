@@ -99,7 +99,7 @@ __device__ __forceinline__ void theta_sd(const double* xi, const double* ni, con
   if (DIM == 3 && !DERIV) {
     const double r0 = xi[0] - yj[0], r1 = xi[1] - yj[1], r2 = xi[2] - yj[2];
     const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
-    const double ri = d2 > kSamePointTol2 ? rsqrt_fast(d2) : 0.0;  // self pair: every value 0
+    const double ri = pair_keep(d2) ? rsqrt_fast(d2) : 0.0;  // self pair: every value 0
     const double rn = fma(r2, nj[2], fma(r1, nj[1], r0 * nj[0]));
     constexpr double c4 = 1.0 / (4 * kPi);
     if (PDE == LAPLACE) {

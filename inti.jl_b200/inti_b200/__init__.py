@@ -21,6 +21,7 @@ from .geometry import (
     Quadrature,
     circle_quadrature,
     curve_quadrature,
+    ball_hex_quadrature,
     disk_triangle_quadrature,
     ellipsoid_quadrature,
     gauss_legendre,
@@ -37,6 +38,7 @@ __all__ = list(_core_all) + [
     "kite_quadrature",
     "circle_quadrature",
     "curve_quadrature",
+    "ball_hex_quadrature",
     "disk_triangle_quadrature",
     "ellipsoid_quadrature",
     "p2_sphere_quadrature",

@@ -525,3 +525,68 @@ def disk_triangle_quadrature(m: int, radius: float = 1.0, a: float | None = None
     q = Quadrature(np.concatenate(coords), None, np.concatenate(weights), len(wh))
     q.meta.update(shape="disk", radius=radius, order=4)
     return q
+
+
+# ----------------------------------------------------------------------------
+# volumes (3D): the ball in curved hexahedra
+# ----------------------------------------------------------------------------
+def _cube_rule(order: int):
+    """TensorProductQuadrature(GL, GL, GL) on [0,1]³, first coordinate fastest."""
+    x, w = gauss_legendre_for_order(order)
+    X = np.array([[a, b, c] for c in x for b in x for a in x])
+    W = np.array([wa * wb * wc for wc in w for wb in w for wa in w])
+    return X, W
+
+
+def _ball_blocks(radius: float, a: float):
+    """Seven maps [0,1]³ -> ball: the central cube [-a, a]³ and six blocks
+    blending a face of that cube into the matching cube-sphere patch of the
+    bounding sphere, P(s,t,ρ) = (1-ρ) L(s,t) + ρ C(s,t) with C = R p/|p| for
+    p on the unit cube face (the patch map of `ellipsoid_quadrature`).  Each
+    returns (points, |det DP|)."""
+
+    def centre(s, t, r):
+        x = np.stack([-a + 2 * a * s, -a + 2 * a * t, -a + 2 * a * r], axis=-1)
+        return x, np.full(s.shape, 8 * a ** 3)
+
+    def outer(pid):
+        def f(s, t, r):
+            u, v = -1 + 2 * s, -1 + 2 * t
+            p, pu, pv = unit_sphere_patch(u, v, pid)
+            L, Lu, Lv = a * p, a * pu, a * pv
+            xh, xu, xv = _sphere_map(u, v, pid)
+            C, Cu, Cv = radius * xh, radius * xu, radius * xv
+            rr = r[..., None]
+            x = (1 - rr) * L + rr * C
+            xs = 2 * ((1 - rr) * Lu + rr * Cu)  # d/ds = 2 d/du
+            xt = 2 * ((1 - rr) * Lv + rr * Cv)
+            xr = C - L
+            det = np.abs(np.sum(xs * np.cross(xt, xr), axis=-1))
+            return x, det
+
+        return f
+
+    return [centre] + [outer(pid) for pid in range(1, 7)]
+
+
+def ball_hex_quadrature(m: int, qorder: int = 5, radius: float = 1.0, a: float | None = None) -> Quadrature:
+    """The ball of the given radius as 7 blocks x m³ curved hexahedra
+    (7 m³ elements), each with the tensor Gauss-Legendre rule of the given
+    order mapped through its block: x = P(y0 + h x̂), w = ŵ h³ |det DP|.
+    The outer faces lie on the cube-sphere patches of
+    ``ellipsoid_quadrature(·, ·, scaling=(R, R, R))``.  A volume quadrature
+    for the volume potential (no normals); meta ``order`` is the rule's
+    order (the default VDIM interpolation order)."""
+    a = 0.5 * radius if a is None else a
+    X, W = _cube_rule(qorder)
+    h = 1.0 / m
+    cells = np.array([(i, j, k) for k in range(m) for j in range(m) for i in range(m)], dtype=np.float64)
+    st = (cells[:, None, :] + X[None, :, :]) * h  # (m³, nq, 3)
+    coords, weights = [], []
+    for block in _ball_blocks(radius, a):
+        x, det = block(st[..., 0], st[..., 1], st[..., 2])
+        coords.append(x.reshape(-1, 3))
+        weights.append((W[None, :] * h ** 3 * det).reshape(-1))
+    q = Quadrature(np.concatenate(coords), None, np.concatenate(weights), len(W))
+    q.meta.update(shape="ball", radius=radius, order=qorder)
+    return q

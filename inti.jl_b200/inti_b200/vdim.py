@@ -1,5 +1,5 @@
 """Volume density interpolation (VDIM) correction of the volume potential
-(src/vdim.jl:30-130, 261-285; src/api.jl:282-378), 2D Laplace.
+(src/vdim.jl:30-130, 261-285; src/api.jl:282-378), Laplace in 2D and 3D.
 
     V + δV  with  δV_ij = w_j(i),  L_e w(i) = Θ[i, :]  (least squares),
 

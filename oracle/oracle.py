@@ -12,6 +12,7 @@ import os
 import subprocess
 from pathlib import Path
 
+import itertools
 import math
 
 import numpy as np
@@ -288,58 +289,71 @@ def dim_element_conds(pde, k, coords, normals, nq, elements=None):
 
 
 # ----------------------------------------------------------------------------
-# VDIM (src/vdim.jl:30-130, 261-285), 2D Laplace, restated with dense
-# coefficient arrays C[i, j] <-> x^i y^j; particular solutions of ΔP = p by
-# the Almansi expansion P = Σ_j a_j r^(2j+2) Δ^j p.
+# VDIM (src/vdim.jl:30-130, 261-285), Laplace in 2D and 3D, restated with
+# dense coefficient arrays C[i, j(, k)] <-> x^i y^j (z^k); particular
+# solutions of ΔP = p by the Almansi expansion P = Σ_j a_j r^(2j+2) Δ^j p.
 # ----------------------------------------------------------------------------
+def _ax(d, sl, nd):
+    """Index selecting `sl` along axis d of an nd-array."""
+    return tuple(sl if a == d else slice(None) for a in range(nd))
+
+
+def _along(v, d, nd):
+    """1-D array v shaped to broadcast along axis d."""
+    return v.reshape(tuple(-1 if a == d else 1 for a in range(nd)))
+
+
 def _pl_lap(C):
     out = np.zeros_like(C)
-    out[:-2, :] += C[2:, :] * (np.arange(2, C.shape[0])[:, None] * np.arange(1, C.shape[0] - 1)[:, None])
-    out[:, :-2] += C[:, 2:] * (np.arange(2, C.shape[1])[None, :] * np.arange(1, C.shape[1] - 1)[None, :])
+    nd, n = C.ndim, C.shape[0]
+    for d in range(nd):
+        k = np.arange(2, n)
+        out[_ax(d, slice(None, -2), nd)] += C[_ax(d, slice(2, None), nd)] * _along(k * (k - 1), d, nd)
     return out
 
 
 def _pl_r2(C):
     out = np.zeros_like(C)
-    out[2:, :] += C[:-2, :]
-    out[:, 2:] += C[:, :-2]
+    for d in range(C.ndim):
+        out[_ax(d, slice(2, None), C.ndim)] += C[_ax(d, slice(None, -2), C.ndim)]
     return out
 
 
 def _pl_eval(C, X):
-    i, j = np.nonzero(C)
-    return (C[i, j][None, :] * X[:, 0:1] ** i[None, :] * X[:, 1:2] ** j[None, :]).sum(axis=1)
+    idx = np.nonzero(C)
+    terms = C[idx][None, :]
+    for d, e in enumerate(idx):
+        terms = terms * X[:, d:d + 1] ** e[None, :]
+    return terms.sum(axis=1)
 
 
 def _pl_dx(C, d):
     out = np.zeros_like(C)
-    if d == 0:
-        out[:-1, :] = C[1:, :] * np.arange(1, C.shape[0])[:, None]
-    else:
-        out[:, :-1] = C[:, 1:] * np.arange(1, C.shape[1])[None, :]
+    nd, n = C.ndim, C.shape[0]
+    out[_ax(d, slice(None, -1), nd)] = C[_ax(d, slice(1, None), nd)] * _along(np.arange(1, n), d, nd)
     return out
 
 
-def vdim_basis(order, size=None):
-    """[(p, P)] for x^a y^b/(a! b!), a + b <= order (first index fastest)."""
+def vdim_basis(order, size=None, dim=2):
+    """[(p, P)] for x^α/α!, |α| <= order, the first index fastest."""
     size = size or order + 2 * (order // 2 + 1) + 3
     out = []
-    for b in range(order + 1):
-        for a in range(order + 1):
-            if a + b > order:
-                continue
-            p = np.zeros((size, size))
-            p[a, b] = 1.0 / (math.factorial(a) * math.factorial(b))
-            m, P, term, j, c = a + b, np.zeros((size, size)), p.copy(), 0, 0.0
-            while np.any(term):
-                c = 1.0 / (2 * (2 * m + 2)) if j == 0 else -c / ((2 * j + 2) * (2 * m - 2 * j + 2))
-                T = term
-                for _ in range(j + 1):
-                    T = _pl_r2(T)
-                P = P + c * T
-                term = _pl_lap(term)
-                j += 1
-            out.append((p, P))
+    for rev in itertools.product(range(order + 1), repeat=dim):
+        alpha = rev[::-1]
+        if sum(alpha) > order:
+            continue
+        p = np.zeros((size,) * dim)
+        p[alpha] = 1.0 / math.prod(math.factorial(a) for a in alpha)
+        m, P, term, j, c = sum(alpha), np.zeros((size,) * dim), p.copy(), 0, 0.0
+        while np.any(term):
+            c = 1.0 / (2 * (2 * m + dim)) if j == 0 else -c / ((2 * j + 2) * (2 * m - 2 * j + dim))
+            T = term
+            for _ in range(j + 1):
+                T = _pl_r2(T)
+            P = P + c * T
+            term = _pl_lap(term)
+            j += 1
+        out.append((p, P))
     return out
 
 
@@ -352,11 +366,11 @@ def vdim(tcoords, vcoords, vweights, nq, bcoords, bnormals, bweights, bnq, green
     T, Y = _c(tcoords), _c(vcoords)
     m = T.shape[0]
     mu = np.broadcast_to(np.asarray(green_multiplier, dtype=np.float64), (m,))
-    basis = vdim_basis(order)
+    dim = Y.shape[1]
+    basis = vdim_basis(order, dim=dim)
     b = np.stack([_pl_eval(p, Y) for p, _ in basis], axis=1)
     g0 = np.stack([_pl_eval(P, bcoords) for _, P in basis], axis=1)
-    g1 = np.stack([_pl_eval(_pl_dx(P, 0), bcoords) * bnormals[:, 0] + _pl_eval(_pl_dx(P, 1), bcoords) * bnormals[:, 1]
-                   for _, P in basis], axis=1)
+    g1 = np.stack([sum(_pl_eval(_pl_dx(P, d), bcoords) * bnormals[:, d] for d in range(dim)) for _, P in basis], axis=1)
     near_b, bS, bD = bdim_targets(LAPLACE, 0.0, T, bcoords, bnormals, bweights, bnq, mu, maxdist=maxdist)
     ipS, ixS, dvS = targets_csr(near_b, bS, bnq, len(bcoords))
     ipD, ixD, dvD = targets_csr(near_b, bD, bnq, len(bcoords))

@@ -314,3 +314,30 @@ def test_vdim_disk_known_answers(order):
         Vc = V0 + O.csr_apply(ip, ix, dv, f)
         err0, err = np.max(np.abs(V0 - exact)), np.max(np.abs(Vc - exact))
         assert err < 1e-6 and err < err0 / 1e3, (err, err0)
+
+
+# VDIM in the unit ball (3D Laplace): V[1] = (3 - r^2)/6 and
+# V[r^2] = 1/4 - r^4/20 inside (the Newton potential of radial densities).
+def test_vdim_ball_known_answers():
+    Y = G.ball_hex_quadrature(2)
+    B = G.ellipsoid_quadrature(16, 5, scaling=(1.0, 1.0, 1.0))
+    near, vals = O.vdim(Y.coords, Y.coords, Y.weights, Y.nq, B.coords, B.normals, B.weights, B.nq, -1.0, 2,
+                        same=True)
+    ip, ix, dv = O.targets_csr(near, vals, Y.nq, len(Y))
+    r2 = (Y.coords ** 2).sum(1)
+    for f, exact in ((np.ones(len(Y)), (3 - r2) / 6), (r2, 0.25 - r2 ** 2 / 20)):
+        V0 = O.apply(O.LAPLACE, O.SL, 0.0, Y.coords, None, Y.coords, None, Y.weights, f)
+        Vc = V0 + O.csr_apply(ip, ix, dv, f)
+        err0, err = np.max(np.abs(V0 - exact)), np.max(np.abs(Vc - exact))
+        assert err < 1e-6 and err < err0 / 1e3, (err, err0)
+
+
+def test_ball_quadrature_moments():
+    """Volume and second moment of the curved-hexahedron ball converge."""
+    errs = []
+    for m in (2, 3):
+        Y = G.ball_hex_quadrature(m)
+        r2 = (Y.coords ** 2).sum(1)
+        errs.append(max(abs(Y.weights.sum() - 4 * np.pi / 3), abs((Y.weights * r2).sum() - 4 * np.pi / 5)))
+        assert np.all(np.sqrt(r2) < 1.0) and Y.nq == 27 and len(Y) == 7 * m ** 3 * 27
+    assert errs[1] < 1e-4 and errs[1] < errs[0] / 10, errs
