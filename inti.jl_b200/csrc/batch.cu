@@ -9,10 +9,10 @@
 // (node, rhs) over the concatenated nodes.
 //
 // Two arithmetic forms of the pair product:
-//  * FP64 on CUDA cores (mrhs_fp64): each thread owns one target and a
-//    chunk of 16 right-hand sides; source tiles and their densities are
-//    staged in shared memory; the kernel value is computed once per pair and
-//    applied to the 16 columns.
+//  * FP64 (mrhs_mma): a CTA owns 64 targets and 64 right-hand sides; per
+//    source tile the CUDA cores evaluate each kernel value once into shared
+//    memory and the warps multiply that tile with the staged densities on
+//    the FP64 MMA path (fp64_mma.cuh).
 //  * TF32 on the tensor cores (mrhs_tc.cu): the kernel tile is generated by
 //    CUDA cores into shared memory and multiplied with the staged density
 //    block by tcgen05.mma into a TMEM accumulator.
@@ -23,12 +23,14 @@
 #include <algorithm>
 #include <cmath>
 #include <memory>
+#include <mutex>
 #include <numeric>
 #include <vector>
 
 #include "batch.h"
 #include "common.h"
 #include "device_common.cuh"
+#include "fp64_mma.cuh"
 #include "internal.h"
 
 namespace inti {
@@ -78,57 +80,124 @@ __device__ __forceinline__ double2 lap_kernels(const double* x, const double* y,
   return make_double2(v, 0.0);
 }
 
-constexpr int kMrhsBlock = 128;
-constexpr int kMrhsTile = 32;
-constexpr int kMrhsCols = 16;  // right-hand sides per thread
+constexpr int kMrhsBlock = 128;  // targets per work item
 
-// Y[c][i] = alpha * (scale * sum_j K_ij w_j X[c][j]) + beta * Y[c][i]
-// for the targets of item blockIdx.x and columns blockIdx.y*16 .. +15.
+// FP64 form on the MMA path: one CTA = 64 targets x 64 right-hand sides;
+// per tile of kMmaJ sources the CUDA cores evaluate K(x_i, y_j) w_j once per
+// pair into A (complex: slots (Re, Im)), the density rows are staged as B
+// (complex: row Re -> (Xr, Xi), row Im -> (-Xi, Xr) per column, so the
+// accumulator pairs are (Re, Im) of Y), and the warps multiply A B with the
+// FP64 MMA.  The next tile's densities and source records are loaded into
+// registers while the MMA runs and stored to shared memory after it.
+// Grid: x = 2 per 128-target work item, y = 64-column groups.
+constexpr int kMmaJ = 24;
+constexpr int kMmaCols = 64;
+constexpr int kMmaXPer = kMmaJ * kMmaCols / kMmaThreads;  // densities per thread per tile
+constexpr int kMmaSrcVals = 7 * kMmaJ;                    // x, n, w per source
+static_assert(kMmaJ * kMmaCols % kMmaThreads == 0 && kMmaSrcVals <= kMmaThreads, "staging split");
+
+template <bool CPLX>
+struct MrhsShape {
+  using Sh = MmaShape<2, 4, CPLX ? 4 : 2, kMmaJ * (CPLX ? 2 : 1), CPLX ? 2 : 1>;
+  static constexpr int NA = CPLX ? 2 : 1;
+  static constexpr size_t smem_bytes() {
+    return sizeof(double) * ((size_t)Sh::MT * Sh::LDA + (size_t)Sh::kK * Sh::LDB + kMmaSrcVals) +
+           (CPLX ? sizeof(double2) * kExpiTable : 0);
+  }
+};
+
 template <int PDE, int KIND>
-__global__ void __launch_bounds__(kMrhsBlock) mrhs_fp64(BatchArgs a) {
+__global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
   constexpr bool CPLX = PDE == HELMHOLTZ;
-  __shared__ double sx[kMrhsTile * 3], sn[kMrhsTile * 3], sw[kMrhsTile];
-  __shared__ double2 sX[kMrhsTile * kMrhsCols];
-  __shared__ double2 tab[kExpiTable];
-  const int item = blockIdx.x;
+  using MS = MrhsShape<CPLX>;
+  using Sh = typename MS::Sh;
+  constexpr int NA = MS::NA;
+  static_assert(Sh::MT == 64 && kMmaThreads % Sh::MT == 0 && kMmaJ % (kMmaThreads / Sh::MT) == 0, "shape");
+  extern __shared__ __align__(16) double smem_d[];
+  double* As = smem_d;
+  double* Bs = As + Sh::MT * Sh::LDA;
+  double* ssrc = Bs + Sh::kK * Sh::LDB;  // [x y z](J) [n](J) [w](J)
+  double* sx = ssrc;
+  double* sn = ssrc + 3 * kMmaJ;
+  double* sw = ssrc + 6 * kMmaJ;
+  double2* tab = reinterpret_cast<double2*>(ssrc + kMmaSrcVals);
+  const int tid = threadIdx.x;
+  const int item = blockIdx.x >> 1;
   const int s = a.item_surf[item];
   const int64_t off = a.off[s], n = a.off[s + 1] - off;
-  const int64_t i_loc = (int64_t)a.item_block[item] * kMrhsBlock + threadIdx.x;
-  const bool active = i_loc < n;
-  const int64_t i = off + min(i_loc, n - 1);
-  const int c0 = blockIdx.y * kMrhsCols;
-  const int ncol = min(kMrhsCols, a.nrhs - c0);
+  const int64_t base = (int64_t)a.item_block[item] * 128 + (blockIdx.x & 1) * Sh::MT;
+  if (base >= n) return;  // second half of a short last block (uniform per CTA)
+  const int c0 = blockIdx.y * kMmaCols;
+  const int ncol = min(kMmaCols, a.nrhs - c0);
   if (CPLX)
-    for (int q = threadIdx.x; q < kExpiTable; q += kMrhsBlock) tab[q] = a.expi[q];
-  double xi[3] = {a.coords[3 * i], a.coords[3 * i + 1], a.coords[3 * i + 2]};
-  double2 acc[kMrhsCols];
-#pragma unroll
-  for (int c = 0; c < kMrhsCols; ++c) acc[c] = make_double2(0.0, 0.0);
+    for (int q = tid; q < kExpiTable; q += kMmaThreads) tab[q] = a.expi[q];
+  // phase-1 role: target m, sources r0, r0 + R, ...
+  constexpr int R = kMmaThreads / Sh::MT;
+  const int m = tid % Sh::MT, r0 = tid / Sh::MT;
+  const int64_t i = off + min(base + m, n - 1);
+  const double xi[3] = {a.coords[3 * i], a.coords[3 * i + 1], a.coords[3 * i + 2]};
   const double kT = a.k * kExpiTable / (2 * kPi), delta = 2 * kPi / kExpiTable;
-  for (int64_t j0 = 0; j0 < n; j0 += kMrhsTile) {
-    __syncthreads();
-    for (int q = threadIdx.x; q < kMrhsTile; q += kMrhsBlock) {
+  // staging roles: density element e = tid + r*256 -> (source e % J, column e / J)
+  // (consecutive threads read consecutive nodes of one column); source value tid
+  double2 xpre[kMmaXPer];
+  double spre = 0.0;
+  auto prefetch = [&](int64_t j0) {
+#pragma unroll
+    for (int r = 0; r < kMmaXPer; ++r) {
+      const int e = tid + r * kMmaThreads, q = e % kMmaJ, c = e / kMmaJ;
       const int64_t j = j0 + q;
-      const bool in = j < n;
-      for (int c = 0; c < 3; ++c) {
-        sx[3 * q + c] = in ? a.coords[3 * (off + j) + c] : 0.0;
-        sn[3 * q + c] = (in && a.normals) ? a.normals[3 * (off + j) + c] : 0.0;
-      }
-      sw[q] = in ? a.weights[off + j] : 0.0;
-    }
-    for (int q = threadIdx.x; q < kMrhsTile * kMrhsCols; q += kMrhsBlock) {
-      const int jj = q / kMrhsCols, c = q % kMrhsCols;
-      const int64_t j = j0 + jj;
       double2 v = make_double2(0.0, 0.0);
       if (j < n && c < ncol) {
         const int64_t idx = (int64_t)(c0 + c) * a.ldx + off + j;
         v = CPLX ? reinterpret_cast<const double2*>(a.x)[idx] : make_double2(a.x[idx], 0.0);
       }
-      sX[q] = v;
+      xpre[r] = v;
     }
+    if (tid < kMmaSrcVals) {
+      const int f = tid / kMmaJ, q = tid % kMmaJ;  // field 0..6 of source q
+      const int64_t j = j0 + q;
+      double v = 0.0;
+      if (j < n) {
+        if (f < 3) v = a.coords[3 * (off + j) + f];
+        else if (f < 6) v = a.normals ? a.normals[3 * (off + j) + f - 3] : 0.0;
+        else v = a.weights[off + j];
+      }
+      spre = v;
+    }
+  };
+  auto store_staged = [&]() {
+#pragma unroll
+    for (int r = 0; r < kMmaXPer; ++r) {
+      const int e = tid + r * kMmaThreads, q = e % kMmaJ, c = e / kMmaJ;
+      const double2 v = xpre[r];
+      if (CPLX) {
+        const int col = Sh::bcol(2 * q, 2 * c);
+        *reinterpret_cast<double2*>(&Bs[(2 * q) * Sh::LDB + col]) = v;
+        *reinterpret_cast<double2*>(&Bs[(2 * q + 1) * Sh::LDB + col]) = make_double2(-v.y, v.x);
+      } else {
+        Bs[q * Sh::LDB + Sh::bcol(q, c)] = v.x;
+      }
+    }
+    if (tid < kMmaSrcVals) {
+      const int f = tid / kMmaJ, q = tid % kMmaJ;
+      if (f < 3) sx[3 * q + f] = spre;
+      else if (f < 6) sn[3 * q + f - 3] = spre;
+      else sw[q] = spre;
+    }
+  };
+  double acc[4][Sh::kNT][2];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < Sh::kNT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+  prefetch(0);
+  for (int64_t j0 = 0; j0 < n; j0 += kMmaJ) {
+    __syncthreads();  // the previous tile's A and B are consumed
+    store_staged();
     __syncthreads();
-    const int cnt = (int)(n - j0 < kMrhsTile ? n - j0 : kMrhsTile);
-    for (int q = 0; q < cnt; ++q) {
+    // phase 1: kernel values into A
+#pragma unroll 2
+    for (int q = r0; q < kMmaJ; q += R) {
       double2 kv;
       if (CPLX) {
         const KPair kp = helm_kernels(xi, &sx[3 * q], &sn[3 * q], a.k, kT, delta, tab, KIND != SL, KIND != DL);
@@ -136,42 +205,57 @@ __global__ void __launch_bounds__(kMrhsBlock) mrhs_fp64(BatchArgs a) {
           kv = kp.sl;
         else if (KIND == DL)
           kv = kp.dl;
-        else  // c1*DL + c2*SL, complex coefficients
+        else
           kv = make_double2(a.c1r * kp.dl.x - a.c1i * kp.dl.y + a.c2r * kp.sl.x - a.c2i * kp.sl.y,
                             a.c1r * kp.dl.y + a.c1i * kp.dl.x + a.c2r * kp.sl.y + a.c2i * kp.sl.x);
       } else {
         kv = lap_kernels(xi, &sx[3 * q], &sn[3 * q], a.c1r, a.c2r, KIND);
       }
       const double w = sw[q];
-      kv.x *= w;
-      kv.y *= w;
-#pragma unroll
-      for (int c = 0; c < kMrhsCols; ++c) {
-        const double2 xv = sX[q * kMrhsCols + c];
-        acc[c].x = fma(kv.x, xv.x, fma(-kv.y, xv.y, acc[c].x));
-        acc[c].y = fma(kv.x, xv.y, fma(kv.y, xv.x, acc[c].y));
+      if (CPLX) {
+        *reinterpret_cast<double2*>(&As[m * Sh::LDA + NA * q]) = make_double2(kv.x * w, kv.y * w);
+      } else {
+        As[m * Sh::LDA + q] = kv.x * w;
       }
     }
+    __syncthreads();
+    if (j0 + kMmaJ < n) prefetch(j0 + kMmaJ);  // in flight during the MMA phase
+    // phase 2: Y += A B on the FP64 MMA path
+    mma_tile<Sh>(As, Bs, acc);
   }
-  if (!active) return;
   const double sc = 1.0 / (4 * kPi);
 #pragma unroll
-  for (int c = 0; c < kMrhsCols; ++c) {
-    if (c >= ncol) break;
-    const int64_t idx = (int64_t)(c0 + c) * a.ldy + i;
-    double yr = sc * acc[c].x, yi = sc * acc[c].y;
-    double orr = a.ar * yr - a.ai * yi, oi = a.ar * yi + a.ai * yr;
-    if (CPLX) {
-      double2* Y = reinterpret_cast<double2*>(a.y);
-      if (!a.beta_zero) {
-        const double2 yo = Y[idx];
-        orr += a.br * yo.x - a.bi * yo.y;
-        oi += a.br * yo.y + a.bi * yo.x;
+  for (int mt = 0; mt < 4; ++mt) {
+    const int64_t il = base + mma_row<Sh>(mt);
+    if (il >= n) continue;
+    const int64_t iy = off + il;
+#pragma unroll
+    for (int nt = 0; nt < Sh::kNT; ++nt) {
+      const int col = mma_col<Sh>(nt);
+      if (CPLX) {
+        const int c = col / 2;
+        if (c >= ncol) continue;
+        const int64_t idx = (int64_t)(c0 + c) * a.ldy + iy;
+        const double yr = sc * acc[mt][nt][0], yi = sc * acc[mt][nt][1];
+        double orr = a.ar * yr - a.ai * yi, oi = a.ar * yi + a.ai * yr;
+        double2* Y = reinterpret_cast<double2*>(a.y);
+        if (!a.beta_zero) {
+          const double2 yo = Y[idx];
+          orr += a.br * yo.x - a.bi * yo.y;
+          oi += a.br * yo.y + a.bi * yo.x;
+        }
+        Y[idx] = make_double2(orr, oi);
+      } else {
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int c = col + e;
+          if (c >= ncol) continue;
+          const int64_t idx = (int64_t)(c0 + c) * a.ldy + iy;
+          double o = a.ar * sc * acc[mt][nt][e];
+          if (!a.beta_zero) o += a.br * a.y[idx];
+          a.y[idx] = o;
+        }
       }
-      Y[idx] = make_double2(orr, oi);
-    } else {
-      if (!a.beta_zero) orr += a.br * a.y[idx];
-      a.y[idx] = orr;
     }
   }
 }
@@ -355,11 +439,17 @@ void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t l
     if (!cplx) throw Error(INTI_E_UNSUPPORTED, "the tensor-core form is implemented for Helmholtz");
     mrhs_tc_launch(b, a);
   } else if (precision == INTI_FP64) {
-    dim3 grid((unsigned)b->nitems, (unsigned)((nrhs + kMrhsCols - 1) / kMrhsCols));
+    dim3 grid((unsigned)(2 * b->nitems), (unsigned)((nrhs + kMmaCols - 1) / kMmaCols));
     ProfScope ps(ctx, "batch");
     auto go = [&](auto pc, auto kc) {
       constexpr int P = decltype(pc)::value, K = decltype(kc)::value;
-      mrhs_fp64<P, K><<<grid, kMrhsBlock, 0, ctx->stream>>>(a);
+      constexpr size_t smem = MrhsShape<P == HELMHOLTZ>::smem_bytes();
+      // the attribute is set once per kernel, outside any stream capture
+      static std::once_flag once;
+      std::call_once(once, [] {
+        cudaFuncSetAttribute(mrhs_mma<P, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      });
+      mrhs_mma<P, K><<<grid, kMmaThreads, smem, ctx->stream>>>(a);
     };
     if (cplx) {
       if (b->kind == SL) go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, SL>());

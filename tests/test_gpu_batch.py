@@ -45,17 +45,19 @@ def per_surface(op, quads, kind, corrs, X, cD=1.0, cS=1.0, ctx=None):
 
 @pytest.mark.parametrize("kind", ["SL", "DL", "CF"])
 @pytest.mark.parametrize("pde", ["helmholtz", "laplace"])
-def test_batch_fp64_matches_single_surface_operators(ctx, kind, pde):
+@pytest.mark.parametrize("nrhs", [5, 70])
+def test_batch_fp64_matches_single_surface_operators(ctx, kind, pde, nrhs):
+    """70 columns: two 64-column groups, the second ragged."""
     quads = stars()
     op = inti.Helmholtz(k=5.0, dim=3) if pde == "helmholtz" else inti.Laplace(dim=3)
     corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
     cD, cS = (1.0, -5.0j) if pde == "helmholtz" else (1.0, 0.5)
     B = inti.BatchOperator(op, quads, kind, corrs, cD, cS, ctx=ctx)
-    X = rhs(B.n, 5, pde == "helmholtz")
+    X = rhs(B.n, nrhs, pde == "helmholtz")
     ref = per_surface(op, quads, kind, corrs, X, cD, cS, ctx)
     assert relerr(B.apply(X), ref) < 1e-12
     # alpha / beta
-    Y0 = rhs(B.n, 5, pde == "helmholtz", 9)
+    Y0 = rhs(B.n, nrhs, pde == "helmholtz", 9)
     got = B.apply(X, Y=Y0, alpha=0.5, beta=2.0)
     assert relerr(got, 0.5 * ref + 2.0 * Y0) < 1e-12
 
