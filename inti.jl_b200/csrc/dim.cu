@@ -18,10 +18,12 @@
 
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "common.h"
 #include "device_common.cuh"
+#include "fp64_mma.cuh"
 #include "internal.h"
 
 namespace inti {
@@ -206,6 +208,155 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
 #pragma unroll
     for (int q = 0; q < NS; ++q)
       if (q < ns) out[q] = make_double2(Sc::re(acc[q]), Sc::im(acc[q]));
+  }
+}
+
+// Theta partials on the FP64 MMA path (3D value kernels): per tile of J
+// sources the CUDA cores evaluate (S w, D w) once per pair into A (complex:
+// slots Sr, Si, Dr, Di), the trace rows are staged as B (real: rows g1, -g0;
+// complex, with (Re, Im) column pairs: (g1r, g1i), (-g1i, g1r), (-g0r, -g0i),
+// (g0i, -g0r)), and the warps multiply A B with the FP64 MMA.  The next
+// tile's traces and source records are loaded during the MMA phase.  Same
+// partial layout as dim_theta.
+template <int PDE>
+struct ThetaMma;
+template <>
+struct ThetaMma<LAPLACE> {
+  static constexpr int J = 16, NA = 2, kMaxNs = 32;
+  using Sh = MmaShape<8, 1, 4, J * NA, 1>;  // 256 targets x 32 columns
+};
+template <>
+struct ThetaMma<HELMHOLTZ> {
+  static constexpr int J = 8, NA = 4, kMaxNs = 24;
+  using Sh = MmaShape<4, 2, 3, J * NA, 2>;  // 128 targets x 24 complex columns
+};
+template <int PDE>
+constexpr size_t theta_mma_smem() {
+  using Sh = typename ThetaMma<PDE>::Sh;
+  return sizeof(double) * ((size_t)Sh::MT * Sh::LDA + (size_t)Sh::kK * Sh::LDB + 7 * ThetaMma<PDE>::J) +
+         (PDE == HELMHOLTZ ? sizeof(double2) * kExpiTable : 0);
+}
+
+template <int PDE>
+__global__ void __launch_bounds__(kMmaThreads, 2) dim_theta_mma(
+    int64_t m, int64_t n, int ns, const double* __restrict__ tx, const double* __restrict__ x,
+    const double* __restrict__ nrm, const double* __restrict__ w, const double2* __restrict__ g0,
+    const double2* __restrict__ g1, double k, double kT, double delta, const double2* __restrict__ tab_g,
+    int tiles_per_split, double2* __restrict__ partial) {
+  using TM = ThetaMma<PDE>;
+  using Sh = typename TM::Sh;
+  constexpr bool CPLX = PDE == HELMHOLTZ;
+  constexpr int J = TM::J, NA = TM::NA;
+  constexpr int R = kMmaThreads / Sh::MT;                            // threads per target in phase 1
+  constexpr int XPER = (J * TM::kMaxNs + kMmaThreads - 1) / kMmaThreads;  // trace values per thread
+  static_assert(J % R == 0 && 7 * J <= kMmaThreads, "shape");
+  extern __shared__ __align__(16) double smem_d[];
+  double* As = smem_d;
+  double* Bs = As + Sh::MT * Sh::LDA;
+  double* sx = Bs + Sh::kK * Sh::LDB;
+  double* sn = sx + 3 * J;
+  double* sw = sx + 6 * J;
+  double2* tab = reinterpret_cast<double2*>(sx + 7 * J);
+  const int tid = threadIdx.x;
+  const int64_t base = (int64_t)blockIdx.x * Sh::MT;
+  const int mloc = tid % Sh::MT, r0 = tid / Sh::MT;
+  const int64_t ii = min(base + mloc, m - 1);
+  const double xi[3] = {tx[3 * ii], tx[3 * ii + 1], tx[3 * ii + 2]};
+  for (int q = tid; q < Sh::kK * Sh::LDB; q += kMmaThreads) Bs[q] = 0.0;  // padding columns stay zero
+  if (CPLX)
+    for (int q = tid; q < kExpiTable; q += kMmaThreads) tab[q] = tab_g[q];
+  const int64_t ntile = (n + J - 1) / J;
+  const int64_t t0 = (int64_t)blockIdx.y * tiles_per_split;
+  const int64_t t1 = min(ntile, t0 + tiles_per_split);
+  const int tot = J * ns;  // trace values per tile and array
+  double2 p0[XPER], p1[XPER];
+  double spre = 0.0;
+  auto prefetch = [&](int64_t t) {
+    const int64_t j0 = t * J;
+#pragma unroll
+    for (int r = 0; r < XPER; ++r) {
+      const int e = tid + r * kMmaThreads;
+      const int64_t j = j0 + e / ns;
+      const bool in = e < tot && j < n;
+      const int64_t idx = j0 * ns + e;  // traces are node-major, ns per node
+      p0[r] = in ? g0[idx] : make_double2(0.0, 0.0);
+      p1[r] = in ? g1[idx] : make_double2(0.0, 0.0);
+    }
+    if (tid < 7 * J) {
+      const int f = tid / J, q = tid % J;
+      const int64_t j = j0 + q;
+      double v = 0.0;
+      if (j < n) v = f < 3 ? x[3 * j + f] : (f < 6 ? nrm[3 * j + f - 3] : w[j]);
+      spre = v;
+    }
+  };
+  auto store_staged = [&]() {
+#pragma unroll
+    for (int r = 0; r < XPER; ++r) {
+      const int e = tid + r * kMmaThreads;
+      if (e >= tot) continue;
+      const int q = e / ns, kk = e % ns;
+      const double2 a0 = p0[r], a1 = p1[r];
+      if (CPLX) {
+        const int k0 = NA * q;
+        *reinterpret_cast<double2*>(&Bs[(k0 + 0) * Sh::LDB + Sh::bcol(k0 + 0, 2 * kk)]) = a1;
+        *reinterpret_cast<double2*>(&Bs[(k0 + 1) * Sh::LDB + Sh::bcol(k0 + 1, 2 * kk)]) = make_double2(-a1.y, a1.x);
+        *reinterpret_cast<double2*>(&Bs[(k0 + 2) * Sh::LDB + Sh::bcol(k0 + 2, 2 * kk)]) = make_double2(-a0.x, -a0.y);
+        *reinterpret_cast<double2*>(&Bs[(k0 + 3) * Sh::LDB + Sh::bcol(k0 + 3, 2 * kk)]) = make_double2(a0.y, -a0.x);
+      } else {
+        Bs[(2 * q) * Sh::LDB + Sh::bcol(2 * q, kk)] = a1.x;
+        Bs[(2 * q + 1) * Sh::LDB + Sh::bcol(2 * q + 1, kk)] = -a0.x;
+      }
+    }
+    if (tid < 7 * J) {
+      const int f = tid / J, q = tid % J;
+      if (f < 3) sx[3 * q + f] = spre;
+      else if (f < 6) sn[3 * q + f - 3] = spre;
+      else sw[q] = spre;
+    }
+  };
+  double acc[4][Sh::kNT][2];
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+    for (int nt = 0; nt < Sh::kNT; ++nt) acc[mt][nt][0] = acc[mt][nt][1] = 0.0;
+  if (t0 < t1) prefetch(t0);
+  for (int64_t t = t0; t < t1; ++t) {
+    __syncthreads();  // previous tile consumed (and B zeroed, table loaded)
+    store_staged();
+    __syncthreads();
+#pragma unroll 2
+    for (int q = r0; q < J; q += R) {
+      double2 sv, dv;
+      theta_sd<PDE, 3, false>(xi, xi, &sx[3 * q], &sn[3 * q], k, kT, delta, tab, sv, dv);
+      const double wq = sw[q];
+      if (CPLX) {
+        double* a = &As[mloc * Sh::LDA + NA * q];
+        *reinterpret_cast<double2*>(a) = make_double2(sv.x * wq, sv.y * wq);
+        *reinterpret_cast<double2*>(a + 2) = make_double2(dv.x * wq, dv.y * wq);
+      } else {
+        *reinterpret_cast<double2*>(&As[mloc * Sh::LDA + NA * q]) = make_double2(sv.x * wq, dv.x * wq);
+      }
+    }
+    __syncthreads();
+    if (t + 1 < t1) prefetch(t + 1);
+    mma_tile<Sh>(As, Bs, acc);
+  }
+#pragma unroll
+  for (int mt = 0; mt < 4; ++mt) {
+    const int64_t i = base + mma_row<Sh>(mt);
+    if (i >= m) continue;
+    double2* out = partial + ((int64_t)blockIdx.y * m + i) * ns;
+#pragma unroll
+    for (int nt = 0; nt < Sh::kNT; ++nt) {
+      const int col = mma_col<Sh>(nt);
+      if (CPLX) {
+        if (col / 2 < ns) out[col / 2] = make_double2(acc[mt][nt][0], acc[mt][nt][1]);
+      } else {
+        if (col < ns) out[col] = make_double2(acc[mt][nt][0], 0.0);
+        if (col + 1 < ns) out[col + 1] = make_double2(acc[mt][nt][1], 0.0);
+      }
+    }
   }
 }
 
@@ -548,6 +699,34 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
   auto run = [&](auto pde_c, auto dim_c) {
     constexpr int P = decltype(pde_c)::value;
     constexpr int D = decltype(dim_c)::value;
+    const int64_t tot = m * ns;
+    if constexpr (D == 3) {
+      if (!derivative && ns <= ThetaMma<P>::kMaxNs) {
+        // FP64 MMA form; split over sources for >= 8 waves of 2 CTAs per SM
+        using TM = ThetaMma<P>;
+        const int64_t blocks = (m + TM::Sh::MT - 1) / TM::Sh::MT;
+        const int64_t ntile = (n + TM::J - 1) / TM::J;
+        const int64_t want = (int64_t)ctx->num_sms * 16;
+        int split = (int)std::max<int64_t>(1, std::min<int64_t>({ntile, (want + blocks - 1) / blocks, 64}));
+        const int tps = (int)((ntile + split - 1) / split);
+        split = (int)((ntile + tps - 1) / tps);
+        wk.part.ensure(sizeof(double2) * (size_t)split * m * ns);
+        constexpr size_t smem = theta_mma_smem<P>();
+        static std::once_flag once;
+        std::call_once(once, [] {
+          cudaFuncSetAttribute(dim_theta_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        });
+        ProfScope pd(ctx, "dim");
+        dim_theta_mma<P><<<dim3((unsigned)blocks, (unsigned)split), kMmaThreads, smem, ctx->stream>>>(
+            m, n, ns, tx, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re, k_re * kExpiTable / (2 * kPi),
+            2 * kPi / kExpiTable, P == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, tps, wk.part.as<double2>());
+        ctx->launches++;
+        dim_theta_reduce<P, D, false><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
+            m, ns, split, tx, tn, wk.d_xs.as<double>(), mu, k_re, wk.part.as<double2>(), wk.theta.as<double2>());
+        ctx->launches++;
+        return;
+      }
+    }
     // split over sources so the grid covers the device
     const int64_t blocks = (m + kThetaBlock - 1) / kThetaBlock;
     const int64_t ntile = (n + kThetaTile - 1) / kThetaTile;
@@ -556,7 +735,6 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
     const int tps = (int)((ntile + split - 1) / split);
     split = (int)((ntile + tps - 1) / tps);
     wk.part.ensure(sizeof(double2) * (size_t)split * m * ns);
-    const int64_t tot = m * ns;
     auto theta_go = [&](auto nsb, auto deriv_c) {
       constexpr int NSB = decltype(nsb)::value;
       constexpr bool DV = decltype(deriv_c)::value;
