@@ -559,6 +559,33 @@ static int apply_common(inti_op* op, const double* x, int64_t ldx, double* y, in
     const int64_t nout = transpose ? op->source->n : op->target->n;
     require(ldx >= nin && ldy >= nout, INTI_E_SHAPE, "leading dimension smaller than the vector length");
     const bool bz = !beta || (beta[0] == 0.0 && beta[1] == 0.0);
+    if (!transpose && nrhs >= kMrhsMinColumns && op_mrhs_supported(op)) {
+      // all columns at once: each kernel value evaluated once per 64 columns
+      const double* xd = x;
+      double* yd = y;
+      int64_t lx = ldx, ly = ldy;
+      const size_t cx = sizeof(double) * comps * nin, cy = sizeof(double) * comps * nout;
+      if (!on_device) {
+        op->mx.ensure(cx * nrhs);
+        op->my.ensure(cy * nrhs);
+        INTI_CUDA(cudaMemcpy2DAsync(op->mx.p, cx, x, sizeof(double) * comps * ldx, cx, nrhs, cudaMemcpyHostToDevice,
+                                    ctx->stream));
+        if (!bz)
+          INTI_CUDA(cudaMemcpy2DAsync(op->my.p, cy, y, sizeof(double) * comps * ldy, cy, nrhs,
+                                      cudaMemcpyHostToDevice, ctx->stream));
+        xd = op->mx.as<double>();
+        yd = op->my.as<double>();
+        lx = nin;
+        ly = nout;
+      }
+      op_apply_mrhs(op, xd, lx, yd, ly, nrhs, alpha, beta);
+      if (!on_device) {
+        INTI_CUDA(cudaMemcpy2DAsync(y, sizeof(double) * comps * ldy, op->my.p, cy, cy, nrhs, cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+        sync_and_check(ctx);
+      }
+      return;
+    }
     if (transpose && !op->tpartial.p) op_prepare_transpose(op);
     for (int32_t r = 0; r < nrhs; ++r) {
       const double* xr = x + (size_t)r * ldx * comps;

@@ -89,29 +89,31 @@ constexpr int kMrhsBlock = 128;  // targets per work item
 // accumulator pairs are (Re, Im) of Y), and the warps multiply A B with the
 // FP64 MMA.  The next tile's densities and source records are loaded into
 // registers while the MMA runs and stored to shared memory after it.
-// Grid: x = 2 per 128-target work item, y = 64-column groups.
+// Grid: x = 2 per 128-target work item, y = groups of RHS columns.  RHS =
+// columns per CTA: 64, or 16 (complex) / 32 (real) for narrow applies.
 constexpr int kMmaJ = 24;
-constexpr int kMmaCols = 64;
-constexpr int kMmaXPer = kMmaJ * kMmaCols / kMmaThreads;  // densities per thread per tile
-constexpr int kMmaSrcVals = 7 * kMmaJ;                    // x, n, w per source
-static_assert(kMmaJ * kMmaCols % kMmaThreads == 0 && kMmaSrcVals <= kMmaThreads, "staging split");
+constexpr int kMmaSrcVals = 7 * kMmaJ;  // x, n, w per source
+static_assert(kMmaSrcVals <= kMmaThreads, "staging split");
 
-template <bool CPLX>
+template <bool CPLX, int RHS>
 struct MrhsShape {
-  using Sh = MmaShape<2, 4, CPLX ? 4 : 2, kMmaJ * (CPLX ? 2 : 1), CPLX ? 2 : 1>;
   static constexpr int NA = CPLX ? 2 : 1;
+  using Sh = MmaShape<2, 4, RHS * NA / 32, kMmaJ * NA, CPLX ? 2 : 1>;
+  static_assert(Sh::NCOL == RHS * NA, "columns");
+  static constexpr int XPER = (kMmaJ * RHS + kMmaThreads - 1) / kMmaThreads;  // densities per thread
   static constexpr size_t smem_bytes() {
     return sizeof(double) * ((size_t)Sh::MT * Sh::LDA + (size_t)Sh::kK * Sh::LDB + kMmaSrcVals) +
            (CPLX ? sizeof(double2) * kExpiTable : 0);
   }
 };
 
-template <int PDE, int KIND>
+template <int PDE, int KIND, int RHS>
 __global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
   constexpr bool CPLX = PDE == HELMHOLTZ;
-  using MS = MrhsShape<CPLX>;
+  using MS = MrhsShape<CPLX, RHS>;
   using Sh = typename MS::Sh;
   constexpr int NA = MS::NA;
+  constexpr int XPER = MS::XPER;
   static_assert(Sh::MT == 64 && kMmaThreads % Sh::MT == 0 && kMmaJ % (kMmaThreads / Sh::MT) == 0, "shape");
   extern __shared__ __align__(16) double smem_d[];
   double* As = smem_d;
@@ -123,31 +125,46 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
   double2* tab = reinterpret_cast<double2*>(ssrc + kMmaSrcVals);
   const int tid = threadIdx.x;
   const int item = blockIdx.x >> 1;
-  const int s = a.item_surf[item];
-  const int64_t off = a.off[s], n = a.off[s + 1] - off;
-  const int64_t base = (int64_t)a.item_block[item] * 128 + (blockIdx.x & 1) * Sh::MT;
-  if (base >= n) return;  // second half of a short last block (uniform per CTA)
-  const int c0 = blockIdx.y * kMmaCols;
-  const int ncol = min(kMmaCols, a.nrhs - c0);
+  // targets toff + [0, tn), sources off + [0, n) (one surface, or the operator)
+  int64_t toff, tn, off, n, blk;
+  const double* tc;
+  if (a.tcoords) {
+    toff = 0;
+    tn = a.gm;
+    off = 0;
+    n = a.gn;
+    blk = item;
+    tc = a.tcoords;
+  } else {
+    const int s = a.item_surf[item];
+    off = toff = a.off[s];
+    n = tn = a.off[s + 1] - off;
+    blk = a.item_block[item];
+    tc = a.coords;
+  }
+  const int64_t base = blk * 128 + (blockIdx.x & 1) * Sh::MT;
+  if (base >= tn) return;  // second half of a short last block (uniform per CTA)
+  const int c0 = blockIdx.y * RHS;
+  const int ncol = min(RHS, a.nrhs - c0);
   if (CPLX)
     for (int q = tid; q < kExpiTable; q += kMmaThreads) tab[q] = a.expi[q];
   // phase-1 role: target m, sources r0, r0 + R, ...
   constexpr int R = kMmaThreads / Sh::MT;
   const int m = tid % Sh::MT, r0 = tid / Sh::MT;
-  const int64_t i = off + min(base + m, n - 1);
-  const double xi[3] = {a.coords[3 * i], a.coords[3 * i + 1], a.coords[3 * i + 2]};
+  const int64_t i = toff + min(base + m, tn - 1);
+  const double xi[3] = {tc[3 * i], tc[3 * i + 1], tc[3 * i + 2]};
   const double kT = a.k * kExpiTable / (2 * kPi), delta = 2 * kPi / kExpiTable;
   // staging roles: density element e = tid + r*256 -> (source e % J, column e / J)
   // (consecutive threads read consecutive nodes of one column); source value tid
-  double2 xpre[kMmaXPer];
+  double2 xpre[XPER];
   double spre = 0.0;
   auto prefetch = [&](int64_t j0) {
 #pragma unroll
-    for (int r = 0; r < kMmaXPer; ++r) {
+    for (int r = 0; r < XPER; ++r) {
       const int e = tid + r * kMmaThreads, q = e % kMmaJ, c = e / kMmaJ;
       const int64_t j = j0 + q;
       double2 v = make_double2(0.0, 0.0);
-      if (j < n && c < ncol) {
+      if (j < n && c < ncol) {  // c < ncol <= RHS also bounds e < J * RHS
         const int64_t idx = (int64_t)(c0 + c) * a.ldx + off + j;
         v = CPLX ? reinterpret_cast<const double2*>(a.x)[idx] : make_double2(a.x[idx], 0.0);
       }
@@ -167,8 +184,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
   };
   auto store_staged = [&]() {
 #pragma unroll
-    for (int r = 0; r < kMmaXPer; ++r) {
+    for (int r = 0; r < XPER; ++r) {
       const int e = tid + r * kMmaThreads, q = e % kMmaJ, c = e / kMmaJ;
+      if (c >= RHS) continue;  // (J * RHS not a multiple of the block)
       const double2 v = xpre[r];
       if (CPLX) {
         const int col = Sh::bcol(2 * q, 2 * c);
@@ -227,8 +245,8 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
 #pragma unroll
   for (int mt = 0; mt < 4; ++mt) {
     const int64_t il = base + mma_row<Sh>(mt);
-    if (il >= n) continue;
-    const int64_t iy = off + il;
+    if (il >= tn) continue;
+    const int64_t iy = toff + il;
 #pragma unroll
     for (int nt = 0; nt < Sh::kNT; ++nt) {
       const int col = mma_col<Sh>(nt);
@@ -408,6 +426,45 @@ inti_batch* batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* q
   return b.release();
 }
 
+// Launch of the FP64 MMA kernel for one (pde, kind); the dynamic shared
+// memory attribute is set once per kernel, outside any stream capture.
+// blocks = 128-target work items; the column width per CTA is 64, or the
+// narrow one when all columns fit in it.
+static void mrhs_mma_launch(inti_ctx* ctx, int pde, int kind, const BatchArgs& a, int64_t blocks) {
+  auto go = [&](auto pc, auto kc) {
+    constexpr int P = decltype(pc)::value, K = decltype(kc)::value;
+    constexpr int narrow = P == HELMHOLTZ ? 16 : 32;
+    auto launch = [&](auto rc) {
+      constexpr int RHS = decltype(rc)::value;
+      constexpr size_t smem = MrhsShape<P == HELMHOLTZ, RHS>::smem_bytes();
+      auto* kern = &mrhs_mma<P, K, RHS>;
+      static std::once_flag once;
+      std::call_once(once, [kern] {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      });
+      const dim3 grid((unsigned)(2 * blocks), (unsigned)((a.nrhs + RHS - 1) / RHS));
+      kern<<<grid, kMmaThreads, smem, ctx->stream>>>(a);
+    };
+    if (a.nrhs <= narrow)
+      launch(std::integral_constant<int, narrow>());
+    else
+      launch(std::integral_constant<int, 64>());
+  };
+  using H = std::integral_constant<int, HELMHOLTZ>;
+  using Lp = std::integral_constant<int, LAPLACE>;
+  if (pde == INTI_HELMHOLTZ) {
+    if (kind == SL) go(H(), std::integral_constant<int, SL>());
+    else if (kind == DL) go(H(), std::integral_constant<int, DL>());
+    else go(H(), std::integral_constant<int, CF>());
+  } else {
+    if (kind == SL) go(Lp(), std::integral_constant<int, SL>());
+    else if (kind == DL) go(Lp(), std::integral_constant<int, DL>());
+    else go(Lp(), std::integral_constant<int, CF>());
+  }
+  ctx->launches++;
+  INTI_CUDA(cudaGetLastError());
+}
+
 void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
                         int32_t nrhs, const double* alpha, const double* beta) {
   inti_ctx* ctx = b->ctx;
@@ -439,28 +496,8 @@ void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t l
     if (!cplx) throw Error(INTI_E_UNSUPPORTED, "the tensor-core form is implemented for Helmholtz");
     mrhs_tc_launch(b, a);
   } else if (precision == INTI_FP64) {
-    dim3 grid((unsigned)(2 * b->nitems), (unsigned)((nrhs + kMmaCols - 1) / kMmaCols));
     ProfScope ps(ctx, "batch");
-    auto go = [&](auto pc, auto kc) {
-      constexpr int P = decltype(pc)::value, K = decltype(kc)::value;
-      constexpr size_t smem = MrhsShape<P == HELMHOLTZ>::smem_bytes();
-      // the attribute is set once per kernel, outside any stream capture
-      static std::once_flag once;
-      std::call_once(once, [] {
-        cudaFuncSetAttribute(mrhs_mma<P, K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      });
-      mrhs_mma<P, K><<<grid, kMmaThreads, smem, ctx->stream>>>(a);
-    };
-    if (cplx) {
-      if (b->kind == SL) go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, SL>());
-      else if (b->kind == DL) go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, DL>());
-      else go(std::integral_constant<int, HELMHOLTZ>(), std::integral_constant<int, CF>());
-    } else {
-      if (b->kind == SL) go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, SL>());
-      else if (b->kind == DL) go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, DL>());
-      else go(std::integral_constant<int, LAPLACE>(), std::integral_constant<int, CF>());
-    }
-    ctx->launches++;
+    mrhs_mma_launch(ctx, b->pde, b->kind, a, b->nitems);
   } else {
     throw Error(INTI_E_ARG, "batch precision must be FP64 or TF32");
   }
@@ -474,6 +511,58 @@ void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t l
     else
       csr_mrhs<false><<<grid, 256, 0, ctx->stream>>>(m, b->corr->rowptr.as<int64_t>(), b->corr->col.as<int32_t>(),
                                                      b->corr->val.as<double>(), x, ldx, y, ldy, nrhs, a.ar, a.ai);
+    ctx->launches++;
+    INTI_CUDA(cudaGetLastError());
+  }
+}
+
+bool op_mrhs_supported(const inti_op* op) {
+  return op->precision == INTI_FP64 && op->dim == 3 && (op->kind == SL || op->kind == DL || op->kind == CF) &&
+         (op->kind == SL || op->source->has_normals);
+}
+
+void op_apply_mrhs(inti_op* op, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
+                   const double* alpha, const double* beta) {
+  inti_ctx* ctx = op->ctx;
+  const bool cplx = op->pde == INTI_HELMHOLTZ;
+  BatchArgs a{};
+  a.tcoords = op->target->coords.as<double>();
+  a.gm = op->target->n;
+  a.gn = op->source->n;
+  a.coords = op->source->coords.as<double>();
+  a.normals = op->source->has_normals ? op->source->normals.as<double>() : nullptr;
+  a.weights = op->source->weights.as<double>();
+  a.x = x;
+  a.ldx = ldx;
+  a.y = y;
+  a.ldy = ldy;
+  a.nrhs = nrhs;
+  a.k = op->k;
+  // CF: c1*DL + c2*SL; single kernels ignore the coefficients
+  a.c1r = op->c1[0];
+  a.c1i = op->c1[1];
+  a.c2r = op->c2[0];
+  a.c2i = op->c2[1];
+  a.ar = alpha ? alpha[0] : 1.0;
+  a.ai = alpha ? alpha[1] : 0.0;
+  a.br = beta ? beta[0] : 0.0;
+  a.bi = beta ? beta[1] : 0.0;
+  a.beta_zero = a.br == 0.0 && a.bi == 0.0;
+  a.expi = cplx ? expi_table_f64(ctx) : nullptr;
+  const int64_t blocks = (a.gm + kMrhsBlock - 1) / kMrhsBlock;
+  {
+    ProfScope ps(ctx, "mrhs");
+    mrhs_mma_launch(ctx, op->pde, op->kind, a, blocks);
+  }
+  if (op->corr) {
+    const inti_csr* c = op->corr;
+    dim3 grid((unsigned)((a.gm + 255) / 256), (unsigned)nrhs);
+    if (cplx)
+      csr_mrhs<true><<<grid, 256, 0, ctx->stream>>>(a.gm, c->rowptr.as<int64_t>(), c->col.as<int32_t>(),
+                                                    c->val.as<double>(), x, ldx, y, ldy, nrhs, a.ar, a.ai);
+    else
+      csr_mrhs<false><<<grid, 256, 0, ctx->stream>>>(a.gm, c->rowptr.as<int64_t>(), c->col.as<int32_t>(),
+                                                     c->val.as<double>(), x, ldx, y, ldy, nrhs, a.ar, a.ai);
     ctx->launches++;
     INTI_CUDA(cudaGetLastError());
   }

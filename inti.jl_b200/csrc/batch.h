@@ -45,6 +45,11 @@ struct BatchArgs {
   double ar, ai, br, bi;
   bool beta_zero;
   const double2* expi;
+  // single-operator form of the FP64 MMA kernel (tcoords != null): targets
+  // tcoords[0, gm), sources coords/normals/weights[0, gn), work item b =
+  // target block b; off, item_surf and item_block are unused
+  const double* tcoords = nullptr;
+  int64_t gm = 0, gn = 0;
 };
 
 void mrhs_tc_launch(inti_batch* b, const BatchArgs& a);
@@ -56,5 +61,11 @@ void batch_gmres(inti_batch* b, const double* shift, const double* B, double* X,
                  inti_gmres_stats* stats);
 void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t ldx, double* y, int64_t ldy,
                         int32_t nrhs, const double* alpha, const double* beta);
+// y = alpha*(A + C) x + beta*y for nrhs device columns of a 3D FP64 SL, DL or
+// combined-field operator, each kernel value evaluated once for 64 columns
+// (the batch FP64 MMA kernel in single-operator form).
+bool op_mrhs_supported(const inti_op* op);
+void op_apply_mrhs(inti_op* op, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
+                   const double* alpha, const double* beta);
 
 }  // namespace inti

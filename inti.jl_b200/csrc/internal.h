@@ -32,6 +32,7 @@ struct inti_op {
   inti::DevBuf xbuf, ybuf;  // staging for host-pointer applies
   inti::DevBuf tpartial;  // transpose: tsplit x n double2
   inti::DevBuf gpartial;  // source gradients: split x n x (2 dim + 2)
+  inti::DevBuf mx, my;    // staging of host columns for multi-column applies
   int split = 1;
   int tpt = 4;  // targets per thread of the pair kernel (autotuned with split)
   int tsplit = 1;
@@ -46,6 +47,10 @@ struct inti_op {
 };
 
 namespace inti {
+
+// Applies of this many columns or more (FP64 3D SL/DL/CF operators) take the
+// multi-column MMA kernel instead of one pair product per column.
+constexpr int kMrhsMinColumns = 8;
 
 void sync_and_check(inti_ctx* ctx);
 PairLaunch make_launch(inti_op* op, const double* xdev);
