@@ -218,32 +218,32 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
 // (g0i, -g0r)), and the warps multiply A B with the FP64 MMA.  The next
 // tile's traces and source records are loaded during the MMA phase.  Same
 // partial layout as dim_theta.
-template <int PDE>
+template <int PDE, bool WIDE>
 struct ThetaMma;
-template <>
-struct ThetaMma<LAPLACE> {
+template <bool WIDE>
+struct ThetaMma<LAPLACE, WIDE> {
   static constexpr int J = 16, NA = 2, kMaxNs = 32;
   using Sh = MmaShape<8, 1, 4, J * NA, 1>;  // 256 targets x 32 columns
 };
-template <>
-struct ThetaMma<HELMHOLTZ> {
-  static constexpr int J = 8, NA = 4, kMaxNs = 24;
-  using Sh = MmaShape<4, 2, 3, J * NA, 2>;  // 128 targets x 24 complex columns
+template <bool WIDE>
+struct ThetaMma<HELMHOLTZ, WIDE> {
+  static constexpr int J = 8, NA = 4, kMaxNs = WIDE ? 32 : 24;
+  using Sh = MmaShape<4, 2, WIDE ? 4 : 3, J * NA, 2>;  // 128 targets x 24 or 32 complex columns
 };
-template <int PDE>
+template <int PDE, bool WIDE>
 constexpr size_t theta_mma_smem() {
-  using Sh = typename ThetaMma<PDE>::Sh;
-  return sizeof(double) * ((size_t)Sh::MT * Sh::LDA + (size_t)Sh::kK * Sh::LDB + 7 * ThetaMma<PDE>::J) +
+  using Sh = typename ThetaMma<PDE, WIDE>::Sh;
+  return sizeof(double) * ((size_t)Sh::MT * Sh::LDA + (size_t)Sh::kK * Sh::LDB + 7 * ThetaMma<PDE, WIDE>::J) +
          (PDE == HELMHOLTZ ? sizeof(double2) * kExpiTable : 0);
 }
 
-template <int PDE>
+template <int PDE, bool WIDE>
 __global__ void __launch_bounds__(kMmaThreads, 2) dim_theta_mma(
     int64_t m, int64_t n, int ns, const double* __restrict__ tx, const double* __restrict__ x,
     const double* __restrict__ nrm, const double* __restrict__ w, const double2* __restrict__ g0,
     const double2* __restrict__ g1, double k, double kT, double delta, const double2* __restrict__ tab_g,
     int tiles_per_split, double2* __restrict__ partial) {
-  using TM = ThetaMma<PDE>;
+  using TM = ThetaMma<PDE, WIDE>;
   using Sh = typename TM::Sh;
   constexpr bool CPLX = PDE == HELMHOLTZ;
   constexpr int J = TM::J, NA = TM::NA;
@@ -701,9 +701,10 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
     constexpr int D = decltype(dim_c)::value;
     const int64_t tot = m * ns;
     if constexpr (D == 3) {
-      if (!derivative && ns <= ThetaMma<P>::kMaxNs) {
-        // FP64 MMA form; split over sources for >= 8 waves of 2 CTAs per SM
-        using TM = ThetaMma<P>;
+      // FP64 MMA form; split over sources for >= 8 waves of 2 CTAs per SM
+      auto mma = [&](auto wide_c) {
+        constexpr bool WIDE = decltype(wide_c)::value;
+        using TM = ThetaMma<P, WIDE>;
         const int64_t blocks = (m + TM::Sh::MT - 1) / TM::Sh::MT;
         const int64_t ntile = (n + TM::J - 1) / TM::J;
         const int64_t want = (int64_t)ctx->num_sms * 16;
@@ -711,20 +712,30 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
         const int tps = (int)((ntile + split - 1) / split);
         split = (int)((ntile + tps - 1) / tps);
         wk.part.ensure(sizeof(double2) * (size_t)split * m * ns);
-        constexpr size_t smem = theta_mma_smem<P>();
+        constexpr size_t smem = theta_mma_smem<P, WIDE>();
+        auto* kern = &dim_theta_mma<P, WIDE>;
         static std::once_flag once;
-        std::call_once(once, [] {
-          cudaFuncSetAttribute(dim_theta_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        std::call_once(once, [kern] {
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         });
         ProfScope pd(ctx, "dim");
-        dim_theta_mma<P><<<dim3((unsigned)blocks, (unsigned)split), kMmaThreads, smem, ctx->stream>>>(
+        kern<<<dim3((unsigned)blocks, (unsigned)split), kMmaThreads, smem, ctx->stream>>>(
             m, n, ns, tx, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re, k_re * kExpiTable / (2 * kPi),
             2 * kPi / kExpiTable, P == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, tps, wk.part.as<double2>());
         ctx->launches++;
         dim_theta_reduce<P, D, false><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
             m, ns, split, tx, tn, wk.d_xs.as<double>(), mu, k_re, wk.part.as<double2>(), wk.theta.as<double2>());
         ctx->launches++;
+      };
+      if (!derivative && ns <= ThetaMma<P, false>::kMaxNs) {
+        mma(std::false_type());
         return;
+      }
+      if constexpr (P == HELMHOLTZ) {
+        if (!derivative && ns <= ThetaMma<P, true>::kMaxNs) {
+          mma(std::true_type());
+          return;
+        }
       }
     }
     // split over sources so the grid covers the device
