@@ -21,6 +21,11 @@ gmres   (extra key) time to ||b - Lx|| <= 1e-10 ||b|| for the 3D Laplace
         combined field ½I + D + S on the (1, 0.7, 0.5) ellipsoid, N = 200,934,
         plain FP64 GMRES versus FP32-inner / FP64-outer refinement.
 
+Other workloads (--workload): c2_dl, c3_dl_fp64, c3_dl_fp32c, c3_sl_fp64, c1
+(single operators); c4 (batched surfaces x 64 right-hand sides, TF32 tensor
+cores and FP64 MMA, --nsurf surfaces); c5 (adjoint); csr (correction SpMV
+bandwidth); dim_c2, dim_c3 (GPU construction of the DIM correction).
+
 --impl reference times the reference's CPU algorithm for the same step
 (Inti's on-the-fly row sums, restated in C++ as the oracle) on all host
 cores, each step a bounded sample of rows scaled to the metric.
@@ -46,9 +51,9 @@ METRIC = "G kernel-pairs/s"
 UNIT = "Gpairs/s"
 # Algorithmic flops per pair (FMA = 2 flops; special functions counted apart)
 FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10}
-# DRAM bytes (read + write) of one pair-kernel launch on this workload, from
-# the ncu capture summarised in profiles/pair_forward_helmholtz_sl_fp64_p2sphere62k.md
-PAIR_TRAFFIC_BYTES = 4.516e6
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pair-kernel
+# launch on the default workload, from an ncu capture of that launch
+PAIR_TRAFFIC_BYTES = 4.51e6
 # Algorithmic flops per pair of the source-gradient (adjoint) pass
 ADJ_FLOPS_PER_PAIR = {"laplace_dl": 40, "laplace_sl": 19}
 
@@ -245,6 +250,51 @@ def gmres_c3(ctx) -> dict:
     return out
 
 
+def bench_dim(args, ctx, peaks, torch) -> dict:
+    """GPU construction of the on-surface DIM correction (bdim_correction,
+    src/bdim.jl:50-196) of the C2 operator (Helmholtz k = 10, P2 sphere,
+    N = 62,208, ns = 18) or the C3 operator (Laplace, ellipsoid, N = 200,934,
+    ns = 27): traces, the Θ pair product over all node pairs on the FP64 MMA
+    path, per-element least squares, CSR assembly.  value = seconds per
+    construction (wall clock around the call, synchronised)."""
+    import inti_b200 as inti
+
+    if args.workload == "dim_c2":
+        q, op, work = inti.p2_sphere_quadrature(36), inti.Helmholtz(k=10.0, dim=3), "helmholtz3d_dim_k10_p2sphere_N62208"
+        flops_pair = 24 + 34 + 16 * 18  # S and D values, 2 complex multiply-adds per column
+    else:
+        q, op, work = inti.ellipsoid_quadrature(61, 5), inti.Laplace(dim=3), "laplace3d_dim_ellipsoid_N200934"
+        flops_pair = 11 + 18 + 4 * 27
+    n = len(q)
+    for _ in range(args.warmup):
+        inti.bdim_correction(op, q, q, ctx=ctx)
+    ctx.synchronize()
+    clocks = Clocks(0)
+    launches0 = ctx.launch_count
+    ctx.set_profiling(True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
+    ctx.synchronize()
+    wall = (time.perf_counter() - t0) / args.steps
+    theta_ms, theta_launches = ctx.profile("dim")
+    ctx.set_profiling(False)
+    clk = clocks.stop()
+    theta_ms /= args.steps
+    achieved = float(n) * n * flops_pair / (theta_ms * 1e-3) / 1e12
+    fp64 = peaks["fp64_flops"] / 1e12
+    return {"metric": "DIM construction time", "value": wall, "unit": "s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall * 1e3, "higher_is_better": False, "scaling": "none",
+            "vs_baseline": None, "dtype": "c128" if isinstance(op, inti.Helmholtz) else "f64", "data": "synthetic",
+            "config": {"workload": work, "n": n, "nnz_per_row": dS.nnz // n, "l2": "inputs (traces, partials) "
+                       "larger than L2 are not flushed: each step rebuilds everything"},
+            "roofline": {"bound": "fp64", "kernel": "dim_theta_mma + dim_theta_reduce", "kernel_ms": theta_ms,
+                         "achieved": achieved, "peak": fp64, "unit": "TFLOP/s", "frac": achieved / fp64,
+                         "flops_per_pair": flops_pair, "traffic": None,
+                         "peak_source": "FP64 FMA throughput measured in this run (inti_measure_peaks), of measured"},
+            "gpu_launches": (ctx.launch_count - launches0) // args.steps, "clocks": clk}
+
+
 def build_c4(ctx, nsurf: int = 32, nrhs: int = 64, seed: int = 4):
     """32 seeded star surfaces r = 1 + 0.2*sum a_lm Y_lm (l <= 3), n x n cells
     per cube-sphere patch with n in [6, 27] (N_s = 54 n^2: 1,944 .. 39,366
@@ -274,7 +324,7 @@ def build_c4(ctx, nsurf: int = 32, nrhs: int = 64, seed: int = 4):
 def bench_batch(args, ctx, peaks, torch) -> dict:
     """Batched multi-RHS apply (config 4): value = kernel pairs x right-hand
     sides per second through the TF32 tensor-core path."""
-    B, X, pairs, cfg, quads = build_c4(ctx)
+    B, X, pairs, cfg, quads = build_c4(ctx, nsurf=args.nsurf)
     nrhs = X.shape[1]
     dev = torch.device("cuda:0")
     stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
@@ -590,7 +640,9 @@ def main() -> None:
                     help="N > 1: split the target rows of one operator over the ranks (strong scaling, y "
                          "all-gathered every step) or run independent replicas (weak scaling)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr"])
+                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr",
+                             "dim_c2", "dim_c3"])
+    ap.add_argument("--nsurf", type=int, default=32, help="c4: number of star surfaces (32 = the batched workload)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
@@ -614,9 +666,11 @@ def main() -> None:
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     ctx = inti.Context(local)
     peaks = ctx.measure_peaks()
-    if args.workload in ("c4", "c5", "csr"):
+    if args.workload in ("c4", "c5", "csr", "dim_c2", "dim_c3"):
         if args.workload == "csr":
             line = bench_csr(args, ctx, torch)
+        elif args.workload.startswith("dim"):
+            line = bench_dim(args, ctx, peaks, torch)
         else:
             line = (bench_batch if args.workload == "c4" else bench_adjoint)(args, ctx, peaks, torch)
         if rank == 0:

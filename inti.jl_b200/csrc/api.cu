@@ -270,7 +270,8 @@ int inti_ctx_destroy(inti_ctx* ctx) {
     ctx->err_flag.release();
     for (inti::DevBuf* d : {&ctx->krylov.V, &ctx->krylov.w, &ctx->krylov.r, &ctx->krylov.e, &ctx->krylov.w_outer,
                             &ctx->krylov.partial, &ctx->krylov.h, &ctx->krylov.y, &ctx->krylov.nrm, &ctx->krylov.b,
-                            &ctx->krylov.x, &ctx->expi64, &ctx->expi32})
+                            &ctx->krylov.x, &ctx->expi64, &ctx->expi32, &ctx->dimwork.d_xs, &ctx->dimwork.g0,
+                            &ctx->dimwork.g1, &ctx->dimwork.theta, &ctx->dimwork.part, &ctx->dimwork.mu})
       d->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
   }

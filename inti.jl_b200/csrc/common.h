@@ -94,6 +94,11 @@ struct inti_ctx {
   struct {
     inti::DevBuf V, w, r, e, w_outer, partial, h, y, nrm, b, x;
   } krylov;
+  // DIM construction workspace kept between constructions: source points,
+  // traces, Theta, its partial sums, green multipliers.
+  struct {
+    inti::DevBuf d_xs, g0, g1, theta, part, mu;
+  } dimwork;
 };
 
 struct inti_quad {

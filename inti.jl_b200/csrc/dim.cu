@@ -612,9 +612,15 @@ static void nq_dispatch(int nq, F&& f) {
 // Steps 1-3 shared by both forms: monopole centres and traces on the source
 // nodes, then Theta for m targets (coordinates tx, normals tn or NULL, green
 // multipliers mu or NULL for -1/2, all on the device).
+// Work arrays of one construction: the context's buffers, kept between
+// constructions (hundreds of MB at N = 2e5, whose cudaMalloc/cudaFree per
+// call would dominate the host time and synchronise the device).
 struct DimWork {
   int ns = 0;
-  DevBuf d_xs, g0, g1, theta, part;
+  DevBuf &d_xs, &g0, &g1, &theta, &part, &mu;
+  explicit DimWork(inti_ctx* c)
+      : d_xs(c->dimwork.d_xs), g0(c->dimwork.g0), g1(c->dimwork.g1), theta(c->dimwork.theta),
+        part(c->dimwork.part), mu(c->dimwork.mu) {}
 };
 
 static void dim_source_setup(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
@@ -796,14 +802,14 @@ static std::unique_ptr<inti_csr> new_csr(inti_ctx* ctx, int64_t m, int64_t n, in
 void dim_correction(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* q,
                     int derivative, const double* green_multiplier, inti_csr** dS,
                     inti_csr** dD) {
-  DimWork wk;
+  DimWork wk(ctx);
   dim_source_setup(ctx, pde, k_re, k_im, q, wk);
   const int64_t n = q->n;
   const int nq = q->nq;
   const int64_t nel = n / nq;
   const int ns = wk.ns;
   const bool cplx = pde == INTI_HELMHOLTZ;
-  DevBuf d_mu;
+  DevBuf& d_mu = wk.mu;
   if (green_multiplier) {
     for (int64_t i = 0; i < n; ++i)
       if (!std::isfinite(green_multiplier[i])) throw Error(INTI_E_NONFINITE, "green_multiplier contains NaN/Inf");
@@ -844,7 +850,7 @@ void dim_correction_targets(inti_ctx* ctx, int pde, double k_re, double k_im, co
   if (target->ctx != ctx) throw Error(INTI_E_STATE, "target belongs to another context");
   if (!green_multiplier) throw Error(INTI_E_ARG, "off-surface targets need a green multiplier per target");
   if (std::isnan(maxdist) || maxdist < 0) throw Error(INTI_E_ARG, "maxdist must be >= 0");
-  DimWork wk;
+  DimWork wk(ctx);
   dim_source_setup(ctx, pde, k_re, k_im, q, wk);
   if (target->dim != q->dim) throw Error(INTI_E_SHAPE, "target and source dimensions differ");
   if (derivative && !target->has_normals) throw Error(INTI_E_ARG, "derivative corrections need target normals");
