@@ -315,7 +315,7 @@ def build_c4(ctx, nsurf: int = 32, nrhs: int = 64, seed: int = 4):
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     X = np.concatenate([np.exp(1j * k * (q.coords @ d.T)) for q in quads], axis=0)
     pairs = float(sum(len(q) ** 2 for q in quads))
-    cfg = {"workload": "helmholtz3d_cfie_k5_32stars_64rhs_dim", "surfaces": nsurf, "n_total": B.n,
+    cfg = {"workload": f"helmholtz3d_cfie_k5_{nsurf}stars_64rhs_dim", "surfaces": nsurf, "n_total": B.n,
            "n_min": int(min(len(q) for q in quads)), "n_max": int(max(len(q) for q in quads)), "nrhs": nrhs,
            "sum_n2": pairs, "dim_setup_s": t_dim}
     return B, X, pairs, cfg, quads
