@@ -46,7 +46,10 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
     y[c] = sx[DIM * jj + c];
     ny[c] = KIND == DL ? sn[DIM * jj + c] : 0.0;
   }
-  double s = 0.0, a[DIM], b[DIM];
+  // DL: the source's own normal factors out of two sums, accumulated as
+  // scalars and applied at the end: s = n_y . a, and b = P*h - n_y*G with
+  // h = sum g K' r (P = 3 in 3D, 2 in 2D) and G = sum g K'
+  double s = 0.0, G = 0.0, a[DIM], b[DIM];
 #pragma unroll
   for (int c = 0; c < DIM; ++c) a[c] = b[c] = 0.0;
   const int64_t ntile = (m + kAdjTile - 1) / kAdjTile;
@@ -84,12 +87,12 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
 #pragma unroll
           for (int c = 1; c < DIM; ++c) rn = fma(r[c], ny[c], rn);
           const double gr3 = gi * ri3;
-          s = fma(gr3, rn, s);
-          const double f = 3.0 * gr3 * rn * ri * ri;
+          G += gr3;
+          const double h = gr3 * rn * (ri * ri);
 #pragma unroll
           for (int c = 0; c < DIM; ++c) {
             a[c] = fma(gr3, r[c], a[c]);
-            b[c] = fma(f, r[c], fma(-gr3, ny[c], b[c]));
+            b[c] = fma(h, r[c], b[c]);
           }
         }
       } else {
@@ -103,16 +106,24 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
 #pragma unroll
           for (int c = 1; c < DIM; ++c) rn = fma(r[c], ny[c], rn);
           const double gd = gi * id2;
-          s = fma(gd, rn, s);
-          const double f = 2.0 * gd * rn * id2;
+          G += gd;
+          const double h = gd * rn * id2;
 #pragma unroll
           for (int c = 0; c < DIM; ++c) {
             a[c] = fma(gd, r[c], a[c]);
-            b[c] = fma(f, r[c], fma(-gd, ny[c], b[c]));
+            b[c] = fma(h, r[c], b[c]);
           }
         }
       }
     }
+  }
+  if (KIND == DL) {
+    constexpr double P = DIM == 3 ? 3.0 : 2.0;
+    s = a[0] * ny[0];
+#pragma unroll
+    for (int c = 1; c < DIM; ++c) s = fma(a[c], ny[c], s);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) b[c] = fma(P, b[c], -G * ny[c]);
   }
   if (j < n) {
     double* o = partial + ((int64_t)blockIdx.y * n + j) * W;
