@@ -133,18 +133,27 @@ void op_apply_device(inti_op* op, const double* x, double* y, const double* alph
 
 void op_apply_transpose_device(inti_op* op, const double* x, double* y, const double* alpha,
                                const double* beta) {
+  // the forward pair product with targets and sources swapped (op_prepare_transpose)
   PairLaunch L = make_launch(op, x);
-  L.split = op->tsplit;
+  L.kind = transposed_kind(op->kind);
+  L.m = op->source->n;
+  L.n = op->target->n;
+  L.tcoords = op->source->coords.as<double>();
+  L.tnormals = op->source->has_normals ? op->source->normals.as<double>() : nullptr;
+  L.scoords = op->target->coords.as<double>();
+  L.snormals = op->target->has_normals ? op->target->normals.as<double>() : nullptr;
+  L.sweights = op->tones.as<double>();
+  L.packed = op->tpacked.p;
   L.partial = op->tpartial.p;
-  pair_transpose_launch(op->ctx, L);
-  // reduce: y = alpha*(sum partial + C^T x) + beta*y (partial is double2)
-  PairLaunch R = L;
-  R.m = op->source->n;
-  R.precision = INTI_FP64;
-  R.pde = INTI_HELMHOLTZ;  // double2 partial layout
-  const bool cplx = op->pde == INTI_HELMHOLTZ;
-  transpose_epilogue(op->ctx, R.m, op->tsplit, op->tpartial.p, op->corrT.get(), x, y, alpha,
-                     beta, cplx);
+  L.split = op->tsplit;
+  L.tpt = op->ttpt;
+  L.n_tiles = op->tn_tiles;
+  {
+    ProfScope pt(op->ctx, "transpose");
+    pair_launch(op->ctx, L);
+  }
+  // y = alpha*(w_j * scale * sum partial + C^T x) + beta*y
+  pair_epilogue(op->ctx, L, op->corrT.get(), x, y, alpha, beta, op->source->weights.as<double>());
 }
 
 }  // namespace inti

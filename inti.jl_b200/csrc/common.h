@@ -182,13 +182,12 @@ int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precisi
                     int64_t n, int tpt = 4);
 // Enqueue pack + pair kernels (results in L.partial); returns launches.
 int pair_launch(inti_ctx* ctx, const PairLaunch& L);
-// y = alpha*(scale*sum_s partial + C x) + beta*y; complex when cplx.
+// y = alpha*(scale*rowscale_i*sum_s partial + C x) + beta*y (rowscale NULL:
+// 1); complex when cplx.
 int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x,
-                  double* y, const double* alpha, const double* beta);
+                  double* y, const double* alpha, const double* beta, const double* rowscale = nullptr);
 // Dense assembly of A.
 int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out);
-// Transpose apply partials: y_j = sum_i K(x_i,y_j) w_j x_i.
-int pair_transpose_launch(inti_ctx* ctx, const PairLaunch& L);
 
 // CSR: y = alpha*C*x + beta*y (alpha/beta complex pairs); transpose via col scatter.
 int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, const double* alpha,

@@ -30,13 +30,13 @@ struct inti_op {
   inti::DevBuf packed;    // packed source records, n_tiles * tile
   inti::DevBuf partial;   // split x m accumulators
   inti::DevBuf xbuf, ybuf;  // staging for host-pointer applies
-  inti::DevBuf tpartial;  // transpose: tsplit x n double2
+  inti::DevBuf tpartial, tpacked, tones;  // A^T: partials, packed target records, unit weights
   inti::DevBuf gpartial;  // source gradients: split x n x (2 dim + 2)
   inti::DevBuf mx, my;    // staging of host columns for multi-column applies
   int split = 1;
   int tpt = 4;  // targets per thread of the pair kernel (autotuned with split)
-  int tsplit = 1;
-  int64_t n_tiles = 1;
+  int tsplit = 1, ttpt = 4;  // A^T launch shape
+  int64_t n_tiles = 1, tn_tiles = 1;
   // Derived operators kept for repeated solves: the FP32C twin used by the
   // mixed-precision GMRES, and (on a double layer) the combined-field operator
   // fused with the single layer `fused_sl` under coefficients fused_c.
@@ -73,9 +73,7 @@ std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, co
                                             const inti_csr* b, const double* cb, int64_t m, int64_t n,
                                             bool cplx);
 void op_prepare_transpose(inti_op* op);
-void transpose_epilogue(inti_ctx* ctx, int64_t n, int split, const void* partial,
-                        const inti_csr* corrT, const double* x, double* y, const double* alpha,
-                        const double* beta, bool cplx);
+int transposed_kind(int kind);
 inti_csr* csr_create_host(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz,
                           const int64_t* rowptr, const int32_t* col, const double* val,
                           int dtype);

@@ -268,69 +268,40 @@ void op_autotune(inti_op* op, bool measure) {
   set(pick.first, pick.second);
 }
 
+// A^T as a forward product with the roles swapped: (A^T g)_j =
+// w_j sum_i K(x_i, y_j) g_i, and K(x_i, y_j) = K'(y_j, x_i) with K' the
+// kernel of the swapped roles (the kernels of src/kernels.jl:137-204,
+// 347-413 satisfy SL(x,y) = SL(y,x), DL(x,y) = ADL(y,x), ADL(x,y) = DL(y,x),
+// HS(x,y) = HS(y,x), the normal travelling with its point).  So A^T runs on
+// the pair kernel with targets = the source nodes (and their normals),
+// sources = the target nodes with unit weights, density g, and w_j applied
+// per row in the epilogue.
+int transposed_kind(int kind) { return kind == DL ? ADL : kind == ADL ? DL : kind; }
+
 void op_prepare_transpose(inti_op* op) {
   if (op->kind == CF) throw Error(INTI_E_UNSUPPORTED, "transpose of a combined-field operator");
-  const int64_t ntile = (op->target->n + 63) / 64;
-  const int64_t blocks = (op->source->n + 127) / 128;
-  const int64_t want = (int64_t)op->ctx->num_sms * 8;
-  op->tsplit = (int)std::max<int64_t>(1, std::min<int64_t>(ntile, (want + blocks - 1) / blocks));
-  op->tpartial.ensure(sizeof(double2) * (size_t)op->tsplit * op->source->n);
-  if (op->corr && !op->corrT) op->corrT = csr_transpose(op->ctx, op->corr);
-}
-
-__global__ void transpose_epilogue_kernel(int64_t n, int split, const double2* partial,
-                                          const int64_t* rowptr, const int32_t* col,
-                                          const double* val, const double* x, double* y,
-                                          double ar, double ai, double br, double bi, bool bz,
-                                          bool cplx) {
-  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  double sr = 0.0, si = 0.0;
-  for (int s = 0; s < split; ++s) {
-    const double2 v = partial[(int64_t)s * n + j];
-    sr += v.x;
-    si += v.y;
-  }
-  if (rowptr) {
-    for (int64_t p = rowptr[j]; p < rowptr[j + 1]; ++p) {
-      const int32_t i = col[p];
-      if (cplx) {
-        const double vr = val[2 * p], vi = val[2 * p + 1];
-        const double xr = x[2 * i], xi = x[2 * i + 1];
-        sr = fma(vr, xr, fma(-vi, xi, sr));
-        si = fma(vr, xi, fma(vi, xr, si));
-      } else {
-        sr = fma(val[p], x[i], sr);
-      }
-    }
-  }
-  if (cplx) {
-    double yr = ar * sr - ai * si, yi = ar * si + ai * sr;
-    if (!bz) {
-      yr += br * y[2 * j] - bi * y[2 * j + 1];
-      yi += br * y[2 * j + 1] + bi * y[2 * j];
-    }
-    y[2 * j] = yr;
-    y[2 * j + 1] = yi;
+  inti_ctx* ctx = op->ctx;
+  const int kt = transposed_kind(op->kind);
+  const int64_t m2 = op->source->n, n2 = op->target->n;
+  const int tile = pair_tile(op->precision);
+  op->tn_tiles = std::max<int64_t>(1, (n2 + tile - 1) / tile);
+  // the context's timed shape for this problem when there is one, else the heuristic
+  const std::string key = std::to_string(op->pde) + "/" + std::to_string(kt) + "/" + std::to_string(op->dim) +
+                          "/" + std::to_string(op->precision) + "/" + std::to_string(m2) + "/" + std::to_string(n2);
+  auto it = ctx->tuned.find(key);
+  if (it != ctx->tuned.end()) {
+    op->ttpt = it->second.first;
+    op->tsplit = it->second.second;
   } else {
-    double yr = ar * sr;
-    if (!bz) yr += br * y[j];
-    y[j] = yr;
+    op->ttpt = 4;
+    op->tsplit = pair_plan_split(ctx, op->pde, kt, op->dim, op->precision, m2, n2, 4);
   }
-}
-
-void transpose_epilogue(inti_ctx* ctx, int64_t n, int split, const void* partial,
-                        const inti_csr* corrT, const double* x, double* y, const double* alpha,
-                        const double* beta, bool cplx) {
-  const double ar = alpha ? alpha[0] : 1.0, ai = alpha ? alpha[1] : 0.0;
-  const double br = beta ? beta[0] : 0.0, bi = beta ? beta[1] : 0.0;
-  const bool bz = br == 0.0 && bi == 0.0;
-  transpose_epilogue_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(
-      n, split, static_cast<const double2*>(partial), corrT ? corrT->rowptr.as<int64_t>() : nullptr,
-      corrT ? corrT->col.as<int32_t>() : nullptr, corrT ? corrT->val.as<double>() : nullptr, x, y,
-      ar, ai, br, bi, bz, cplx);
-  INTI_CUDA(cudaGetLastError());
-  ctx->launches += 1;
+  op->tpacked.ensure((size_t)op->tn_tiles * tile * pair_record_bytes(op->pde, kt, op->dim, op->precision));
+  op->tpartial.ensure((size_t)op->tsplit * m2 * pair_partial_bytes(op->pde, op->precision));
+  std::vector<double> ones((size_t)std::max<int64_t>(n2, 1), 1.0);
+  op->tones.ensure(sizeof(double) * ones.size());
+  INTI_CUDA(cudaMemcpy(op->tones.p, ones.data(), sizeof(double) * ones.size(), cudaMemcpyHostToDevice));
+  if (op->corr && !op->corrT) op->corrT = csr_transpose(ctx, op->corr);
 }
 
 }  // namespace inti

@@ -463,6 +463,7 @@ struct EpiArgs {
   double* y;
   double ar, ai, br, bi;
   bool beta_zero;
+  const double* rowscale = nullptr;  // per-row factor of the pair sum (A^T: the source weights)
 };
 
 template <class P, bool CPLX>
@@ -476,8 +477,9 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
     sr += v.x;
     si += v.y;
   }
-  sr *= e.scale;
-  si *= e.scale;
+  const double sc = e.rowscale ? e.scale * e.rowscale[i] : e.scale;
+  sr *= sc;
+  si *= sc;
   if (e.rowptr) {
     const int64_t p0 = e.rowptr[i], p1 = e.rowptr[i + 1];
     for (int64_t p = p0; p < p1; ++p) {
@@ -527,62 +529,6 @@ __global__ void assemble_kernel(int64_t m, int64_t n, const double* tc, const do
   }
 }
 
-// ---------------------------------------------------------------------------
-// Transpose apply z_j = w_j * sum_i K(x_i, y_j) g_i: each thread owns source
-// nodes, target tiles are staged in shared memory (plain loads; this is the
-// adjoint's density gradient, not the forward hot loop).
-// ---------------------------------------------------------------------------
-template <int PDE, int KIND, int DIM>
-__global__ void __launch_bounds__(kBlock) transpose_kernel(int64_t m, int64_t n, const double* tc,
-                                                          const double* tn, const double* sc,
-                                                          const double* sn, const double* w,
-                                                          const double* g, double k, int tiles_per_split,
-                                                          double2* partial) {
-  constexpr int T = 64;
-  __shared__ double stc[T * DIM], stn[T * DIM], sg[T * 2];
-  const int64_t j = blockIdx.x * (int64_t)kBlock + threadIdx.x;
-  const int64_t jj = min(j, n - 1);
-  double y[DIM], ny[DIM];
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    y[c] = sc[DIM * jj + c];
-    ny[c] = sn ? sn[DIM * jj + c] : 0.0;
-  }
-  const int64_t ntile = (m + T - 1) / T;
-  const int64_t i0 = (int64_t)blockIdx.y * tiles_per_split;
-  const int64_t i1 = min(ntile, i0 + tiles_per_split);
-  double ar = 0.0, ai = 0.0;
-  for (int64_t t = i0; t < i1; ++t) {
-    __syncthreads();
-    for (int q = threadIdx.x; q < T; q += kBlock) {
-      const int64_t i = t * T + q;
-      const bool in = i < m;
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        stc[q * DIM + c] = in ? tc[DIM * i + c] : 0.0;
-        stn[q * DIM + c] = (in && tn) ? tn[DIM * i + c] : 0.0;
-      }
-      if (PDE == HELMHOLTZ) {
-        sg[2 * q] = in ? g[2 * i] : 0.0;
-        sg[2 * q + 1] = in ? g[2 * i + 1] : 0.0;
-      } else {
-        sg[2 * q] = in ? g[i] : 0.0;
-        sg[2 * q + 1] = 0.0;
-      }
-    }
-    __syncthreads();
-    for (int q = 0; q < T; ++q) {
-      const double2 kv = kernel_value<PDE, KIND, DIM>(&stc[q * DIM], &stn[q * DIM], y, ny, k);
-      const double gr = sg[2 * q], gi = sg[2 * q + 1];
-      ar = fma(kv.x, gr, fma(-kv.y, gi, ar));
-      ai = fma(kv.x, gi, fma(kv.y, gr, ai));
-    }
-  }
-  if (j < n) {
-    const double wj = w[j];
-    partial[(int64_t)blockIdx.y * n + j] = make_double2(ar * wj, ai * wj);
-  }
-}
 
 // ---------------------------------------------------------------------------
 // Host-side dispatch
@@ -804,8 +750,9 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
 }
 
 int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x,
-                  double* y, const double* alpha, const double* beta) {
+                  double* y, const double* alpha, const double* beta, const double* rowscale) {
   EpiArgs e;
+  e.rowscale = rowscale;
   e.m = L.m;
   e.split = L.split;
   e.partial = L.partial;
@@ -857,25 +804,6 @@ int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {
 }
 
 // Transpose: the roles of the two node sets swap; partial is split x n double2.
-int pair_transpose_launch(inti_ctx* ctx, const PairLaunch& L) {
-  const int64_t ntile = (L.m + 63) / 64;
-  const int tps = (int)((ntile + L.split - 1) / L.split);
-  if (L.kind == CF) throw Error(INTI_E_UNSUPPORTED, "transpose of a combined-field operator");
-  dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
-    using T = decltype(tag);
-    if constexpr (T::kind != CF) {
-      dim3 grid((unsigned)((L.n + kBlock - 1) / kBlock), (unsigned)L.split);
-      ProfScope pt(ctx, "transpose");
-      transpose_kernel<T::pde, T::kind, T::dim><<<grid, kBlock, 0, ctx->stream>>>(
-          L.m, L.n, L.tcoords, L.tnormals, L.scoords, L.snormals, L.sweights, L.x, L.k, tps,
-          static_cast<double2*>(L.partial));
-    }
-  });
-  INTI_CUDA(cudaGetLastError());
-  ctx->launches += 1;
-  return 1;
-}
-
 // ===========================================================================
 // Allocation-free apply.
 //
