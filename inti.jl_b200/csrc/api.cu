@@ -725,6 +725,10 @@ int inti_batch_apply(inti_batch* b, int precision, const double* x, int64_t ldx,
       batch_apply_device(b, precision, x, ldx, y, ldy, nrhs, alpha, beta);
       return;
     }
+    if (precision == INTI_TF32) {  // copies overlapped with the compute, surface group by group
+      batch_apply_host_tf32(b, x, ldx, y, ldy, nrhs, alpha, beta);
+      return;
+    }
     // staging buffers are kept on the handle: no allocation per call once they fit
     DevBuf &xd = b->xstage, &yd = b->ystage;
     const size_t bx = sizeof(double) * comps * (size_t)ldx * nrhs, by = sizeof(double) * comps * (size_t)ldy * nrhs;

@@ -568,4 +568,23 @@ void op_apply_mrhs(inti_op* op, const double* x, int64_t ldx, double* y, int64_t
   }
 }
 
+// Rows [row0, row1) of Y += alpha*C*X for the block-diagonal correction (the
+// rows of a group of surfaces in the pipelined host apply).
+void batch_correction_rows(inti_batch* b, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
+                           double ar, double ai, int64_t row0, int64_t row1) {
+  if (!b->corr || row1 <= row0) return;
+  inti_ctx* ctx = b->ctx;
+  const bool cplx = b->pde == INTI_HELMHOLTZ;
+  const dim3 grid((unsigned)((row1 - row0 + 255) / 256), (unsigned)nrhs);
+  const int64_t* rp = b->corr->rowptr.as<int64_t>() + row0;  // entries keep their global positions
+  if (cplx)
+    csr_mrhs<true><<<grid, 256, 0, ctx->stream>>>(row1 - row0, rp, b->corr->col.as<int32_t>(),
+                                                  b->corr->val.as<double>(), x, ldx, y + 2 * row0, ldy, nrhs, ar, ai);
+  else
+    csr_mrhs<false><<<grid, 256, 0, ctx->stream>>>(row1 - row0, rp, b->corr->col.as<int32_t>(),
+                                                   b->corr->val.as<double>(), x, ldx, y + row0, ldy, nrhs, ar, ai);
+  ctx->launches++;
+  INTI_CUDA(cudaGetLastError());
+}
+
 }  // namespace inti

@@ -22,6 +22,19 @@ struct inti_batch {
   // offsets, 256-target work items, work counter
   inti::DevBuf tc_b, tc_src, tc_counter, tc_toff, tc_items;
   inti::DevBuf xstage, ystage;  // staging for host-pointer applies
+  // pipelined host-pointer TF32 apply: surface groups (contiguous surface
+  // ranges grp_s[g] .. grp_s[g+1]-1), their items stored group after group
+  // (largest surface first within a group) starting at grp_item[g], and the
+  // copy streams and events
+  std::vector<int> grp_s, grp_item;
+  inti::DevBuf tc_items_grp;
+  cudaStream_t s_in = nullptr, s_out = nullptr;
+  std::vector<cudaEvent_t> ev;
+  ~inti_batch() {
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (s_in) cudaStreamDestroy(s_in);
+    if (s_out) cudaStreamDestroy(s_out);
+  }
   int64_t tc_ntiles = 0;
   int tc_nitems = 0;
 };
@@ -53,6 +66,12 @@ struct BatchArgs {
 };
 
 void mrhs_tc_launch(inti_batch* b, const BatchArgs& a);
+// Host-pointer TF32 apply with the copies overlapped: surface groups are
+// copied in, computed and copied out on three streams.
+void batch_apply_host_tf32(inti_batch* b, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
+                           const double* alpha, const double* beta);
+void batch_correction_rows(inti_batch* b, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
+                           double ar, double ai, int64_t row0, int64_t row1);
 inti_batch* batch_create(inti_ctx* ctx, int32_t nsurf, const inti_quad* const* quads, int pde, int kind,
                          double k_re, double k_im, const double* c_dl, const double* c_sl,
                          const inti_csr* const* corr_dl, const inti_csr* const* corr_sl);

@@ -514,12 +514,12 @@ __global__ void tc_pack_sources(int nsurf, const int64_t* off, const int64_t* to
 
 // Density blocks: for column group cg and tile (surface s, local tile lt),
 // B[n][k] in the canonical K-major layout (see the header), TF32.
-__global__ void tc_pack_density(int nsurf, const int64_t* off, const int64_t* toff, int64_t ntiles,
-                                const double* weights, const double* x, int64_t ldx, int nrhs, int cg,
-                                uint32_t* out) {
+__global__ void tc_pack_density(int nsurf, const int64_t* off, const int64_t* toff, int64_t tile0,
+                                int64_t tile1, int64_t ntiles, const double* weights, const double* x,
+                                int64_t ldx, int nrhs, int cg, uint32_t* out) {
   const int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  const int64_t tile = gid / (TC_N * TC_K / 4);  // one thread per 16-byte chunk
-  if (tile >= ntiles) return;
+  const int64_t tile = tile0 + gid / (TC_N * TC_K / 4);  // one thread per 16-byte chunk
+  if (tile >= tile1) return;
   const int rem = (int)(gid % (TC_N * TC_K / 4));
   const int nn = rem / (TC_K / 4), kc = rem % (TC_K / 4);  // column n, K chunk
   int s = 0;
@@ -612,64 +612,110 @@ void measure_peak_tf32(inti_ctx* ctx, double* tf32_flops) {
   *tf32_flops = 2.0 * 128 * TC_N * 8 * (TC_K / 8) * (double)rounds * ctx->num_sms / (ms * 1e-3);
 }
 
-void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
+// Tile offsets, 256-target items (largest surfaces first), packed source
+// records and kernel attributes: built once per batch (an apply after the
+// first only enqueues work, so it can be captured into a CUDA graph).
+static void tc_setup(inti_batch* b) {
+  if (b->tc_src.p) return;
   inti_ctx* ctx = b->ctx;
   const int nsurf = (int)b->off.size() - 1;
-  // tile offsets and 256-target items (largest surfaces first), built once
-  if (!b->tc_src.p) {
-    std::vector<int64_t> toff(nsurf + 1, 0);
-    for (int s = 0; s < nsurf; ++s) toff[s + 1] = toff[s] + (b->off[s + 1] - b->off[s] + TC_J - 1) / TC_J;
-    std::vector<int> order(nsurf);
-    for (int s = 0; s < nsurf; ++s) order[s] = s;
-    std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
-      return b->off[p + 1] - b->off[p] > b->off[q + 1] - b->off[q];
-    });
-    std::vector<int32_t> isurf, iblk;
-    for (int s : order)
-      for (int64_t t = 0; t * TC_ROWS < b->off[s + 1] - b->off[s]; ++t) {
-        isurf.push_back(s);
-        iblk.push_back((int32_t)t);
-      }
-    b->tc_ntiles = toff[nsurf];
-    b->tc_nitems = (int)isurf.size();
-    b->tc_toff.ensure(sizeof(int64_t) * (nsurf + 1));
-    INTI_CUDA(cudaMemcpy(b->tc_toff.p, toff.data(), sizeof(int64_t) * (nsurf + 1), cudaMemcpyHostToDevice));
-    b->tc_items.ensure(sizeof(int32_t) * 2 * b->tc_nitems);
-    INTI_CUDA(cudaMemcpy(b->tc_items.p, isurf.data(), sizeof(int32_t) * b->tc_nitems, cudaMemcpyHostToDevice));
-    INTI_CUDA(cudaMemcpy(b->tc_items.as<int32_t>() + b->tc_nitems, iblk.data(), sizeof(int32_t) * b->tc_nitems,
-                         cudaMemcpyHostToDevice));
-    b->tc_src.ensure(sizeof(float) * TC_S_FLOATS * TC_J * b->tc_ntiles);
-    const int64_t slots = b->tc_ntiles * TC_J;
-    tc_pack_sources<<<(unsigned)((slots + 255) / 256), 256, 0, ctx->stream>>>(
-        nsurf, b->d_off.as<int64_t>(), b->tc_toff.as<int64_t>(), b->coords.as<double>(),
-        b->kind == SL ? nullptr : b->normals.as<double>(), b->tc_src.as<float>());
-    ctx->launches++;
-    b->tc_counter.ensure(sizeof(int));
-    // once per batch (not per launch): an apply after the first only enqueues
-    // work, so it can be captured into a CUDA graph
-    for (const void* kern : {(const void*)mrhs_tc_kernel<SL>, (const void*)mrhs_tc_kernel<DL>,
-                             (const void*)mrhs_tc_kernel<CF>, (const void*)mrhs_tc_kernel<CFI>})
-      INTI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-  }
-  const int ncg = (a.nrhs + TC_R - 1) / TC_R;
-  b->tc_b.ensure((size_t)ncg * b->tc_ntiles * TC_B_BYTES);
-  {
-    ProfScope pp(ctx, "batch_pack");
-    for (int cg = 0; cg < ncg; ++cg) {
-      const int64_t chunks = b->tc_ntiles * (TC_N * TC_K / 4);
-      tc_pack_density<<<(unsigned)((chunks + 255) / 256), 256, 0, ctx->stream>>>(
-          nsurf, b->d_off.as<int64_t>(), b->tc_toff.as<int64_t>(), b->tc_ntiles, b->weights.as<double>(), a.x,
-          a.ldx, a.nrhs, cg, b->tc_b.as<uint32_t>());
-      ctx->launches++;
+  std::vector<int64_t> toff(nsurf + 1, 0);
+  for (int s = 0; s < nsurf; ++s) toff[s + 1] = toff[s] + (b->off[s + 1] - b->off[s] + TC_J - 1) / TC_J;
+  std::vector<int> order(nsurf);
+  for (int s = 0; s < nsurf; ++s) order[s] = s;
+  std::stable_sort(order.begin(), order.end(), [&](int p, int q) {
+    return b->off[p + 1] - b->off[p] > b->off[q + 1] - b->off[q];
+  });
+  std::vector<int32_t> isurf, iblk;
+  for (int s : order)
+    for (int64_t t = 0; t * TC_ROWS < b->off[s + 1] - b->off[s]; ++t) {
+      isurf.push_back(s);
+      iblk.push_back((int32_t)t);
     }
+  b->tc_ntiles = toff[nsurf];
+  b->tc_nitems = (int)isurf.size();
+  b->tc_toff.ensure(sizeof(int64_t) * (nsurf + 1));
+  INTI_CUDA(cudaMemcpy(b->tc_toff.p, toff.data(), sizeof(int64_t) * (nsurf + 1), cudaMemcpyHostToDevice));
+  b->tc_items.ensure(sizeof(int32_t) * 2 * b->tc_nitems);
+  INTI_CUDA(cudaMemcpy(b->tc_items.p, isurf.data(), sizeof(int32_t) * b->tc_nitems, cudaMemcpyHostToDevice));
+  INTI_CUDA(cudaMemcpy(b->tc_items.as<int32_t>() + b->tc_nitems, iblk.data(), sizeof(int32_t) * b->tc_nitems,
+                       cudaMemcpyHostToDevice));
+  // surface groups for the pipelined host apply: contiguous surface ranges of
+  // about equal pair work, at most 8
+  std::vector<double> work(nsurf);
+  double total = 0.0;
+  for (int s = 0; s < nsurf; ++s) {
+    const double ns = (double)(b->off[s + 1] - b->off[s]);
+    work[s] = ns * ns;
+    total += work[s];
   }
+  const int ngrp = std::min(nsurf, 8);
+  b->grp_s.assign(1, 0);
+  double acc = 0.0;
+  for (int s = 0; s + 1 < nsurf; ++s) {
+    acc += work[s];
+    const int made = (int)b->grp_s.size();  // groups started so far
+    if (made >= ngrp) break;
+    // a new group at s + 1 once this one holds its share of the work, or when
+    // every remaining surface has to start a group of its own
+    if (acc >= total * made / ngrp || nsurf - (s + 1) == ngrp - made) b->grp_s.push_back(s + 1);
+  }
+  b->grp_s.push_back(nsurf);
+  std::vector<int32_t> gs, gb;
+  b->grp_item.assign(1, 0);
+  for (size_t g = 0; g + 1 < b->grp_s.size(); ++g) {
+    for (int s : order)
+      if (s >= b->grp_s[g] && s < b->grp_s[g + 1])
+        for (int64_t t = 0; t * TC_ROWS < b->off[s + 1] - b->off[s]; ++t) {
+          gs.push_back(s);
+          gb.push_back((int32_t)t);
+        }
+    b->grp_item.push_back((int)gs.size());
+  }
+  b->tc_items_grp.ensure(sizeof(int32_t) * 2 * gs.size());
+  INTI_CUDA(cudaMemcpy(b->tc_items_grp.p, gs.data(), sizeof(int32_t) * gs.size(), cudaMemcpyHostToDevice));
+  INTI_CUDA(cudaMemcpy(b->tc_items_grp.as<int32_t>() + gs.size(), gb.data(), sizeof(int32_t) * gb.size(),
+                       cudaMemcpyHostToDevice));
+  b->tc_src.ensure(sizeof(float) * TC_S_FLOATS * TC_J * b->tc_ntiles);
+  const int64_t slots = b->tc_ntiles * TC_J;
+  tc_pack_sources<<<(unsigned)((slots + 255) / 256), 256, 0, ctx->stream>>>(
+      nsurf, b->d_off.as<int64_t>(), b->tc_toff.as<int64_t>(), b->coords.as<double>(),
+      b->kind == SL ? nullptr : b->normals.as<double>(), b->tc_src.as<float>());
+  ctx->launches++;
+  b->tc_counter.ensure(sizeof(int));
+  for (const void* kern : {(const void*)mrhs_tc_kernel<SL>, (const void*)mrhs_tc_kernel<DL>,
+                           (const void*)mrhs_tc_kernel<CF>, (const void*)mrhs_tc_kernel<CFI>})
+    INTI_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+}
+
+// Density blocks of tiles [tile0, tile1) for every 64-column group.
+static void tc_pack(inti_batch* b, const double* x, int64_t ldx, int nrhs, int64_t tile0, int64_t tile1) {
+  inti_ctx* ctx = b->ctx;
+  const int nsurf = (int)b->off.size() - 1;
+  const int ncg = (nrhs + TC_R - 1) / TC_R;
+  b->tc_b.ensure((size_t)ncg * b->tc_ntiles * TC_B_BYTES);
+  if (tile1 <= tile0) return;
+  ProfScope pp(ctx, "batch_pack");
+  for (int cg = 0; cg < ncg; ++cg) {
+    const int64_t chunks = (tile1 - tile0) * (TC_N * TC_K / 4);
+    tc_pack_density<<<(unsigned)((chunks + 255) / 256), 256, 0, ctx->stream>>>(
+        nsurf, b->d_off.as<int64_t>(), b->tc_toff.as<int64_t>(), tile0, tile1, b->tc_ntiles,
+        b->weights.as<double>(), x, ldx, nrhs, cg, b->tc_b.as<uint32_t>());
+    ctx->launches++;
+  }
+}
+
+// The tensor-core kernel over nitems work items (item_surf[i], item_block[i]).
+static void tc_run(inti_batch* b, const BatchArgs& a, const int32_t* item_surf, const int32_t* item_block,
+                   int nitems) {
+  inti_ctx* ctx = b->ctx;
   TcArgs t;
   t.off = b->d_off.as<int64_t>();
   t.toff = b->tc_toff.as<int64_t>();
-  t.item_surf = b->tc_items.as<int32_t>();
-  t.item_block = b->tc_items.as<int32_t>() + b->tc_nitems;
-  t.nitems = b->tc_nitems;
-  t.ncolgroups = ncg;
+  t.item_surf = item_surf;
+  t.item_block = item_block;
+  t.nitems = nitems;
+  t.ncolgroups = (a.nrhs + TC_R - 1) / TC_R;
   t.src = b->tc_src.as<float>();
   t.bpack = b->tc_b.as<uint32_t>();
   t.ntiles = b->tc_ntiles;
@@ -705,6 +751,79 @@ void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
     launch(mrhs_tc_kernel<CF>);
   ctx->launches++;
   INTI_CUDA(cudaGetLastError());
+}
+
+void mrhs_tc_launch(inti_batch* b, const BatchArgs& a) {
+  tc_setup(b);
+  tc_pack(b, a.x, a.ldx, a.nrhs, 0, b->tc_ntiles);
+  tc_run(b, a, b->tc_items.as<int32_t>(), b->tc_items.as<int32_t>() + b->tc_nitems, b->tc_nitems);
+}
+
+void batch_apply_host_tf32(inti_batch* b, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
+                           const double* alpha, const double* beta) {
+  inti_ctx* ctx = b->ctx;
+  if (b->pde != INTI_HELMHOLTZ) throw Error(INTI_E_UNSUPPORTED, "the tensor-core form is implemented for Helmholtz");
+  const size_t pitch_x = sizeof(double2) * ldx, pitch_y = sizeof(double2) * ldy;
+  DevBuf &xd = b->xstage, &yd = b->ystage;
+  xd.ensure(pitch_x * nrhs);
+  yd.ensure(pitch_y * nrhs);
+  tc_setup(b);
+  const int ngrp = (int)b->grp_s.size() - 1;
+  if (!b->s_in) {
+    INTI_CUDA(cudaStreamCreateWithFlags(&b->s_in, cudaStreamNonBlocking));
+    INTI_CUDA(cudaStreamCreateWithFlags(&b->s_out, cudaStreamNonBlocking));
+  }
+  while ((int)b->ev.size() < 2 * ngrp + 2) {
+    cudaEvent_t e;
+    INTI_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    b->ev.push_back(e);
+  }
+  BatchArgs a{};
+  a.x = xd.as<double>();
+  a.ldx = ldx;
+  a.y = yd.as<double>();
+  a.ldy = ldy;
+  a.nrhs = nrhs;
+  a.ar = alpha ? alpha[0] : 1.0;
+  a.ai = alpha ? alpha[1] : 0.0;
+  a.br = beta ? beta[0] : 0.0;
+  a.bi = beta ? beta[1] : 0.0;
+  a.beta_zero = a.br == 0.0 && a.bi == 0.0;
+  std::vector<int64_t> toff(b->off.size());
+  for (size_t s = 0; s + 1 < b->off.size(); ++s)
+    toff[s + 1] = toff[s] + (b->off[s + 1] - b->off[s] + TC_J - 1) / TC_J;
+  // the input stream starts after the work already queued on the context's stream
+  INTI_CUDA(cudaEventRecord(b->ev[2 * ngrp], ctx->stream));
+  INTI_CUDA(cudaStreamWaitEvent(b->s_in, b->ev[2 * ngrp], 0));
+  INTI_CUDA(cudaStreamWaitEvent(b->s_out, b->ev[2 * ngrp], 0));
+  const int32_t* gs = b->tc_items_grp.as<int32_t>();
+  const int32_t* gb = gs + b->grp_item.back();
+  for (int g = 0; g < ngrp; ++g) {
+    const int s0 = b->grp_s[g], s1 = b->grp_s[g + 1];
+    const int64_t r0 = b->off[s0], rows = b->off[s1] - r0;
+    const size_t width = sizeof(double2) * rows;
+    // in: X rows (and Y rows when beta != 0) of this group, all columns
+    INTI_CUDA(cudaMemcpy2DAsync(xd.as<double2>() + r0, pitch_x, reinterpret_cast<const double2*>(x) + r0, pitch_x,
+                                width, nrhs, cudaMemcpyHostToDevice, b->s_in));
+    if (!a.beta_zero)
+      INTI_CUDA(cudaMemcpy2DAsync(yd.as<double2>() + r0, pitch_y, reinterpret_cast<const double2*>(y) + r0,
+                                  pitch_y, width, nrhs, cudaMemcpyHostToDevice, b->s_in));
+    INTI_CUDA(cudaEventRecord(b->ev[2 * g], b->s_in));
+    INTI_CUDA(cudaStreamWaitEvent(ctx->stream, b->ev[2 * g], 0));
+    // compute: this group's density tiles, items and correction rows
+    tc_pack(b, a.x, ldx, nrhs, toff[s0], toff[s1]);
+    const int i0 = b->grp_item[g], i1 = b->grp_item[g + 1];
+    tc_run(b, a, gs + i0, gb + i0, i1 - i0);
+    batch_correction_rows(b, a.x, ldx, a.y, ldy, nrhs, a.ar, a.ai, r0, r0 + rows);
+    INTI_CUDA(cudaEventRecord(b->ev[2 * g + 1], ctx->stream));
+    // out: Y rows of this group
+    INTI_CUDA(cudaStreamWaitEvent(b->s_out, b->ev[2 * g + 1], 0));
+    INTI_CUDA(cudaMemcpy2DAsync(reinterpret_cast<double2*>(y) + r0, pitch_y, yd.as<double2>() + r0, pitch_y, width,
+                                nrhs, cudaMemcpyDeviceToHost, b->s_out));
+  }
+  INTI_CUDA(cudaEventRecord(b->ev[2 * ngrp + 1], b->s_out));
+  INTI_CUDA(cudaStreamWaitEvent(ctx->stream, b->ev[2 * ngrp + 1], 0));
+  sync_and_check(ctx);
 }
 
 }  // namespace inti
