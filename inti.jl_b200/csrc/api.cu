@@ -120,6 +120,15 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
   L.c1[1] = op->c1[1];
   L.c2[0] = op->c2[0];
   L.c2[1] = op->c2[1];
+  if (op->symm) {
+    L.symm = true;
+    L.sym_nb = op->sym_nb;
+    L.sym_nitems = op->sym_nitems;
+    L.sym_items = op->sym_tab.as<int32_t>();
+    L.sym_rowptr = L.sym_items + 3 * op->sym_nitems;
+    L.sym_rowitems = L.sym_rowptr + op->sym_nb + 1;
+    L.zpart = op->zpart.p;
+  }
   return L;
 }
 
@@ -135,6 +144,7 @@ void op_apply_transpose_device(inti_op* op, const double* x, double* y, const do
                                const double* beta) {
   // the forward pair product with targets and sources swapped (op_prepare_transpose)
   PairLaunch L = make_launch(op, x);
+  L.symm = false;  // the swapped product runs one-sided
   L.kind = transposed_kind(op->kind);
   L.m = op->source->n;
   L.n = op->target->n;
@@ -546,6 +556,16 @@ int inti_op_tuning(const inti_op* op, int32_t* targets_per_thread, int32_t* spli
 int inti_ctx_set_autotune(inti_ctx* ctx, int enable) {
   if (!ctx) return INTI_E_ARG;
   return guarded(ctx, [&] { ctx->autotune = enable != 0; });
+}
+
+int inti_ctx_set_symmetric(inti_ctx* ctx, int enable) {
+  if (!ctx) return INTI_E_ARG;
+  return guarded(ctx, [&] { ctx->symmetric = enable != 0; });
+}
+
+int inti_op_symmetric(const inti_op* op) {
+  if (!op) return -INTI_E_ARG;
+  return op->symm ? 1 : 0;
 }
 
 int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype) {

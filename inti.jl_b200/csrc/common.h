@@ -89,6 +89,9 @@ struct inti_ctx {
   // key "pde/kind/dim/precision/m/n" -> (targets per thread, split)
   bool autotune = true;
   std::map<std::string, std::pair<int, int>> tuned;
+  // square operators created while this is set use the symmetric pair
+  // kernel (inti_ctx_set_symmetric)
+  bool symmetric = true;
   // GMRES workspace kept between solves: Krylov basis, work vectors, the
   // reduction scratch and the staged right-hand side / solution.
   struct {
@@ -164,6 +167,14 @@ struct PairLaunch {
   int tpt = 4;             // targets per thread of the pair kernel (2 or 4)
   int64_t n_tiles;         // padded source tiles
   int* err_flag;
+  // symmetric form (target set == source set; pair_symm): work items
+  // (I, J0, J1), per row block the list of its items, column partials
+  bool symm = false;
+  int sym_nb = 0, sym_nitems = 0;
+  const int32_t* sym_items = nullptr;     // 3 x nitems
+  const int32_t* sym_rowptr = nullptr;    // nb + 1
+  const int32_t* sym_rowitems = nullptr;  // nitems
+  void* zpart = nullptr;                  // nb x (n_tiles * tile)
 };
 
 // Message for inti_last_error(NULL) from entry points that take no context.
@@ -177,6 +188,12 @@ int pair_tile(int precision);
 int pair_record_bytes(int pde, int kind, int dim, int precision);
 // Bytes of one partial accumulator per target per split.
 int pair_partial_bytes(int pde, int precision);
+// Symmetric form: node block of 128*tpt nodes; work items of row blocks
+// against chunks of `ch` source blocks (the longest first), the table laid
+// out as items (3 x nitems), row pointers (nb + 1), row items (nitems).
+int pair_symm_block(int tpt);
+void pair_symm_plan(int64_t n, int tpt, int ch, std::vector<int32_t>& table, int& nb, int& nitems);
+int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int precision, int64_t n, int tpt);
 // Choose the split for a problem on this device.
 int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
                     int64_t n, int tpt = 4);

@@ -36,6 +36,11 @@ struct inti_op {
   int split = 1;
   int tpt = 4;  // targets per thread of the pair kernel (autotuned with split)
   int tsplit = 1, ttpt = 4;  // A^T launch shape
+  // symmetric form (target set == source set, pair_symm): plan table and
+  // column partials; split holds the source blocks per work item
+  bool symm = false;
+  int sym_nb = 0, sym_nitems = 0;
+  inti::DevBuf sym_tab, zpart;
   int64_t n_tiles = 1, tn_tiles = 1;
   // Derived operators kept for repeated solves: the FP32C twin used by the
   // mixed-precision GMRES, and (on a double layer) the combined-field operator
@@ -69,6 +74,10 @@ inti_op* op_clone_precision(const inti_op* op, int precision);
 // problem, else (measure = true, autotuning on, problem large enough) the
 // fastest candidate timed now, else the occupancy heuristic.
 void op_autotune(inti_op* op, bool measure);
+// Square operators (target === source, 3D SL/DL/combined field): switch to
+// the symmetric form when the context allows it and its column partials fit.
+void op_symm_init(inti_op* op);
+void op_symm_configure(inti_op* op, int tpt, int ch);
 std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
                                             const inti_csr* b, const double* cb, int64_t m, int64_t n,
                                             bool cplx);

@@ -65,6 +65,7 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   const int64_t big = std::max(target->n, source->n);
   op->xbuf.ensure(sizeof(double) * comps * big);
   op->ybuf.ensure(sizeof(double) * comps * big);
+  op_symm_init(op.get());
   op_autotune(op.get(), false);
   return op.release();
 }
@@ -169,6 +170,7 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   const int64_t big = std::max(target->n, source->n);
   op->xbuf.ensure(sizeof(double) * comps * big);
   op->ybuf.ensure(sizeof(double) * comps * big);
+  op_symm_init(op.get());
   op_autotune(op.get(), false);
   return op.release();
 }
@@ -199,8 +201,49 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
   const int64_t big = std::max(op->target->n, op->source->n);
   t->xbuf.ensure(sizeof(double) * comps * big);
   t->ybuf.ensure(sizeof(double) * comps * big);
+  op_symm_init(t.get());
   op_autotune(t.get(), false);
   return t.release();
+}
+
+// Column partials of the symmetric form are nb x n values; above this size
+// (N of a few hundred thousand) the operator keeps the one-sided kernel.
+constexpr double kSymmMaxPartialBytes = 2.0e9;
+
+void op_symm_configure(inti_op* op, int tpt, int ch) {
+  std::vector<int32_t> tab;
+  int nb = 0, nitems = 0;
+  pair_symm_plan(op->source->n, tpt, ch, tab, nb, nitems);
+  INTI_CUDA(cudaStreamSynchronize(op->ctx->stream));  // no launch is reading the old table
+  op->sym_tab.ensure(sizeof(int32_t) * tab.size());
+  INTI_CUDA(cudaMemcpy(op->sym_tab.p, tab.data(), sizeof(int32_t) * tab.size(), cudaMemcpyHostToDevice));
+  op->sym_nb = nb;
+  op->sym_nitems = nitems;
+  op->tpt = tpt;
+  op->split = ch;
+  const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
+  const int64_t npad = op->n_tiles * pair_tile(op->precision);
+  op->partial.ensure(pb * nitems * pair_symm_block(tpt));
+  op->zpart.ensure(pb * nb * npad);
+}
+
+void op_symm_init(inti_op* op) {
+  inti_ctx* ctx = op->ctx;
+  op->symm = false;
+  if (!ctx->symmetric || op->target != op->source || op->dim != 3 ||
+      !(op->kind == SL || op->kind == DL || op->kind == CF))
+    return;
+  const int64_t n = op->source->n;
+  const int tile = pair_tile(op->precision);
+  const int64_t bmax = pair_symm_block(4), bmin = pair_symm_block(2);
+  const int64_t npad = (n + bmax - 1) / bmax * bmax;  // whole blocks for both node-block sizes
+  const double zbytes = (double)((n + bmin - 1) / bmin) * npad * pair_partial_bytes(op->pde, op->precision);
+  if (zbytes > kSymmMaxPartialBytes) return;
+  op->symm = true;
+  op->n_tiles = npad / tile;
+  op->packed.ensure((size_t)npad * pair_record_bytes(op->pde, op->kind, op->dim, op->precision));
+  const int tpt = 2;
+  op_symm_configure(op, tpt, pair_symm_default_ch(ctx, op->pde, op->kind, op->precision, n, tpt));
 }
 
 // Problems below this many pairs keep the heuristic shape (a timing pass
@@ -212,7 +255,52 @@ void op_autotune(inti_op* op, bool measure) {
   const int64_t m = op->target->n, n = op->source->n;
   const std::string key = std::to_string(op->pde) + "/" + std::to_string(op->kind) + "/" +
                           std::to_string(op->dim) + "/" + std::to_string(op->precision) + "/" +
-                          std::to_string(m) + "/" + std::to_string(n);
+                          std::to_string(m) + "/" + std::to_string(n) + (op->symm ? "/symmetric" : "");
+  if (op->symm) {
+    // symmetric form: 4 or 2 targets per thread, each with the default number
+    // of source blocks per item, half and twice it
+    auto cached = ctx->tuned.find(key);
+    if (cached != ctx->tuned.end()) {
+      if (cached->second.first != op->tpt || cached->second.second != op->split)
+        op_symm_configure(op, cached->second.first, cached->second.second);
+      return;
+    }
+    if (!measure || !ctx->autotune || (double)m * (double)n < kTuneMinPairs) return;
+    std::vector<std::pair<int, int>> cand;
+    for (int tpt : {4, 2}) {
+      const int c0 = pair_symm_default_ch(ctx, op->pde, op->kind, op->precision, n, tpt);
+      for (int ch : {c0, std::max(1, c0 / 2), 2 * c0})
+        if (std::find(cand.begin(), cand.end(), std::make_pair(tpt, ch)) == cand.end()) cand.emplace_back(tpt, ch);
+    }
+    const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
+    INTI_CUDA(cudaMemsetAsync(op->xbuf.p, 0, sizeof(double) * comps * n, ctx->stream));
+    cudaEvent_t e0, e1;
+    INTI_CUDA(cudaEventCreate(&e0));
+    INTI_CUDA(cudaEventCreate(&e1));
+    float best = -1.0f;
+    std::pair<int, int> pick(op->tpt, op->split);
+    for (auto& c : cand) {
+      op_symm_configure(op, c.first, c.second);
+      PairLaunch L = make_launch(op, op->xbuf.as<double>());
+      pair_launch(ctx, L);  // warm-up of this shape
+      INTI_CUDA(cudaEventRecord(e0, ctx->stream));
+      pair_launch(ctx, L);
+      INTI_CUDA(cudaEventRecord(e1, ctx->stream));
+      INTI_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.0f;
+      INTI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      if (best < 0.0f || ms < best) {
+        best = ms;
+        pick = c;
+      }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    sync_and_check(ctx);
+    ctx->tuned[key] = pick;
+    op_symm_configure(op, pick.first, pick.second);
+    return;
+  }
   const size_t pbytes = (size_t)pair_partial_bytes(op->pde, op->precision);
   auto set = [&](int tpt, int split) {
     op->tpt = tpt;

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <mutex>
 #include <string>
@@ -466,17 +467,10 @@ struct EpiArgs {
   const double* rowscale = nullptr;  // per-row factor of the pair sum (A^T: the source weights)
 };
 
-template <class P, bool CPLX>
-__global__ void pair_epilogue_kernel(EpiArgs e) {
-  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= e.m) return;
-  const P* part = static_cast<const P*>(e.partial);
-  double sr = 0.0, si = 0.0;
-  for (int s = 0; s < e.split; ++s) {
-    const double2 v = load_partial(part + (int64_t)s * e.m + i);
-    sr += v.x;
-    si += v.y;
-  }
+// Kernel constant, correction row, alpha/beta and the store for row i, given
+// the row's pair sum (sr, si).
+template <bool CPLX>
+__device__ __forceinline__ void epilogue_finish(const EpiArgs& e, int64_t i, double sr, double si) {
   const double sc = e.rowscale ? e.scale * e.rowscale[i] : e.scale;
   sr *= sc;
   si *= sc;
@@ -507,6 +501,279 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
     if (!e.beta_zero) yr += e.br * e.y[i];
     e.y[i] = yr;
   }
+}
+
+template <class P, bool CPLX>
+__global__ void pair_epilogue_kernel(EpiArgs e) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= e.m) return;
+  const P* part = static_cast<const P*>(e.partial);
+  double sr = 0.0, si = 0.0;
+  for (int s = 0; s < e.split; ++s) {
+    const double2 v = load_partial(part + (int64_t)s * e.m + i);
+    sr += v.x;
+    si += v.y;
+  }
+  epilogue_finish<CPLX>(e, i, sr, si);
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric form for square operators (the target set is the source set),
+// single layer, double layer and combined field in 3D.
+//
+// Every kernel value of an unordered pair {a, b} serves both products:
+//   SL: G(x_a, x_b) = G(x_b, x_a);
+//   DL: K(x_a, x_b) p_b = d(r.p_b) and K(x_b, x_a) p_a = -d(r.p_a) with the
+//       same radial factor d (r = x_a - x_b, p the packed dipoles w sigma n);
+// so the distance, the reciprocal square root and the phase are computed
+// once per unordered pair.  Nodes are cut into blocks of BT = 128*TPT; a CTA
+// takes one work item (row block I, source blocks J0 <= J < J1, J >= I):
+// its threads hold the targets of block I (coordinates and their own packed
+// charge/dipole), source tiles of the blocks J stream through shared memory
+// as in pair_forward.  For J == I every ordered pair is evaluated (the
+// forward step).  For J > I the row sums go to the target registers and the
+// column sums of each source are reduced over the CTA (warp shuffles, then
+// the four warps in a fixed order) and stored in zpart[I][j].  The epilogue
+// adds, for node i of block B, the row partials of the items of row B and
+// zpart[I][i] for I < B: a fixed order, so the result is deterministic.
+// ---------------------------------------------------------------------------
+struct SymArgs {
+  int64_t npad;           // packed records: nb * BT (zero charges past n)
+  const int32_t* items;   // (I, J0, J1) per CTA
+  const void* packed;
+  void* ypart;            // [item][BT]
+  void* zpart;            // [nb][npad]
+  double k, kT, delta;
+  const void* expi;
+  int* err;
+};
+
+// Both products of one unordered pair: y_t += K(x_t, x_s) c_s and
+// z_s += K(x_s, x_t) c_t, with c the packed charge/dipole records of the
+// target t and the source s (layouts of Rec), r = x_t - x_s.
+template <int PDE, int KIND, class R>
+__device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* __restrict__ s, R kT, R delta, R k,
+                                              const typename MathOps<R>::R2* __restrict__ tab, R& ar, R& ai,
+                                              R& zr, R& zi) {
+  using M = MathOps<R>;
+  const R r0 = t[0] - s[0], r1 = t[1] - s[1], r2 = t[2] - s[2];
+  const R d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
+  const bool keep = M::keep(d2);
+  if (PDE == LAPLACE) {
+    if (KIND == SL) {
+      const R ri = keep ? M::rsq(d2) : R(0);
+      ar = fma(ri, s[3], ar);
+      zr = fma(ri, t[3], zr);
+    } else {
+      const R rs = fma(r2, s[5], fma(r1, s[4], r0 * s[3]));
+      const R rt = fma(r2, t[5], fma(r1, t[4], r0 * t[3]));
+      if (KIND == DL) {
+        const R ri3 = keep ? M::rsq3(d2) : R(0);
+        ar = fma(rs, ri3, ar);
+        zr = fma(-rt, ri3, zr);
+      } else {  // CF: charge after the dipole
+        const R ri = keep ? M::rsq(d2) : R(0);
+        const R ri3 = ri * ri * ri;
+        ar = fma(ri, s[6], fma(rs, ri3, ar));
+        zr = fma(ri, t[6], fma(-rt, ri3, zr));
+      }
+    }
+  } else {
+    const R ri = keep ? M::rsq(d2) : R(0);
+    R sn, cs;
+    expi_table_eval(d2 * ri, kT, tab, delta, cs, sn);
+    if (KIND == SL) {
+      const R gr = ri * cs, gi = ri * sn;
+      ar = fma(gr, s[3], fma(-gi, s[4], ar));
+      ai = fma(gr, s[4], fma(gi, s[3], ai));
+      zr = fma(gr, t[3], fma(-gi, t[4], zr));
+      zi = fma(gr, t[4], fma(gi, t[3], zi));
+    } else {  // dipole Re [3..5], Im [6..8]; CF: charge [9], [10]
+      const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
+      const R id2 = ri * ri;
+      const R gr = er * id2, gi = ei * id2;
+      const R A = fma(r2, s[5], fma(r1, s[4], r0 * s[3])), B = fma(r2, s[8], fma(r1, s[7], r0 * s[6]));
+      const R At = fma(r2, t[5], fma(r1, t[4], r0 * t[3])), Bt = fma(r2, t[8], fma(r1, t[7], r0 * t[6]));
+      ar = fma(gr, A, fma(-gi, B, ar));
+      ai = fma(gr, B, fma(gi, A, ai));
+      zr = fma(-gr, At, fma(gi, Bt, zr));
+      zi = fma(-gr, Bt, fma(-gi, At, zi));
+      if (KIND == CF) {
+        const R hr = cs * ri, hi = sn * ri;
+        ar = fma(hr, s[9], fma(-hi, s[10], ar));
+        ai = fma(hr, s[10], fma(hi, s[9], ai));
+        zr = fma(hr, t[9], fma(-hi, t[10], zr));
+        zi = fma(hr, t[10], fma(hi, t[9], zi));
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void put_partial(double* p, double r, double) { *p = r; }
+__device__ __forceinline__ void put_partial(double2* p, double r, double i) { *p = make_double2(r, i); }
+__device__ __forceinline__ void put_partial(float2* p, float r, float) { *p = make_float2(r, 0.f); }
+__device__ __forceinline__ void put_partial(float4* p, float r, float i) { *p = make_float4(r, 0.f, i, 0.f); }
+
+template <int PDE, int KIND, class R, int TILE, int TPT>
+__global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
+  using RC = Rec<PDE, KIND, 3, R>;
+  constexpr bool CPLX = RC::cplx;
+  using P = typename PartialT<R, CPLX>::T;
+  using R2 = typename MathOps<R>::R2;
+  constexpr int BT = kBlock * TPT;
+  static_assert(BT % TILE == 0, "whole source tiles per node block");
+  constexpr int TPB = BT / TILE;
+  constexpr int NU = RC::used;
+  constexpr int kWarps = kBlock / 32;
+  constexpr uint32_t kStageBytes = TILE * RC::n * sizeof(R);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  R* stage0 = reinterpret_cast<R*>(smem_raw);
+  R* stage1 = reinterpret_cast<R*>(smem_raw + kStageBytes);
+  R2* tab = reinterpret_cast<R2*>(smem_raw + 2 * kStageBytes);  // Helmholtz only
+  R* zsm = reinterpret_cast<R*>(smem_raw + 2 * kStageBytes + (CPLX ? kExpiTable * sizeof(R2) : 0));
+  __shared__ __align__(8) uint64_t full[2];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int I = a.items[3 * blockIdx.x], J0 = a.items[3 * blockIdx.x + 1], J1 = a.items[3 * blockIdx.x + 2];
+  const R* src = static_cast<const R*>(a.packed);
+  R tg[TPT][NU];
+  Acc<R, CPLX> acc[TPT];
+#pragma unroll
+  for (int u = 0; u < TPT; ++u) {
+    const int64_t i = (int64_t)I * BT + u * kBlock + tid;
+#pragma unroll
+    for (int c = 0; c < NU; ++c) tg[u][c] = src[i * RC::n + c];
+  }
+  const R k = R(a.k), kT = R(a.kT), delta = R(a.delta);
+  if (CPLX) {
+    const R2* g = static_cast<const R2*>(a.expi);
+    for (int q = tid; q < kExpiTable; q += kBlock) tab[q] = g[q];
+  }
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int64_t t0 = (int64_t)J0 * TPB, t1 = (int64_t)J1 * TPB;
+  int64_t issued = t0;
+  if (tid == 0) {
+    for (int s = 0; s < 2 && issued < t1; ++s, ++issued) {
+      mbar_arrive_expect_tx(&full[s], kStageBytes);
+      bulk_copy_g2s(s ? stage1 : stage0, src + issued * TILE * RC::n, kStageBytes, &full[s]);
+    }
+  }
+  for (int64_t t = t0; t < t1; ++t) {
+    const int st = (int)((t - t0) & 1);
+    const uint32_t parity = (uint32_t)(((t - t0) >> 1) & 1);
+    const bool ok = mbar_wait_bounded(&full[st], parity);
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) {
+        atomicExch(a.err, kErrWaitTimeout);
+        for (int64_t q = t + 1; q < issued; ++q)
+          mbar_wait_bounded(&full[(q - t0) & 1], (uint32_t)(((q - t0) >> 1) & 1));
+      }
+      return;
+    }
+    const R* sp = st ? stage1 : stage0;
+    const bool diag = t / TPB == I;
+    R* zb = zsm + st * (kWarps * TILE * 2);
+    if (diag) {
+#pragma unroll 1
+      for (int g = 0; g < TILE; g += kGroup) {
+#pragma unroll 2
+        for (int s = 0; s < kGroup; ++s) {
+          const R* rec = sp + (g + s) * RC::n;
+#pragma unroll
+          for (int u = 0; u < TPT; ++u) {
+            Target<R, 3, false> tt;
+            tt.x[0] = tg[u][0];
+            tt.x[1] = tg[u][1];
+            tt.x[2] = tg[u][2];
+            pair_step<PDE, KIND, 3, R>(tt, rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) acc[u].fold();
+      }
+    } else {
+#pragma unroll 1
+      for (int g = 0; g < TILE; g += kGroup) {
+#pragma unroll 2
+        for (int s = 0; s < kGroup; ++s) {
+          const R* rec = sp + (g + s) * RC::n;
+          R zr = R(0), zi = R(0);
+#pragma unroll
+          for (int u = 0; u < TPT; ++u)
+            pair_sym_step<PDE, KIND, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(), zr, zi);
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) {
+            zr += __shfl_xor_sync(0xffffffffu, zr, o);
+            if (CPLX) zi += __shfl_xor_sync(0xffffffffu, zi, o);
+          }
+          if (lane == 0) {
+            zb[(warp * TILE + g + s) * 2] = zr;
+            zb[(warp * TILE + g + s) * 2 + 1] = zi;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < TPT; ++u) acc[u].fold();
+      }
+    }
+    __syncthreads();  // the stage is read and this tile's column sums are in zb
+    if (!diag) {
+      P* zp = static_cast<P*>(a.zpart) + (int64_t)I * a.npad + t * TILE;
+      for (int s = tid; s < TILE; s += kBlock) {
+        R vr = zb[s * 2], vi = zb[s * 2 + 1];
+#pragma unroll
+        for (int w = 1; w < kWarps; ++w) {
+          vr += zb[(w * TILE + s) * 2];
+          vi += zb[(w * TILE + s) * 2 + 1];
+        }
+        put_partial(zp + s, vr, vi);
+      }
+    }
+    if (tid == 0 && issued < t1) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&full[st], kStageBytes);
+      bulk_copy_g2s(st ? stage1 : stage0, src + issued * TILE * RC::n, kStageBytes, &full[st]);
+      ++issued;
+    }
+  }
+  P* out = static_cast<P*>(a.ypart) + (int64_t)blockIdx.x * BT;
+#pragma unroll
+  for (int u = 0; u < TPT; ++u) store_partial(out + u * kBlock + tid, acc[u]);
+}
+
+// Row sums of the symmetric form: the item partials of row block B and the
+// column partials of the row blocks above.
+struct SymEpi {
+  int64_t npad;
+  int bt;
+  const int32_t* rowptr;    // nb + 1
+  const int32_t* rowitems;  // items of each row block
+  const void* zpart;
+};
+
+template <class P, bool CPLX>
+__global__ void pair_symm_epilogue_kernel(EpiArgs e, SymEpi s) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= e.m) return;
+  const int B = (int)(i / s.bt), il = (int)(i % s.bt);
+  const P* yp = static_cast<const P*>(e.partial);
+  const P* zp = static_cast<const P*>(s.zpart);
+  double sr = 0.0, si = 0.0;
+  for (int q = s.rowptr[B]; q < s.rowptr[B + 1]; ++q) {
+    const double2 v = load_partial(yp + (int64_t)s.rowitems[q] * s.bt + il);
+    sr += v.x;
+    si += v.y;
+  }
+  for (int r = 0; r < B; ++r) {
+    const double2 v = load_partial(zp + (int64_t)r * s.npad + i);
+    sr += v.x;
+    si += v.y;
+  }
+  epilogue_finish<CPLX>(e, i, sr, si);
 }
 
 // ---------------------------------------------------------------------------
@@ -700,6 +967,75 @@ int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precisi
   return best;
 }
 
+// Dynamic shared memory of the symmetric kernel: two source stages, the
+// e^{i m delta} table, two buffers of per-warp column sums.
+template <class T, class R>
+static size_t symm_smem() {
+  constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
+  return fwd_smem<T, R>() + 2 * (size_t)(kBlock / 32) * TILE * 2 * sizeof(R);
+}
+
+template <class T>
+constexpr bool symm_kind() {
+  return T::dim == 3 && (T::kind == SL || T::kind == DL || T::kind == CF);
+}
+
+int pair_symm_block(int tpt) { return kBlock * tpt; }
+
+void pair_symm_plan(int64_t n, int tpt, int ch, std::vector<int32_t>& table, int& nb, int& nitems) {
+  const int bt = pair_symm_block(tpt);
+  nb = (int)std::max<int64_t>(1, (n + bt - 1) / bt);
+  ch = std::max(1, ch);
+  std::vector<std::array<int32_t, 3>> it;
+  for (int I = 0; I < nb; ++I)
+    for (int J0 = I; J0 < nb; J0 += ch) it.push_back({I, J0, std::min(J0 + ch, nb)});
+  std::stable_sort(it.begin(), it.end(), [](const std::array<int32_t, 3>& a, const std::array<int32_t, 3>& b) {
+    return a[2] - a[1] > b[2] - b[1];
+  });
+  nitems = (int)it.size();
+  table.assign((size_t)3 * nitems + nb + 1 + nitems, 0);
+  int32_t* items = table.data();
+  int32_t* rowptr = items + 3 * nitems;
+  int32_t* rowitems = rowptr + nb + 1;
+  for (int q = 0; q < nitems; ++q) {
+    items[3 * q] = it[q][0];
+    items[3 * q + 1] = it[q][1];
+    items[3 * q + 2] = it[q][2];
+    ++rowptr[it[q][0] + 1];
+  }
+  for (int I = 0; I < nb; ++I) rowptr[I + 1] += rowptr[I];
+  std::vector<int32_t> fill(rowptr, rowptr + nb);
+  for (int q = 0; q < nitems; ++q) rowitems[fill[it[q][0]]++] = q;
+}
+
+int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int precision, int64_t n, int tpt) {
+  int occ = 1;
+  dispatch(pde, kind, 3, [&](auto tag) {
+    using T = decltype(tag);
+    if constexpr (symm_kind<T>()) {
+      const void* fn;
+      size_t sm;
+      if (precision == INTI_FP32C) {
+        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, float, kTile32, 2>
+                      : (const void*)&pair_symm<T::pde, T::kind, float, kTile32, 4>;
+        sm = symm_smem<T, float>();
+      } else {
+        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, double, kTile64, 2>
+                      : (const void*)&pair_symm<T::pde, T::kind, double, kTile64, 4>;
+        sm = symm_smem<T, double>();
+      }
+      INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      INTI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, kBlock, sm));
+    }
+  });
+  occ = std::max(occ, 1);
+  const int bt = pair_symm_block(tpt);
+  const int64_t nb = std::max<int64_t>(1, (n + bt - 1) / bt);
+  const int64_t pairs = nb * (nb + 1) / 2;         // block pairs J >= I
+  const int64_t want = (int64_t)ctx->num_sms * occ * 8;  // about 8 waves of items
+  return (int)std::max<int64_t>(1, std::min<int64_t>(nb, (pairs + want - 1) / want));
+}
+
 int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
   const int tile = pair_tile(L.precision);
   const int64_t npad = L.n_tiles * tile;
@@ -717,6 +1053,29 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
             L.n, npad, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
             make_double2(L.c2[0], L.c2[1]), static_cast<R*>(L.packed));
       }
+      if constexpr (symm_kind<T>()) {
+        if (L.symm) {
+          SymArgs a;
+          a.npad = npad;
+          a.items = L.sym_items;
+          a.packed = L.packed;
+          a.ypart = L.partial;
+          a.zpart = L.zpart;
+          a.k = L.k;
+          a.kT = L.k * kExpiTable / (2 * kPi);
+          a.delta = 2 * kPi / kExpiTable;
+          a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
+          a.err = L.err_flag;
+          const size_t sm = symm_smem<T, R>();
+          auto fn = L.tpt == 2 ? &pair_symm<T::pde, T::kind, R, TILE, 2> : &pair_symm<T::pde, T::kind, R, TILE, 4>;
+          INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+          ProfScope pp(ctx, "pair");
+          fn<<<(unsigned)L.sym_nitems, kBlock, sm, ctx->stream>>>(a);
+          launches = 2;
+          return;
+        }
+      }
+      if (L.symm) throw Error(INTI_E_UNSUPPORTED, "symmetric form of this kernel");
       FwdArgs a;
       a.m = L.m;
       a.n_tiles = L.n_tiles;
@@ -771,6 +1130,28 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
   const unsigned gb = (unsigned)((L.m + tb - 1) / tb);
   const bool cplx = L.pde == HELMHOLTZ;
   ProfScope pe(ctx, "epilogue");
+  if (L.symm) {
+    SymEpi se;
+    se.npad = L.n_tiles * pair_tile(L.precision);
+    se.bt = pair_symm_block(L.tpt);
+    se.rowptr = L.sym_rowptr;
+    se.rowitems = L.sym_rowitems;
+    se.zpart = L.zpart;
+    if (L.precision == INTI_FP32C) {
+      if (cplx)
+        pair_symm_epilogue_kernel<float4, true><<<gb, tb, 0, ctx->stream>>>(e, se);
+      else
+        pair_symm_epilogue_kernel<float2, false><<<gb, tb, 0, ctx->stream>>>(e, se);
+    } else {
+      if (cplx)
+        pair_symm_epilogue_kernel<double2, true><<<gb, tb, 0, ctx->stream>>>(e, se);
+      else
+        pair_symm_epilogue_kernel<double, false><<<gb, tb, 0, ctx->stream>>>(e, se);
+    }
+    INTI_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return 1;
+  }
   if (L.precision == INTI_FP32C) {
     if (cplx)
       pair_epilogue_kernel<float4, true><<<gb, tb, 0, ctx->stream>>>(e);

@@ -115,6 +115,11 @@ class Context:
         default; see ``GpuOperator.tuning``)."""
         self.check(self.lib.inti_ctx_set_autotune(self.handle, int(bool(enable))))
 
+    def set_symmetric(self, enable: bool) -> None:
+        """Use the symmetric pair kernel for square operators created
+        afterwards (on by default; see ``GpuOperator.tuning``)."""
+        self.check(self.lib.inti_ctx_set_symmetric(self.handle, int(bool(enable))))
+
     def selftest_math(self) -> dict:
         """Accuracy of the device's fast rsqrt / e^{iθ} helpers (see the ABI)."""
         out = (C.c_double * 5)()
@@ -527,7 +532,8 @@ class GpuOperator(_Map):
         """Launch shape of the pair kernel: targets per thread and split."""
         t, s = C.c_int32(), C.c_int32()
         self.ctx.check(self.ctx.lib.inti_op_tuning(self.handle, C.byref(t), C.byref(s)))
-        return {"targets_per_thread": t.value, "split": s.value}
+        return {"targets_per_thread": t.value, "split": s.value,
+                "symmetric": bool(self.ctx.lib.inti_op_symmetric(self.handle) == 1)}
 
     def grad_sources_device(self, g_ptr: int, sigma_ptr: int, dsigma_ptr: int, dcoords_ptr: int,
                             dnormals_ptr: int, dweights_ptr: int) -> None:

@@ -1,0 +1,83 @@
+"""Symmetric pair kernel of square operators (target === source): each
+unordered pair is evaluated once for both products.  Checked against the
+one-sided kernel (a context with the symmetric form off) and the oracle, on
+surfaces of many node blocks with a ragged last block, for the single layer,
+double layer and combined field, Laplace and Helmholtz, FP64 and FP32C, with
+the DIM correction, alpha/beta and repeated applies."""
+import numpy as np
+import pytest
+
+import inti_b200 as inti
+import oracle as O
+from helpers import density, oracle_apply, relerr
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def one_sided():
+    c = inti.Context(0)
+    c.set_symmetric(False)
+    return c
+
+
+def _op(pde):
+    return inti.Laplace(dim=3) if pde == O.LAPLACE else inti.Helmholtz(k=6.0, dim=3)
+
+
+@pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
+@pytest.mark.parametrize("kname", ["SL", "DL"])
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32c", 5e-5)])
+def test_symmetric_matches_one_sided_and_oracle(ctx, one_sided, pde, kname, prec, tol):
+    q = inti.ellipsoid_quadrature(9, 5)  # 4,374 nodes: 9 blocks of 512, the last ragged
+    K = inti.SingleLayerKernel if kname == "SL" else inti.DoubleLayerKernel
+    okind = O.SL if kname == "SL" else O.DL
+    k = 0.0 if pde == O.LAPLACE else 6.0
+    A = inti.GpuOperator(K(_op(pde)), q, q, None, prec, ctx)
+    B = inti.GpuOperator(K(_op(pde)), q, q, None, prec, one_sided)
+    assert A.tuning["symmetric"] and not B.tuning["symmetric"]
+    x = density(len(q), pde == O.HELMHOLTZ, 3)
+    ya, yb = A @ x, B @ x
+    ref = oracle_apply(pde, okind, k, q, q, x)
+    assert relerr(ya, ref) < tol and relerr(yb, ref) < tol
+    if prec == "fp64":
+        assert relerr(ya, yb) < 1e-13
+    assert np.array_equal(A @ x, ya)  # deterministic
+
+
+@pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
+def test_symmetric_combined_field_with_correction(ctx, one_sided, pde):
+    q = inti.ellipsoid_quadrature(8, 5)  # 3,456 nodes
+    op = _op(pde)
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    cS = -6.0j if pde == O.HELMHOLTZ else 0.7
+    CF = inti.CombinedFieldOperator(D, S, 1.0, cS)
+    assert CF.tuning["symmetric"]
+    cs = inti.CorrectionMatrix.from_csr(*S.correction.arrays(), S.shape, ctx=one_sided)
+    cd = inti.CorrectionMatrix.from_csr(*D.correction.arrays(), D.shape, ctx=one_sided)
+    S2 = inti.GpuOperator(S.kernel, q, q, cs, "fp64", one_sided)
+    D2 = inti.GpuOperator(D.kernel, q, q, cd, "fp64", one_sided)
+    cplx = pde == O.HELMHOLTZ
+    x = density(len(q), cplx, 4)
+    y0 = density(len(q), cplx, 5)
+    alpha, beta = (0.5 + 0.5j, -1.0 + 0.25j) if cplx else (0.5, -1.0)
+    got = CF.mul(y0.copy(), x, alpha=alpha, beta=beta)
+    want = alpha * (D2 @ x + cS * (S2 @ x)) + beta * y0
+    assert relerr(got, want) < 1e-12
+
+
+def test_symmetric_gmres_matches_one_sided(ctx, one_sided):
+    """The solver's fused combined field and its FP32C twin on the symmetric
+    kernel give the same solution as on the one-sided one."""
+    q = inti.ellipsoid_quadrature(8, 5)
+    op = inti.Laplace(dim=3)
+    b = density(len(q), False, 6)
+    xs = []
+    for c in (ctx, one_sided):
+        S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=c)
+        for mode in ("fp64", "mixed"):
+            x, st = inti.gmres(0.5 * inti.I + D + S, b, rtol=1e-10, restart=50, maxiter=200, mode=mode)
+            assert st["converged"] == 1, st
+            xs.append(x)
+    for x in xs[1:]:
+        assert relerr(x, xs[0]) < 1e-8
