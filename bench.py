@@ -6,7 +6,9 @@ Workload (the single-GPU configuration the headline metric is quoted on):
 sphere meshed by 10,368 quadratic triangles with the 6-point VR rule
 (N = 62,208 nodes), plus its DIM correction (6 nonzeros per row) applied as a
 CSR SpMV fused into the pair kernel's epilogue.  Density: complex Gaussian,
-seed 1.  One step = one y = (A + δS) σ over all N² node pairs.
+seed 1.  One step = one y = (A + δS) σ over all N² node pairs (the symmetric
+kernel of square operators evaluates each unordered pair once for both
+products; the metric counts the N² ordered pairs of the product).
 
 value   kernel-pairs/s (G) with σ and y resident in HBM; L2 flushed between
         steps (a 256 MiB write, untimed), each step timed with CUDA events on
@@ -52,8 +54,9 @@ UNIT = "Gpairs/s"
 # Algorithmic flops per pair (FMA = 2 flops; special functions counted apart)
 FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pair-kernel
-# launch on the default workload, from an ncu capture of that launch
-PAIR_TRAFFIC_BYTES = 4.51e6
+# launch on the default workload, from an ncu capture of that launch (the
+# symmetric kernel: source records read, column partials written)
+PAIR_TRAFFIC_BYTES = 66.43e6
 # Algorithmic flops per pair of the source-gradient (adjoint) pass
 ADJ_FLOPS_PER_PAIR = {"laplace_dl": 40, "laplace_sl": 19}
 
@@ -773,11 +776,23 @@ def main() -> None:
     fp32 = cfg["precision"] == "fp32c"
     achieved = float(m_loc) * n * FLOPS_PER_PAIR[fkey] / (kern_ms * 1e-3) / 1e12
     peak = peaks["fp32_flops" if fp32 else "fp64_flops"] / 1e12
+    shape = A.tuning
+    sym = bool(shape.get("symmetric"))
+    if sym:  # diagonal node blocks evaluate every ordered pair, the others each unordered pair once
+        bt = 128 * shape["targets_per_thread"]
+        nb = -(-n // bt)
+        evals = float(nb * (nb + 1) // 2) * bt * bt
+    else:
+        evals = float(m_loc) * n
     roofline = {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak,
                 "traffic": PAIR_TRAFFIC_BYTES if args.workload == "c2" else None,
-                "kernel": f"pair_forward ({fkey}, {'float' if fp32 else 'double'})", "kernel_ms": kern_ms,
+                "kernel": f"{'pair_symm' if sym else 'pair_forward'} ({fkey}, {'float' if fp32 else 'double'})",
+                "kernel_ms": kern_ms,
                 "flops_per_pair": FLOPS_PER_PAIR[fkey],
+                "form": ("symmetric: one kernel evaluation per unordered pair serves both products; achieved "
+                         "counts the metric's M*N ordered pairs" if sym else "one-sided"),
+                "kernel_evaluations_per_step": evals,
                 "peak_source": f"{'FP32' if fp32 else 'FP64'} FMA throughput measured in this run "
                                "(inti_measure_peaks), of measured",
                 "share_of_step": pair_ms / max(sum(step_ms), 1e-9),
