@@ -609,6 +609,24 @@ __device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* 
   }
 }
 
+// Warp sums of four values v[0..3] (one per source), reduce-scattered: lanes
+// 0, 8, 16, 24 return the totals of v[0], v[1], v[2], v[3].  Levels 16 and 8
+// exchange halves of the set instead of reducing every value over all five
+// levels: 6 adds and 6 shuffles for four sums instead of 20 each.
+template <class R>
+__device__ __forceinline__ R warp_sum4(const R (&v)[4], int lane) {
+  const bool b4 = lane & 16, b3 = lane & 8;
+  R k0 = b4 ? v[2] : v[0], k1 = b4 ? v[3] : v[1];
+  k0 += __shfl_xor_sync(0xffffffffu, b4 ? v[0] : v[2], 16);
+  k1 += __shfl_xor_sync(0xffffffffu, b4 ? v[1] : v[3], 16);
+  R k = b3 ? k1 : k0;
+  k += __shfl_xor_sync(0xffffffffu, b3 ? k0 : k1, 8);
+  k += __shfl_xor_sync(0xffffffffu, k, 4);
+  k += __shfl_xor_sync(0xffffffffu, k, 2);
+  k += __shfl_xor_sync(0xffffffffu, k, 1);
+  return k;
+}
+
 __device__ __forceinline__ void put_partial(double* p, double r, double) { *p = r; }
 __device__ __forceinline__ void put_partial(double2* p, double r, double i) { *p = make_double2(r, i); }
 __device__ __forceinline__ void put_partial(float2* p, float r, float) { *p = make_float2(r, 0.f); }
@@ -699,21 +717,23 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
     } else {
 #pragma unroll 1
       for (int g = 0; g < TILE; g += kGroup) {
-#pragma unroll 2
-        for (int s = 0; s < kGroup; ++s) {
-          const R* rec = sp + (g + s) * RC::n;
-          R zr = R(0), zi = R(0);
+#pragma unroll 1
+        for (int s = 0; s < kGroup; s += 4) {
+          R zr[4], zi[4];
 #pragma unroll
-          for (int u = 0; u < TPT; ++u)
-            pair_sym_step<PDE, KIND, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(), zr, zi);
+          for (int v = 0; v < 4; ++v) {
+            const R* rec = sp + (g + s + v) * RC::n;
+            zr[v] = zi[v] = R(0);
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            zr += __shfl_xor_sync(0xffffffffu, zr, o);
-            if (CPLX) zi += __shfl_xor_sync(0xffffffffu, zi, o);
+            for (int u = 0; u < TPT; ++u)
+              pair_sym_step<PDE, KIND, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(), zr[v], zi[v]);
           }
-          if (lane == 0) {
-            zb[(warp * TILE + g + s) * 2] = zr;
-            zb[(warp * TILE + g + s) * 2 + 1] = zi;
+          const R sr = warp_sum4(zr, lane);
+          const R si = CPLX ? warp_sum4(zi, lane) : R(0);
+          if ((lane & 7) == 0) {
+            const int v = lane >> 3;
+            zb[(warp * TILE + g + s + v) * 2] = sr;
+            zb[(warp * TILE + g + s + v) * 2 + 1] = si;
           }
         }
 #pragma unroll
