@@ -206,9 +206,10 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
   return t.release();
 }
 
-// Column partials of the symmetric form are nb x n values; above this size
-// (N of a few hundred thousand) the operator keeps the one-sided kernel.
-constexpr double kSymmMaxPartialBytes = 2.0e9;
+// Column partials of the symmetric form are nb x n values (N^2/256 at 2
+// targets per thread); above this size (N of about 5e5 real, 3.5e5 complex)
+// the operator keeps the one-sided kernel.
+constexpr double kSymmMaxPartialBytes = 8.0e9;
 
 void op_symm_configure(inti_op* op, int tpt, int ch) {
   std::vector<int32_t> tab;
