@@ -56,7 +56,7 @@ FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "lap
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pair-kernel
 # launch on the default workload, from an ncu capture of that launch (the
 # symmetric kernel: source records read, column partials written)
-PAIR_TRAFFIC_BYTES = 66.43e6
+PAIR_TRAFFIC_BYTES = 67.32e6
 # Algorithmic flops per pair of the source-gradient (adjoint) pass
 ADJ_FLOPS_PER_PAIR = {"laplace_dl": 40, "laplace_sl": 19}
 
