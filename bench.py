@@ -639,9 +639,11 @@ def main() -> None:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-gmres", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--shard", default="rows", choices=["rows", "replicas"],
-                    help="N > 1: split the target rows of one operator over the ranks (strong scaling, y "
-                         "all-gathered every step) or run independent replicas (weak scaling)")
+    ap.add_argument("--shard", default="items", choices=["items", "rows", "replicas"],
+                    help="N > 1: split the symmetric work items of one square operator over the ranks (strong "
+                         "scaling, partial y all-reduced every step; operators without the symmetric form fall "
+                         "back to rows), split its target rows (y all-gathered every step), or run independent "
+                         "replicas (weak scaling)")
     ap.add_argument("--workload", default="c2",
                     choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr",
                              "dim_c2", "dim_c3"])
@@ -690,8 +692,15 @@ def main() -> None:
     comps = 2 if S.is_complex else 1
     xs = torch.from_numpy(np.ascontiguousarray(sigma).view(np.float64).copy()).to(dev)
     shard = args.shard if world > 1 else "none"
+    if shard == "items" and not S.tuning["symmetric"]:
+        shard = "rows"
     A, m_loc, yfull = S, n, None
-    if shard == "rows":
+    if shard == "items":
+        # every rank holds the whole operator and computes its share of the
+        # node pairs as a partial y over all rows; one all-reduce sums them
+        S.set_shard(rank, world)
+        ys = torch.zeros(comps * n, dtype=torch.float64, device=dev)
+    elif shard == "rows":
         # rank r computes target rows [r0, r1) of the one operator (all sources
         # on every rank, correction rows sliced); y is all-gathered each step
         from inti_b200 import shard as SH
@@ -715,6 +724,8 @@ def main() -> None:
         A.apply_device(xs.data_ptr(), ys.data_ptr())
         if yfull is not None:
             dist.all_gather_into_tensor(yfull, ys)
+        if shard == "items":
+            dist.all_reduce(ys)
 
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
@@ -749,20 +760,36 @@ def main() -> None:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    job_pairs = pairs if shard == "rows" else world * pairs  # whole-job pairs per step
+    job_pairs = pairs if shard in ("rows", "items") else world * pairs  # whole-job pairs per step
     value = job_pairs / (ms * 1e-3) / 1e9
 
-    # e2e through the public API with pinned host buffers (sharded: each rank
-    # uploads sigma and reads back its own row block)
+    # e2e through the public API with pinned host buffers (row shards: each
+    # rank uploads sigma and reads back its own row block; item shards: each
+    # rank uploads sigma, the partial products are all-reduced on the device
+    # and every rank reads back y)
     hx = torch.from_numpy(sigma.copy()).pin_memory().numpy()
     hy = torch.zeros(m_loc, dtype=torch.complex128 if S.is_complex else torch.float64).pin_memory().numpy()
+    if shard == "items":
+        hx_t = torch.from_numpy(np.ascontiguousarray(sigma).view(np.float64).copy()).pin_memory()
+        hy_t = torch.zeros(comps * n, dtype=torch.float64).pin_memory()
+
+        def e2e_step():
+            with torch.cuda.stream(stream):
+                xs.copy_(hx_t, non_blocking=True)
+                A.apply_device(xs.data_ptr(), ys.data_ptr())
+                dist.all_reduce(ys)
+                hy_t.copy_(ys, non_blocking=True)
+            stream.synchronize()
+    else:
+        def e2e_step():
+            A.mul(hy, hx)
     for _ in range(2):
-        A.mul(hy, hx)
+        e2e_step()
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        A.mul(hy, hx)
+        e2e_step()
     e2e_s = (time.perf_counter() - t0) / args.steps
     if dist:
         t = torch.tensor([e2e_s], device=dev)
@@ -802,12 +829,15 @@ def main() -> None:
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "strong" if args.shard == "rows" else "weak",
+        "scaling": "weak" if args.shard == "replicas" else "strong",
         "vs_baseline": None, "dtype": dtype, "data": "synthetic",
-        "config": dict(cfg, parallelism=(f"rows{world}" if args.shard == "rows" else f"replicas{world}"),
+        "config": dict(cfg, parallelism=(f"replicas{world}" if args.shard == "replicas" else
+                                         f"{'rows' if shard in ('rows', 'none') else shard}{world}"),
                        l2="flushed between steps",
                        **({"exchange": "NCCL all_gather of y every step (inside the timed region)"}
-                          if shard == "rows" else {})),
+                          if shard == "rows" else {}),
+                       **({"exchange": "NCCL all_reduce of the partial y every step (inside the timed region)"}
+                          if shard == "items" else {})),
         "e2e": e2e, "gpu_launches": launches, "roofline": roofline, "clocks": clk,
         "peaks_measured": {k: v / 1e12 for k, v in peaks.items()},
     }

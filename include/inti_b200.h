@@ -204,6 +204,17 @@ int inti_ctx_set_autotune(inti_ctx* ctx, int enable);  /* default on */
  * reference, which evaluates every ordered pair (src/nystrom.jl:117-124). */
 int inti_ctx_set_symmetric(inti_ctx* ctx, int enable);  /* default on */
 int inti_op_symmetric(const inti_op* op);
+/* Item shard of a symmetric operator for one process per GPU: after
+ * inti_op_set_shard(op, r, P), inti_op_apply on rank r computes this rank's
+ * share of the unordered node pairs (every P-th work item, largest first,
+ * so the shares balance) as a partial y over all rows; rank 0 adds the
+ * correction and beta*y.  The sum of the P partials (one all-reduce) is
+ * alpha*(A + C)x + beta*y.  nranks = 1 restores the whole operator.
+ * Multi-column applies of a shard run column by column; transposes and
+ * GMRES refuse shards.  Operators without the symmetric form return
+ * INTI_E_UNSUPPORTED (shard them by target rows: an operator on a row block
+ * of targets).  No counterpart in the reference (single process). */
+int inti_op_set_shard(inti_op* op, int rank, int nranks);
 
 /* ---- BDIM correction on the GPU (src/bdim.jl:50-196) ------------------- */
 /* green_multiplier: n values or NULL for -1/2 (on the surface,

@@ -128,6 +128,11 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
     L.sym_rowptr = L.sym_items + 3 * op->sym_nitems;
     L.sym_rowitems = L.sym_rowptr + op->sym_nb + 1;
     L.zpart = op->zpart.p;
+    if (op->shard_n > 1) {
+      L.sym_launch_items = op->shard_items;
+      L.sym_launch = op->shard_tab.as<int32_t>();
+      L.sym_launch_ids = L.sym_launch + 3 * op->shard_items;
+    }
   }
   return L;
 }
@@ -136,6 +141,19 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
 void op_apply_device(inti_op* op, const double* x, double* y, const double* alpha,
                      const double* beta) {
   PairLaunch L = make_launch(op, x);
+  if (op->shard_n > 1) {
+    // this rank's items only: the partials of the others' items are zero, and
+    // the correction and beta*y belong to rank 0 (the ranks' y are summed)
+    const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
+    INTI_CUDA(cudaMemsetAsync(op->partial.p, 0, pb * op->sym_nitems * pair_symm_block(op->tpt), op->ctx->stream));
+    INTI_CUDA(cudaMemsetAsync(op->zpart.p, 0, pb * op->sym_nb * op->n_tiles * pair_tile(op->precision),
+                              op->ctx->stream));
+    pair_launch(op->ctx, L);
+    const double zero[2] = {0.0, 0.0};
+    const bool lead = op->shard_rank == 0;
+    pair_epilogue(op->ctx, L, lead ? op->corr : nullptr, x, y, alpha, lead ? beta : zero);
+    return;
+  }
   pair_launch(op->ctx, L);
   pair_epilogue(op->ctx, L, op->corr, x, y, alpha, beta);
 }
@@ -563,6 +581,12 @@ int inti_ctx_set_symmetric(inti_ctx* ctx, int enable) {
   return guarded(ctx, [&] { ctx->symmetric = enable != 0; });
 }
 
+int inti_op_set_shard(inti_op* op, int rank, int nranks) {
+  if (!op) return INTI_E_ARG;
+  inti_ctx* ctx = op->ctx;
+  return guarded(ctx, [&] { op_set_shard(op, rank, nranks); });
+}
+
 int inti_op_symmetric(const inti_op* op) {
   if (!op) return -INTI_E_ARG;
   return op->symm ? 1 : 0;
@@ -589,7 +613,8 @@ static int apply_common(inti_op* op, const double* x, int64_t ldx, double* y, in
     const int64_t nout = transpose ? op->source->n : op->target->n;
     require(ldx >= nin && ldy >= nout, INTI_E_SHAPE, "leading dimension smaller than the vector length");
     const bool bz = !beta || (beta[0] == 0.0 && beta[1] == 0.0);
-    if (!transpose && nrhs >= kMrhsMinColumns && op_mrhs_supported(op)) {
+    require(!(transpose && op->shard_n > 1), INTI_E_UNSUPPORTED, "transpose of an item-sharded operator");
+    if (!transpose && nrhs >= kMrhsMinColumns && op_mrhs_supported(op) && op->shard_n == 1) {
       // all columns at once: each kernel value evaluated once per 64 columns
       const double* xd = x;
       double* yd = y;

@@ -175,6 +175,10 @@ struct PairLaunch {
   const int32_t* sym_rowptr = nullptr;    // nb + 1
   const int32_t* sym_rowitems = nullptr;  // nitems
   void* zpart = nullptr;                  // nb x (n_tiles * tile)
+  // a shard of the items (inti_op_set_shard): launch these, with their ids
+  int sym_launch_items = 0;
+  const int32_t* sym_launch = nullptr;    // 3 x sym_launch_items
+  const int32_t* sym_launch_ids = nullptr;
 };
 
 // Message for inti_last_error(NULL) from entry points that take no context.

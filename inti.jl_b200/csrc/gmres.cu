@@ -337,6 +337,7 @@ void gmres_solve(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const doubl
     if (!op) throw Error(INTI_E_ARG, "operator is NULL");
     if (op->ctx != ctx) throw Error(INTI_E_STATE, "operator belongs to another context");
     if (op->precision != INTI_FP64) throw Error(INTI_E_ARG, "GMRES takes FP64 operators (MIXED builds its FP32C twins)");
+    if (op->shard_n > 1) throw Error(INTI_E_STATE, "GMRES takes whole operators, not item shards");
     if (op->target->n != op->source->n) throw Error(INTI_E_SHAPE, "operators must be square");
     if (!q) q = op->source;
     if (op->source->n != q->n) throw Error(INTI_E_SHAPE, "operators differ in size");

@@ -41,6 +41,10 @@ struct inti_op {
   bool symm = false;
   int sym_nb = 0, sym_nitems = 0;
   inti::DevBuf sym_tab, zpart;
+  // item shard of this operator (inti_op_set_shard): rank, ranks, and the
+  // rank's items (3 x n) followed by their ids
+  int shard_rank = 0, shard_n = 1, shard_items = 0;
+  inti::DevBuf shard_tab;
   int64_t n_tiles = 1, tn_tiles = 1;
   // Derived operators kept for repeated solves: the FP32C twin used by the
   // mixed-precision GMRES, and (on a double layer) the combined-field operator
@@ -78,6 +82,9 @@ void op_autotune(inti_op* op, bool measure);
 // the symmetric form when the context allows it and its column partials fit.
 void op_symm_init(inti_op* op);
 void op_symm_configure(inti_op* op, int tpt, int ch);
+// Restrict the symmetric form to the work items of rank `rank` of `nranks`
+// (round robin over the items, largest first); nranks = 1 lifts it.
+void op_set_shard(inti_op* op, int rank, int nranks);
 std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
                                             const inti_csr* b, const double* cb, int64_t m, int64_t n,
                                             bool cplx);

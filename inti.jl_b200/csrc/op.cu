@@ -226,6 +226,32 @@ void op_symm_configure(inti_op* op, int tpt, int ch) {
   const int64_t npad = op->n_tiles * pair_tile(op->precision);
   op->partial.ensure(pb * nitems * pair_symm_block(tpt));
   op->zpart.ensure(pb * nb * npad);
+  if (op->shard_n > 1) op_set_shard(op, op->shard_rank, op->shard_n);  // the items changed
+}
+
+void op_set_shard(inti_op* op, int rank, int nranks) {
+  if (nranks < 1 || rank < 0 || rank >= nranks) throw Error(INTI_E_ARG, "shard rank must be in [0, nranks)");
+  if (nranks > 1 && !op->symm)
+    throw Error(INTI_E_UNSUPPORTED, "item shards need the symmetric form (a square 3D SL/DL/combined-field "
+                                    "operator); shard other operators by target rows");
+  op->shard_rank = rank;
+  op->shard_n = nranks;
+  op->shard_items = 0;
+  if (nranks == 1) return;
+  std::vector<int32_t> tab;
+  int nb = 0, nitems = 0;
+  pair_symm_plan(op->source->n, op->tpt, op->split, tab, nb, nitems);
+  std::vector<int32_t> items, ids;
+  for (int q = rank; q < nitems; q += nranks) {
+    for (int c = 0; c < 3; ++c) items.push_back(tab[3 * q + c]);
+    ids.push_back(q);
+  }
+  op->shard_items = (int)ids.size();
+  items.insert(items.end(), ids.begin(), ids.end());
+  INTI_CUDA(cudaStreamSynchronize(op->ctx->stream));
+  op->shard_tab.ensure(sizeof(int32_t) * std::max<size_t>(items.size(), 1));
+  if (!items.empty())
+    INTI_CUDA(cudaMemcpy(op->shard_tab.p, items.data(), sizeof(int32_t) * items.size(), cudaMemcpyHostToDevice));
 }
 
 void op_symm_init(inti_op* op) {

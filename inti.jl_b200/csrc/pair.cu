@@ -540,6 +540,7 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
 struct SymArgs {
   int64_t npad;           // packed records: nb * BT (zero charges past n)
   const int32_t* items;   // (I, J0, J1) per CTA
+  const int32_t* ids;     // row-partial slot of each CTA's item (NULL: the CTA index)
   const void* packed;
   void* ypart;            // [item][BT]
   void* zpart;            // [nb][npad]
@@ -760,7 +761,7 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
       ++issued;
     }
   }
-  P* out = static_cast<P*>(a.ypart) + (int64_t)blockIdx.x * BT;
+  P* out = static_cast<P*>(a.ypart) + (int64_t)(a.ids ? a.ids[blockIdx.x] : (int)blockIdx.x) * BT;
 #pragma unroll
   for (int u = 0; u < TPT; ++u) store_partial(out + u * kBlock + tid, acc[u]);
 }
@@ -1077,7 +1078,8 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
         if (L.symm) {
           SymArgs a;
           a.npad = npad;
-          a.items = L.sym_items;
+          a.items = L.sym_launch ? L.sym_launch : L.sym_items;
+          a.ids = L.sym_launch ? L.sym_launch_ids : nullptr;
           a.packed = L.packed;
           a.ypart = L.partial;
           a.zpart = L.zpart;
@@ -1090,7 +1092,8 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
           auto fn = L.tpt == 2 ? &pair_symm<T::pde, T::kind, R, TILE, 2> : &pair_symm<T::pde, T::kind, R, TILE, 4>;
           INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
           ProfScope pp(ctx, "pair");
-          fn<<<(unsigned)L.sym_nitems, kBlock, sm, ctx->stream>>>(a);
+          const int grid = L.sym_launch ? L.sym_launch_items : L.sym_nitems;
+          if (grid > 0) fn<<<(unsigned)grid, kBlock, sm, ctx->stream>>>(a);
           launches = 2;
           return;
         }

@@ -535,6 +535,14 @@ class GpuOperator(_Map):
         return {"targets_per_thread": t.value, "split": s.value,
                 "symmetric": bool(self.ctx.lib.inti_op_symmetric(self.handle) == 1)}
 
+    def set_shard(self, rank: int, nranks: int) -> None:
+        """Compute only rank ``rank``'s share of the node pairs (symmetric
+        operators): each apply returns a partial product over all rows, and
+        the ranks' partials sum to the whole (one all-reduce).  Rank 0
+        carries the correction and ``beta*y``.  ``nranks=1`` restores the
+        whole operator."""
+        self.ctx.check(self.ctx.lib.inti_op_set_shard(self.handle, int(rank), int(nranks)))
+
     def grad_sources_device(self, g_ptr: int, sigma_ptr: int, dsigma_ptr: int, dcoords_ptr: int,
                             dnormals_ptr: int, dweights_ptr: int) -> None:
         """Stream-ordered ``grad_sources`` on device pointers (no copies, no

@@ -86,3 +86,44 @@ def test_row_sharded_product_matches_single_process():
         p.join(timeout=120)
         assert p.exitcode == 0
     assert np.array_equal(got, full)
+
+
+def _rank_items(rank, world, port, out):
+    """The item-shard exchange: each rank holds a share of the pair terms of
+    the product over all rows (here: the source columns j with j % world ==
+    rank, a stand-in for its work items), rank 0 adds the correction, and one
+    all-reduce sums the partials (NCCL all_reduce on the GPUs)."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        q, (indptr, indices, data), sigma = _problem()
+        part = np.where(np.arange(len(q)) % world == rank, sigma, 0.0)
+        y = O.apply(O.LAPLACE, O.DL, 0.0, q.coords, q.normals, q.coords, q.normals, q.weights, part)
+        if rank == 0:
+            y = y + O.csr_apply(indptr, indices, data, sigma)
+        t = torch.from_numpy(y)
+        dist.all_reduce(t)
+        if rank == 0:
+            out.put(t.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+def test_item_sharded_product_matches_single_process():
+    q, (indptr, indices, data), sigma = _problem()
+    full = O.apply(O.LAPLACE, O.DL, 0.0, q.coords, q.normals, q.coords, q.normals, q.weights, sigma) + \
+        O.csr_apply(indptr, indices, data, sigma)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    out = ctx.Queue()
+    world = 2
+    procs = [ctx.Process(target=_rank_items, args=(r, world, port, out)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = out.get(timeout=120)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert np.max(np.abs(got - full)) <= 1e-13 * np.max(np.abs(full))
