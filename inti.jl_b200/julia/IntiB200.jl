@@ -199,6 +199,44 @@ LinearMaps._unsafe_mul!(y::AbstractVector, A::B200Map, x::AbstractVector) = appl
 LinearMaps._unsafe_mul!(y::AbstractVector, A::B200Map, x::AbstractVector, α::Number, β::Number) =
     apply!(y, A, x, α, β)
 
+# Many columns in one call: from 8 columns on, FP64 3D SL/DL/combined-field
+# operators evaluate each kernel value once for up to 64 columns.
+function apply!(Y::AbstractMatrix, A::B200Map{T}, X::AbstractMatrix, α = true, β = false) where {T}
+    XX = Matrix{T}(X)
+    YY = Y isa Matrix{T} ? Y : Matrix{T}(Y)
+    a = Float64[real(α), imag(complex(α))]
+    b = Float64[real(β), imag(complex(β))]
+    GC.@preserve XX YY a b check(ccall((:inti_op_apply, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Cvoid}, Int64, Int32, Ptr{Float64}, Ptr{Float64}, Cint),
+        A.h.ptr, XX, size(XX, 1), YY, size(YY, 1), size(XX, 2), a, b, 0), A.ctx.ptr)
+    YY === Y || copyto!(Y, YY)
+    return Y
+end
+LinearMaps._unsafe_mul!(Y::AbstractMatrix, A::B200Map, X::AbstractMatrix) = apply!(Y, A, X)
+LinearMaps._unsafe_mul!(Y::AbstractMatrix, A::B200Map, X::AbstractMatrix, α::Number, β::Number) =
+    apply!(Y, A, X, α, β)
+
+"""
+    set_symmetric!(ctx, flag)
+
+Square operators created afterwards use (`true`, the default) or skip the
+symmetric pair kernel, which evaluates each unordered node pair once for both
+products.
+"""
+set_symmetric!(ctx::Context, flag::Bool) =
+    check(ccall((:inti_ctx_set_symmetric, LIB), Cint, (Ptr{Cvoid}, Cint), ctx.ptr, flag), ctx.ptr)
+
+"""
+    set_shard!(A::B200Map, rank, nranks)
+
+One process per GPU: `A` computes only rank `rank`'s share of the node pairs
+(a symmetric operator), so `mul!` returns a partial product and the sum over
+the ranks (one `MPI.Allreduce!`) is the whole; rank 0 carries the correction
+and `β*y`. `nranks = 1` restores the whole operator.
+"""
+set_shard!(A::B200Map, rank::Integer, nranks::Integer) =
+    check(ccall((:inti_op_set_shard, LIB), Cint, (Ptr{Cvoid}, Cint, Cint), A.h.ptr, rank, nranks), A.ctx.ptr)
+
 as_linearmap(h::OpHandle, ::Type{T}, m, n, ctx) where {T} = B200Map{T}(h, m, n, ctx)
 
 """
@@ -210,7 +248,8 @@ The GPU counterpart of `assemble_matrix`/`assemble_fmm` (src/nystrom.jl:
 function assemble_b200(iop::Inti.IntegralOperator; precision = :fp64, correction = nothing,
                        ctx = default_context())
     tgt = upload(Inti.target(iop); ctx)
-    src = upload(Inti.source(iop); ctx)
+    # one handle for target === source: the library then uses its symmetric pair kernel
+    src = Inti.source(iop) === Inti.target(iop) ? tgt : upload(Inti.source(iop); ctx)
     corr = correction === nothing ? nothing : upload(correction; ctx)
     h = op_handle(Inti.kernel(iop), tgt, src, corr, precision)
     return as_linearmap(h, eltype(iop), size(iop)..., ctx)

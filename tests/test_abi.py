@@ -57,3 +57,15 @@ def test_context_creation_reports_missing_device():
     assert lib.inti_last_error(None)
     with pytest.raises(inti_b200.InticError):
         inti_b200.Context(0)
+
+
+def test_julia_binding_calls_only_declared_exports():
+    """Every ccall of inti.jl_b200/julia/IntiB200.jl names a function the
+    header declares and the library exports (Julia itself is absent here)."""
+    text = (ROOT / "inti.jl_b200" / "julia" / "IntiB200.jl").read_text()
+    called = sorted(set(re.findall(r"ccall\(\(:(inti_[a-z0-9_]+)", text)))
+    assert len(called) >= 10
+    lib = L.load()
+    declared = set(header_functions())
+    for name in called:
+        assert name in declared and hasattr(lib, name), name
