@@ -81,3 +81,30 @@ def test_symmetric_gmres_matches_one_sided(ctx, one_sided):
             xs.append(x)
     for x in xs[1:]:
         assert relerr(x, xs[0]) < 1e-8
+
+
+@pytest.mark.parametrize("n", [1, 7, 511, 512, 513, 1025])
+@pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
+def test_symmetric_edge_sizes(ctx, n, pde):
+    """Node counts around the block size (512 or 256 nodes): a single node,
+    a partial block, exact blocks and one node past them; points with
+    arbitrary normals and weights (no element structure needed)."""
+    r = np.random.default_rng(n)
+    X = r.standard_normal((n, 3))
+    N = r.standard_normal((n, 3))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    W = r.uniform(0.5, 1.5, n)
+    q = inti.Quadrature(X, N, W, 0)
+    cplx = pde == O.HELMHOLTZ
+    k = 0.0 if pde == O.LAPLACE else 3.0
+    x = density(n, cplx, 2)
+    op = inti.Laplace(dim=3) if pde == O.LAPLACE else inti.Helmholtz(k=3.0, dim=3)
+    for K, okind in ((inti.SingleLayerKernel, O.SL), (inti.DoubleLayerKernel, O.DL)):
+        A = inti.GpuOperator(K(op), q, q, None, "fp64", ctx)
+        assert A.tuning["symmetric"]
+        ref = oracle_apply(pde, okind, k, q, q, x)
+        got = A @ x
+        if n == 1:
+            assert np.all(got == 0)  # the self pair is excluded
+        else:
+            assert relerr(got, ref) < 1e-12
