@@ -225,8 +225,12 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def gmres_c3(ctx) -> dict:
-    """Combined-field Laplace solve on the ellipsoid (N = 200,934)."""
+def gmres_c3(ctx, cpu_seconds: float | None = None) -> dict:
+    """Combined-field Laplace solve on the ellipsoid (N = 200,934).  With
+    cpu_seconds, also the CPU estimate of the same FP64 solve: the oracle's
+    D and S row sums (the reference's on-the-fly matvec) timed on a sample
+    of rows on all host cores, extrapolated to a full product and multiplied
+    by the GPU solve's count of operator applications."""
     import inti_b200 as inti
 
     q = inti.ellipsoid_quadrature(61, 5)
@@ -250,6 +254,28 @@ def gmres_c3(ctx) -> dict:
                      "relres_fp64": st["relres"], "converged": bool(st["converged"])}
     if out["fp64"]["converged"] and out["mixed"]["converged"]:
         out["mixed_speedup_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    if cpu_seconds:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        nt, n = host_cores(), len(q)
+        rows = max(8 * nt, 32)
+        per_row = 0.0
+        for kind in (O.DL, O.SL):
+            args = (O.LAPLACE, kind, 0.0, q.coords, q.normals, q.coords, q.normals, q.weights, b)
+            t0 = time.perf_counter()
+            O.apply_rows_block(*args, 0, rows, nthreads=nt)
+            dt = time.perf_counter() - t0
+            r2 = int(min(n, max(rows, rows * cpu_seconds / 2 / max(dt, 1e-6))))
+            t0 = time.perf_counter()
+            O.apply_rows_block(*args, 0, r2, nthreads=nt)
+            per_row += (time.perf_counter() - t0) / r2
+        matvec = per_row * n
+        out["cpu_fp64_estimate"] = {
+            "seconds": matvec * out["fp64"]["fp64_applies"], "matvec_s": matvec, "cores": nt,
+            "kind": "port, extrapolated",
+            "sample": "D and S row sums of the C++ FP64 restatement on a sample of rows, scaled to a full "
+                      "product and multiplied by the FP64 solve's operator applications"}
     return out
 
 
@@ -844,7 +870,7 @@ def main() -> None:
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(q, S, sigma, args.cpu_seconds, host_cores())
     if not args.no_gmres and world == 1 and args.workload == "c2":
-        line["gmres"] = gmres_c3(ctx)
+        line["gmres"] = gmres_c3(ctx, None if args.no_cpu else min(args.cpu_seconds, 10.0))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
