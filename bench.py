@@ -23,7 +23,7 @@ gmres   (extra key) time to ||b - Lx|| <= 1e-10 ||b|| for the 3D Laplace
         combined field ½I + D + S on the (1, 0.7, 0.5) ellipsoid, N = 200,934,
         plain FP64 GMRES versus FP32-inner / FP64-outer refinement.
 
-Other workloads (--workload): c2_dl, c3_dl_fp64, c3_dl_fp32c, c3_sl_fp64, c1
+Other workloads (--workload): c2_dl, c2_adl, c2_hs, c3_dl_fp64, c3_dl_fp32c, c3_sl_fp64, c1
 (single operators); c4 (batched surfaces x 64 right-hand sides, TF32 tensor
 cores and FP64 MMA, --nsurf surfaces); c5 (adjoint); csr (correction SpMV
 bandwidth); dim_c2, dim_c3 (GPU construction of the DIM correction).
@@ -52,7 +52,10 @@ import numpy as np  # noqa: E402
 METRIC = "G kernel-pairs/s"
 UNIT = "Gpairs/s"
 # Algorithmic flops per pair (FMA = 2 flops; special functions counted apart)
-FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10}
+FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "laplace_dl": 18, "laplace2d_dl": 10,
+                  # the same count for the adjoint double layer (r.n_x in place of r.n_y) and the
+                  # hypersingular kernel: + n_x.n_y, the 1/d^5 term and its complex factor
+                  "helmholtz_adl": 34, "helmholtz_hs": 60}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pair-kernel
 # launch on the default workload, from an ncu capture of that launch (the
 # symmetric kernel: source records read, column partials written)
@@ -132,6 +135,13 @@ def build_workload(name: str, ctx):
         op = inti.Helmholtz(k=10.0, dim=3)
         kern, key, prec, dt = inti.DoubleLayerKernel(op), "helmholtz_dl", "fp64", "c128"
         wl = "helmholtz3d_dl_k10_p2sphere_N62208_dim"
+    elif name in ("c2_adl", "c2_hs"):
+        q = inti.p2_sphere_quadrature(36)
+        op = inti.Helmholtz(k=10.0, dim=3)
+        hs = name == "c2_hs"
+        kern = inti.HyperSingularKernel(op) if hs else inti.AdjointDoubleLayerKernel(op)
+        key, prec, dt = ("helmholtz_hs" if hs else "helmholtz_adl"), "fp64", "c128"
+        wl = f"helmholtz3d_{'hs' if hs else 'adl'}_k10_p2sphere_N62208_dim"
     elif name in ("c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64"):
         q = inti.ellipsoid_quadrature(61, 5)
         op = inti.Laplace(dim=3)
@@ -147,10 +157,11 @@ def build_workload(name: str, ctx):
         wl = "laplace2d_dl_kite_N1000_dim"
     else:
         raise SystemExit(f"unknown workload {name}")
+    deriv = isinstance(kern, (inti.AdjointDoubleLayerKernel, inti.HyperSingularKernel))
     t0 = time.perf_counter()
-    dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
+    dS, dD = inti.bdim_correction(op, q, q, derivative=deriv, ctx=ctx)  # derivative: (ADL, HS) corrections
     t_dim = time.perf_counter() - t0
-    corr = dS if isinstance(kern, inti.SingleLayerKernel) else dD
+    corr = dS if isinstance(kern, (inti.SingleLayerKernel, inti.AdjointDoubleLayerKernel)) else dD
     A = inti.GpuOperator(kern, q, q, corr, prec, ctx)
     n = len(q)
     if A.is_complex:
@@ -671,7 +682,7 @@ def main() -> None:
                          "back to rows), split its target rows (y all-gathered every step), or run independent "
                          "replicas (weak scaling)")
     ap.add_argument("--workload", default="c2",
-                    choices=["c2", "c2_dl", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr",
+                    choices=["c2", "c2_dl", "c2_adl", "c2_hs", "c3_dl_fp64", "c3_dl_fp32c", "c3_sl_fp64", "c1", "c4", "c5", "csr",
                              "dim_c2", "dim_c3"])
     ap.add_argument("--nsurf", type=int, default=32, help="c4: number of star surfaces (32 = the batched workload)")
     args = ap.parse_args()

@@ -160,9 +160,22 @@ void op_apply_device(inti_op* op, const double* x, double* y, const double* alph
 
 void op_apply_transpose_device(inti_op* op, const double* x, double* y, const double* alpha,
                                const double* beta) {
+  if (op->symm) {
+    // square operator: the symmetric product of the transposed kernel with
+    // unit weights on the same node blocks, work items and partial buffers
+    PairLaunch L = make_launch(op, x);
+    L.kind = transposed_kind(op->kind);
+    L.sweights = op->tones.as<double>();
+    L.packed = op->tpacked.p;
+    {
+      ProfScope pt(op->ctx, "transpose");
+      pair_launch(op->ctx, L);
+    }
+    pair_epilogue(op->ctx, L, op->corrT.get(), x, y, alpha, beta, op->source->weights.as<double>());
+    return;
+  }
   // the forward pair product with targets and sources swapped (op_prepare_transpose)
   PairLaunch L = make_launch(op, x);
-  L.symm = false;  // the swapped product runs one-sided
   L.kind = transposed_kind(op->kind);
   L.m = op->source->n;
   L.n = op->target->n;

@@ -190,6 +190,7 @@ const float2* expi_table_f32(inti_ctx* ctx);
 int pair_tile(int precision);
 // Bytes of one packed source record.
 int pair_record_bytes(int pde, int kind, int dim, int precision);
+int pair_symm_record_bytes(int pde, int kind, int precision);  // packed record of the symmetric form
 // Bytes of one partial accumulator per target per split.
 int pair_partial_bytes(int pde, int precision);
 // Symmetric form: node block of 128*tpt nodes; work items of row blocks

@@ -232,8 +232,8 @@ void op_symm_configure(inti_op* op, int tpt, int ch) {
 void op_set_shard(inti_op* op, int rank, int nranks) {
   if (nranks < 1 || rank < 0 || rank >= nranks) throw Error(INTI_E_ARG, "shard rank must be in [0, nranks)");
   if (nranks > 1 && !op->symm)
-    throw Error(INTI_E_UNSUPPORTED, "item shards need the symmetric form (a square 3D SL/DL/combined-field "
-                                    "operator); shard other operators by target rows");
+    throw Error(INTI_E_UNSUPPORTED, "item shards need the symmetric form (a square 3D operator); "
+                                    "shard other operators by target rows");
   op->shard_rank = rank;
   op->shard_n = nranks;
   op->shard_items = 0;
@@ -257,9 +257,7 @@ void op_set_shard(inti_op* op, int rank, int nranks) {
 void op_symm_init(inti_op* op) {
   inti_ctx* ctx = op->ctx;
   op->symm = false;
-  if (!ctx->symmetric || op->target != op->source || op->dim != 3 ||
-      !(op->kind == SL || op->kind == DL || op->kind == CF))
-    return;
+  if (!ctx->symmetric || op->target != op->source || op->dim != 3) return;
   const int64_t n = op->source->n;
   const int tile = pair_tile(op->precision);
   const int64_t bmax = pair_symm_block(4), bmin = pair_symm_block(2);
@@ -268,7 +266,7 @@ void op_symm_init(inti_op* op) {
   if (zbytes > kSymmMaxPartialBytes) return;
   op->symm = true;
   op->n_tiles = npad / tile;
-  op->packed.ensure((size_t)npad * pair_record_bytes(op->pde, op->kind, op->dim, op->precision));
+  op->packed.ensure((size_t)npad * pair_symm_record_bytes(op->pde, op->kind, op->precision));
   const int tpt = 2;
   op_symm_configure(op, tpt, pair_symm_default_ch(ctx, op->pde, op->kind, op->precision, n, tpt));
 }
@@ -383,7 +381,8 @@ void op_autotune(inti_op* op, bool measure) {
   set(pick.first, pick.second);
 }
 
-// A^T as a forward product with the roles swapped: (A^T g)_j =
+// A^T as a forward product with the roles swapped (square operators with the
+// symmetric form: the symmetric product of the swapped kernel): (A^T g)_j =
 // w_j sum_i K(x_i, y_j) g_i, and K(x_i, y_j) = K'(y_j, x_i) with K' the
 // kernel of the swapped roles (the kernels of src/kernels.jl:137-204,
 // 347-413 satisfy SL(x,y) = SL(y,x), DL(x,y) = ADL(y,x), ADL(x,y) = DL(y,x),
@@ -412,6 +411,8 @@ void op_prepare_transpose(inti_op* op) {
     op->tsplit = pair_plan_split(ctx, op->pde, kt, op->dim, op->precision, m2, n2, 4);
   }
   op->tpacked.ensure((size_t)op->tn_tiles * tile * pair_record_bytes(op->pde, kt, op->dim, op->precision));
+  if (op->symm)  // the symmetric form packs all npad = n_tiles * tile nodes in its own records
+    op->tpacked.ensure((size_t)op->n_tiles * tile * pair_symm_record_bytes(op->pde, kt, op->precision));
   op->tpartial.ensure((size_t)op->tsplit * m2 * pair_partial_bytes(op->pde, op->precision));
   std::vector<double> ones((size_t)std::max<int64_t>(n2, 1), 1.0);
   op->tones.ensure(sizeof(double) * ones.size());

@@ -519,12 +519,14 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
 
 // ---------------------------------------------------------------------------
 // Symmetric form for square operators (the target set is the source set),
-// single layer, double layer and combined field in 3D.
+// every 3D kernel: single layer, double layer, combined field, adjoint double
+// layer and hypersingular.
 //
 // Every kernel value of an unordered pair {a, b} serves both products:
 //   SL: G(x_a, x_b) = G(x_b, x_a);
 //   DL: K(x_a, x_b) p_b = d(r.p_b) and K(x_b, x_a) p_a = -d(r.p_a) with the
 //       same radial factor d (r = x_a - x_b, p the packed dipoles w sigma n);
+//   ADL and HS: see pair_sym_step;
 // so the distance, the reciprocal square root and the phase are computed
 // once per unordered pair.  Nodes are cut into blocks of BT = 128*TPT; a CTA
 // takes one work item (row block I, source blocks J0 <= J < J1, J >= I):
@@ -549,10 +551,60 @@ struct SymArgs {
   int* err;
 };
 
+// Records of the symmetric form.  SL, DL and CF use the layouts of Rec.  The
+// adjoint double layer and the hypersingular kernel take the normal of the
+// target, so both ends of a pair need their normal and their charge:
+//   x y z n_x n_y n_z q [0]     (Laplace)
+//   x y z n_x n_y n_z qr qi     (Helmholtz)
+// with q = w sigma; eight elements, 64 bytes (FP64) or 32 bytes (FP32).
+template <int PDE, int KIND, class R>
+struct SymRec {
+  static constexpr bool normal = (KIND == ADL || KIND == HS);
+  static constexpr bool cplx = (PDE == HELMHOLTZ);
+  static constexpr int used = normal ? (cplx ? 8 : 7) : Rec<PDE, KIND, 3, R>::used;
+  static constexpr int n = normal ? 8 : Rec<PDE, KIND, 3, R>::n;
+};
+
+template <int PDE, class R>
+__global__ void pack_sym_normal(int64_t n, int64_t npad, const double* __restrict__ xs,
+                                const double* __restrict__ ns, const double* __restrict__ w,
+                                const double* __restrict__ sigma, R* __restrict__ out) {
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= npad) return;
+  R rec[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) rec[c] = R(0);
+  if (j < n) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      rec[c] = R(xs[3 * j + c]);
+      rec[3 + c] = R(ns[3 * j + c]);
+    }
+    const double wj = w[j];
+    if (PDE == HELMHOLTZ) {
+      rec[6] = R(wj * sigma[2 * j]);
+      rec[7] = R(wj * sigma[2 * j + 1]);
+    } else {
+      rec[6] = R(wj * sigma[j]);
+    }
+  }
+  R* o = out + j * 8;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) o[c] = rec[c];
+}
+
 // Both products of one unordered pair: y_t += K(x_t, x_s) c_s and
 // z_s += K(x_s, x_t) c_t, with c the packed charge/dipole records of the
-// target t and the source s (layouts of Rec), r = x_t - x_s.
-template <int PDE, int KIND, class R>
+// target t and the source s (layouts of SymRec), r = x_t - x_s.  With COL
+// false only the row product is formed (the diagonal blocks of the
+// adjoint double layer and hypersingular forms, which evaluate every ordered
+// pair).
+//   ADL: K(x_t, x_s) q_s = (r.n_t) f q_s and K(x_s, x_t) q_t = -(r.n_s) f q_t
+//        with the same radial factor f (1/d^3; e^{ikd}(1/d - ik)/d^2);
+//   HS : K(x_t, x_s) q_s = h q_s and K(x_s, x_t) q_t = h q_t with
+//        h = a (r.n_t)(r.n_s) + b (n_t.n_s), a and b functions of d alone
+//        (Laplace: a = -3/d^5, b = 1/d^3), so h is symmetric in the pair.
+template <int PDE, int KIND, class R, bool COL = true>
 __device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* __restrict__ s, R kT, R delta, R k,
                                               const typename MathOps<R>::R2* __restrict__ tab, R& ar, R& ai,
                                               R& zr, R& zi) {
@@ -560,6 +612,59 @@ __device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* 
   const R r0 = t[0] - s[0], r1 = t[1] - s[1], r2 = t[2] - s[2];
   const R d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
   const bool keep = M::keep(d2);
+  if (KIND == ADL || KIND == HS) {
+    const R rnt = fma(r2, t[5], fma(r1, t[4], r0 * t[3]));
+    const R rns = COL || KIND == HS ? fma(r2, s[5], fma(r1, s[4], r0 * s[3])) : R(0);
+    if (PDE == LAPLACE) {
+      if (KIND == ADL) {
+        const R ri3 = keep ? M::rsq3(d2) : R(0);
+        ar = fma(rnt * ri3, s[6], ar);
+        if (COL) zr = fma(-rns * ri3, t[6], zr);
+      } else {
+        const R nn = fma(t[5], s[5], fma(t[4], s[4], t[3] * s[3]));
+        const R ri = keep ? M::rsq(d2) : R(0);
+        const R id2 = ri * ri;
+        const R h = fma(R(-3) * rnt * rns, id2, nn) * (id2 * ri);
+        ar = fma(h, s[6], ar);
+        if (COL) zr = fma(h, t[6], zr);
+      }
+    } else {
+      const R ri = keep ? M::rsq(d2) : R(0);
+      const R d = d2 * ri;
+      R sn, cs;
+      expi_table_eval(d, kT, tab, delta, cs, sn);
+      const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);  // e^{ikd}(1/d - ik)
+      const R id2 = ri * ri;
+      R hr, hi, gr = R(0), gi = R(0);  // row factor h, column factor g
+      if (KIND == ADL) {
+        const R br = er * id2, bi = ei * id2;
+        hr = br * rnt;
+        hi = bi * rnt;
+        if (COL) {
+          gr = -br * rns;
+          gi = -bi * rns;
+        }
+      } else {
+        // b = e^{ikd}(1/d - ik)/d^2; a = e^{ikd}(k^2 d^2 - 3 + 3ikd)/d^5
+        const R nn = fma(t[5], s[5], fma(t[4], s[4], t[3] * s[3]));
+        const R fr = fma(k * d, k * d, R(-3)), fi = R(3) * k * d;
+        const R sa = id2 * id2 * ri;
+        const R a_r = sa * fma(cs, fr, -sn * fi), a_i = sa * fma(cs, fi, sn * fr);
+        const R u = rnt * rns;
+        hr = fma(a_r, u, er * id2 * nn);
+        hi = fma(a_i, u, ei * id2 * nn);
+        gr = hr;
+        gi = hi;
+      }
+      ar = fma(hr, s[6], fma(-hi, s[7], ar));
+      ai = fma(hr, s[7], fma(hi, s[6], ai));
+      if (COL) {
+        zr = fma(gr, t[6], fma(-gi, t[7], zr));
+        zi = fma(gr, t[7], fma(gi, t[6], zi));
+      }
+    }
+    return;
+  }
   if (PDE == LAPLACE) {
     if (KIND == SL) {
       const R ri = keep ? M::rsq(d2) : R(0);
@@ -635,7 +740,7 @@ __device__ __forceinline__ void put_partial(float4* p, float r, float i) { *p = 
 
 template <int PDE, int KIND, class R, int TILE, int TPT>
 __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
-  using RC = Rec<PDE, KIND, 3, R>;
+  using RC = SymRec<PDE, KIND, R>;
   constexpr bool CPLX = RC::cplx;
   using P = typename PartialT<R, CPLX>::T;
   using R2 = typename MathOps<R>::R2;
@@ -705,11 +810,17 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
           const R* rec = sp + (g + s) * RC::n;
 #pragma unroll
           for (int u = 0; u < TPT; ++u) {
-            Target<R, 3, false> tt;
-            tt.x[0] = tg[u][0];
-            tt.x[1] = tg[u][1];
-            tt.x[2] = tg[u][2];
-            pair_step<PDE, KIND, 3, R>(tt, rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
+            if constexpr (RC::normal) {
+              R unused_r, unused_i;
+              pair_sym_step<PDE, KIND, R, false>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(),
+                                                 unused_r, unused_i);
+            } else {
+              Target<R, 3, false> tt;
+              tt.x[0] = tg[u][0];
+              tt.x[1] = tg[u][1];
+              tt.x[2] = tg[u][2];
+              pair_step<PDE, KIND, 3, R>(tt, rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
+            }
           }
         }
 #pragma unroll
@@ -993,12 +1104,20 @@ int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precisi
 template <class T, class R>
 static size_t symm_smem() {
   constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
-  return fwd_smem<T, R>() + 2 * (size_t)(kBlock / 32) * TILE * 2 * sizeof(R);
+  const size_t table = T::pde == HELMHOLTZ ? (size_t)kExpiTable * 2 * sizeof(R) : 0;
+  return 2 * (size_t)TILE * SymRec<T::pde, T::kind, R>::n * sizeof(R) + table +
+         2 * (size_t)(kBlock / 32) * TILE * 2 * sizeof(R);
 }
 
 template <class T>
 constexpr bool symm_kind() {
-  return T::dim == 3 && (T::kind == SL || T::kind == DL || T::kind == CF);
+  return T::dim == 3;
+}
+
+int pair_symm_record_bytes(int pde, int kind, int precision) {
+  const bool normal = kind == ADL || kind == HS;
+  if (!normal) return pair_record_bytes(pde, kind, 3, precision);
+  return 8 * (precision == INTI_FP32C ? 4 : 8);
 }
 
 int pair_symm_block(int tpt) { return kBlock * tpt; }
@@ -1070,9 +1189,14 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       const int pb = 256;
       {
         ProfScope ps(ctx, "pack");
-        pack_sources<T::pde, T::kind, T::dim, R><<<(unsigned)((npad + pb - 1) / pb), pb, 0, ctx->stream>>>(
-            L.n, npad, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
-            make_double2(L.c2[0], L.c2[1]), static_cast<R*>(L.packed));
+        const unsigned gp = (unsigned)((npad + pb - 1) / pb);
+        if (L.symm && (T::kind == ADL || T::kind == HS))
+          pack_sym_normal<T::pde, R><<<gp, pb, 0, ctx->stream>>>(L.n, npad, L.scoords, L.snormals, L.sweights,
+                                                                 L.x, static_cast<R*>(L.packed));
+        else
+          pack_sources<T::pde, T::kind, T::dim, R><<<gp, pb, 0, ctx->stream>>>(
+              L.n, npad, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
+              make_double2(L.c2[0], L.c2[1]), static_cast<R*>(L.packed));
       }
       if constexpr (symm_kind<T>()) {
         if (L.symm) {

@@ -2,8 +2,9 @@
 unordered pair is evaluated once for both products.  Checked against the
 one-sided kernel (a context with the symmetric form off) and the oracle, on
 surfaces of many node blocks with a ragged last block, for the single layer,
-double layer and combined field, Laplace and Helmholtz, FP64 and FP32C, with
-the DIM correction, alpha/beta and repeated applies."""
+double layer, combined field, adjoint double layer and hypersingular kernel,
+Laplace and Helmholtz, FP64 and FP32C, with the DIM correction, alpha/beta
+and repeated applies."""
 import numpy as np
 import pytest
 
@@ -25,13 +26,16 @@ def _op(pde):
     return inti.Laplace(dim=3) if pde == O.LAPLACE else inti.Helmholtz(k=6.0, dim=3)
 
 
+KERNELS = {"SL": (inti.SingleLayerKernel, O.SL), "DL": (inti.DoubleLayerKernel, O.DL),
+           "ADL": (inti.AdjointDoubleLayerKernel, O.ADL), "HS": (inti.HyperSingularKernel, O.HS)}
+
+
 @pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
-@pytest.mark.parametrize("kname", ["SL", "DL"])
+@pytest.mark.parametrize("kname", ["SL", "DL", "ADL", "HS"])
 @pytest.mark.parametrize("prec,tol", [("fp64", 1e-12), ("fp32c", 5e-5)])
 def test_symmetric_matches_one_sided_and_oracle(ctx, one_sided, pde, kname, prec, tol):
     q = inti.ellipsoid_quadrature(9, 5)  # 4,374 nodes: 9 blocks of 512, the last ragged
-    K = inti.SingleLayerKernel if kname == "SL" else inti.DoubleLayerKernel
-    okind = O.SL if kname == "SL" else O.DL
+    K, okind = KERNELS[kname]
     k = 0.0 if pde == O.LAPLACE else 6.0
     A = inti.GpuOperator(K(_op(pde)), q, q, None, prec, ctx)
     B = inti.GpuOperator(K(_op(pde)), q, q, None, prec, one_sided)
@@ -64,6 +68,49 @@ def test_symmetric_combined_field_with_correction(ctx, one_sided, pde):
     got = CF.mul(y0.copy(), x, alpha=alpha, beta=beta)
     want = alpha * (D2 @ x + cS * (S2 @ x)) + beta * y0
     assert relerr(got, want) < 1e-12
+
+
+@pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
+def test_symmetric_adjoint_double_layer_hypersingular_with_correction(ctx, one_sided, pde):
+    """adj_double_layer_hypersingular on the surface (DIM correction): the
+    symmetric operators against one-sided ones carrying the same corrections,
+    with alpha/beta."""
+    q = inti.ellipsoid_quadrature(8, 5)
+    A, H = inti.adj_double_layer_hypersingular(op=_op(pde), target=q, source=q, correction={"method": "dim"},
+                                              ctx=ctx)
+    assert A.tuning["symmetric"] and H.tuning["symmetric"]
+    cplx = pde == O.HELMHOLTZ
+    x, y0 = density(len(q), cplx, 7), density(len(q), cplx, 8)
+    alpha, beta = (0.25 - 1.0j, 0.5 + 0.5j) if cplx else (-0.75, 1.5)
+    for P in (A, H):
+        c = inti.CorrectionMatrix.from_csr(*P.correction.arrays(), P.shape, ctx=one_sided)
+        P2 = inti.GpuOperator(P.kernel, q, q, c, "fp64", one_sided)
+        assert not P2.tuning["symmetric"]
+        got = P.mul(y0.copy(), x, alpha=alpha, beta=beta)
+        want = alpha * (P2 @ x) + beta * y0
+        assert relerr(got, want) < 1e-12
+
+
+@pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
+@pytest.mark.parametrize("kname", ["SL", "DL", "ADL", "HS"])
+def test_symmetric_transpose_matches_one_sided(ctx, one_sided, pde, kname):
+    """A^T of a square operator runs the symmetric product of the swapped
+    kernel (DL <-> ADL) with unit weights; against the one-sided transpose
+    (itself checked against the oracle's dense transpose) and, on sampled
+    columns, against the oracle's rows of the swapped kernel."""
+    q = inti.ellipsoid_quadrature(9, 5)
+    K, okind = KERNELS[kname]
+    A = inti.GpuOperator(K(_op(pde)), q, q, None, "fp64", ctx)
+    B = inti.GpuOperator(K(_op(pde)), q, q, None, "fp64", one_sided)
+    cplx = pde == O.HELMHOLTZ
+    g = density(len(q), cplx, 9)
+    ya = A.rmatvec(g)
+    assert relerr(ya, B.rmatvec(g)) < 1e-13
+    swapped = {O.DL: O.ADL, O.ADL: O.DL}.get(okind, okind)
+    k = 0.0 if pde == O.LAPLACE else 6.0
+    rows = np.arange(0, len(q), 97)
+    ref = O.apply(pde, swapped, k, q.coords, q.normals, q.coords, q.normals, np.ones(len(q)), g, rows=rows)
+    assert relerr(ya[rows], q.weights[rows] * ref) < 1e-12
 
 
 def test_symmetric_gmres_matches_one_sided(ctx, one_sided):
@@ -99,7 +146,7 @@ def test_symmetric_edge_sizes(ctx, n, pde):
     k = 0.0 if pde == O.LAPLACE else 3.0
     x = density(n, cplx, 2)
     op = inti.Laplace(dim=3) if pde == O.LAPLACE else inti.Helmholtz(k=3.0, dim=3)
-    for K, okind in ((inti.SingleLayerKernel, O.SL), (inti.DoubleLayerKernel, O.DL)):
+    for K, okind in KERNELS.values():
         A = inti.GpuOperator(K(op), q, q, None, "fp64", ctx)
         assert A.tuning["symmetric"]
         ref = oracle_apply(pde, okind, k, q, q, x)
