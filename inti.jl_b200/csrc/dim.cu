@@ -91,9 +91,10 @@ struct S<true> {
 };
 
 // S and D kernel values of one pair (without the weight), sharing r, 1/d and
-// e^{ikd}: the 3D single/double layer from the refined hardware rsqrt and the
-// tabulated e^{ikd} of the pair kernels (tab: the device table, read-only);
-// other kinds and 2D through kernel_value.
+// e^{ikd}: in 3D the single/double layer (DERIV false) or the adjoint double
+// layer / hypersingular pair (DERIV true, target normal ni) from the refined
+// hardware rsqrt and the tabulated e^{ikd} of the pair kernels (tab: the
+// device table, read-only); 2D through kernel_value.
 template <int PDE, int DIM, bool DERIV>
 __device__ __forceinline__ void theta_sd(const double* xi, const double* ni, const double* yj,
                                          const double* nj, double k, double kT, double delta,
@@ -115,6 +116,36 @@ __device__ __forceinline__ void theta_sd(const double* xi, const double* ni, con
       // e^{ikd} (1/d - ik) (r.n_y) / (4 pi d^2)
       const double h = c4 * rn * ri * ri;
       dv = make_double2(h * fma(c, ri, k * s), h * fma(s, ri, -k * c));
+    }
+  } else if (DIM == 3) {
+    // derivative: (ADL, HS) with the target normal n_x = ni, source normal n_y
+    const double r0 = xi[0] - yj[0], r1 = xi[1] - yj[1], r2 = xi[2] - yj[2];
+    const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
+    const double ri = pair_keep(d2) ? rsqrt_fast(d2) : 0.0;
+    const double rnx = fma(r2, ni[2], fma(r1, ni[1], r0 * ni[0]));
+    const double rny = fma(r2, nj[2], fma(r1, nj[1], r0 * nj[0]));
+    const double nn = fma(ni[2], nj[2], fma(ni[1], nj[1], ni[0] * nj[0]));
+    constexpr double c4 = 1.0 / (4 * kPi);
+    const double id2 = ri * ri;
+    if (PDE == LAPLACE) {
+      const double ri3 = id2 * ri;
+      sv = make_double2(-c4 * rnx * ri3, 0.0);
+      dv = make_double2(c4 * fma(-3.0 * rnx * rny, id2, nn) * ri3, 0.0);
+    } else {
+      const double d = d2 * ri;
+      double c, s;  // e^{ikd}
+      expi_table_eval(d, kT, tab, delta, c, s);
+      // -e^{ikd} (1/d - ik) (r.n_x) / (4 pi d^2)
+      const double f = -c4 * rnx * id2;
+      sv = make_double2(f * fma(c, ri, k * s), f * fma(s, ri, -k * c));
+      // e^{ikd} [(1/d - ik) p + (k^2 d^2 - 3 + 3ikd) s5] / (4 pi) with
+      // p = (n_x.n_y)/d^2, s5 = (r.n_x)(r.n_y)/d^5
+      const double kd = k * d;
+      const double fr = fma(kd, kd, -3.0), fi = 3.0 * kd;
+      const double p = nn * id2;
+      const double s5 = (rnx * rny) * (id2 * id2 * ri);
+      const double wr = c4 * fma(ri, p, fr * s5), wi = c4 * fma(-k, p, fi * s5);
+      dv = make_double2(fma(c, wr, -s * wi), fma(c, wi, s * wr));
     }
   } else {
     constexpr int KS = DERIV ? ADL : SL;
@@ -211,7 +242,8 @@ __global__ void __launch_bounds__(kThetaBlock) dim_theta(
   }
 }
 
-// Theta partials on the FP64 MMA path (3D value kernels): per tile of J
+// Theta partials on the FP64 MMA path (3D; DERIV: the (ADL, HS) pair of the
+// derivative corrections in place of (S, D)): per tile of J
 // sources the CUDA cores evaluate (S w, D w) once per pair into A (complex:
 // slots Sr, Si, Dr, Di), the trace rows are staged as B (real: rows g1, -g0;
 // complex, with (Re, Im) column pairs: (g1r, g1i), (-g1i, g1r), (-g0r, -g0i),
@@ -237,9 +269,10 @@ constexpr size_t theta_mma_smem() {
          (PDE == HELMHOLTZ ? sizeof(double2) * kExpiTable : 0);
 }
 
-template <int PDE, bool WIDE>
+template <int PDE, bool WIDE, bool DERIV>
 __global__ void __launch_bounds__(kMmaThreads, 2) dim_theta_mma(
-    int64_t m, int64_t n, int ns, const double* __restrict__ tx, const double* __restrict__ x,
+    int64_t m, int64_t n, int ns, const double* __restrict__ tx, const double* __restrict__ tn,
+    const double* __restrict__ x,
     const double* __restrict__ nrm, const double* __restrict__ w, const double2* __restrict__ g0,
     const double2* __restrict__ g1, double k, double kT, double delta, const double2* __restrict__ tab_g,
     int tiles_per_split, double2* __restrict__ partial) {
@@ -262,6 +295,12 @@ __global__ void __launch_bounds__(kMmaThreads, 2) dim_theta_mma(
   const int mloc = tid % Sh::MT, r0 = tid / Sh::MT;
   const int64_t ii = min(base + mloc, m - 1);
   const double xi[3] = {tx[3 * ii], tx[3 * ii + 1], tx[3 * ii + 2]};
+  double ni[3] = {0.0, 0.0, 0.0};  // target normal: derivative corrections only
+  if (DERIV) {
+    ni[0] = tn[3 * ii];
+    ni[1] = tn[3 * ii + 1];
+    ni[2] = tn[3 * ii + 2];
+  }
   for (int q = tid; q < Sh::kK * Sh::LDB; q += kMmaThreads) Bs[q] = 0.0;  // padding columns stay zero
   if (CPLX)
     for (int q = tid; q < kExpiTable; q += kMmaThreads) tab[q] = tab_g[q];
@@ -328,7 +367,7 @@ __global__ void __launch_bounds__(kMmaThreads, 2) dim_theta_mma(
 #pragma unroll 2
     for (int q = r0; q < J; q += R) {
       double2 sv, dv;
-      theta_sd<PDE, 3, false>(xi, xi, &sx[3 * q], &sn[3 * q], k, kT, delta, tab, sv, dv);
+      theta_sd<PDE, 3, DERIV>(xi, ni, &sx[3 * q], &sn[3 * q], k, kT, delta, tab, sv, dv);
       const double wq = sw[q];
       if (CPLX) {
         double* a = &As[mloc * Sh::LDA + NA * q];
@@ -708,8 +747,9 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
     const int64_t tot = m * ns;
     if constexpr (D == 3) {
       // FP64 MMA form; split over sources for >= 8 waves of 2 CTAs per SM
-      auto mma = [&](auto wide_c) {
+      auto mma = [&](auto wide_c, auto deriv_c) {
         constexpr bool WIDE = decltype(wide_c)::value;
+        constexpr bool DV = decltype(deriv_c)::value;
         using TM = ThetaMma<P, WIDE>;
         const int64_t blocks = (m + TM::Sh::MT - 1) / TM::Sh::MT;
         const int64_t ntile = (n + TM::J - 1) / TM::J;
@@ -719,27 +759,34 @@ static void dim_theta_run(inti_ctx* ctx, int pde, double k_re, const inti_quad* 
         split = (int)((ntile + tps - 1) / tps);
         wk.part.ensure(sizeof(double2) * (size_t)split * m * ns);
         constexpr size_t smem = theta_mma_smem<P, WIDE>();
-        auto* kern = &dim_theta_mma<P, WIDE>;
+        auto* kern = &dim_theta_mma<P, WIDE, DV>;
         static std::once_flag once;
         std::call_once(once, [kern] {
           cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         });
         ProfScope pd(ctx, "dim");
         kern<<<dim3((unsigned)blocks, (unsigned)split), kMmaThreads, smem, ctx->stream>>>(
-            m, n, ns, tx, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re, k_re * kExpiTable / (2 * kPi),
-            2 * kPi / kExpiTable, P == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, tps, wk.part.as<double2>());
+            m, n, ns, tx, tn, X, NR, W, wk.g0.as<double2>(), wk.g1.as<double2>(), k_re,
+            k_re * kExpiTable / (2 * kPi), 2 * kPi / kExpiTable, P == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, tps,
+            wk.part.as<double2>());
         ctx->launches++;
-        dim_theta_reduce<P, D, false><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
+        dim_theta_reduce<P, D, DV><<<(unsigned)((tot + 255) / 256), 256, 0, ctx->stream>>>(
             m, ns, split, tx, tn, wk.d_xs.as<double>(), mu, k_re, wk.part.as<double2>(), wk.theta.as<double2>());
         ctx->launches++;
       };
-      if (!derivative && ns <= ThetaMma<P, false>::kMaxNs) {
-        mma(std::false_type());
+      auto mma_d = [&](auto wide_c) {
+        if (derivative)
+          mma(wide_c, std::true_type());
+        else
+          mma(wide_c, std::false_type());
+      };
+      if (ns <= ThetaMma<P, false>::kMaxNs) {
+        mma_d(std::false_type());
         return;
       }
       if constexpr (P == HELMHOLTZ) {
-        if (!derivative && ns <= ThetaMma<P, true>::kMaxNs) {
-          mma(std::true_type());
+        if (ns <= ThetaMma<P, true>::kMaxNs) {
+          mma_d(std::true_type());
           return;
         }
       }

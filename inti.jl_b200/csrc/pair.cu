@@ -645,14 +645,18 @@ __device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* 
           gi = -bi * rns;
         }
       } else {
-        // b = e^{ikd}(1/d - ik)/d^2; a = e^{ikd}(k^2 d^2 - 3 + 3ikd)/d^5
+        // h = b (n_t.n_s) + a (r.n_t)(r.n_s) with b = e^{ikd}(1/d - ik)/d^2 and
+        // a = e^{ikd}(k^2 d^2 - 3 + 3ikd)/d^5, i.e. h = e^{ikd} W with the
+        // bracket W = (1/d - ik) p + (k^2 d^2 - 3 + 3ikd) s formed in real
+        // arithmetic from p = (n_t.n_s)/d^2 and s = (r.n_t)(r.n_s)/d^5
         const R nn = fma(t[5], s[5], fma(t[4], s[4], t[3] * s[3]));
-        const R fr = fma(k * d, k * d, R(-3)), fi = R(3) * k * d;
-        const R sa = id2 * id2 * ri;
-        const R a_r = sa * fma(cs, fr, -sn * fi), a_i = sa * fma(cs, fi, sn * fr);
-        const R u = rnt * rns;
-        hr = fma(a_r, u, er * id2 * nn);
-        hi = fma(a_i, u, ei * id2 * nn);
+        const R kd = k * d;
+        const R fr = fma(kd, kd, R(-3)), fi = R(3) * kd;
+        const R p = nn * id2;
+        const R s5 = (rnt * rns) * (id2 * id2 * ri);
+        const R wr = fma(ri, p, fr * s5), wi = fma(-k, p, fi * s5);
+        hr = fma(cs, wr, -sn * wi);
+        hi = fma(cs, wi, sn * wr);
         gr = hr;
         gi = hi;
       }
