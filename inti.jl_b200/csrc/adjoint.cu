@@ -29,29 +29,33 @@ namespace inti {
 
 constexpr int kAdjBlock = 128;
 constexpr int kAdjTile = 128;
+constexpr int kAdjSpt = 2;  // sources per thread: each staged target serves two pairs
 
 // partial layout per (split, source): [s, a_0..a_{D-1}, b_0..b_{D-1}, pad]
-template <int KIND, int DIM>
+template <int KIND, int DIM, int SPT>
 __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
     int64_t m, int64_t n, const double* __restrict__ tx, const double* __restrict__ g,
     const double* __restrict__ sx, const double* __restrict__ sn, int tiles_per_split,
     double* __restrict__ partial) {
   constexpr int W = 2 * DIM + 2;
   __shared__ double stx[kAdjTile * DIM], sg[kAdjTile];
-  const int64_t j = blockIdx.x * (int64_t)kAdjBlock + threadIdx.x;
-  const int64_t jj = min(j, n - 1);
-  double y[DIM], ny[DIM];
-#pragma unroll
-  for (int c = 0; c < DIM; ++c) {
-    y[c] = sx[DIM * jj + c];
-    ny[c] = KIND == DL ? sn[DIM * jj + c] : 0.0;
-  }
+  const int64_t j0 = blockIdx.x * (int64_t)(kAdjBlock * SPT) + threadIdx.x;
+  double y[SPT][DIM], ny[SPT][DIM];
   // DL: the source's own normal factors out of two sums, accumulated as
   // scalars and applied at the end: s = n_y . a, and b = P*h - n_y*G with
   // h = sum g K' r (P = 3 in 3D, 2 in 2D) and G = sum g K'
-  double s = 0.0, G = 0.0, a[DIM], b[DIM];
+  double s[SPT], G[SPT], a[SPT][DIM], b[SPT][DIM];
 #pragma unroll
-  for (int c = 0; c < DIM; ++c) a[c] = b[c] = 0.0;
+  for (int u = 0; u < SPT; ++u) {
+    const int64_t jj = min(j0 + u * kAdjBlock, n - 1);
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      y[u][c] = sx[DIM * jj + c];
+      ny[u][c] = KIND == DL ? sn[DIM * jj + c] : 0.0;
+      a[u][c] = b[u][c] = 0.0;
+    }
+    s[u] = G[u] = 0.0;
+  }
   const int64_t ntile = (m + kAdjTile - 1) / kAdjTile;
   const int64_t t0 = (int64_t)blockIdx.y * tiles_per_split;
   const int64_t t1 = min(ntile, t0 + tiles_per_split);
@@ -67,71 +71,81 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
     __syncthreads();
 #pragma unroll 2
     for (int q = 0; q < kAdjTile; ++q) {
-      double r[DIM];
+      double xt[DIM];
 #pragma unroll
-      for (int c = 0; c < DIM; ++c) r[c] = stx[q * DIM + c] - y[c];
-      double d2 = r[0] * r[0];
-#pragma unroll
-      for (int c = 1; c < DIM; ++c) d2 = fma(r[c], r[c], d2);
-      if (!pair_keep(d2)) continue;
+      for (int c = 0; c < DIM; ++c) xt[c] = stx[q * DIM + c];
       const double gi = sg[q];
-      if (DIM == 3) {
-        const double ri = rsqrt_fast(d2);
-        const double ri3 = ri * ri * ri;
-        if (KIND == SL) {
-          s = fma(gi, ri, s);
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) b[c] = fma(gi * ri3, r[c], b[c]);
-        } else {
-          double rn = r[0] * ny[0];
+      for (int u = 0; u < SPT; ++u) {
+        double r[DIM];
 #pragma unroll
-          for (int c = 1; c < DIM; ++c) rn = fma(r[c], ny[c], rn);
-          const double gr3 = gi * ri3;
-          G += gr3;
-          const double h = gr3 * rn * (ri * ri);
+        for (int c = 0; c < DIM; ++c) r[c] = xt[c] - y[u][c];
+        double d2 = r[0] * r[0];
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            a[c] = fma(gr3, r[c], a[c]);
-            b[c] = fma(h, r[c], b[c]);
+        for (int c = 1; c < DIM; ++c) d2 = fma(r[c], r[c], d2);
+        const bool keep = pair_keep(d2);  // the self pair adds zero to every sum
+        if (DIM == 3) {
+          const double ri = keep ? rsqrt_fast(d2) : 0.0;
+          const double ri3 = ri * ri * ri;
+          if (KIND == SL) {
+            s[u] = fma(gi, ri, s[u]);
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) b[u][c] = fma(gi * ri3, r[c], b[u][c]);
+          } else {
+            double rn = r[0] * ny[u][0];
+#pragma unroll
+            for (int c = 1; c < DIM; ++c) rn = fma(r[c], ny[u][c], rn);
+            const double gr3 = gi * ri3;
+            G[u] += gr3;
+            const double h = gr3 * rn * (ri * ri);
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+              a[u][c] = fma(gr3, r[c], a[u][c]);
+              b[u][c] = fma(h, r[c], b[u][c]);
+            }
           }
-        }
-      } else {
-        const double id2 = 1.0 / d2;
-        if (KIND == SL) {
-          s = fma(gi, log(d2), s);  // scaled by -1/(4 pi) at the end
-#pragma unroll
-          for (int c = 0; c < DIM; ++c) b[c] = fma(gi * id2, r[c], b[c]);
         } else {
-          double rn = r[0] * ny[0];
+          const double id2 = keep ? 1.0 / d2 : 0.0;
+          if (KIND == SL) {
+            s[u] = fma(gi, keep ? log(d2) : 0.0, s[u]);  // scaled by -1/(4 pi) at the end
 #pragma unroll
-          for (int c = 1; c < DIM; ++c) rn = fma(r[c], ny[c], rn);
-          const double gd = gi * id2;
-          G += gd;
-          const double h = gd * rn * id2;
+            for (int c = 0; c < DIM; ++c) b[u][c] = fma(gi * id2, r[c], b[u][c]);
+          } else {
+            double rn = r[0] * ny[u][0];
 #pragma unroll
-          for (int c = 0; c < DIM; ++c) {
-            a[c] = fma(gd, r[c], a[c]);
-            b[c] = fma(h, r[c], b[c]);
+            for (int c = 1; c < DIM; ++c) rn = fma(r[c], ny[u][c], rn);
+            const double gd = gi * id2;
+            G[u] += gd;
+            const double h = gd * rn * id2;
+#pragma unroll
+            for (int c = 0; c < DIM; ++c) {
+              a[u][c] = fma(gd, r[c], a[u][c]);
+              b[u][c] = fma(h, r[c], b[u][c]);
+            }
           }
         }
       }
     }
   }
-  if (KIND == DL) {
-    constexpr double P = DIM == 3 ? 3.0 : 2.0;
-    s = a[0] * ny[0];
 #pragma unroll
-    for (int c = 1; c < DIM; ++c) s = fma(a[c], ny[c], s);
+  for (int u = 0; u < SPT; ++u) {
+    if (KIND == DL) {
+      constexpr double P = DIM == 3 ? 3.0 : 2.0;
+      s[u] = a[u][0] * ny[u][0];
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) b[c] = fma(P, b[c], -G * ny[c]);
-  }
-  if (j < n) {
-    double* o = partial + ((int64_t)blockIdx.y * n + j) * W;
-    o[0] = s;
+      for (int c = 1; c < DIM; ++c) s[u] = fma(a[u][c], ny[u][c], s[u]);
 #pragma unroll
-    for (int c = 0; c < DIM; ++c) {
-      o[1 + c] = a[c];
-      o[1 + DIM + c] = b[c];
+      for (int c = 0; c < DIM; ++c) b[u][c] = fma(P, b[u][c], -G[u] * ny[u][c]);
+    }
+    const int64_t j = j0 + u * kAdjBlock;
+    if (j < n) {
+      double* o = partial + ((int64_t)blockIdx.y * n + j) * W;
+      o[0] = s[u];
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) {
+        o[1 + c] = a[u][c];
+        o[1 + DIM + c] = b[u][c];
+      }
     }
   }
 }
@@ -191,7 +205,7 @@ void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsi
     if (dnormals) { o_n.ensure(sizeof(double) * dim * n); DN = o_n.as<double>(); }
     if (dweights) { o_w.ensure(sizeof(double) * n); DW = o_w.as<double>(); }
   }
-  const int64_t blocks = (n + kAdjBlock - 1) / kAdjBlock;
+  const int64_t blocks = (n + kAdjBlock * kAdjSpt - 1) / (kAdjBlock * kAdjSpt);
   const int64_t ntile = (m + kAdjTile - 1) / kAdjTile;
   const int64_t want = (int64_t)ctx->num_sms * 8;
   int split = (int)std::max<int64_t>(1, std::min<int64_t>(ntile, (want + blocks - 1) / blocks));
@@ -209,7 +223,7 @@ void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsi
     constexpr int D = decltype(dim_c)::value;
     {
       ProfScope pa(ctx, "adjoint");
-      adjoint_sources<K, D><<<dim3((unsigned)blocks, (unsigned)split), kAdjBlock, 0, ctx->stream>>>(
+      adjoint_sources<K, D, kAdjSpt><<<dim3((unsigned)blocks, (unsigned)split), kAdjBlock, 0, ctx->stream>>>(
           m, n, TX, G, SX, SN, tps, part);
     }
     adjoint_reduce<K, D><<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>(

@@ -1,7 +1,8 @@
 """Hand-written adjoint: gradients of J = ½‖u − u*‖², u = D[σ] at exterior
 targets, with respect to σ and every node's coordinates, normal and weight,
 checked against central finite differences (h = 1e-6, FP64) and against a
-forward-mode (dual number) restatement of the CPU matvec."""
+forward-mode (dual number) restatement of the CPU matvec; single and double
+layer, 3D and 2D, one and many thread blocks of sources."""
 import numpy as np
 import pytest
 
@@ -93,3 +94,42 @@ def test_device_gradients_match_host(ctx):
     op.grad_sources_device(gd.data_ptr(), sd.data_ptr(), outs["sigma"].data_ptr(), 0, 0, 0)
     ctx.synchronize()
     assert torch.isnan(outs["weights"]).all()
+
+
+@pytest.mark.parametrize("dim", [3, 2])
+@pytest.mark.parametrize("kind,okind", [(inti.DoubleLayerKernel, O.DL), (inti.SingleLayerKernel, O.SL)])
+def test_gradients_many_source_blocks(ctx, dim, kind, okind):
+    """Sources over many thread blocks (two sources per thread, the last
+    block ragged) and targets over several chunks, in 3D and 2D: dJ/dsigma
+    against the transpose apply, the geometry gradients against central
+    differences."""
+    if dim == 3:
+        q = inti.ellipsoid_quadrature(8, 5)  # 3,456 sources
+        d = np.random.default_rng(7).standard_normal((300, 3))
+        tgt = inti.points(1.6 * d / np.linalg.norm(d, axis=1, keepdims=True))
+    else:
+        q = inti.kite_quadrature(200, 9)  # 1,000 sources
+        t = np.linspace(0, 2 * np.pi, 300, endpoint=False)
+        tgt = inti.points(np.stack([3.0 * np.cos(t), 3.0 * np.sin(t)], axis=1))
+    op = inti.GpuOperator(kind(inti.Laplace(dim=dim)), tgt, q, ctx=ctx)
+    sigma = density(len(q), False, 12)
+    ustar = density(len(tgt), False, 13) * 0.01
+    g = op @ sigma - ustar
+    grad = op.grad_sources(g, sigma)
+    assert relerr(grad["sigma"], op.rmatvec(g)) < 1e-13
+    r = np.random.default_rng(14)
+    h = 1e-6
+    base = {"coords": q.coords, "normals": q.normals, "weights": q.weights, "sigma": sigma}
+
+    def Jd(p):
+        u = O.apply(O.LAPLACE, okind, 0.0, tgt.coords, None, p["coords"], p["normals"], p["weights"], p["sigma"])
+        return 0.5 * np.sum((u - ustar) ** 2)
+
+    for name in ("coords", "normals", "weights"):
+        if okind == O.SL and name == "normals":
+            assert np.all(grad[name] == 0)
+            continue
+        v = r.standard_normal(base[name].shape)
+        fd = (Jd(dict(base, **{name: base[name] + h * v})) - Jd(dict(base, **{name: base[name] - h * v}))) / (2 * h)
+        ad = float(np.sum(grad[name] * v))
+        assert abs(ad - fd) <= 1e-6 * max(abs(fd), 1e-8), (name, ad, fd)
