@@ -189,6 +189,8 @@ const float2* expi_table_f32(inti_ctx* ctx);
 // Source records per tile (must match the kernel template parameter).
 int pair_tile(int precision);
 // Bytes of one packed source record.
+// Most source chunks (partial sums per target) of one pair-kernel launch.
+constexpr int kMaxSplit = 256;
 int pair_record_bytes(int pde, int kind, int dim, int precision);
 int pair_symm_record_bytes(int pde, int kind, int precision);  // packed record of the symmetric form
 // Bytes of one partial accumulator per target per split.

@@ -339,11 +339,11 @@ void op_autotune(inti_op* op, bool measure) {
   }
   if (!measure || !ctx->autotune || (double)m * (double)n < kTuneMinPairs) return;
   // candidates: 4 or 2 targets per thread, each with the heuristic split,
-  // half of it and twice it (at most one chunk per source tile, 64 chunks)
+  // half of it and twice it (at most one chunk per source tile, kMaxSplit chunks)
   std::vector<std::pair<int, int>> cand;
   for (int tpt : {4, 2}) {
     const int s0 = pair_plan_split(ctx, op->pde, op->kind, op->dim, op->precision, m, n, tpt);
-    const int hi = (int)std::min<int64_t>({(int64_t)2 * s0, op->n_tiles, 64});
+    const int hi = (int)std::min<int64_t>({(int64_t)2 * s0, op->n_tiles, (int64_t)kMaxSplit});
     for (int sp : {s0, std::max(1, s0 / 2), hi})
       if (std::find(cand.begin(), cand.end(), std::make_pair(tpt, sp)) == cand.end()) cand.emplace_back(tpt, sp);
   }

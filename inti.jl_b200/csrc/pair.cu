@@ -1083,10 +1083,11 @@ int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precisi
   const int64_t blocks = (m + kBlock * tpt - 1) / (kBlock * tpt);
   const int64_t slots = (int64_t)ctx->num_sms * occ;
   // Smallest split whose last wave is >= 90% full (or that reaches 8
-  // waves), never more chunks than source tiles.
+  // waves), never more chunks than source tiles.  Up to kMaxSplit chunks:
+  // few target blocks (potentials at a few thousand points) need many.
   int best = 1;
   double best_eff = -1.0;
-  for (int s = 1; s <= 64 && s <= n_tiles; ++s) {
+  for (int s = 1; s <= kMaxSplit && s <= n_tiles; ++s) {
     const int64_t tps = (n_tiles + s - 1) / s;
     const int64_t eff_s = (n_tiles + tps - 1) / tps;  // chunks actually used
     const double waves = (double)(blocks * eff_s) / (double)slots;

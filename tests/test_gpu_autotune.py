@@ -28,7 +28,7 @@ def test_autotuned_shape_gives_the_same_operator(symmetric):
     B = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp64", plain)
     ta, tb = A.tuning, B.tuning
     assert ta["symmetric"] == tb["symmetric"] == symmetric
-    assert ta["targets_per_thread"] in (2, 4) and 1 <= ta["split"] <= 64
+    assert ta["targets_per_thread"] in (2, 4) and 1 <= ta["split"] <= 256
     assert tb["targets_per_thread"] == (2 if symmetric else 4)
     # the choice is cached per context and problem shape
     assert inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp64", tuned).tuning == ta
@@ -46,3 +46,20 @@ def test_small_operators_keep_the_heuristic_shape():
     A = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp64", tuned)
     B = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp64", plain)
     assert A.tuning == B.tuning
+
+
+@pytest.mark.parametrize("kname", ["SL", "DL"])
+def test_few_targets_many_source_chunks(ctx, kname):
+    """A potential at a few hundred points from 21,600 sources: one or two
+    target blocks, so the heuristic cuts the sources into more than 64
+    chunks; the product still matches the oracle."""
+    q = G.ellipsoid_quadrature(20, 5)
+    d = np.random.default_rng(4).standard_normal((300, 3))
+    tgt = inti.points(1.7 * d / np.linalg.norm(d, axis=1, keepdims=True))
+    op = inti.Helmholtz(k=3.0, dim=3)
+    K, okind = (inti.SingleLayerKernel, O.SL) if kname == "SL" else (inti.DoubleLayerKernel, O.DL)
+    A = inti.GpuOperator(K(op), tgt, q, None, "fp64", ctx)
+    assert A.tuning["split"] > 64
+    sigma = density(len(q), True, 8)
+    ref = O.apply(O.HELMHOLTZ, okind, 3.0, tgt.coords, None, q.coords, q.normals, q.weights, sigma)
+    assert relerr(A @ sigma, ref) < 1e-12
