@@ -161,8 +161,8 @@ int inti_op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im,
 int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype);
 /* Y = alpha*(A*X + C*X) + beta*Y for nrhs columns (leading dimensions ldx,
  * ldy in elements).  alpha, beta: 2 doubles each (re, im); NULL means 1, 0.
- * beta = 0 does not read Y.  FP64 3D SL, DL and combined-field operators
- * apply 8 or more columns in one pass that evaluates each kernel value once
+ * beta = 0 does not read Y.  FP64 3D operators (every kernel) apply 8 or
+ * more columns in one pass that evaluates each kernel value once
  * per 64 columns (16 complex / 32 real when all columns fit), the pair tile
  * multiplied with the columns on the FP64 MMA path; other operators and
  * fewer columns run one pair product per column.  Results agree to rounding

@@ -80,6 +80,42 @@ __device__ __forceinline__ double2 lap_kernels(const double* x, const double* y,
   return make_double2(v, 0.0);
 }
 
+// Adjoint double layer (KIND ADL) or hypersingular (HS) value without the
+// 1/(4 pi) factor, with the target normal nx: ADL = -e^{ikd}(1/d - ik)(r.n_x)/d^2
+// (Laplace: -(r.n_x)/d^3); HS = e^{ikd} [(1/d - ik) p + (k^2 d^2 - 3 + 3ikd) s]
+// with p = (n_x.n_y)/d^2, s = (r.n_x)(r.n_y)/d^5 (Laplace: (n_x.n_y - 3 (r.n_x)(r.n_y)/d^2)/d^3).
+template <int PDE, int KIND>
+__device__ __forceinline__ double2 normal_kernels(const double* x, const double* nx, const double* y,
+                                                  const double* ny, double k, double kT, double delta,
+                                                  const double2* tab) {
+  const double r0 = x[0] - y[0], r1 = x[1] - y[1], r2 = x[2] - y[2];
+  const double d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
+  const double ri = pair_keep(d2) ? rsqrt_fast(d2) : 0.0;
+  const double id2 = ri * ri;
+  const double rnx = fma(r2, nx[2], fma(r1, nx[1], r0 * nx[0]));
+  if (PDE == LAPLACE) {
+    if (KIND == ADL) return make_double2(-rnx * (id2 * ri), 0.0);
+    const double rny = fma(r2, ny[2], fma(r1, ny[1], r0 * ny[0]));
+    const double nn = fma(nx[2], ny[2], fma(nx[1], ny[1], nx[0] * ny[0]));
+    return make_double2(fma(-3.0 * rnx * rny, id2, nn) * (id2 * ri), 0.0);
+  }
+  const double d = d2 * ri;
+  double cs, sn;
+  expi_table_eval(d, kT, tab, delta, cs, sn);
+  if (KIND == ADL) {
+    const double f = -rnx * id2;
+    return make_double2(f * fma(cs, ri, k * sn), f * fma(sn, ri, -k * cs));
+  }
+  const double rny = fma(r2, ny[2], fma(r1, ny[1], r0 * ny[0]));
+  const double nn = fma(nx[2], ny[2], fma(nx[1], ny[1], nx[0] * ny[0]));
+  const double kd = k * d;
+  const double fr = fma(kd, kd, -3.0), fi = 3.0 * kd;
+  const double p = nn * id2;
+  const double s5 = (rnx * rny) * (id2 * id2 * ri);
+  const double wr = fma(ri, p, fr * s5), wi = fma(-k, p, fi * s5);
+  return make_double2(fma(cs, wr, -sn * wi), fma(cs, wi, sn * wr));
+}
+
 constexpr int kMrhsBlock = 128;  // targets per work item
 
 // FP64 form on the MMA path: one CTA = 64 targets x 64 right-hand sides;
@@ -153,6 +189,14 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
   const int m = tid % Sh::MT, r0 = tid / Sh::MT;
   const int64_t i = toff + min(base + m, tn - 1);
   const double xi[3] = {tc[3 * i], tc[3 * i + 1], tc[3 * i + 2]};
+  constexpr bool TN = KIND == ADL || KIND == HS;  // kernels with the target normal
+  double ni[3] = {0.0, 0.0, 0.0};
+  if (TN) {
+    const double* tnr = a.tcoords ? a.tnormals : a.normals;
+    ni[0] = tnr[3 * i];
+    ni[1] = tnr[3 * i + 1];
+    ni[2] = tnr[3 * i + 2];
+  }
   const double kT = a.k * kExpiTable / (2 * kPi), delta = 2 * kPi / kExpiTable;
   // staging roles: density element e = tid + r*256 -> (source e % J, column e / J)
   // (consecutive threads read consecutive nodes of one column); source value tid
@@ -217,7 +261,9 @@ __global__ void __launch_bounds__(kMmaThreads, 2) mrhs_mma(BatchArgs a) {
 #pragma unroll 2
     for (int q = r0; q < kMmaJ; q += R) {
       double2 kv;
-      if (CPLX) {
+      if (TN) {
+        kv = normal_kernels<PDE, KIND>(xi, ni, &sx[3 * q], &sn[3 * q], a.k, kT, delta, tab);
+      } else if (CPLX) {
         const KPair kp = helm_kernels(xi, &sx[3 * q], &sn[3 * q], a.k, kT, delta, tab, KIND != SL, KIND != DL);
         if (KIND == SL)
           kv = kp.sl;
@@ -452,15 +498,19 @@ static void mrhs_mma_launch(inti_ctx* ctx, int pde, int kind, const BatchArgs& a
   };
   using H = std::integral_constant<int, HELMHOLTZ>;
   using Lp = std::integral_constant<int, LAPLACE>;
-  if (pde == INTI_HELMHOLTZ) {
-    if (kind == SL) go(H(), std::integral_constant<int, SL>());
-    else if (kind == DL) go(H(), std::integral_constant<int, DL>());
-    else go(H(), std::integral_constant<int, CF>());
-  } else {
-    if (kind == SL) go(Lp(), std::integral_constant<int, SL>());
-    else if (kind == DL) go(Lp(), std::integral_constant<int, DL>());
-    else go(Lp(), std::integral_constant<int, CF>());
-  }
+  auto by_kind = [&](auto pc) {
+    switch (kind) {
+      case SL: return go(pc, std::integral_constant<int, SL>());
+      case DL: return go(pc, std::integral_constant<int, DL>());
+      case ADL: return go(pc, std::integral_constant<int, ADL>());
+      case HS: return go(pc, std::integral_constant<int, HS>());
+      default: return go(pc, std::integral_constant<int, CF>());
+    }
+  };
+  if (pde == INTI_HELMHOLTZ)
+    by_kind(H());
+  else
+    by_kind(Lp());
   ctx->launches++;
   INTI_CUDA(cudaGetLastError());
 }
@@ -517,8 +567,10 @@ void batch_apply_device(inti_batch* b, int precision, const double* x, int64_t l
 }
 
 bool op_mrhs_supported(const inti_op* op) {
-  return op->precision == INTI_FP64 && op->dim == 3 && (op->kind == SL || op->kind == DL || op->kind == CF) &&
-         (op->kind == SL || op->source->has_normals);
+  const bool snormal = op->kind == DL || op->kind == CF || op->kind == HS;
+  const bool tnormal = op->kind == ADL || op->kind == HS;
+  return op->precision == INTI_FP64 && op->dim == 3 && (!snormal || op->source->has_normals) &&
+         (!tnormal || op->target->has_normals);
 }
 
 void op_apply_mrhs(inti_op* op, const double* x, int64_t ldx, double* y, int64_t ldy, int32_t nrhs,
@@ -527,6 +579,7 @@ void op_apply_mrhs(inti_op* op, const double* x, int64_t ldx, double* y, int64_t
   const bool cplx = op->pde == INTI_HELMHOLTZ;
   BatchArgs a{};
   a.tcoords = op->target->coords.as<double>();
+  a.tnormals = op->target->has_normals ? op->target->normals.as<double>() : nullptr;
   a.gm = op->target->n;
   a.gn = op->source->n;
   a.coords = op->source->coords.as<double>();

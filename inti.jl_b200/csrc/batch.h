@@ -62,6 +62,7 @@ struct BatchArgs {
   // tcoords[0, gm), sources coords/normals/weights[0, gn), work item b =
   // target block b; off, item_surf and item_block are unused
   const double* tcoords = nullptr;
+  const double* tnormals = nullptr;  // adjoint double layer / hypersingular
   int64_t gm = 0, gn = 0;
 };
 

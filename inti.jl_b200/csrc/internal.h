@@ -57,7 +57,7 @@ struct inti_op {
 
 namespace inti {
 
-// Applies of this many columns or more (FP64 3D SL/DL/CF operators) take the
+// Applies of this many columns or more (FP64 3D operators, every kernel) take the
 // multi-column MMA kernel instead of one pair product per column.
 constexpr int kMrhsMinColumns = 8;
 

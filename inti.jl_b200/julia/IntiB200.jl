@@ -199,8 +199,8 @@ LinearMaps._unsafe_mul!(y::AbstractVector, A::B200Map, x::AbstractVector) = appl
 LinearMaps._unsafe_mul!(y::AbstractVector, A::B200Map, x::AbstractVector, α::Number, β::Number) =
     apply!(y, A, x, α, β)
 
-# Many columns in one call: from 8 columns on, FP64 3D SL/DL/combined-field
-# operators evaluate each kernel value once for up to 64 columns.
+# Many columns in one call: from 8 columns on, FP64 3D operators (every
+# kernel) evaluate each kernel value once for up to 64 columns.
 function apply!(Y::AbstractMatrix, A::B200Map{T}, X::AbstractMatrix, α = true, β = false) where {T}
     XX = Matrix{T}(X)
     YY = Y isa Matrix{T} ? Y : Matrix{T}(Y)

@@ -1,5 +1,7 @@
 """Multi-column applies of single operators (inti_op_apply with nrhs >= 8):
-the FP64 MMA kernel evaluates each kernel value once for up to 64 columns.
+the FP64 MMA kernel evaluates each kernel value once for up to 64 columns,
+for the single and double layer, the combined field, the adjoint double
+layer and the hypersingular kernel.
 Checked against the same operator applied one column at a time (itself
 checked against the oracle), on-surface with the DIM correction and off the
 surface, for 8 columns, and for 70 (two column groups, the second ragged),
@@ -17,18 +19,25 @@ pytestmark = pytest.mark.gpu
 def _ops(kind, pde, on_surface, ctx):
     q = inti.ellipsoid_quadrature(5, 5)
     op = inti.Helmholtz(k=4.0, dim=3) if pde == "helmholtz" else inti.Laplace(dim=3)
+    deriv = kind in ("ADL", "HS")
     if on_surface:
-        S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+        S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"},
+                                        derivative=deriv, ctx=ctx)
         tq = q
     else:
         r = np.random.default_rng(3)
         d = r.standard_normal((700, 3))
-        tq = inti.points(1.6 * d / np.linalg.norm(d, axis=1, keepdims=True))
-        S = inti.GpuOperator(inti.SingleLayerKernel(op), tq, q, None, "fp64", ctx)
-        D = inti.GpuOperator(inti.DoubleLayerKernel(op), tq, q, None, "fp64", ctx)
-    if kind == "SL":
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        nt = r.standard_normal((700, 3))
+        nt /= np.linalg.norm(nt, axis=1, keepdims=True)
+        tq = inti.Quadrature(1.6 * d, nt, np.ones(700), 0)  # off-surface targets with normals
+        K1, K2 = ((inti.AdjointDoubleLayerKernel, inti.HyperSingularKernel) if deriv
+                  else (inti.SingleLayerKernel, inti.DoubleLayerKernel))
+        S = inti.GpuOperator(K1(op), tq, q, None, "fp64", ctx)
+        D = inti.GpuOperator(K2(op), tq, q, None, "fp64", ctx)
+    if kind in ("SL", "ADL"):
         return S, q, tq
-    if kind == "DL":
+    if kind in ("DL", "HS"):
         return D, q, tq
     cS = -4.0j if pde == "helmholtz" else 0.7
     return inti.CombinedFieldOperator(D, S, 1.0, cS), q, tq
@@ -38,7 +47,7 @@ def _cols(A, X):
     return np.stack([A @ X[:, c] for c in range(X.shape[1])], axis=1)
 
 
-@pytest.mark.parametrize("kind", ["SL", "DL", "CF"])
+@pytest.mark.parametrize("kind", ["SL", "DL", "CF", "ADL", "HS"])
 @pytest.mark.parametrize("pde", ["helmholtz", "laplace"])
 @pytest.mark.parametrize("on_surface", [True, False])
 @pytest.mark.parametrize("nrhs", [8, 70])
@@ -53,11 +62,12 @@ def test_multi_column_apply_matches_columns(ctx, kind, pde, on_surface, nrhs):
     launches = ctx.launch_count - before
     assert launches <= 2  # one MMA launch (+ the correction SpMV), not one product per column
     assert relerr(Y, _cols(A, X)) < 1e-12
-    if kind == "SL" and not on_surface:  # and against the oracle directly
+    if kind in ("SL", "ADL", "HS") and not on_surface:  # and against the oracle directly
         pde_o = O.HELMHOLTZ if pde == "helmholtz" else O.LAPLACE
         k = 4.0 if pde == "helmholtz" else 0.0
+        okind = {"SL": O.SL, "ADL": O.ADL, "HS": O.HS}[kind]
         for c in (0, nrhs - 1):
-            ref = O.apply(pde_o, O.SL, k, tq.coords, None, q.coords, q.normals, q.weights, X[:, c])
+            ref = O.apply(pde_o, okind, k, tq.coords, tq.normals, q.coords, q.normals, q.weights, X[:, c])
             assert relerr(Y[:, c], ref) < 1e-12
 
 
