@@ -248,7 +248,6 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
         ai = fma(hr, qi, fma(hi, qr, ai));
       }
     } else {  // HS
-      const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);
       const R id2 = ri * ri;
       R rn = r[0] * t.n[0];
       rn = fma(r[1], t.n[1], rn);
@@ -261,15 +260,19 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
         NA = fma(t.n[c], s[3 + c], NA);
         NB = fma(t.n[c], s[6 + c], NB);
       }
-      // b = e(1/d - ik) id2 ; a = e (3(ikd-1) + k^2 d^2) id2^2 / d
-      const R br = er * id2, bi = ei * id2;
-      const R fr = fma(k * d, k * d, R(-3)), fi = R(3) * k * d;
-      const R sa = id2 * id2 * ri;
-      const R a_r = sa * fma(cs, fr, -sn * fi), a_i = sa * fma(cs, fi, sn * fr);
-      // value = a (r.nx)(r.p) + b (nx.p), p complex = A + iB (r.p), NA + iNB (nx.p)
-      const R tr = rn * A, ti = rn * B;
-      ar += fma(a_r, tr, -a_i * ti) + fma(br, NA, -bi * NB);
-      ai += fma(a_r, ti, a_i * tr) + fma(br, NB, bi * NA);
+      // value = a (r.nx)(r.p) + b (nx.p) with b = e^{ikd}(1/d - ik)/d^2,
+      // a = e^{ikd}(k^2 d^2 - 3 + 3ikd)/d^5 and the complex dipole sums
+      // r.p = A + iB, nx.p = NA + iNB; formed as e^{ikd} W with
+      // W = (k^2 d^2 - 3 + 3ikd) U + (1/d - ik) P, U = (r.nx)(A + iB)/d^5,
+      // P = (NA + iNB)/d^2
+      const R kd = k * d;
+      const R fr = fma(kd, kd, R(-3)), fi = R(3) * kd;
+      const R u = rn * (id2 * id2 * ri);
+      const R ur = u * A, ui = u * B, pr = NA * id2, pi = NB * id2;
+      const R wr = fma(fr, ur, fma(-fi, ui, fma(ri, pr, k * pi)));
+      const R wi = fma(fr, ui, fma(fi, ur, fma(ri, pi, -k * pr)));
+      ar = fma(cs, wr, fma(-sn, wi, ar));
+      ai = fma(cs, wi, fma(sn, wr, ai));
     }
   }
 }
