@@ -636,10 +636,10 @@ __device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* 
       const R d = d2 * ri;
       R sn, cs;
       expi_table_eval(d, kT, tab, delta, cs, sn);
-      const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);  // e^{ikd}(1/d - ik)
       const R id2 = ri * ri;
       R hr, hi, gr = R(0), gi = R(0);  // row factor h, column factor g
       if (KIND == ADL) {
+        const R er = fma(cs, ri, k * sn), ei = fma(sn, ri, -k * cs);  // e^{ikd}(1/d - ik)
         const R br = er * id2, bi = ei * id2;
         hr = br * rnt;
         hi = bi * rnt;
@@ -818,7 +818,7 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
 #pragma unroll
           for (int u = 0; u < TPT; ++u) {
             if constexpr (RC::normal) {
-              R unused_r, unused_i;
+              R unused_r = R(0), unused_i = R(0);  // the column half is not formed
               pair_sym_step<PDE, KIND, R, false>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(),
                                                  unused_r, unused_i);
             } else {
