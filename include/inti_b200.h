@@ -198,7 +198,8 @@ int inti_ctx_set_autotune(inti_ctx* ctx, int enable);  /* default on */
  * symmetric in the pair).  The partial sums are reduced in a fixed order, so results
  * are deterministic; they differ from the one-sided kernel's by rounding.
  * The column partials take N^2 / (256 or 512) values; operators whose
- * partials would exceed 8 GB keep the one-sided kernel.  For such operators
+ * partials would exceed a quarter of the device memory free at creation (or
+ * 64 GB) keep the one-sided kernel.  For symmetric operators
  * inti_op_tuning reports the targets per thread and the source blocks per
  * work item.  inti_ctx_set_symmetric(ctx, 0) makes operators created
  * afterwards use the one-sided kernel; inti_op_symmetric returns 1 when an

@@ -207,9 +207,13 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
 }
 
 // Column partials of the symmetric form are nb x n values (N^2/256 at 2
-// targets per thread); above this size (N of about 5e5 real, 3.5e5 complex)
-// the operator keeps the one-sided kernel.
-constexpr double kSymmMaxPartialBytes = 8.0e9;
+// targets per thread).  An operator takes the symmetric form while they fit
+// in a quarter of the device memory free at its creation and 64 GB (N of
+// about 1.4e6 real, 1e6 complex on an empty 180 GB device); larger ones keep
+// the one-sided kernel.  Writing and summing the partials costs O(N^2/256)
+// memory traffic against the O(N^2) pair evaluations they save.
+constexpr double kSymmMaxPartialBytes = 64.0e9;
+constexpr double kSymmMaxFreeShare = 0.25;
 
 void op_symm_configure(inti_op* op, int tpt, int ch) {
   std::vector<int32_t> tab;
@@ -263,7 +267,9 @@ void op_symm_init(inti_op* op) {
   const int64_t bmax = pair_symm_block(4), bmin = pair_symm_block(2);
   const int64_t npad = (n + bmax - 1) / bmax * bmax;  // whole blocks for both node-block sizes
   const double zbytes = (double)((n + bmin - 1) / bmin) * npad * pair_partial_bytes(op->pde, op->precision);
-  if (zbytes > kSymmMaxPartialBytes) return;
+  size_t free_b = 0, total_b = 0;
+  INTI_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  if (zbytes > std::min(kSymmMaxPartialBytes, kSymmMaxFreeShare * (double)free_b)) return;
   op->symm = true;
   op->n_tiles = npad / tile;
   op->packed.ensure((size_t)npad * pair_symm_record_bytes(op->pde, op->kind, op->precision));
