@@ -188,9 +188,9 @@ int inti_op_destroy(inti_op* op);
  * reference (launch configuration). */
 int inti_op_tuning(const inti_op* op, int32_t* targets_per_thread, int32_t* split);
 int inti_ctx_set_autotune(inti_ctx* ctx, int enable);  /* default on */
-/* Square operators (target === source, the same inti_quad) of every 3D
- * kernel (single layer, double layer, combined field, adjoint double layer,
- * hypersingular) use a symmetric pair kernel: each unordered pair's distance,
+/* Square operators (target === source, the same inti_quad) of every kernel
+ * (single layer, double layer, combined field, adjoint double layer,
+ * hypersingular; 3D and the 2D Laplace kernels) use a symmetric pair kernel: each unordered pair's distance,
  * reciprocal square root and phase are computed once and serve both
  * y_i += K(x_i, x_j) w_j x_j and y_j += K(x_j, x_i) w_i x_i (G(x, y) =
  * G(y, x); the double-layer and adjoint-double-layer radial factors are shared

@@ -192,7 +192,7 @@ int pair_tile(int precision);
 // Most source chunks (partial sums per target) of one pair-kernel launch.
 constexpr int kMaxSplit = 256;
 int pair_record_bytes(int pde, int kind, int dim, int precision);
-int pair_symm_record_bytes(int pde, int kind, int precision);  // packed record of the symmetric form
+int pair_symm_record_bytes(int pde, int kind, int dim, int precision);  // packed record of the symmetric form
 // Bytes of one partial accumulator per target per split.
 int pair_partial_bytes(int pde, int precision);
 // Symmetric form: node block of 128*tpt nodes; work items of row blocks
@@ -200,7 +200,7 @@ int pair_partial_bytes(int pde, int precision);
 // out as items (3 x nitems), row pointers (nb + 1), row items (nitems).
 int pair_symm_block(int tpt);
 void pair_symm_plan(int64_t n, int tpt, int ch, std::vector<int32_t>& table, int& nb, int& nitems);
-int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int precision, int64_t n, int tpt);
+int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t n, int tpt);
 // Choose the split for a problem on this device.
 int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,
                     int64_t n, int tpt = 4);

@@ -78,7 +78,7 @@ inti_op* op_clone_precision(const inti_op* op, int precision);
 // problem, else (measure = true, autotuning on, problem large enough) the
 // fastest candidate timed now, else the occupancy heuristic.
 void op_autotune(inti_op* op, bool measure);
-// Square operators (target === source, 3D, every kernel): switch to
+// Square operators (target === source, every kernel, 2D and 3D): switch to
 // the symmetric form when the context allows it and its column partials fit.
 void op_symm_init(inti_op* op);
 void op_symm_configure(inti_op* op, int tpt, int ch);

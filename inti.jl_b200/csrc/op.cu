@@ -261,7 +261,7 @@ void op_set_shard(inti_op* op, int rank, int nranks) {
 void op_symm_init(inti_op* op) {
   inti_ctx* ctx = op->ctx;
   op->symm = false;
-  if (!ctx->symmetric || op->target != op->source || op->dim != 3) return;
+  if (!ctx->symmetric || op->target != op->source) return;
   const int64_t n = op->source->n;
   const int tile = pair_tile(op->precision);
   const int64_t bmax = pair_symm_block(4), bmin = pair_symm_block(2);
@@ -272,9 +272,9 @@ void op_symm_init(inti_op* op) {
   if (zbytes > std::min(kSymmMaxPartialBytes, kSymmMaxFreeShare * (double)free_b)) return;
   op->symm = true;
   op->n_tiles = npad / tile;
-  op->packed.ensure((size_t)npad * pair_symm_record_bytes(op->pde, op->kind, op->precision));
+  op->packed.ensure((size_t)npad * pair_symm_record_bytes(op->pde, op->kind, op->dim, op->precision));
   const int tpt = 2;
-  op_symm_configure(op, tpt, pair_symm_default_ch(ctx, op->pde, op->kind, op->precision, n, tpt));
+  op_symm_configure(op, tpt, pair_symm_default_ch(ctx, op->pde, op->kind, op->dim, op->precision, n, tpt));
 }
 
 // Problems below this many pairs keep the heuristic shape (a timing pass
@@ -299,7 +299,7 @@ void op_autotune(inti_op* op, bool measure) {
     if (!measure || !ctx->autotune || (double)m * (double)n < kTuneMinPairs) return;
     std::vector<std::pair<int, int>> cand;
     for (int tpt : {4, 2}) {
-      const int c0 = pair_symm_default_ch(ctx, op->pde, op->kind, op->precision, n, tpt);
+      const int c0 = pair_symm_default_ch(ctx, op->pde, op->kind, op->dim, op->precision, n, tpt);
       for (int ch : {c0, std::max(1, c0 / 2), 2 * c0})
         if (std::find(cand.begin(), cand.end(), std::make_pair(tpt, ch)) == cand.end()) cand.emplace_back(tpt, ch);
     }
@@ -418,7 +418,7 @@ void op_prepare_transpose(inti_op* op) {
   }
   op->tpacked.ensure((size_t)op->tn_tiles * tile * pair_record_bytes(op->pde, kt, op->dim, op->precision));
   if (op->symm)  // the symmetric form packs all npad = n_tiles * tile nodes in its own records
-    op->tpacked.ensure((size_t)op->n_tiles * tile * pair_symm_record_bytes(op->pde, kt, op->precision));
+    op->tpacked.ensure((size_t)op->n_tiles * tile * pair_symm_record_bytes(op->pde, kt, op->dim, op->precision));
   op->tpartial.ensure((size_t)op->tsplit * m2 * pair_partial_bytes(op->pde, op->precision));
   std::vector<double> ones((size_t)std::max<int64_t>(n2, 1), 1.0);
   op->tones.ensure(sizeof(double) * ones.size());

@@ -522,8 +522,8 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
 
 // ---------------------------------------------------------------------------
 // Symmetric form for square operators (the target set is the source set),
-// every 3D kernel: single layer, double layer, combined field, adjoint double
-// layer and hypersingular.
+// every kernel: single layer, double layer, combined field (3D), adjoint
+// double layer and hypersingular, in 3D and for the 2D Laplace kernels.
 //
 // Every kernel value of an unordered pair {a, b} serves both products:
 //   SL: G(x_a, x_b) = G(x_b, x_a);
@@ -557,43 +557,47 @@ struct SymArgs {
 // Records of the symmetric form.  SL, DL and CF use the layouts of Rec.  The
 // adjoint double layer and the hypersingular kernel take the normal of the
 // target, so both ends of a pair need their normal and their charge:
-//   x y z n_x n_y n_z q [0]     (Laplace)
-//   x y z n_x n_y n_z qr qi     (Helmholtz)
-// with q = w sigma; eight elements, 64 bytes (FP64) or 32 bytes (FP32).
-template <int PDE, int KIND, class R>
+//   x [DIM] | n [DIM] | q            (Laplace; 3D: 8 elements with one pad,
+//                                     2D: 6 (FP64) or 8 (FP32))
+//   x y z | n_x n_y n_z | qr qi      (Helmholtz: 8 elements)
+// with q = w sigma; padded to a multiple of 16 bytes.
+template <int PDE, int KIND, int DIM, class R>
 struct SymRec {
   static constexpr bool normal = (KIND == ADL || KIND == HS);
   static constexpr bool cplx = (PDE == HELMHOLTZ);
-  static constexpr int used = normal ? (cplx ? 8 : 7) : Rec<PDE, KIND, 3, R>::used;
-  static constexpr int n = normal ? 8 : Rec<PDE, KIND, 3, R>::n;
+  static constexpr int align = 16 / sizeof(R);
+  static constexpr int nused = 2 * DIM + (cplx ? 2 : 1);
+  static constexpr int used = normal ? nused : Rec<PDE, KIND, DIM, R>::used;
+  static constexpr int n = normal ? (nused + align - 1) / align * align : Rec<PDE, KIND, DIM, R>::n;
 };
 
-template <int PDE, class R>
+template <int PDE, int DIM, class R>
 __global__ void pack_sym_normal(int64_t n, int64_t npad, const double* __restrict__ xs,
                                 const double* __restrict__ ns, const double* __restrict__ w,
                                 const double* __restrict__ sigma, R* __restrict__ out) {
+  constexpr int NR = SymRec<PDE, HS, DIM, R>::n;
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= npad) return;
-  R rec[8];
+  R rec[NR];
 #pragma unroll
-  for (int c = 0; c < 8; ++c) rec[c] = R(0);
+  for (int c = 0; c < NR; ++c) rec[c] = R(0);
   if (j < n) {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      rec[c] = R(xs[3 * j + c]);
-      rec[3 + c] = R(ns[3 * j + c]);
+    for (int c = 0; c < DIM; ++c) {
+      rec[c] = R(xs[DIM * j + c]);
+      rec[DIM + c] = R(ns[DIM * j + c]);
     }
     const double wj = w[j];
     if (PDE == HELMHOLTZ) {
-      rec[6] = R(wj * sigma[2 * j]);
-      rec[7] = R(wj * sigma[2 * j + 1]);
+      rec[2 * DIM] = R(wj * sigma[2 * j]);
+      rec[2 * DIM + 1] = R(wj * sigma[2 * j + 1]);
     } else {
-      rec[6] = R(wj * sigma[j]);
+      rec[2 * DIM] = R(wj * sigma[j]);
     }
   }
-  R* o = out + j * 8;
+  R* o = out + j * NR;
 #pragma unroll
-  for (int c = 0; c < 8; ++c) o[c] = rec[c];
+  for (int c = 0; c < NR; ++c) o[c] = rec[c];
 }
 
 // Both products of one unordered pair: y_t += K(x_t, x_s) c_s and
@@ -607,10 +611,47 @@ __global__ void pack_sym_normal(int64_t n, int64_t npad, const double* __restric
 //   HS : K(x_t, x_s) q_s = h q_s and K(x_s, x_t) q_t = h q_t with
 //        h = a (r.n_t)(r.n_s) + b (n_t.n_s), a and b functions of d alone
 //        (Laplace: a = -3/d^5, b = 1/d^3), so h is symmetric in the pair.
-template <int PDE, int KIND, class R, bool COL = true>
+// 2D Laplace (kernel constants in the epilogue as in pair_step):
+//   SL : log(d^2), symmetric;   DL : (r.p)/d^2, column -(r.p_t)/d^2;
+//   ADL: (r.n_t) q/d^2, column -(r.n_s) q_t/d^2;
+//   HS : h = (n_t.n_s - 2 (r.n_t)(r.n_s)/d^2)/d^2, symmetric.
+template <int KIND, class R, bool COL>
+__device__ __forceinline__ void pair_sym_step_2d(const R* __restrict__ t, const R* __restrict__ s, R& ar,
+                                                 R& zr) {
+  using M = MathOps<R>;
+  const R r0 = t[0] - s[0], r1 = t[1] - s[1];
+  const R d2 = fma(r1, r1, r0 * r0);
+  const bool keep = M::keep(d2);
+  if (KIND == SL) {
+    const R l = keep ? M::lg(d2) : R(0);
+    ar = fma(l, s[2], ar);
+    if (COL) zr = fma(l, t[2], zr);
+    return;
+  }
+  const R id2 = keep ? R(1) / d2 : R(0);
+  if (KIND == DL) {
+    ar = fma(fma(r1, s[3], r0 * s[2]), id2, ar);
+    if (COL) zr = fma(-fma(r1, t[3], r0 * t[2]), id2, zr);
+  } else if (KIND == ADL) {
+    ar = fma(fma(r1, t[3], r0 * t[2]) * id2, s[4], ar);
+    if (COL) zr = fma(-fma(r1, s[3], r0 * s[2]) * id2, t[4], zr);
+  } else if (KIND == HS) {
+    const R rnt = fma(r1, t[3], r0 * t[2]), rns = fma(r1, s[3], r0 * s[2]);
+    const R nn = fma(t[3], s[3], t[2] * s[2]);
+    const R h = fma(R(-2) * rnt * rns, id2, nn) * id2;
+    ar = fma(h, s[4], ar);
+    if (COL) zr = fma(h, t[4], zr);
+  }
+}
+
+template <int PDE, int KIND, int DIM, class R, bool COL = true>
 __device__ __forceinline__ void pair_sym_step(const R* __restrict__ t, const R* __restrict__ s, R kT, R delta, R k,
                                               const typename MathOps<R>::R2* __restrict__ tab, R& ar, R& ai,
                                               R& zr, R& zi) {
+  if constexpr (DIM == 2) {
+    pair_sym_step_2d<KIND, R, COL>(t, s, ar, zr);
+    return;
+  }
   using M = MathOps<R>;
   const R r0 = t[0] - s[0], r1 = t[1] - s[1], r2 = t[2] - s[2];
   const R d2 = fma(r2, r2, fma(r1, r1, r0 * r0));
@@ -745,9 +786,9 @@ __device__ __forceinline__ void put_partial(double2* p, double r, double i) { *p
 __device__ __forceinline__ void put_partial(float2* p, float r, float) { *p = make_float2(r, 0.f); }
 __device__ __forceinline__ void put_partial(float4* p, float r, float i) { *p = make_float4(r, 0.f, i, 0.f); }
 
-template <int PDE, int KIND, class R, int TILE, int TPT>
+template <int PDE, int KIND, int DIM, class R, int TILE, int TPT>
 __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
-  using RC = SymRec<PDE, KIND, R>;
+  using RC = SymRec<PDE, KIND, DIM, R>;
   constexpr bool CPLX = RC::cplx;
   using P = typename PartialT<R, CPLX>::T;
   using R2 = typename MathOps<R>::R2;
@@ -819,14 +860,13 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
           for (int u = 0; u < TPT; ++u) {
             if constexpr (RC::normal) {
               R unused_r = R(0), unused_i = R(0);  // the column half is not formed
-              pair_sym_step<PDE, KIND, R, false>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(),
-                                                 unused_r, unused_i);
+              pair_sym_step<PDE, KIND, DIM, R, false>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(),
+                                                      unused_r, unused_i);
             } else {
-              Target<R, 3, false> tt;
-              tt.x[0] = tg[u][0];
-              tt.x[1] = tg[u][1];
-              tt.x[2] = tg[u][2];
-              pair_step<PDE, KIND, 3, R>(tt, rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
+              Target<R, DIM, false> tt;
+#pragma unroll
+              for (int c = 0; c < DIM; ++c) tt.x[c] = tg[u][c];
+              pair_step<PDE, KIND, DIM, R>(tt, rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi());
             }
           }
         }
@@ -845,7 +885,8 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
             zr[v] = zi[v] = R(0);
 #pragma unroll
             for (int u = 0; u < TPT; ++u)
-              pair_sym_step<PDE, KIND, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(), zr[v], zi[v]);
+              pair_sym_step<PDE, KIND, DIM, R>(tg[u], rec, kT, delta, k, tab, acc[u].gr(), acc[u].gi(), zr[v],
+                                               zi[v]);
           }
           const R sr = warp_sum4(zr, lane);
           const R si = CPLX ? warp_sum4(zi, lane) : R(0);
@@ -1113,19 +1154,23 @@ template <class T, class R>
 static size_t symm_smem() {
   constexpr int TILE = std::is_same<R, float>::value ? kTile32 : kTile64;
   const size_t table = T::pde == HELMHOLTZ ? (size_t)kExpiTable * 2 * sizeof(R) : 0;
-  return 2 * (size_t)TILE * SymRec<T::pde, T::kind, R>::n * sizeof(R) + table +
+  return 2 * (size_t)TILE * SymRec<T::pde, T::kind, T::dim, R>::n * sizeof(R) + table +
          2 * (size_t)(kBlock / 32) * TILE * 2 * sizeof(R);
 }
 
 template <class T>
 constexpr bool symm_kind() {
-  return T::dim == 3;
+  return true;  // every kernel of the dispatch (3D, and 2D Laplace)
 }
 
-int pair_symm_record_bytes(int pde, int kind, int precision) {
-  const bool normal = kind == ADL || kind == HS;
-  if (!normal) return pair_record_bytes(pde, kind, 3, precision);
-  return 8 * (precision == INTI_FP32C ? 4 : 8);
+int pair_symm_record_bytes(int pde, int kind, int dim, int precision) {
+  int bytes = 0;
+  dispatch(pde, kind, dim, [&](auto tag) {
+    using T = decltype(tag);
+    bytes = precision == INTI_FP32C ? SymRec<T::pde, T::kind, T::dim, float>::n * 4
+                                    : SymRec<T::pde, T::kind, T::dim, double>::n * 8;
+  });
+  return bytes;
 }
 
 int pair_symm_block(int tpt) { return kBlock * tpt; }
@@ -1156,20 +1201,20 @@ void pair_symm_plan(int64_t n, int tpt, int ch, std::vector<int32_t>& table, int
   for (int q = 0; q < nitems; ++q) rowitems[fill[it[q][0]]++] = q;
 }
 
-int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int precision, int64_t n, int tpt) {
+int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t n, int tpt) {
   int occ = 1;
-  dispatch(pde, kind, 3, [&](auto tag) {
+  dispatch(pde, kind, dim, [&](auto tag) {
     using T = decltype(tag);
     if constexpr (symm_kind<T>()) {
       const void* fn;
       size_t sm;
       if (precision == INTI_FP32C) {
-        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, float, kTile32, 2>
-                      : (const void*)&pair_symm<T::pde, T::kind, float, kTile32, 4>;
+        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, T::dim, float, kTile32, 2>
+                      : (const void*)&pair_symm<T::pde, T::kind, T::dim, float, kTile32, 4>;
         sm = symm_smem<T, float>();
       } else {
-        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, double, kTile64, 2>
-                      : (const void*)&pair_symm<T::pde, T::kind, double, kTile64, 4>;
+        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, T::dim, double, kTile64, 2>
+                      : (const void*)&pair_symm<T::pde, T::kind, T::dim, double, kTile64, 4>;
         sm = symm_smem<T, double>();
       }
       INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -1199,8 +1244,9 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
         ProfScope ps(ctx, "pack");
         const unsigned gp = (unsigned)((npad + pb - 1) / pb);
         if (L.symm && (T::kind == ADL || T::kind == HS))
-          pack_sym_normal<T::pde, R><<<gp, pb, 0, ctx->stream>>>(L.n, npad, L.scoords, L.snormals, L.sweights,
-                                                                 L.x, static_cast<R*>(L.packed));
+          pack_sym_normal<T::pde, T::dim, R><<<gp, pb, 0, ctx->stream>>>(L.n, npad, L.scoords, L.snormals,
+                                                                         L.sweights, L.x,
+                                                                         static_cast<R*>(L.packed));
         else
           pack_sources<T::pde, T::kind, T::dim, R><<<gp, pb, 0, ctx->stream>>>(
               L.n, npad, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
@@ -1221,7 +1267,8 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
           a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
           a.err = L.err_flag;
           const size_t sm = symm_smem<T, R>();
-          auto fn = L.tpt == 2 ? &pair_symm<T::pde, T::kind, R, TILE, 2> : &pair_symm<T::pde, T::kind, R, TILE, 4>;
+          auto fn = L.tpt == 2 ? &pair_symm<T::pde, T::kind, T::dim, R, TILE, 2>
+                               : &pair_symm<T::pde, T::kind, T::dim, R, TILE, 4>;
           INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
           ProfScope pp(ctx, "pair");
           const int grid = L.sym_launch ? L.sym_launch_items : L.sym_nitems;

@@ -3,8 +3,8 @@ unordered pair is evaluated once for both products.  Checked against the
 one-sided kernel (a context with the symmetric form off) and the oracle, on
 surfaces of many node blocks with a ragged last block, for the single layer,
 double layer, combined field, adjoint double layer and hypersingular kernel,
-Laplace and Helmholtz, FP64 and FP32C, with the DIM correction, alpha/beta
-and repeated applies."""
+Laplace (3D and 2D) and Helmholtz, FP64 and FP32C, with the DIM correction,
+alpha/beta and repeated applies."""
 import numpy as np
 import pytest
 
@@ -155,3 +155,53 @@ def test_symmetric_edge_sizes(ctx, n, pde):
             assert np.all(got == 0)  # the self pair is excluded
         else:
             assert relerr(got, ref) < 1e-12
+
+
+# FP32C against the FP64 oracle on the 4,500-node kite: on a curve r.n is
+# O(d^2) between neighbouring nodes and cancels in FP32 coordinates, so even
+# exact sums of the FP32 pair values (a numpy restatement: FP32 coordinates,
+# products and quotients, FP64 sums) are off by 9.6e-4 (DL), 6.9e-4 (ADL),
+# 1.4e-4 (HS) and 2.9e-7 (SL); the bounds are about twice those floors.
+FP32_2D_TOL = {"SL": 5e-5, "DL": 2e-3, "ADL": 2e-3, "HS": 5e-4}
+
+
+@pytest.mark.parametrize("kname", ["SL", "DL", "ADL", "HS"])
+@pytest.mark.parametrize("prec", ["fp64", "fp32c"])
+def test_symmetric_2d_laplace(ctx, one_sided, kname, prec):
+    """2D Laplace kernels on the symmetric form (log(d^2) once per unordered
+    pair for the single layer): against the one-sided kernel and the oracle,
+    and the transposes of the two forms against each other."""
+    q = inti.kite_quadrature(900, 9)  # 4,500 nodes: 9 blocks of 512, the last ragged
+    K, okind = KERNELS[kname]
+    A = inti.GpuOperator(K(inti.Laplace(dim=2)), q, q, None, prec, ctx)
+    B = inti.GpuOperator(K(inti.Laplace(dim=2)), q, q, None, prec, one_sided)
+    assert A.tuning["symmetric"] and not B.tuning["symmetric"]
+    x = density(len(q), False, 21)
+    ya, yb = A @ x, B @ x
+    ref = oracle_apply(O.LAPLACE, okind, 0.0, q, q, x)
+    tol = 1e-12 if prec == "fp64" else FP32_2D_TOL[kname]
+    assert relerr(ya, ref) < tol and relerr(yb, ref) < tol
+    if prec == "fp64":
+        assert relerr(ya, yb) < 1e-13
+        assert relerr(A.rmatvec(x), B.rmatvec(x)) < 1e-13
+    else:  # the same FP32 pair values (r_ts = -r_st exactly), summed in another order
+        assert relerr(ya, yb) < 1e-4
+    assert np.array_equal(A @ x, ya)
+
+
+@pytest.mark.parametrize("n", [1, 7, 257, 513])
+def test_symmetric_2d_edge_sizes(ctx, n):
+    r = np.random.default_rng(100 + n)
+    X = r.standard_normal((n, 2))
+    N = r.standard_normal((n, 2))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    q = inti.Quadrature(X, N, r.uniform(0.5, 1.5, n), 0)
+    x = density(n, False, 3)
+    for K, okind in KERNELS.values():
+        A = inti.GpuOperator(K(inti.Laplace(dim=2)), q, q, None, "fp64", ctx)
+        assert A.tuning["symmetric"]
+        got = A @ x
+        if n == 1:
+            assert np.all(got == 0)
+        else:
+            assert relerr(got, oracle_apply(O.LAPLACE, okind, 0.0, q, q, x)) < 1e-12
