@@ -33,16 +33,23 @@ def test_row_blocks_reproduce_full_product(ctx, case, world):
     assert relerr(np.concatenate(parts), full) < 1e-13
 
 
-@pytest.mark.parametrize("pde", ["helmholtz", "laplace"])
+@pytest.mark.parametrize("pde", ["helmholtz", "laplace", "laplace2d"])
+@pytest.mark.parametrize("kname", ["DL", "HS"])
 @pytest.mark.parametrize("world", [2, 3])
-def test_item_shards_sum_to_the_full_product(ctx, pde, world):
+def test_item_shards_sum_to_the_full_product(ctx, pde, kname, world):
     """Item shards of a symmetric operator (inti_op_set_shard): the ranks'
     partial products over all rows, summed (the all-reduce of one process
-    per GPU), give alpha*(A + C)x + beta*y; rank 0 carries C and beta*y."""
-    q = G.ellipsoid_quadrature(8, 5)  # 3,456 nodes: several node blocks
-    op = inti.Helmholtz(k=6.0, dim=3) if pde == "helmholtz" else inti.Laplace(dim=3)
-    dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
-    A = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, "fp64", ctx)
+    per GPU), give alpha*(A + C)x + beta*y; rank 0 carries C and beta*y.
+    Double layer and hypersingular kernel, 3D and 2D."""
+    if pde == "laplace2d":
+        q, op = G.kite_quadrature(700, 9), inti.Laplace(dim=2)  # 3,500 nodes
+    else:
+        q = G.ellipsoid_quadrature(8, 5)  # 3,456 nodes: several node blocks
+        op = inti.Helmholtz(k=6.0, dim=3) if pde == "helmholtz" else inti.Laplace(dim=3)
+    hs = kname == "HS"
+    dS, dD = inti.bdim_correction(op, q, q, derivative=hs, ctx=ctx)
+    K = inti.HyperSingularKernel if hs else inti.DoubleLayerKernel
+    A = inti.GpuOperator(K(op), q, q, dD, "fp64", ctx)
     assert A.tuning["symmetric"]
     cplx = A.is_complex
     x, y0 = density(len(q), cplx, 11), density(len(q), cplx, 12)
