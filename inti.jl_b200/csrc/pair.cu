@@ -925,6 +925,211 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
   for (int u = 0; u < TPT; ++u) store_partial(out + u * kBlock + tid, acc[u]);
 }
 
+// ---------------------------------------------------------------------------
+// Paired-FP32 form of the symmetric kernel for the FP32C Laplace single
+// layer, double layer and combined field (3D).  The FP32 kernels are bound by
+// instruction issue, not by the FP32 pipe; sm_100 issues two FP32 lanes per
+// instruction (__fadd2_rn, __fmul2_rn, __ffma2_rn).  Each thread holds its
+// targets in pairs (u, u + 1) as float2, and the records carry every value
+// twice (x x y y z z | p_x p_x p_y p_y p_z p_z | q q), so one 16-byte shared
+// load yields two ready operand pairs.  Per lane the arithmetic is that of
+// pair_sym_step (the reciprocal square root and the self-pair test stay per
+// lane); the column sum over the thread's targets is formed per lane and the
+// two lanes added, so results differ from the scalar kernel by rounding only.
+// ---------------------------------------------------------------------------
+template <int KIND>
+struct RecX2 {
+  static constexpr int vals = (KIND == SL ? 4 : KIND == DL ? 6 : 7);  // x y z [p] [q]
+  static constexpr int n = (2 * vals + 3) / 4 * 4;                      // floats per record
+};
+
+template <int KIND>
+__global__ void pack_sources_x2(int64_t n, int64_t npad, const double* __restrict__ xs,
+                                const double* __restrict__ ns, const double* __restrict__ w,
+                                const double* __restrict__ sigma, double c1, double c2,
+                                float* __restrict__ out) {
+  constexpr int NR = RecX2<KIND>::n;
+  const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (j >= npad) return;
+  float v[RecX2<KIND>::vals];
+#pragma unroll
+  for (int c = 0; c < RecX2<KIND>::vals; ++c) v[c] = 0.f;
+  if (j < n) {
+    v[0] = (float)xs[3 * j];
+    v[1] = (float)xs[3 * j + 1];
+    v[2] = (float)xs[3 * j + 2];
+    const double q = w[j] * sigma[j];
+    if (KIND == SL) {
+      v[3] = (float)q;
+    } else {
+      const double qd = KIND == CF ? c1 * q : q;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) v[3 + c] = (float)(qd * ns[3 * j + c]);
+      if (KIND == CF) v[6] = (float)(c2 * q);
+    }
+  }
+  float* o = out + j * NR;
+#pragma unroll
+  for (int c = 0; c < NR; ++c) o[c] = c / 2 < RecX2<KIND>::vals ? v[c / 2] : 0.f;
+}
+
+// One source against a pair of targets: the row products into (ar.x, ar.y);
+// with COL the column terms into zq (ri q_t, CF) and zd (r.p_t ri^3).
+template <int KIND, bool COL>
+__device__ __forceinline__ void pair_x2_step(const float2 (&t)[RecX2<KIND>::vals], const float2* __restrict__ s,
+                                             float2& ar, float2& zq, float2& zd) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 r0 = __ffma2_rn(s[0], m1, t[0]);  // t - s, one rounding per lane
+  const float2 r1 = __ffma2_rn(s[1], m1, t[1]);
+  const float2 r2 = __ffma2_rn(s[2], m1, t[2]);
+  const float2 d2 = __ffma2_rn(r2, r2, __ffma2_rn(r1, r1, __fmul2_rn(r0, r0)));
+  float2 ri;
+  ri.x = d2.x > 1.0e-28f ? rsqrt_fast(d2.x) : 0.f;
+  ri.y = d2.y > 1.0e-28f ? rsqrt_fast(d2.y) : 0.f;
+  if (KIND == SL) {
+    ar = __ffma2_rn(ri, s[3], ar);
+    if (COL) zq = __ffma2_rn(ri, t[3], zq);
+    return;
+  }
+  const float2 ri3 = __fmul2_rn(__fmul2_rn(ri, ri), ri);
+  const float2 rs = __ffma2_rn(r2, s[5], __ffma2_rn(r1, s[4], __fmul2_rn(r0, s[3])));
+  if (KIND == CF) {
+    ar = __ffma2_rn(ri, s[6], __ffma2_rn(rs, ri3, ar));
+  } else {
+    ar = __ffma2_rn(rs, ri3, ar);
+  }
+  if (COL) {
+    const float2 rt = __ffma2_rn(r2, t[5], __ffma2_rn(r1, t[4], __fmul2_rn(r0, t[3])));
+    zd = __ffma2_rn(rt, ri3, zd);
+    if (KIND == CF) zq = __ffma2_rn(ri, t[6], zq);
+  }
+}
+
+template <int KIND, int TPT>
+__global__ void __launch_bounds__(kBlock) pair_symm_x2(SymArgs a) {
+  constexpr int TILE = kTile32;
+  constexpr int NR = RecX2<KIND>::n, NV = RecX2<KIND>::vals;
+  constexpr int BT = kBlock * TPT, NP = TPT / 2;
+  static_assert(TPT % 2 == 0 && BT % TILE == 0, "target pairs, whole source tiles per node block");
+  constexpr int TPB = BT / TILE;
+  constexpr int kWarps = kBlock / 32;
+  constexpr uint32_t kStageBytes = TILE * NR * sizeof(float);
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  float* stage0 = reinterpret_cast<float*>(smem_raw);
+  float* stage1 = reinterpret_cast<float*>(smem_raw + kStageBytes);
+  float* zsm = reinterpret_cast<float*>(smem_raw + 2 * kStageBytes);
+  __shared__ __align__(8) uint64_t full[2];
+
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int I = a.items[3 * blockIdx.x], J0 = a.items[3 * blockIdx.x + 1], J1 = a.items[3 * blockIdx.x + 2];
+  const float* src = static_cast<const float*>(a.packed);
+  float2 tg[NP][NV];  // (target 2p, target 2p + 1), value c
+  float2 g[NP];       // group sums per lane
+  float hr[TPT], lr[TPT];
+#pragma unroll
+  for (int p = 0; p < NP; ++p) {
+    const int64_t i0 = (int64_t)I * BT + (2 * p) * kBlock + tid, i1 = i0 + kBlock;
+#pragma unroll
+    for (int c = 0; c < NV; ++c) tg[p][c] = make_float2(src[i0 * NR + 2 * c], src[i1 * NR + 2 * c]);
+    g[p] = make_float2(0.f, 0.f);
+  }
+#pragma unroll
+  for (int u = 0; u < TPT; ++u) hr[u] = lr[u] = 0.f;
+  auto fold = [&]() {
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      two_sum_fold(hr[2 * p], lr[2 * p], g[p].x);
+      two_sum_fold(hr[2 * p + 1], lr[2 * p + 1], g[p].y);
+    }
+  };
+  if (tid == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int64_t t0 = (int64_t)J0 * TPB, t1 = (int64_t)J1 * TPB;
+  int64_t issued = t0;
+  if (tid == 0) {
+    for (int s = 0; s < 2 && issued < t1; ++s, ++issued) {
+      mbar_arrive_expect_tx(&full[s], kStageBytes);
+      bulk_copy_g2s(s ? stage1 : stage0, src + issued * TILE * NR, kStageBytes, &full[s]);
+    }
+  }
+  for (int64_t t = t0; t < t1; ++t) {
+    const int st = (int)((t - t0) & 1);
+    const uint32_t parity = (uint32_t)(((t - t0) >> 1) & 1);
+    const bool ok = mbar_wait_bounded(&full[st], parity);
+    if (!__syncthreads_and(ok)) {
+      if (tid == 0) {
+        atomicExch(a.err, kErrWaitTimeout);
+        for (int64_t q = t + 1; q < issued; ++q)
+          mbar_wait_bounded(&full[(q - t0) & 1], (uint32_t)(((q - t0) >> 1) & 1));
+      }
+      return;
+    }
+    const float* sp = st ? stage1 : stage0;
+    const bool diag = t / TPB == I;
+    float* zb = zsm + st * (kWarps * TILE * 2);
+    if (diag) {
+#pragma unroll 1
+      for (int gq = 0; gq < TILE; gq += kGroup) {
+#pragma unroll 2
+        for (int s = 0; s < kGroup; ++s) {
+          const float2* rec = reinterpret_cast<const float2*>(sp + (gq + s) * NR);
+          float2 zq, zd;  // not formed
+#pragma unroll
+          for (int p = 0; p < NP; ++p) pair_x2_step<KIND, false>(tg[p], rec, g[p], zq, zd);
+        }
+        fold();
+      }
+    } else {
+#pragma unroll 1
+      for (int gq = 0; gq < TILE; gq += kGroup) {
+#pragma unroll 1
+        for (int s = 0; s < kGroup; s += 4) {
+          float zr[4];
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const float2* rec = reinterpret_cast<const float2*>(sp + (gq + s + v) * NR);
+            float2 zq = make_float2(0.f, 0.f), zd = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int p = 0; p < NP; ++p) pair_x2_step<KIND, true>(tg[p], rec, g[p], zq, zd);
+            // K(x_s, x_t) c_t: SL and CF ri q_t, DL and CF -(r.p_t) ri^3
+            zr[v] = KIND == DL ? -(zd.x + zd.y) : (KIND == SL ? zq.x + zq.y : (zq.x + zq.y) - (zd.x + zd.y));
+          }
+          const float sr = warp_sum4(zr, lane);
+          if ((lane & 7) == 0) {
+            const int v = lane >> 3;
+            zb[(warp * TILE + gq + s + v) * 2] = sr;
+            zb[(warp * TILE + gq + s + v) * 2 + 1] = 0.f;
+          }
+        }
+        fold();
+      }
+    }
+    __syncthreads();  // the stage is read and this tile's column sums are in zb
+    if (!diag) {
+      float2* zp = static_cast<float2*>(a.zpart) + (int64_t)I * a.npad + t * TILE;
+      for (int s = tid; s < TILE; s += kBlock) {
+        float vr = zb[s * 2];
+#pragma unroll
+        for (int w = 1; w < kWarps; ++w) vr += zb[(w * TILE + s) * 2];
+        zp[s] = make_float2(vr, 0.f);
+      }
+    }
+    if (tid == 0 && issued < t1) {
+      fence_proxy_async_smem();
+      mbar_arrive_expect_tx(&full[st], kStageBytes);
+      bulk_copy_g2s(st ? stage1 : stage0, src + issued * TILE * NR, kStageBytes, &full[st]);
+      ++issued;
+    }
+  }
+  float2* out = static_cast<float2*>(a.ypart) + (int64_t)(a.ids ? a.ids[blockIdx.x] : (int)blockIdx.x) * BT;
+#pragma unroll
+  for (int u = 0; u < TPT; ++u) out[u * kBlock + tid] = make_float2(hr[u], lr[u]);
+}
+
 // Row sums of the symmetric form: the item partials of row block B and the
 // column partials of the row blocks above.
 struct SymEpi {
@@ -1163,12 +1368,27 @@ constexpr bool symm_kind() {
   return true;  // every kernel of the dispatch (3D, and 2D Laplace)
 }
 
+// FP32 Laplace SL/DL/CF in 3D run the paired-FP32 symmetric kernel.
+template <class T, class R>
+constexpr bool symm_x2() {
+  return std::is_same<R, float>::value && T::pde == LAPLACE && T::dim == 3 &&
+         (T::kind == SL || T::kind == DL || T::kind == CF);
+}
+
+template <class T>
+static size_t symm_x2_smem() {
+  return 2 * (size_t)kTile32 * RecX2<T::kind>::n * sizeof(float) + 2 * (size_t)(kBlock / 32) * kTile32 * 2 * sizeof(float);
+}
+
 int pair_symm_record_bytes(int pde, int kind, int dim, int precision) {
   int bytes = 0;
   dispatch(pde, kind, dim, [&](auto tag) {
     using T = decltype(tag);
-    bytes = precision == INTI_FP32C ? SymRec<T::pde, T::kind, T::dim, float>::n * 4
-                                    : SymRec<T::pde, T::kind, T::dim, double>::n * 8;
+    if constexpr (symm_x2<T, float>())
+      bytes = precision == INTI_FP32C ? RecX2<T::kind>::n * 4 : SymRec<T::pde, T::kind, T::dim, double>::n * 8;
+    else
+      bytes = precision == INTI_FP32C ? SymRec<T::pde, T::kind, T::dim, float>::n * 4
+                                      : SymRec<T::pde, T::kind, T::dim, double>::n * 8;
   });
   return bytes;
 }
@@ -1209,9 +1429,14 @@ int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int dim, int pr
       const void* fn;
       size_t sm;
       if (precision == INTI_FP32C) {
-        fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, T::dim, float, kTile32, 2>
-                      : (const void*)&pair_symm<T::pde, T::kind, T::dim, float, kTile32, 4>;
-        sm = symm_smem<T, float>();
+        if constexpr (symm_x2<T, float>()) {
+          fn = tpt == 2 ? (const void*)&pair_symm_x2<T::kind, 2> : (const void*)&pair_symm_x2<T::kind, 4>;
+          sm = symm_x2_smem<T>();
+        } else {
+          fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, T::dim, float, kTile32, 2>
+                        : (const void*)&pair_symm<T::pde, T::kind, T::dim, float, kTile32, 4>;
+          sm = symm_smem<T, float>();
+        }
       } else {
         fn = tpt == 2 ? (const void*)&pair_symm<T::pde, T::kind, T::dim, double, kTile64, 2>
                       : (const void*)&pair_symm<T::pde, T::kind, T::dim, double, kTile64, 4>;
@@ -1243,14 +1468,24 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       {
         ProfScope ps(ctx, "pack");
         const unsigned gp = (unsigned)((npad + pb - 1) / pb);
-        if (L.symm && (T::kind == ADL || T::kind == HS))
+        bool done = false;
+        if constexpr (symm_x2<T, R>()) {
+          if (L.symm) {
+            pack_sources_x2<T::kind><<<gp, pb, 0, ctx->stream>>>(L.n, npad, L.scoords, L.snormals, L.sweights, L.x,
+                                                               L.c1[0], L.c2[0], static_cast<float*>(L.packed));
+            done = true;
+          }
+        }
+        if (done) {
+        } else if (L.symm && (T::kind == ADL || T::kind == HS)) {
           pack_sym_normal<T::pde, T::dim, R><<<gp, pb, 0, ctx->stream>>>(L.n, npad, L.scoords, L.snormals,
                                                                          L.sweights, L.x,
                                                                          static_cast<R*>(L.packed));
-        else
+        } else {
           pack_sources<T::pde, T::kind, T::dim, R><<<gp, pb, 0, ctx->stream>>>(
               L.n, npad, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
               make_double2(L.c2[0], L.c2[1]), static_cast<R*>(L.packed));
+        }
       }
       if constexpr (symm_kind<T>()) {
         if (L.symm) {
@@ -1266,9 +1501,16 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
           a.delta = 2 * kPi / kExpiTable;
           a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
           a.err = L.err_flag;
-          const size_t sm = symm_smem<T, R>();
-          auto fn = L.tpt == 2 ? &pair_symm<T::pde, T::kind, T::dim, R, TILE, 2>
-                               : &pair_symm<T::pde, T::kind, T::dim, R, TILE, 4>;
+          size_t sm;
+          void (*fn)(SymArgs);
+          if constexpr (symm_x2<T, R>()) {
+            sm = symm_x2_smem<T>();
+            fn = L.tpt == 2 ? &pair_symm_x2<T::kind, 2> : &pair_symm_x2<T::kind, 4>;
+          } else {
+            sm = symm_smem<T, R>();
+            fn = L.tpt == 2 ? &pair_symm<T::pde, T::kind, T::dim, R, TILE, 2>
+                            : &pair_symm<T::pde, T::kind, T::dim, R, TILE, 4>;
+          }
           INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
           ProfScope pp(ctx, "pair");
           const int grid = L.sym_launch ? L.sym_launch_items : L.sym_nitems;
