@@ -236,6 +236,59 @@ __device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, con
   return make_float2(fmaf(cs, br, -sn * bi), fmaf(cs, bi, sn * br));
 }
 
+// tc_kernel for the two target rows of a generator thread at once: the
+// arithmetic runs on the paired FP32 instructions of sm_100 (two lanes per
+// issue slot); the reciprocal square root, the sine and the cosine stay per
+// lane.  Each lane performs tc_kernel's operations in the same order, so the
+// values are the same bit for bit.
+template <int KIND>
+__device__ __forceinline__ void tc_kernel_x2(const float2 (&x)[3], const float4 s0, const float2 s1,
+                                             const TcConst& c, float2& k0, float2& k1) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float2 r0 = __ffma2_rn(make_float2(s0.x, s0.x), m1, x[0]);  // x - s, one rounding
+  const float2 r1 = __ffma2_rn(make_float2(s0.y, s0.y), m1, x[1]);
+  const float2 r2 = __ffma2_rn(make_float2(s0.z, s0.z), m1, x[2]);
+  const float2 d2 = __ffma2_rn(r2, r2, __ffma2_rn(r1, r1, __fmul2_rn(r0, r0)));
+  float2 ri;
+  ri.x = d2.x > 1.0e-28f ? rsqrt_approx_f32(d2.x) : 0.0f;
+  ri.y = d2.y > 1.0e-28f ? rsqrt_approx_f32(d2.y) : 0.0f;
+  const float2 kd = __fmul2_rn(make_float2(c.k, c.k), __fmul2_rn(d2, ri));
+  float2 sn, cs;
+  sincos_mufu(kd.x, sn.x, cs.x);
+  sincos_mufu(kd.y, sn.y, cs.y);
+  float2 br, bi;
+  if (KIND == SL) {
+    const float2 re = __fmul2_rn(cs, ri), im = __fmul2_rn(sn, ri);
+    k0 = make_float2(re.x, im.x);
+    k1 = make_float2(re.y, im.y);
+    return;
+  }
+  const float2 rn = __ffma2_rn(r2, make_float2(s1.y, s1.y),
+                               __ffma2_rn(r1, make_float2(s1.x, s1.x), __fmul2_rn(r0, make_float2(s0.w, s0.w))));
+  const float2 u = __fmul2_rn(rn, ri);
+  if (KIND == CFI) {
+    br = __fmul2_rn(u, __fmul2_rn(ri, ri));
+    bi = __fmul2_rn(ri, __ffma2_rn(make_float2(-c.k, -c.k), u, make_float2(c.c2i, c.c2i)));
+  } else {
+    const float2 P = __fmul2_rn(u, ri);
+    const float2 Q = __fmul2_rn(P, ri);
+    if (KIND == DL) {
+      br = Q;
+      bi = __fmul2_rn(make_float2(-c.k, -c.k), P);
+    } else {
+      br = __ffma2_rn(make_float2(c.c2r, c.c2r), ri,
+                      __ffma2_rn(make_float2(c.c1r, c.c1r), Q, __fmul2_rn(make_float2(c.kc1i, c.kc1i), P)));
+      bi = __ffma2_rn(make_float2(c.c2i, c.c2i), ri,
+                      __ffma2_rn(make_float2(c.c1i, c.c1i), Q, __fmul2_rn(make_float2(-c.kc1r, -c.kc1r), P)));
+    }
+  }
+  const float2 nsn = make_float2(-sn.x, -sn.y);
+  const float2 re = __ffma2_rn(cs, br, __fmul2_rn(nsn, bi));
+  const float2 im = __ffma2_rn(cs, bi, __fmul2_rn(sn, br));
+  k0 = make_float2(re.x, im.x);
+  k1 = make_float2(re.y, im.y);
+}
+
 // Roles (warp w, one elected lane for the first two):
 //   w = 0       MMA issuer: waits for a stage's A tiles and density block,
 //               issues its 16 MMAs and commits them;
@@ -373,12 +426,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
       const int ra = 32 * (warp & 3) + lane;
       const int j0 = (gw >> 2) * (TC_J / 4);
       const int64_t blk0 = (int64_t)a.item_block[item] * TC_ROWS;
-      float xt[2][3];
+      float2 xt[3];  // (row ra, row ra + 128) coordinates
+      {
+        const int64_t t0i = off + min(blk0 + ra, n - 1), t1i = off + min(blk0 + ra + 128, n - 1);
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        const int64_t ti = off + min(blk0 + ra + 128 * h, n - 1);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) xt[h][c] = (float)a.coords[3 * ti + c];
+        for (int c = 0; c < 3; ++c) xt[c] = make_float2((float)a.coords[3 * t0i + c], (float)a.coords[3 * t1i + c]);
       }
       const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
       for (uint32_t t = 0; t < T; ++t) {
@@ -401,12 +453,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
             const int j = j0 + jq + e;
             const float4 s0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
             const float2 s1 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-              const float2 kv = tc_kernel<KIND>(xt[h], s0, s1, kc);
-              v[h][2 * e] = tf32_bits(kv.x);
-              v[h][2 * e + 1] = tf32_bits(kv.y);
-            }
+            float2 k0, k1;
+            tc_kernel_x2<KIND>(xt, s0, s1, kc, k0, k1);
+            v[0][2 * e] = tf32_bits(k0.x);
+            v[0][2 * e + 1] = tf32_bits(k0.y);
+            v[1][2 * e] = tf32_bits(k1.x);
+            v[1][2 * e + 1] = tf32_bits(k1.y);
           }
 #pragma unroll
           for (int h = 0; h < 2; ++h) tc_st8(lane_base + tc_a_col(gg & 1, h) + 2 * (j0 + jq), v[h]);

@@ -205,3 +205,29 @@ def test_symmetric_2d_edge_sizes(ctx, n):
             assert np.all(got == 0)
         else:
             assert relerr(got, oracle_apply(O.LAPLACE, okind, 0.0, q, q, x)) < 1e-12
+
+
+@pytest.mark.parametrize("n", [1, 7, 513, 1025])
+def test_symmetric_fp32c_edge_sizes(ctx, n):
+    """The paired-FP32 form (FP32C Laplace SL, DL and combined field) at node
+    counts around its 256/512-node blocks: one pair of targets per thread
+    straddling the end of the nodes, padded records, a single node."""
+    r = np.random.default_rng(200 + n)
+    X = r.standard_normal((n, 3))
+    N = r.standard_normal((n, 3))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    q = inti.Quadrature(X, N, r.uniform(0.5, 1.5, n), 0)
+    x = density(n, False, 4)
+    op = inti.Laplace(dim=3)
+    S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp32c", ctx)
+    D = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, None, "fp32c", ctx)
+    CF = inti.CombinedFieldOperator(D, S, 0.5, 2.0)
+    assert S.tuning["symmetric"] and D.tuning["symmetric"] and CF.tuning["symmetric"]
+    rs = oracle_apply(O.LAPLACE, O.SL, 0.0, q, q, x)
+    rd = oracle_apply(O.LAPLACE, O.DL, 0.0, q, q, x)
+    for A, ref in ((S, rs), (D, rd), (CF, 0.5 * rd + 2.0 * rs)):
+        got = A @ x
+        if n == 1:
+            assert np.all(got == 0)
+        else:
+            assert relerr(got, ref) < 5e-5
