@@ -1077,7 +1077,7 @@ __global__ void __launch_bounds__(kBlock) pair_symm_x2(SymArgs a) {
 #pragma unroll 2
         for (int s = 0; s < kGroup; ++s) {
           const float2* rec = reinterpret_cast<const float2*>(sp + (gq + s) * NR);
-          float2 zq, zd;  // not formed
+          float2 zq = make_float2(0.f, 0.f), zd = zq;  // the column half is not formed
 #pragma unroll
           for (int p = 0; p < NP; ++p) pair_x2_step<KIND, false>(tg[p], rec, g[p], zq, zd);
         }
