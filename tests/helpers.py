@@ -72,3 +72,18 @@ def harmonic_traces(pde, k, q, xs, c=0.7):
     if pde == O.LAPLACE:
         return g0.real.copy(), g1.real.copy()
     return g0, g1
+
+
+def block_rows_apply(values, nq, els, sigma):
+    """Rows e*nq + t (e in els, t < nq, in that order) of the element-block
+    correction applied to sigma; `values` are O.bdim block values for the
+    same elements ((len(els)*nq, nq), column a <-> source node e*nq + a)."""
+    els = np.asarray(els)
+    v = np.asarray(values).reshape(len(els), nq, nq)
+    s = np.asarray(sigma)[els[:, None] * nq + np.arange(nq)[None, :]]
+    return np.einsum("eta,ea->et", v, s).reshape(-1)
+
+
+def smooth_density(pde, k, q, xs):
+    """A smooth density: the trace γ₀u of u = G(·, xs), xs off the surface."""
+    return harmonic_traces(pde, k, q, xs, 1.0)[0]

@@ -165,3 +165,68 @@ def test_batch_tf32_apply_replays_in_cuda_graph():
         assert torch.equal(got, ys)
         assert torch.count_nonzero(got) > 0
     del g
+
+
+def _c4_build(ctx):
+    """The batched workload: 32 seeded star surfaces (n in [6, 27] cells per
+    patch edge, 1,944 .. 39,366 nodes), k = 5, D - i k S with per-surface DIM
+    corrections, 64 plane waves e^{i k d.x}."""
+    r = np.random.default_rng(4)
+    ns = r.integers(6, 28, 32)
+    quads = [inti.star_quadrature(inti.star_coefficients(r), int(n)) for n in ns]
+    k = 5.0
+    op = inti.Helmholtz(k=k, dim=3)
+    corrs = [inti.bdim_correction(op, q, q, ctx=ctx) for q in quads]
+    B = inti.BatchOperator(op, quads, "CF", corrs, 1.0, -1j * k, ctx=ctx)
+    d = r.standard_normal((64, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    X = np.concatenate([np.exp(1j * k * (q.coords @ d.T)) for q in quads], axis=0)
+    return quads, corrs, B, X, k
+
+
+def test_c4_batch_sampled_rows_against_oracle(ctx):
+    """The full C4 batch (687,852 nodes, 64 right-hand sides) against the
+    oracle on 64 sampled rows (2 per surface) x 3 columns, in the pattern of
+    test/fmm3d_test.jl:40-42: FP64 batch <= 1e-12 and TF32 batch <= 5e-3
+    against the oracle's D - i k S row sums plus the same correction rows;
+    and the FP64 batch against the oracle's own DIM corrections of the
+    sampled elements (product-level bound)."""
+    import oracle as O
+    from helpers import block_rows_apply
+
+    quads, corrs, B, X, k = _c4_build(ctx)
+    assert B.n == 687_852
+    Y64 = B.apply(X, "fp64")
+    Y32 = B.apply(X, "tf32")
+    r = np.random.default_rng(21)
+    cols = [0, 31, 63]
+    got64, got32, ref_g, ref_o = ([[] for _ in cols] for _ in range(4))
+    for s, q in enumerate(quads):
+        off = B.offsets[s]
+        els = np.sort(r.choice(q.nel, 2, replace=False))
+        rows = els * q.nq + r.integers(0, q.nq, 2)
+        gS, gD = (c.arrays() for c in corrs[s])
+        oS, oD = O.bdim(O.HELMHOLTZ, k, q.coords, q.normals, q.weights, q.nq, elements=els)
+        sel = np.searchsorted(els, rows // q.nq) * q.nq + rows % q.nq
+        for ci, c in enumerate(cols):
+            x = X[off:off + len(q), c]
+            pair = O.apply(O.HELMHOLTZ, O.DL, k, q.coords, q.normals, q.coords, q.normals, q.weights, x, rows=rows) \
+                - 1j * k * O.apply(O.HELMHOLTZ, O.SL, k, q.coords, q.normals, q.coords, q.normals, q.weights, x,
+                                   rows=rows)
+            corr = O.csr_apply(*gD, x)[rows] - 1j * k * O.csr_apply(*gS, x)[rows]
+            # product level: the oracle's own corrections of the sampled elements
+            odd = block_rows_apply(oD, q.nq, els, x) - 1j * k * block_rows_apply(oS, q.nq, els, x)
+            got64[ci].append(Y64[off + rows, c])
+            got32[ci].append(Y32[off + rows, c])
+            ref_g[ci].append(pair + corr)
+            ref_o[ci].append(pair + odd[sel])
+    cat = np.concatenate
+    worst64 = max(relerr(cat(g), cat(f)) for g, f in zip(got64, ref_g))
+    worst32 = max(relerr(cat(g), cat(f)) for g, f in zip(got32, ref_g))
+    worst_dim = max(relerr(cat(g), cat(f)) for g, f in zip(got64, ref_o))
+    print(f"C4 64 sampled rows x {len(cols)} columns vs oracle: fp64 {worst64:.3e}, tf32 {worst32:.3e}, "
+          f"fp64 vs oracle DIM {worst_dim:.3e}")
+    # measured on the B200: 1.0e-14, 1.6e-4, 1.4e-14
+    assert worst64 < 1e-12
+    assert worst32 < 2e-3
+    assert worst_dim < 1e-12

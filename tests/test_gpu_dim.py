@@ -16,8 +16,8 @@ import pytest
 
 import inti_b200 as inti
 import oracle as O
-from helpers import (density, dim_values_close, harmonic_traces, oracle_apply, oracle_dim_csr, relerr,
-                     small_surfaces)
+from helpers import (block_rows_apply, density, dim_values_close, harmonic_traces, oracle_apply, oracle_dim_csr,
+                     relerr, small_surfaces, smooth_density)
 
 pytestmark = pytest.mark.gpu
 
@@ -94,3 +94,34 @@ def test_gauss_law_and_green_identity_on_gpu(ctx):
     g0, g1 = harmonic_traces(O.LAPLACE, 0.0, q, np.array([3.0, 3.0, 3.0]))
     e1 = np.max(np.abs(S @ g1 - D @ g0 - 0.5 * g0)) / np.max(np.abs(g0))
     assert e1 < 1e-2
+
+
+# Product-level bounds of the corrected C1 operators, (A + δ_gpu)σ against
+# (A + δ_oracle)σ with δ_oracle from the oracle's own BDIM.  On the kite the
+# element matrices reach cond(M_e) ≈ 8e14, so the weights are fixed only up
+# to the near-null directions of M_e: rounding-level differences in the
+# traces and in Θ move them there.  An N(0,1) density picks those up; a
+# smooth density (what the correction is built to integrate) does not.
+# Measured on the host with the oracle's own problems: a second QR solver
+# changes the random-density product by 6.8e-3, relative perturbations of
+# the traces of 1e-15 / 1e-14 by 3.1e-2 / 7.8e-2.  The GPU traces (their own
+# log and reciprocal square root) and Θ (FP64 MMA, another summation order)
+# differ at that level.  Measured on the B200: DL 8.5e-2 (random) and
+# 5.8e-10 (smooth), SL 1.2e-3 and 4.8e-9; the bounds below.
+C1_BOUNDS = {"DL": (0.2, 5e-9), "SL": (1e-2, 2e-8)}  # (random N(0,1), smooth)
+
+
+def test_c1_corrected_product_against_oracle_correction(ctx):
+    q = inti.kite_quadrature()
+    assert len(q) == 1000
+    op = inti.Laplace(dim=2)
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    oS, oD = O.bdim(O.LAPLACE, 0.0, q.coords, q.normals, q.weights, q.nq)
+    els = np.arange(q.nel)
+    dens = {"random": density(len(q), False, 1), "smooth": smooth_density(O.LAPLACE, 0.0, q, np.array([3.0, -5.2]))}
+    for name, A, kind, ov in (("DL", D, O.DL, oD), ("SL", S, O.SL, oS)):
+        for which, sigma in dens.items():
+            ref = oracle_apply(O.LAPLACE, kind, 0.0, q, q, sigma) + block_rows_apply(ov, q.nq, els, sigma)
+            err = relerr(A @ sigma, ref)
+            print(f"C1 {name} {which}: (A+dgpu)s vs (A+dora)s rel err {err:.3e}")
+            assert err < C1_BOUNDS[name][0 if which == "random" else 1], (name, which, err)
