@@ -249,7 +249,12 @@ typedef struct {
   int32_t converged;        /* 1 if relres <= rtol */
   int32_t reserved;
   double relres;            /* ||b - L x|| / ||b||, FP64 residual */
-  double seconds;           /* device time of the solve */
+  double seconds;           /* wall time of the whole call: operator set-up it
+                               triggers (fused combined field, FP32C twins and
+                               their timed launch shapes), copies of b and x
+                               in, the solve, and x back (host clock) */
+  double setup_seconds;     /* the operator set-up part of seconds (0 when
+                               cached from an earlier solve) */
 } inti_gmres_stats;
 
 /* coefs: nterms complex pairs; shift: one complex pair.  All ops must share
@@ -320,7 +325,7 @@ int inti_batch_destroy(inti_batch* b);
  * No counterpart in the reference: Inti.jl's operators allocate freely.
  * For callers that cannot call cudaMalloc when they apply the operator (a
  * framework's caching allocator owns the device memory, a solver loop that
- * must not pay for allocation, work issued during stream capture).
+ * must not pay for allocation).
  *
  * y = alpha*(A x + C x) + beta*y with the same kernels as inti_op_apply, but
  * every array is a caller-owned DEVICE pointer on the current device:
@@ -329,7 +334,8 @@ int inti_batch_destroy(inti_batch* b);
  * x (n) and y (m) — complex data interleaved for Helmholtz.  alpha/beta are
  * host pairs (re, im) or NULL for 1, 0.  Work goes to `stream` (NULL: the
  * legacy default stream); synchronize != 0 waits and reports device-side
- * timeouts.
+ * timeouts as INTI_E_TIMEOUT.  With synchronize = 0 no status reports a
+ * timeout: a timed-out call leaves NaN in every entry of y.
  *
  * Scratch lives in a fixed 32 MiB static device array that every GPU loading
  * the library holds until exit; problems whose packed sources plus one

@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -276,6 +277,8 @@ void batch_gmres(inti_batch* b, const double* shift, const double* B, double* X,
                  double rtol, int32_t restart, int32_t maxiter, int32_t mode, int on_device, double* relres_out,
                  inti_gmres_stats* stats) {
   inti_ctx* ctx = b->ctx;
+  // the reported time covers the whole call: buffers, copies in and out, the solve
+  const auto t_enter = std::chrono::steady_clock::now();
   if (b->pde != INTI_HELMHOLTZ) throw Error(INTI_E_UNSUPPORTED, "batched GMRES is implemented for Helmholtz");
   if (!B || !X) throw Error(INTI_E_ARG, "B/X NULL");
   if (nrhs < 1) throw Error(INTI_E_ARG, "nrhs must be >= 1");
@@ -317,10 +320,6 @@ void batch_gmres(inti_batch* b, const double* shift, const double* B, double* X,
   }
   double2* bdev = bd.as<double2>();
   double2* xdev = xd.as<double2>();
-  cudaEvent_t e0, e1;
-  INTI_CUDA(cudaEventCreate(&e0));
-  INTI_CUDA(cudaEventCreate(&e1));
-  INTI_CUDA(cudaEventRecord(e0, ctx->stream));
   const std::vector<double> bn = S.norms(bdev);
   const bool x0 = [&] {
     const std::vector<double> xn = S.norms(xdev);
@@ -377,15 +376,10 @@ void batch_gmres(inti_batch* b, const double* shift, const double* B, double* X,
       if (used == 0 || worst_new >= worst_old) break;  // stagnation
     }
   }
-  INTI_CUDA(cudaEventRecord(e1, ctx->stream));
-  INTI_CUDA(cudaEventSynchronize(e1));
-  float ms = 0;
-  INTI_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
   INTI_CUDA(cudaMemcpy2DAsync(X, sizeof(double2) * ldb, xdev, sizeof(double2) * n, sizeof(double2) * n, nrhs,
                               on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, ctx->stream));
   sync_and_check(ctx);
+  const double wall_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_enter).count();
   double worst = 0;
   for (int q = 0; q < S.nsys; ++q) worst = std::max(worst, rel[q]);
   if (relres_out)
@@ -398,7 +392,8 @@ void batch_gmres(inti_batch* b, const double* shift, const double* B, double* X,
     stats->converged = worst <= rtol ? 1 : 0;
     stats->reserved = 0;
     stats->relres = worst;
-    stats->seconds = ms * 1e-3;
+    stats->seconds = wall_s;
+    stats->setup_seconds = 0.0;
   }
 }
 

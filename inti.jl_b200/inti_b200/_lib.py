@@ -73,6 +73,7 @@ class GmresStats(C.Structure):
         ("reserved", C.c_int32),
         ("relres", C.c_double),
         ("seconds", C.c_double),
+        ("setup_seconds", C.c_double),
     ]
 
     def as_dict(self) -> dict:
