@@ -468,6 +468,7 @@ struct EpiArgs {
   double ar, ai, br, bi;
   bool beta_zero;
   const double* rowscale = nullptr;  // per-row factor of the pair sum (A^T: the source weights)
+  const int* err = nullptr;          // when set and nonzero (a pair kernel timed out): y gets NaN
 };
 
 // Kernel constant, correction row, alpha/beta and the store for row i, given
@@ -510,6 +511,14 @@ template <class P, bool CPLX>
 __global__ void pair_epilogue_kernel(EpiArgs e) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (i >= e.m) return;
+  if (e.err && *e.err) {  // the partial sums are incomplete: make the failure visible in y
+    const double nan = __longlong_as_double(0x7ff8000000000000LL);
+    if (CPLX)
+      reinterpret_cast<double2*>(e.y)[i] = make_double2(nan, nan);
+    else
+      e.y[i] = nan;
+    return;
+  }
   const P* part = static_cast<const P*>(e.partial);
   double sr = 0.0, si = 0.0;
   for (int s = 0; s < e.split; ++s) {
@@ -1634,10 +1643,9 @@ int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {
 //
 // Some callers cannot call cudaMalloc at the moment they need the operator:
 // code running inside a framework whose caching allocator already owns nearly
-// all device memory (so a fresh cudaMalloc fails or fragments it), code that
-// must not pay an allocation's latency or implicit synchronisation in a
-// solver loop, and code that issues work while a stream is being captured,
-// where allocation calls are not permitted.  inti_apply_noalloc serves them:
+// all device memory (so a fresh cudaMalloc fails or fragments it), and code
+// that must not pay an allocation's latency or implicit synchronisation in a
+// solver loop.  inti_apply_noalloc serves them:
 // the caller passes every input and output as device pointers, and the
 // scratch the pair product needs (packed source records and per-chunk partial
 // sums) lives in one fixed array of kNoAllocScratchBytes declared below.  The
@@ -1651,6 +1659,8 @@ int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {
 // on it.  Nothing in the array has to start at zero: the pack kernel writes
 // every record (padding included) and the pair kernel writes every partial
 // slot it owns; only the timeout flag is cleared at the start of each call.
+// If a bounded wait of the pair kernel runs out, the epilogue writes NaN into
+// every entry of y (with synchronize = 0 no status reports the timeout).
 // ===========================================================================
 constexpr size_t kNoAllocScratchBytes = 32u << 20;  // 32 MiB
 constexpr size_t kNoAllocFlagBytes = 256;
@@ -1787,6 +1797,7 @@ int apply_noalloc(int pde, int kind, int dim, double k, int precision, int64_t m
   e.br = beta ? beta[0] : 0.0;
   e.bi = beta ? beta[1] : 0.0;
   e.beta_zero = (e.br == 0.0 && e.bi == 0.0);
+  e.err = flag;
   const unsigned gb = (unsigned)((m + 255) / 256);
   const bool cplx = pde == HELMHOLTZ;
   if (precision == INTI_FP32C) {

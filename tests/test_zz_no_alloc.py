@@ -2,13 +2,14 @@
 
 It exists for callers that cannot allocate device memory at the point where
 they apply the operator — for instance when a framework's caching allocator
-already holds the GPU's memory, inside a solver loop that must not pay for an
-allocation, or while a stream is being captured.  Its scratch is a fixed
-static device array, so these tests check that it reproduces the allocating
-entry point (inti_op_apply, via GpuOperator) on two calls in a row with
-different densities: a second call must not see the first call's leftovers.
-They run on their own and after the rest of the suite (pytest collects this
-file last).
+already holds the GPU's memory, or inside a solver loop that must not pay for
+an allocation.  Its scratch is a fixed static device array, so these tests
+check that it reproduces the allocating entry point (inti_op_apply, via
+GpuOperator) on two calls in a row with different densities: a second call
+must not see the first call's leftovers.  The products are also checked
+against the oracle (pair sums plus the same correction rows).  The tests run
+on their own and after the rest of the suite (pytest collects this file
+last).
 """
 import ctypes as C
 
@@ -16,8 +17,9 @@ import numpy as np
 import pytest
 
 import inti_b200 as inti
+import oracle as O
 from inti_b200 import _lib as L
-from helpers import density, relerr
+from helpers import density, oracle_apply, relerr
 
 pytestmark = pytest.mark.gpu
 
@@ -58,35 +60,61 @@ def _noalloc(ctx, pde, kind, k, prec, q, corr, sigma, alpha=1.0, beta=0.0, y0=No
     return yh
 
 
+SL_, DL_, ADL_, HS_ = inti.SingleLayerKernel, inti.DoubleLayerKernel, inti.AdjointDoubleLayerKernel, \
+    inti.HyperSingularKernel
+# (name, operator, kernel class, ABI kernel, precision, tolerance, correction, surface)
 CASES = [
-    ("helmholtz_sl_fp64", lambda: inti.Helmholtz(k=6.0, dim=3), inti.SingleLayerKernel, L.SL, "fp64", 1e-12),
-    ("laplace_dl_fp64", lambda: inti.Laplace(dim=3), inti.DoubleLayerKernel, L.DL, "fp64", 1e-12),
-    ("laplace_dl_fp32c", lambda: inti.Laplace(dim=3), inti.DoubleLayerKernel, L.DL, "fp32c", 2e-5),
+    ("helmholtz_sl_fp64", lambda: inti.Helmholtz(k=6.0, dim=3), SL_, L.SL, "fp64", 1e-12, True, "p2"),
+    ("laplace_dl_fp64", lambda: inti.Laplace(dim=3), DL_, L.DL, "fp64", 1e-12, True, "ell"),
+    ("laplace_dl_fp32c", lambda: inti.Laplace(dim=3), DL_, L.DL, "fp32c", 2e-5, True, "ell"),
+    ("helmholtz_hs_fp64", lambda: inti.Helmholtz(k=6.0, dim=3), HS_, L.HS, "fp64", 1e-12, True, "p2"),
+    ("laplace_adl_fp64_nocorr", lambda: inti.Laplace(dim=3), ADL_, L.ADL, "fp64", 1e-12, False, "ell"),
+    ("laplace2d_dl_fp64", lambda: inti.Laplace(dim=2), DL_, L.DL, "fp64", 1e-12, True, "kite"),
 ]
+ORACLE_KIND = {L.SL: O.SL, L.DL: O.DL, L.ADL: O.ADL, L.HS: O.HS}
 
 
-@pytest.mark.parametrize("name,mkop,Kc,kind,prec,tol", CASES)
-def test_noalloc_matches_allocating_apply_twice(ctx, name, mkop, Kc, kind, prec, tol):
-    q = inti.p2_sphere_quadrature(6) if "helmholtz" in name else inti.ellipsoid_quadrature(5, 5)
+def _surface(name):
+    return {"p2": lambda: inti.p2_sphere_quadrature(6), "ell": lambda: inti.ellipsoid_quadrature(5, 5),
+            "kite": lambda: inti.kite_quadrature(60, 9)}[name]()
+
+
+@pytest.mark.parametrize("name,mkop,Kc,kind,prec,tol,with_corr,surf", CASES)
+def test_noalloc_matches_allocating_apply_twice(ctx, name, mkop, Kc, kind, prec, tol, with_corr, surf):
+    q = _surface(surf)
     op = mkop()
-    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
-    corr = (S if Kc is inti.SingleLayerKernel else D).correction
+    corr = None
+    if with_corr:
+        derivative = Kc in (ADL_, HS_)
+        if derivative:
+            pair = inti.adj_double_layer_hypersingular(op=op, target=q, source=q, correction={"method": "dim"},
+                                                       ctx=ctx)
+        else:
+            pair = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+        corr = pair[0 if Kc in (SL_, ADL_) else 1].correction
     A = inti.GpuOperator(Kc(op), q, q, corr, prec, ctx)
     pde = op.pde
     k = float(getattr(op, "k", 0.0))
     P = {"fp64": L.FP64, "fp32c": L.FP32C}[prec]
     cplx = pde == L.HELMHOLTZ
+    carr = corr.arrays() if corr is not None else None
     for call, seed in enumerate((3, 4)):  # two calls in a row, different densities
         sigma = density(len(q), cplx, seed)
         ref = A @ sigma
-        got = _noalloc(ctx, pde, kind, k, P, q, corr.arrays(), sigma)
+        got = _noalloc(ctx, pde, kind, k, P, q, carr, sigma)
         assert relerr(got, ref) < tol, (name, call)
-    # alpha/beta, as inti_op_apply
+        # and against the oracle: pair sums plus the same correction rows
+        ora = oracle_apply(pde, ORACLE_KIND[kind], k, q, q, sigma)
+        if carr is not None:
+            ora = ora + O.csr_apply(*carr, sigma)
+        assert relerr(got, ora) < tol, (name, call, "oracle")
+    # alpha/beta as inti_op_apply; complex coefficients for the complex operators
+    alpha, beta = (0.5 + 0.3j, -2.0 + 1.0j) if cplx else (0.5, -2.0)
     sigma = density(len(q), cplx, 5)
     y0 = density(len(q), cplx, 6)
     ref = y0.copy()
-    A.mul(ref, sigma, 0.5, -2.0)
-    got = _noalloc(ctx, pde, kind, k, P, q, corr.arrays(), sigma, 0.5, -2.0, y0)
+    A.mul(ref, sigma, alpha, beta)
+    got = _noalloc(ctx, pde, kind, k, P, q, carr, sigma, alpha, beta, y0)
     assert relerr(got, ref) < tol
 
 
