@@ -17,6 +17,7 @@ from ._lib import (
 from .core import *  # noqa: F401,F403
 from .core import __all__ as _core_all
 from .vdim import polynomial_solutions_vdim, vdim_correction
+from .autodiff import TorchPotential, rrule
 from .geometry import (
     Quadrature,
     circle_quadrature,
@@ -47,6 +48,8 @@ __all__ = list(_core_all) + [
     "gauss_legendre",
     "polynomial_solutions_vdim",
     "vdim_correction",
+    "rrule",
+    "TorchPotential",
     "ArgumentError",
     "DimensionMismatch",
     "NonFiniteError",

@@ -23,6 +23,7 @@ module IntiB200
 using LinearAlgebra
 using SparseArrays
 using LinearMaps
+using ChainRulesCore
 import Inti
 
 const LIB = get(ENV, "INTI_B200_LIB", joinpath(@__DIR__, "..", "_build", "libinti_b200.so"))
@@ -68,6 +69,7 @@ mutable struct QuadHandle
     ptr::Ptr{Cvoid}
     ctx::Context
     n::Int
+    dim::Int
 end
 
 """
@@ -98,7 +100,7 @@ function upload(Q::Inti.Quadrature{N}; ctx = default_context()) where {N}
                     (Ptr{Cvoid}, Cint, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Ref{Ptr{Cvoid}}),
                     ctx.ptr, N, n, X, has_normals ? Nrm : C_NULL, W, nq, out), ctx.ptr)
     end
-    h = QuadHandle(out[], ctx, n)
+    h = QuadHandle(out[], ctx, n, N)
     finalizer(h -> ccall((:inti_quad_destroy, LIB), Cint, (Ptr{Cvoid},), h.ptr), h)
     return h
 end
@@ -112,7 +114,7 @@ function upload(pts::AbstractVector{<:AbstractVector}; ctx = default_context())
     GC.@preserve X check(ccall((:inti_quad_create, LIB), Cint,
         (Ptr{Cvoid}, Cint, Int64, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Int32, Ref{Ptr{Cvoid}}),
         ctx.ptr, N, length(pts), X, C_NULL, C_NULL, 0, out), ctx.ptr)
-    h = QuadHandle(out[], ctx, length(pts))
+    h = QuadHandle(out[], ctx, length(pts), N)
     finalizer(h -> ccall((:inti_quad_destroy, LIB), Cint, (Ptr{Cvoid},), h.ptr), h)
     return h
 end
@@ -215,6 +217,75 @@ end
 LinearMaps._unsafe_mul!(Y::AbstractMatrix, A::B200Map, X::AbstractMatrix) = apply!(Y, A, X)
 LinearMaps._unsafe_mul!(Y::AbstractMatrix, A::B200Map, X::AbstractMatrix, α::Number, β::Number) =
     apply!(Y, A, X, α, β)
+
+"""
+    transpose_apply(A::B200Map, x) -> transpose(A) * x
+
+`inti_op_apply_transpose`: the product with the (unconjugated) transpose,
+correction rows included.
+"""
+function transpose_apply(A::B200Map{T}, x::AbstractVector) where {T}
+    xx = Vector{T}(x)
+    yy = zeros(T, A.n)
+    a, b = Float64[1, 0], Float64[0, 0]
+    GC.@preserve xx yy a b check(ccall((:inti_op_apply_transpose, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ptr{Cvoid}, Int64, Int32, Ptr{Float64}, Ptr{Float64}, Cint),
+        A.h.ptr, xx, A.m, yy, A.n, 1, a, b, 0), A.ctx.ptr)
+    return yy
+end
+
+"""
+    grad_sources(A::B200Map{Float64}, ū, σ)
+
+Cotangents of `σ` and of the source quadrature (coordinates `dim × n`,
+normals `dim × n`, weights `n`) for `u = A σ` with `∂J/∂u = ū`, from the
+hand-written adjoint kernel (`inti_op_grad_sources`, Laplace single and
+double layer, FP64): kernel tiles are recomputed, nothing `m × n` is stored.
+The pair terms only; a correction is not part of it.
+"""
+function grad_sources(A::B200Map{Float64}, ubar::AbstractVector, σ::AbstractVector)
+    src = A.h.keep[2]::QuadHandle
+    g, s = Vector{Float64}(ubar), Vector{Float64}(σ)
+    dσ, dw = zeros(A.n), zeros(A.n)
+    dx, dn = zeros(src.dim, A.n), zeros(src.dim, A.n)
+    GC.@preserve g s dσ dx dn dw check(ccall((:inti_op_grad_sources, LIB), Cint,
+        (Ptr{Cvoid}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Cint),
+        A.h.ptr, g, s, dσ, dx, dn, dw, 0), A.ctx.ptr)
+    return (σ = dσ, coords = dx, normals = dn, weights = dw)
+end
+
+"""
+    ChainRulesCore.rrule(::typeof(*), A::B200Map, σ)
+
+Reverse rule of the device product `u = A * σ` (Inti.jl itself only
+differentiates forward, through ForwardDiff: src/reference_interpolation.jl:
+36-39).  The pullback maps `ū` to `Aᴴ ū` for `σ` (the transpose apply,
+conjugated for complex operators, correction rows included) and, for real
+Laplace single and double layers, to a `Tangent` of the operator holding the
+source-geometry cotangents `coords`, `normals`, `weights` from the adjoint
+kernel.  A DIM correction is held constant: its dependence on the geometry
+is not differentiated.
+"""
+function ChainRulesCore.rrule(::typeof(*), A::B200Map{T}, σ::AbstractVector) where {T}
+    u = A * σ
+    function b200_pullback(ū)
+        ubar = unthunk(ū)
+        if T <: Complex
+            return NoTangent(), NoTangent(), conj.(transpose_apply(A, conj.(ubar)))
+        end
+        dσ = transpose_apply(A, ubar)
+        g = try
+            grad_sources(A, ubar, σ)
+        catch err
+            err isa B200Error || rethrow()
+            nothing  # kernels without source gradients (ADL, HS, FP32C)
+        end
+        g === nothing && return NoTangent(), NoTangent(), dσ
+        Ā = Tangent{typeof(A)}(; coords = g.coords, normals = g.normals, weights = g.weights)
+        return NoTangent(), Ā, dσ
+    end
+    return u, b200_pullback
+end
 
 """
     set_symmetric!(ctx, flag)
@@ -369,16 +440,16 @@ function gmres(L::LinearMaps.LinearMap, b::AbstractVector; rtol = 1e-10, restart
     ops = Ptr{Cvoid}[t[2].h.ptr for t in terms]
     coefs = reduce(vcat, [Float64[real(c), imag(c)] for (c, _) in terms])
     sh = Float64[real(shift[]), imag(shift[])]
-    stats = zeros(UInt8, 40)  # inti_gmres_stats: 6 Int32 + 2 Float64
+    stats = zeros(UInt8, 48)  # inti_gmres_stats: 6 Int32 + 3 Float64
     GC.@preserve ops coefs sh bb x stats check(ccall((:inti_gmres, LIB), Cint,
         (Ptr{Cvoid}, Int32, Ptr{Ptr{Cvoid}}, Ptr{Float64}, Ptr{Float64}, Ptr{Cvoid}, Ptr{Cvoid}, Float64,
          Int32, Int32, Int32, Cint, Ptr{Float64}, Ptr{UInt8}),
         ctx.ptr, length(ops), ops, coefs, sh, bb, x, rtol, restart, maxiter, mode == :mixed ? 1 : 0, 0,
         C_NULL, stats), ctx.ptr)
     ints = reinterpret(Int32, stats[1:24])
-    flts = reinterpret(Float64, stats[25:40])
+    flts = reinterpret(Float64, stats[25:48])
     return x, (iterations = ints[1], outer = ints[2], fp64_applies = ints[3], fp32_applies = ints[4],
-               converged = ints[5] == 1, relres = flts[1], seconds = flts[2])
+               converged = ints[5] == 1, relres = flts[1], seconds = flts[2], setup_seconds = flts[3])
 end
 
 collect_terms!(A::B200Map, c, shift, terms) = push!(terms, (ComplexF64(c), A))
