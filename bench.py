@@ -57,9 +57,21 @@ FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "lap
                   # hypersingular kernel: + n_x.n_y, the 1/d^5 term and its complex factor
                   "helmholtz_adl": 34, "helmholtz_hs": 60}
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pair-kernel
-# launch on the default workload, from an ncu capture of that launch (the
-# symmetric kernel: source records read, column partials written)
-PAIR_TRAFFIC_BYTES = 67.32e6
+# launch per workload, from the ncu capture of that launch summarised in
+# profiles/ (the file named beside each entry); None where no capture exists.
+PAIR_TRAFFIC_BYTES = {"c2": (67.32e6, "profiles/pair_symm_helmholtz_sl_fp64_p2sphere62k.md")}
+# Fallback HBM copy bandwidth (GB/s) when MEASURED_PEAKS.json is absent
+HBM_FALLBACK_GBS = 6650.0
+
+
+def hbm_peak() -> tuple[float, str]:
+    """The measured HBM copy bandwidth of this pool's B200s
+    (MEASURED_PEAKS.json, written by the driver), else the fallback."""
+    try:
+        with open(ROOT / "MEASURED_PEAKS.json") as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs, of measured"
+    except (OSError, KeyError, ValueError):
+        return HBM_FALLBACK_GBS, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent), of fallback"
 # Algorithmic flops per pair of the source-gradient (adjoint) pass
 ADJ_FLOPS_PER_PAIR = {"laplace_dl": 40, "laplace_sl": 19}
 
@@ -224,16 +236,75 @@ def run_reference(args) -> None:
     per = statistics.mean(times)
     value = rows * n / per / 1e9
     full_ms = per * (n / rows) * 1e3
+    sample = (f"{rows} of {n} target rows x {n} sources per step (the C++ FP64 restatement of Inti's "
+              f"on-the-fly row sums): sampled rows, pair sums only (the 6-per-row DIM correction SpMV is not "
+              f"timed), rate extrapolated to the full product")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": full_ms, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "helmholtz3d_sl_k10_p2sphere_N62208_dim", "n": n, "nnz_per_row": 6},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port",
-                         "sample": f"{rows} target rows x {n} sources per step (scaled to a full step)"},
+        "config": {"workload": "helmholtz3d_sl_k10_p2sphere_N62208_dim", "n": n, "nnz_per_row": 6,
+                   "step": "sampled rows, extrapolated, pair sums only", "rows_per_step": rows,
+                   "full_product_ms_extrapolated": full_ms},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": nt, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def solve_both(inti, make_L, b, restart: int) -> dict:
+    """FP64 and MIXED GMRES on L x = b to 1e-10.  `seconds` is the wall time
+    of the whole solve call, from the upload of b to x back on the host.
+    Each mode starts from freshly created operators (`make_L()`, the DIM
+    corrections already built), so its first solve includes the operator
+    set-up it triggers: the fused combined field, and for MIXED the FP32C
+    twins (`setup_s` is that part).  The same operators are then solved a
+    second time, set-up cached, as `seconds_repeat`."""
+    out = {}
+    for mode in ("fp64", "mixed"):
+        L = make_L()
+        _, st = inti.gmres(L, b, rtol=1e-10, restart=restart, maxiter=500, mode=mode)
+        _, st2 = inti.gmres(L, b, rtol=1e-10, restart=restart, maxiter=500, mode=mode)
+        out[mode] = {"seconds": st["seconds"], "setup_s": st["setup_seconds"], "seconds_repeat": st2["seconds"],
+                     "iterations": st["iterations"], "outer": st["outer"],
+                     "fp64_applies": st["fp64_applies"], "fp32_applies": st["fp32_applies"],
+                     "relres_fp64": st["relres"], "converged": bool(st["converged"] and st2["converged"])}
+        del L
+    if out["fp64"]["converged"] and out["mixed"]["converged"]:
+        out["mixed_speedup_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+        out["mixed_speedup_vs_fp64_repeat"] = out["fp64"]["seconds_repeat"] / out["mixed"]["seconds_repeat"]
+    out["timing"] = ("wall time of the whole solve call from the upload of b to x on the host; the first solve "
+                     "of each mode on fresh operators (includes the set-up it triggers), the repeat with it cached")
+    return out
+
+
+def gmres_c2_cfie(ctx) -> dict:
+    """Sound-soft scattering on the C2 sphere (P2, N = 62,208), k = 10: the
+    Brakhage-Werner combined field (1/2 I + D - i k S) sigma = -u_inc
+    (docs/src/examples/helmholtz_scattering.jl:485-495) with u_inc a plane
+    wave, both layers DIM-corrected.  A single-RHS Helmholtz solve that
+    needs more Krylov iterations than the C3 Laplace one."""
+    import inti_b200 as inti
+
+    k = 10.0
+    q = inti.p2_sphere_quadrature(36)
+    op = inti.Helmholtz(k=k, dim=3)
+    t0 = time.perf_counter()
+    dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
+    t_setup = time.perf_counter() - t0
+    d = np.array([0.3, -0.5, 0.81])
+    d /= np.linalg.norm(d)
+    b = -np.exp(1j * k * (q.coords @ d))
+
+    def make_L():
+        S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, "fp64", ctx)
+        D = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, "fp64", ctx)
+        return 0.5 * inti.I + D - 1j * k * S
+
+    out = {"workload": "helmholtz3d_cfie(0.5I+D-ikS)_k10_p2sphere_N62208_dim", "n": len(q), "rtol": 1e-10,
+           "setup_s": t_setup}
+    out.update(solve_both(inti, make_L, b, restart=100))
+    return out
 
 
 def gmres_c3(ctx, cpu_seconds: float | None = None) -> dict:
@@ -247,7 +318,7 @@ def gmres_c3(ctx, cpu_seconds: float | None = None) -> dict:
     q = inti.ellipsoid_quadrature(61, 5)
     op = inti.Laplace(dim=3)
     t0 = time.perf_counter()
-    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    dS, dD = inti.bdim_correction(op, q, q, ctx=ctx)
     t_setup = time.perf_counter() - t0
     r = np.random.default_rng(8)
     src = r.uniform(-1, 1, (64, 3))
@@ -255,16 +326,14 @@ def gmres_c3(ctx, cpu_seconds: float | None = None) -> dict:
     c = r.standard_normal(len(src))
     d = np.linalg.norm(q.coords[:, None, :] - src[None, :, :], axis=2)
     b = (c[None, :] / (4 * np.pi * d)).sum(1)
-    L = 0.5 * inti.I + D + S
+    def make_L():
+        S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, dS, "fp64", ctx)
+        D = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, dD, "fp64", ctx)
+        return 0.5 * inti.I + D + S
+
     out = {"workload": "laplace3d_cfie(0.5I+D+S)_ellipsoid_N200934_dim", "n": len(q), "rtol": 1e-10,
            "setup_s": t_setup}
-    for mode in ("fp64", "mixed"):
-        x, st = inti.gmres(L, b, rtol=1e-10, restart=100, maxiter=500, mode=mode)
-        out[mode] = {"seconds": st["seconds"], "iterations": st["iterations"], "outer": st["outer"],
-                     "fp64_applies": st["fp64_applies"], "fp32_applies": st["fp32_applies"],
-                     "relres_fp64": st["relres"], "converged": bool(st["converged"])}
-    if out["fp64"]["converged"] and out["mixed"]["converged"]:
-        out["mixed_speedup_vs_fp64"] = out["fp64"]["seconds"] / out["mixed"]["seconds"]
+    out.update(solve_both(inti, make_L, b, restart=100))
     if cpu_seconds:
         sys.path.insert(0, str(ROOT / "oracle"))
         import oracle as O
@@ -655,7 +724,7 @@ def bench_csr(args, ctx, torch) -> dict:
         ref = np.array([va[ia[i]:ia[i + 1]] @ xh[ja[ia[i]:ia[i + 1]]] for i in rows])
         out[dt]["sampled_rows_max_relerr"] = float(np.max(np.abs(yh[rows] - ref) / np.maximum(np.abs(ref), 1e-300)))
         del Cm
-    peak = 6557.1  # MEASURED_PEAKS.json hbm_gbs
+    peak, peak_src = hbm_peak()
     return {"metric": "correction SpMV bandwidth", "value": out["f64"]["gbs"], "unit": "GB/s", "n_gpus": 1,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["f64"]["ms"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -663,7 +732,7 @@ def bench_csr(args, ctx, torch) -> dict:
                        "l2": "inputs larger than L2 (>= 470 MB per step)"},
             "roofline": {"bound": "hbm", "achieved": out["f64"]["gbs"], "peak": peak, "unit": "GB/s",
                          "frac": out["f64"]["gbs"] / peak, "traffic": None, "kernel": "csr_kernel<8, real>",
-                         "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured"},
+                         "peak_source": peak_src},
             "complex": out["c128"], "real": out["f64"], "gpu_launches": out["f64"]["launches"]}
 
 
@@ -850,7 +919,10 @@ def main() -> None:
         evals = float(m_loc) * n
     roofline = {"bound": "fp32" if fp32 else "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": achieved / peak,
-                "traffic": PAIR_TRAFFIC_BYTES if args.workload == "c2" else None,
+                "traffic": PAIR_TRAFFIC_BYTES[args.workload][0] if args.workload in PAIR_TRAFFIC_BYTES else None,
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                   f"{PAIR_TRAFFIC_BYTES[args.workload][1]}"
+                                   if args.workload in PAIR_TRAFFIC_BYTES else "no capture"),
                 "kernel": f"{'pair_symm' if sym else 'pair_forward'} ({fkey}, {'float' if fp32 else 'double'})",
                 "kernel_ms": kern_ms,
                 "flops_per_pair": FLOPS_PER_PAIR[fkey],
@@ -882,6 +954,7 @@ def main() -> None:
         line["cpu_baseline"] = cpu_sample(q, S, sigma, args.cpu_seconds, host_cores())
     if not args.no_gmres and world == 1 and args.workload == "c2":
         line["gmres"] = gmres_c3(ctx, None if args.no_cpu else min(args.cpu_seconds, 10.0))
+        line["gmres_helmholtz"] = gmres_c2_cfie(ctx)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
