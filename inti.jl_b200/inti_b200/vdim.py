@@ -1,10 +1,11 @@
 """Volume density interpolation (VDIM) correction of the volume potential
-(src/vdim.jl:30-130, 261-285; src/api.jl:282-378), Laplace in 2D and 3D.
+(src/vdim.jl:30-130, 261-285; src/api.jl:282-378), Laplace in 2D and 3D and
+Helmholtz in 3D.
 
     V + δV  with  δV_ij = w_j(i),  L_e w(i) = Θ[i, :]  (least squares),
 
 where, for the monomials p_n(x) = x^α / α! (|α| <= order) and polynomials P_n
-with ΔP_n = p_n,
+with ΔP_n = p_n (Laplace) or ΔP_n + k²P_n = p_n (Helmholtz),
 
     Θ = S·γ₁P − D·γ₀P − V·p + μ(x)·P(x)
 
@@ -30,6 +31,15 @@ which satisfies ΔP = p exactly.  Any two particular solutions differ by a
 harmonic polynomial H, whose contribution S·γ₁H − D·γ₀H + μH vanishes up to
 the boundary quadrature's error, so the corrections agree with the
 reference's to that accuracy, not to rounding.
+
+For Helmholtz (`solve_helmholtz` in the reference) the polynomial solution
+of ΔP + k²P = p is unique (a polynomial H with ΔH + k²H = 0 is zero: its
+top-degree part would satisfy k²H = 0), so P is the reference's own:
+
+    P = Σ_j (−1)^j Δ^j p / k^(2j+2)   (a finite sum: Δ lowers the degree),
+
+since (Δ + k²)P telescopes to p.  Θ, the volume potential and the
+corrections are then complex.
 """
 from __future__ import annotations
 
@@ -104,20 +114,38 @@ def _laplace_particular(p, m, N):
     return P
 
 
+def _helmholtz_particular(p, k, N):
+    """ΔP + k²P = p: P = Σ_j (−1)^j Δ^j p / k^(2j+2) (the unique polynomial
+    solution)."""
+    P, term, c = {}, dict(p), 1.0 / (k * k)
+    while term:
+        P = _add(P, term, c)
+        term = _laplacian(term, N)
+        c = -c / (k * k)
+    return P
+
+
 def polynomial_solutions_vdim(op, order: int):
     """(multiindices, p, P, ∇P) for every monomial p = x^α/α!, |α| <= order
     (src/vdim.jl:309-345); the multi-indices enumerate the first coordinate
     fastest (Iterators.product)."""
     N = op.dim
-    if op.pde != L.LAPLACE:
-        raise L.UnsupportedError(L.E_UNSUPPORTED, "VDIM is implemented for the Laplace operator")
+    if op.pde == L.HELMHOLTZ:
+        if N != 3:
+            raise L.UnsupportedError(L.E_UNSUPPORTED, "Helmholtz VDIM is implemented in 3D (the 2D Hankel "
+                                                      "kernels are not)")
+        k = float(op.k)
+        if not k > 0:
+            raise L.ArgumentError(L.E_ARG, "Helmholtz VDIM needs a positive wavenumber")
+    elif op.pde != L.LAPLACE:
+        raise L.UnsupportedError(L.E_UNSUPPORTED, "VDIM is implemented for the Laplace and Helmholtz operators")
     multi, ps, Ps, dPs = [], [], [], []
     for t in itertools.product(range(order + 1), repeat=N):
         alpha = t[::-1]
         if sum(alpha) > order:
             continue
         p = {tuple(alpha): 1.0 / math.prod(math.factorial(a) for a in alpha)}
-        P = _laplace_particular(p, sum(alpha), N)
+        P = _helmholtz_particular(p, k, N) if op.pde == L.HELMHOLTZ else _laplace_particular(p, sum(alpha), N)
         multi.append(alpha)
         ps.append(p)
         Ps.append(P)
@@ -171,7 +199,7 @@ def vdim_correction(op, target: Quadrature, source: Quadrature, boundary: Quadra
     indptr = np.zeros(len(target) + 1, np.int64)
     indptr[1:] = np.cumsum(np.where(near >= 0, nq, 0))
     indices = (near[rows][:, None] * nq + np.arange(nq)[None, :]).astype(np.int32)
-    data = np.zeros((len(rows), nq))
+    data = np.zeros((len(rows), nq), theta.dtype)
     for e in np.unique(near[rows]):
         sel = np.nonzero(near[rows] == e)[0]
         Le = b[e * nq:(e + 1) * nq].T                                   # basis x nq

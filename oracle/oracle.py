@@ -334,8 +334,11 @@ def _pl_dx(C, d):
     return out
 
 
-def vdim_basis(order, size=None, dim=2):
-    """[(p, P)] for x^α/α!, |α| <= order, the first index fastest."""
+def vdim_basis(order, size=None, dim=2, k=None):
+    """[(p, P)] for x^α/α!, |α| <= order, the first index fastest.  ΔP = p
+    (Laplace, Almansi expansion) or, with a wavenumber k, ΔP + k²P = p
+    (Helmholtz: P = Σ_j (−1)^j Δ^j p / k^(2j+2), the unique polynomial
+    solution, src/vdim.jl:369-373)."""
     size = size or order + 2 * (order // 2 + 1) + 3
     out = []
     for rev in itertools.product(range(order + 1), repeat=dim):
@@ -345,6 +348,14 @@ def vdim_basis(order, size=None, dim=2):
         p = np.zeros((size,) * dim)
         p[alpha] = 1.0 / math.prod(math.factorial(a) for a in alpha)
         m, P, term, j, c = sum(alpha), np.zeros((size,) * dim), p.copy(), 0, 0.0
+        if k is not None:
+            c = 1.0 / (k * k)
+            while np.any(term):
+                P = P + c * term
+                term = _pl_lap(term)
+                c = -c / (k * k)
+            out.append((p, P))
+            continue
         while np.any(term):
             c = 1.0 / (2 * (2 * m + dim)) if j == 0 else -c / ((2 * j + 2) * (2 * m - 2 * j + dim))
             T = term
@@ -358,34 +369,35 @@ def vdim_basis(order, size=None, dim=2):
 
 
 def vdim(tcoords, vcoords, vweights, nq, bcoords, bnormals, bweights, bnq, green_multiplier, order,
-         maxdist=np.inf, same=False):
-    """(near_elem, values (m, nq)) of δV; `same` when the targets are the volume nodes."""
-    import scipy.sparse as sp
+         maxdist=np.inf, same=False, pde=LAPLACE, k=0.0):
+    """(near_elem, values (m, nq)) of δV (src/vdim.jl:30-130, 261-285);
+    `same` when the targets are the volume nodes; Laplace (2D, 3D) or
+    Helmholtz (3D, wavenumber k)."""
     from scipy.spatial import cKDTree
 
     T, Y = _c(tcoords), _c(vcoords)
     m = T.shape[0]
     mu = np.broadcast_to(np.asarray(green_multiplier, dtype=np.float64), (m,))
     dim = Y.shape[1]
-    basis = vdim_basis(order, dim=dim)
+    basis = vdim_basis(order, dim=dim, k=k if pde == HELMHOLTZ else None)
     b = np.stack([_pl_eval(p, Y) for p, _ in basis], axis=1)
     g0 = np.stack([_pl_eval(P, bcoords) for _, P in basis], axis=1)
     g1 = np.stack([sum(_pl_eval(_pl_dx(P, d), bcoords) * bnormals[:, d] for d in range(dim)) for _, P in basis], axis=1)
-    near_b, bS, bD = bdim_targets(LAPLACE, 0.0, T, bcoords, bnormals, bweights, bnq, mu, maxdist=maxdist)
+    near_b, bS, bD = bdim_targets(pde, k, T, bcoords, bnormals, bweights, bnq, mu, maxdist=maxdist)
     ipS, ixS, dvS = targets_csr(near_b, bS, bnq, len(bcoords))
     ipD, ixD, dvD = targets_csr(near_b, bD, bnq, len(bcoords))
-    theta = np.zeros((m, len(basis)))
+    theta = np.zeros((m, len(basis)), np.complex128 if pde == HELMHOLTZ else np.float64)
     for n in range(len(basis)):
-        sg = apply(LAPLACE, SL, 0.0, T, None, bcoords, bnormals, bweights, g1[:, n]) + csr_apply(ipS, ixS, dvS, g1[:, n])
-        dg = apply(LAPLACE, DL, 0.0, T, None, bcoords, bnormals, bweights, g0[:, n]) + csr_apply(ipD, ixD, dvD, g0[:, n])
-        vb = apply(LAPLACE, SL, 0.0, T, None, Y, None, vweights, b[:, n])
+        sg = apply(pde, SL, k, T, None, bcoords, bnormals, bweights, g1[:, n]) + csr_apply(ipS, ixS, dvS, g1[:, n])
+        dg = apply(pde, DL, k, T, None, bcoords, bnormals, bweights, g0[:, n]) + csr_apply(ipD, ixD, dvD, g0[:, n])
+        vb = apply(pde, SL, k, T, None, Y, None, vweights, b[:, n])
         theta[:, n] = sg - dg - vb + mu * _pl_eval(basis[n][1], T)
     if same:
         near = np.arange(m) // nq
     else:
         d, j = cKDTree(Y).query(T)
         near = np.where(d <= maxdist, j // nq, -1)
-    vals = np.zeros((m, nq))
+    vals = np.zeros((m, nq), theta.dtype)
     for i in np.nonzero(near >= 0)[0]:
         e = near[i]
         Le = b[e * nq:(e + 1) * nq].T

@@ -332,6 +332,27 @@ def test_vdim_ball_known_answers():
         assert err < 1e-6 and err < err0 / 1e3, (err, err0)
 
 
+# VDIM in the unit ball, 3D Helmholtz (src/vdim.jl:369-373: the polynomial
+# solutions of ΔP + k²P = p, unique): V[1] = -1/k² + (1 - ik) e^{ik}
+# sin(kr) / (k³ r) inside, the outgoing volume potential of the indicator
+# (radial, regular at 0, matched to e^{ikr}/r at r = 1; k -> 0 gives the
+# Laplace (3 - r²)/6).
+@pytest.mark.parametrize("k", [2.0, 4.0])
+def test_vdim_ball_helmholtz_known_answer(k):
+    Y = G.ball_hex_quadrature(2)
+    B = G.ellipsoid_quadrature(16, 5, scaling=(1.0, 1.0, 1.0))
+    near, vals = O.vdim(Y.coords, Y.coords, Y.weights, Y.nq, B.coords, B.normals, B.weights, B.nq, -1.0, 2,
+                        same=True, pde=O.HELMHOLTZ, k=k)
+    ip, ix, dv = O.targets_csr(near, vals, Y.nq, len(Y))
+    r = np.sqrt((Y.coords ** 2).sum(1))
+    exact = -1 / k ** 2 + (1 - 1j * k) * np.exp(1j * k) * np.sin(k * r) / (k ** 3 * r)
+    f = np.ones(len(Y))
+    V0 = O.apply(O.HELMHOLTZ, O.SL, k, Y.coords, None, Y.coords, None, Y.weights, f)
+    Vc = V0 + O.csr_apply(ip, ix, dv, f)
+    err0, err = np.max(np.abs(V0 - exact)), np.max(np.abs(Vc - exact))
+    assert err < 1e-6 and err < err0 / 1e3, (err, err0)
+
+
 def test_ball_quadrature_moments():
     """Volume and second moment of the curved-hexahedron ball converge."""
     errs = []
