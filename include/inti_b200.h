@@ -197,9 +197,14 @@ int inti_ctx_set_autotune(inti_ctx* ctx, int enable);  /* default on */
  * and only the dipole or the normal changes; the hypersingular kernel is
  * symmetric in the pair).  The partial sums are reduced in a fixed order, so results
  * are deterministic; they differ from the one-sided kernel's by rounding.
- * The column partials take N^2 / (256 or 512) values; operators whose
- * partials would exceed a quarter of the device memory free at creation (or
- * 64 GB) keep the one-sided kernel.  For symmetric operators
+ * The row and column partials take up to N^2 / (256 or 512) values.  While
+ * they fit the partial budget (2e9 bytes, or a quarter of the device memory
+ * free at creation if less) the work runs in one launch; beyond it the work
+ * items are grouped into panels of source blocks, run one after another with
+ * the partials of one panel at a time, so the operator's memory stays O(N)
+ * plus the budget (inti_op_panels reports the panel count, 1 for one
+ * launch).  inti_ctx_set_partial_budget sets the budget for operators
+ * created afterwards (bytes; 0 restores 2e9).  For symmetric operators
  * inti_op_tuning reports the targets per thread and the source blocks per
  * work item.  inti_ctx_set_symmetric(ctx, 0) makes operators created
  * afterwards use the one-sided kernel; inti_op_symmetric returns 1 when an
@@ -207,6 +212,8 @@ int inti_ctx_set_autotune(inti_ctx* ctx, int enable);  /* default on */
  * reference, which evaluates every ordered pair (src/nystrom.jl:117-124). */
 int inti_ctx_set_symmetric(inti_ctx* ctx, int enable);  /* default on */
 int inti_op_symmetric(const inti_op* op);
+int inti_ctx_set_partial_budget(inti_ctx* ctx, double bytes);
+int inti_op_panels(const inti_op* op);
 /* Item shard of a symmetric operator for one process per GPU: after
  * inti_op_set_shard(op, r, P), inti_op_apply on rank r computes this rank's
  * share of the unordered node pairs (every P-th work item, largest first,

@@ -128,10 +128,21 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
     L.sym_rowptr = L.sym_items + 3 * op->sym_nitems;
     L.sym_rowitems = L.sym_rowptr + op->sym_nb + 1;
     L.zpart = op->zpart.p;
+    L.sym_npanels = (int)op->sym_panels.size();
+    if (L.sym_npanels > 1) {
+      L.sym_panels = op->sym_panels.data();
+      L.sym_table = op->sym_tab.as<int32_t>();
+      L.sym_zld = op->sym_zld;
+      L.sym_acc = op->sym_acc.p;
+      const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
+      L.sym_ypart_bytes = pb * op->sym_nitems * pair_symm_block(op->tpt);
+      L.sym_zpart_bytes = pb * op->sym_nb * op->sym_zld;
+    }
     if (op->shard_n > 1) {
       L.sym_launch_items = op->shard_items;
       L.sym_launch = op->shard_tab.as<int32_t>();
       L.sym_launch_ids = L.sym_launch + 3 * op->shard_items;
+      L.sym_launch_panels = op->shard_panels.data();
     }
   }
   return L;
@@ -144,10 +155,13 @@ void op_apply_device(inti_op* op, const double* x, double* y, const double* alph
   if (op->shard_n > 1) {
     // this rank's items only: the partials of the others' items are zero, and
     // the correction and beta*y belong to rank 0 (the ranks' y are summed)
-    const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
-    INTI_CUDA(cudaMemsetAsync(op->partial.p, 0, pb * op->sym_nitems * pair_symm_block(op->tpt), op->ctx->stream));
-    INTI_CUDA(cudaMemsetAsync(op->zpart.p, 0, pb * op->sym_nb * op->n_tiles * pair_tile(op->precision),
-                              op->ctx->stream));
+    // (with panels pair_launch clears them before each panel)
+    if (L.sym_npanels <= 1) {
+      const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
+      INTI_CUDA(cudaMemsetAsync(op->partial.p, 0, pb * op->sym_nitems * pair_symm_block(op->tpt), op->ctx->stream));
+      INTI_CUDA(cudaMemsetAsync(op->zpart.p, 0, pb * op->sym_nb * op->n_tiles * pair_tile(op->precision),
+                                op->ctx->stream));
+    }
     pair_launch(op->ctx, L);
     const double zero[2] = {0.0, 0.0};
     const bool lead = op->shard_rank == 0;
@@ -603,6 +617,19 @@ int inti_op_set_shard(inti_op* op, int rank, int nranks) {
 int inti_op_symmetric(const inti_op* op) {
   if (!op) return -INTI_E_ARG;
   return op->symm ? 1 : 0;
+}
+
+int inti_ctx_set_partial_budget(inti_ctx* ctx, double bytes) {
+  if (!ctx) return INTI_E_ARG;
+  return guarded(ctx, [&] {
+    if (!(bytes >= 0.0) || !std::isfinite(bytes)) throw Error(INTI_E_ARG, "the partial budget must be >= 0 bytes");
+    ctx->symm_budget = bytes > 0.0 ? bytes : 2.0e9;
+  });
+}
+
+int inti_op_panels(const inti_op* op) {
+  if (!op) return -INTI_E_ARG;
+  return op->symm ? (int)op->sym_panels.size() : 0;
 }
 
 int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype) {

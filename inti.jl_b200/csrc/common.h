@@ -92,6 +92,9 @@ struct inti_ctx {
   // square operators created while this is set use the symmetric pair
   // kernel (inti_ctx_set_symmetric)
   bool symmetric = true;
+  // bytes of row and column partials a symmetric operator may hold before
+  // its work is split into panels (inti_ctx_set_partial_budget)
+  double symm_budget = 2.0e9;
   // GMRES workspace kept between solves: Krylov basis, work vectors, the
   // reduction scratch and the staged right-hand side / solution.
   struct {
@@ -149,6 +152,18 @@ struct ProfScope {
 enum Pde { LAPLACE = INTI_LAPLACE, HELMHOLTZ = INTI_HELMHOLTZ };
 enum Kind { SL = INTI_SL, DL = INTI_DL, ADL = INTI_ADL, HS = INTI_HS, CF = 4 /* c1*DL + c2*SL */ };
 
+// A panel of the symmetric form's work items: those whose source blocks lie
+// in [col0, col0 + ncols).  Panels run one after another, so the column
+// partials of one panel at a time are held (nb x ncols blocks).  Offsets are
+// int32 indices into the plan table: items (3 x nitems), row pointers
+// (rows + 1, panel-local item indices) and row items (nitems); rows = the
+// row blocks with items in the panel (0 .. rows - 1).
+struct SymPanel {
+  int item_off = 0, nitems = 0;
+  int rowptr_off = 0, rowitems_off = 0, rows = 0;
+  int col0 = 0, ncols = 0;
+};
+
 // Per-apply description of the pair product A*x for one right-hand side.
 struct PairLaunch {
   int pde, kind, dim, precision;
@@ -179,6 +194,19 @@ struct PairLaunch {
   int sym_launch_items = 0;
   const int32_t* sym_launch = nullptr;    // 3 x sym_launch_items
   const int32_t* sym_launch_ids = nullptr;
+  // More than one panel: the panels (host array) index the plan table
+  // sym_table; their column partials (rows of sym_zld nodes) are folded
+  // into the running sums sym_acc (n x 8 B real, 16 B complex) after each
+  // panel, and the epilogue reads sym_acc.  A shard launches, per panel p,
+  // the sym_launch_panels[2p + 1] items at sym_launch_panels[2p] of its
+  // table, clearing the sym_ypart_bytes / sym_zpart_bytes of partials first.
+  int sym_npanels = 1;
+  const SymPanel* sym_panels = nullptr;
+  const int32_t* sym_table = nullptr;
+  int64_t sym_zld = 0;
+  void* sym_acc = nullptr;
+  const int32_t* sym_launch_panels = nullptr;
+  size_t sym_ypart_bytes = 0, sym_zpart_bytes = 0;
 };
 
 // Message for inti_last_error(NULL) from entry points that take no context.
@@ -196,10 +224,14 @@ int pair_symm_record_bytes(int pde, int kind, int dim, int precision);  // packe
 // Bytes of one partial accumulator per target per split.
 int pair_partial_bytes(int pde, int precision);
 // Symmetric form: node block of 128*tpt nodes; work items of row blocks
-// against chunks of `ch` source blocks (the longest first), the table laid
-// out as items (3 x nitems), row pointers (nb + 1), row items (nitems).
+// against chunks of `ch` source blocks (the longest first), grouped into
+// panels of `pcols` source blocks (pcols >= nb: one panel).  Per panel the
+// table holds items (3 x nitems), row pointers (rows + 1) and row items
+// (nitems); one panel gives the layout items, row pointers (nb + 1), row
+// items.  nitems returns the largest panel's item count.
 int pair_symm_block(int tpt);
-void pair_symm_plan(int64_t n, int tpt, int ch, std::vector<int32_t>& table, int& nb, int& nitems);
+void pair_symm_plan(int64_t n, int tpt, int ch, int pcols, std::vector<int32_t>& table,
+                    std::vector<SymPanel>& panels, int& nb, int& nitems);
 int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t n, int tpt);
 // Choose the split for a problem on this device.
 int pair_plan_split(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t m,

@@ -149,6 +149,137 @@ __global__ void __launch_bounds__(kStreamThreads) csr_stream_kernel(
   }
 }
 
+// Bulk-staged row blocks, the form used for short rows: as csr_stream_kernel
+// a CTA owns a block of rows whose nonzeros are one contiguous range
+// [p0, p1), but the range's values and column indices are brought into
+// shared memory by the bulk-copy (TMA) engine: one elected thread issues two
+// cp.async.bulk copies of the 16-byte-aligned interiors, completing on one
+// mbarrier, so the whole range is in flight at once instead of one load per
+// thread.  The unaligned head and tail (< 16 bytes of each array) are plain
+// loads.  Shared-memory slots are offset so that the interiors land 16-byte
+// aligned: element p sits at vals[p - (p0 & ~(16/VB - 1))] and
+// cols[p - (p0 & ~3)].  Then each thread forms products with the gathered x
+// in place, and one thread per row sums its segment in order.  A range
+// longer than the buffers takes the warp-per-row path.  The wait is bounded:
+// on a timeout the CTA records the error, waits once more for its copies
+// and leaves.
+constexpr int kBulkThreads = 256;
+constexpr int kBulkNnz = 2560;  // nonzeros staged per CTA
+
+template <bool CPLX>
+constexpr size_t csr_bulk_smem() {
+  return (size_t)(kBulkNnz + 2) * (CPLX ? 16 : 8) + (size_t)(kBulkNnz + 4) * 4;
+}
+
+template <bool CPLX>
+__global__ void __launch_bounds__(kBulkThreads) csr_bulk_kernel(
+    int64_t m, int rows_per_block, const int64_t* __restrict__ rowptr, const int32_t* __restrict__ col,
+    const double* __restrict__ val, const double* __restrict__ x, double* __restrict__ y, double ar,
+    double ai, double br, double bi, bool beta_zero, int* err) {
+  constexpr int VB = CPLX ? 16 : 8;   // bytes per value
+  constexpr int VA = 16 / VB;          // values per 16 bytes
+  extern __shared__ __align__(16) unsigned char csm[];
+  double* sval = reinterpret_cast<double*>(csm);
+  int32_t* scol = reinterpret_cast<int32_t*>(csm + (size_t)(kBulkNnz + 2) * VB);
+  __shared__ __align__(8) uint64_t bar;
+  const int64_t r0 = (int64_t)blockIdx.x * rows_per_block;
+  const int64_t r1 = r0 + rows_per_block < m ? r0 + rows_per_block : m;
+  const int64_t p0 = rowptr[r0], p1 = rowptr[r1];
+  const int tid = threadIdx.x;
+  if (p1 - p0 <= kBulkNnz) {
+    const int64_t sv = p0 & ~(int64_t)(VA - 1), sc = p0 & ~(int64_t)3;  // slot origins
+    const int64_t va = (p0 + VA - 1) & ~(int64_t)(VA - 1), vb = p1 & ~(int64_t)(VA - 1);
+    const int64_t ca = (p0 + 3) & ~(int64_t)3, cb = p1 & ~(int64_t)3;
+    const uint32_t vbytes = vb > va ? (uint32_t)((vb - va) * VB) : 0u;
+    const uint32_t cbytes = cb > ca ? (uint32_t)((cb - ca) * 4) : 0u;
+    const bool bulk = vbytes + cbytes > 0;
+    if (tid == 0 && bulk) {
+      mbar_init(&bar, 1);
+      mbar_fence_init();
+    }
+    __syncthreads();
+    if (tid == 0 && bulk) {
+      mbar_arrive_expect_tx(&bar, vbytes + cbytes);
+      if (vbytes)
+        bulk_copy_g2s(reinterpret_cast<unsigned char*>(sval) + (va - sv) * VB,
+                      reinterpret_cast<const unsigned char*>(val) + va * VB, vbytes, &bar);
+      if (cbytes) bulk_copy_g2s(scol + (ca - sc), col + ca, cbytes, &bar);
+    }
+    // heads and tails outside the aligned interiors
+    for (int64_t p = p0 + tid; p < p1; p += kBulkThreads) {
+      if (p < va || p >= vb) {
+        if (CPLX)
+          reinterpret_cast<double2*>(sval)[p - sv] = reinterpret_cast<const double2*>(val)[p];
+        else
+          sval[p - sv] = val[p];
+      }
+      if (p < ca || p >= cb) scol[p - sc] = col[p];
+    }
+    if (bulk) {
+      const bool ok = mbar_wait_bounded(&bar, 0);
+      if (!__syncthreads_and(ok)) {
+        if (tid == 0) {
+          atomicExch(err, kErrWaitTimeout);
+          mbar_wait_bounded(&bar, 0);
+        }
+        return;
+      }
+    } else {
+      __syncthreads();
+    }
+    // products in place
+    for (int64_t p = p0 + tid; p < p1; p += kBulkThreads) {
+      const int32_t j = scol[p - sc];
+      if (CPLX) {
+        double2* v = reinterpret_cast<double2*>(sval) + (p - sv);
+        const double2 a = *v;
+        const double2 xv = __ldg(reinterpret_cast<const double2*>(x) + j);
+        *v = make_double2(fma(a.x, xv.x, -a.y * xv.y), fma(a.x, xv.y, a.y * xv.x));
+      } else {
+        sval[p - sv] *= __ldg(x + j);
+      }
+    }
+    __syncthreads();
+    for (int64_t row = r0 + tid; row < r1; row += kBulkThreads) {
+      const int64_t a = rowptr[row] - sv, b = rowptr[row + 1] - sv;
+      double sr = 0.0, si = 0.0;
+      for (int64_t q = a; q < b; ++q) {
+        if (CPLX) {
+          const double2 v = reinterpret_cast<const double2*>(sval)[q];
+          sr += v.x;
+          si += v.y;
+        } else {
+          sr += sval[q];
+        }
+      }
+      csr_finish<CPLX>(row, sr, si, y, ar, ai, br, bi, beta_zero);
+    }
+    return;
+  }
+  // overflow: one warp per row, lanes striding the row, shuffle reduction
+  const int warp = tid >> 5, lane = tid & 31;
+  for (int64_t row = r0 + warp; row < r1; row += kBulkThreads / 32) {
+    double sr = 0.0, si = 0.0;
+    for (int64_t p = rowptr[row] + lane; p < rowptr[row + 1]; p += 32) {
+      const int32_t j = __ldg(col + p);
+      if (CPLX) {
+        const double2 v = __ldg(reinterpret_cast<const double2*>(val) + p);
+        const double2 xv = __ldg(reinterpret_cast<const double2*>(x) + j);
+        sr = fma(v.x, xv.x, fma(-v.y, xv.y, sr));
+        si = fma(v.x, xv.y, fma(v.y, xv.x, si));
+      } else {
+        sr = fma(__ldg(val + p), __ldg(x + j), sr);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      sr += __shfl_xor_sync(0xffffffffu, sr, o);
+      if (CPLX) si += __shfl_xor_sync(0xffffffffu, si, o);
+    }
+    if (lane == 0) csr_finish<CPLX>(row, sr, si, y, ar, ai, br, bi, beta_zero);
+  }
+}
+
 template <int G>
 static void csr_go(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, double ar,
                    double ai, double br, double bi, bool bz) {
@@ -175,16 +306,23 @@ int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, cons
   ProfScope pc(ctx, "csr");
   const bool cplx = c->dtype == INTI_C128;
   if (mean <= 64) {
-    // rows per CTA: fill ~80% of the product buffer at the mean row length
-    const int cap = kStreamBytes / (cplx ? 16 : 8);
-    const int rpb = (int)std::max<double>(1.0, std::min<double>(kStreamThreads, 0.8 * cap / std::max(mean, 1.0)));
+    // rows per CTA: fill ~90% of the staging buffers at the mean row length
+    const int rpb = (int)std::max<double>(1.0, std::min<double>(kBulkThreads, 0.9 * kBulkNnz / std::max(mean, 1.0)));
     const unsigned grid = (unsigned)((c->m + rpb - 1) / rpb);
-    if (cplx)
-      csr_stream_kernel<true><<<grid, kStreamThreads, 0, ctx->stream>>>(
-          c->m, rpb, c->rowptr.as<int64_t>(), c->col.as<int32_t>(), c->val.as<double>(), x, y, ar, ai, br, bi, bz);
-    else
-      csr_stream_kernel<false><<<grid, kStreamThreads, 0, ctx->stream>>>(
-          c->m, rpb, c->rowptr.as<int64_t>(), c->col.as<int32_t>(), c->val.as<double>(), x, y, ar, ai, br, bi, bz);
+    int* err = ctx->err_flag.as<int>();
+    if (cplx) {
+      const size_t sm = csr_bulk_smem<true>();
+      INTI_CUDA(cudaFuncSetAttribute(&csr_bulk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      csr_bulk_kernel<true><<<grid, kBulkThreads, sm, ctx->stream>>>(
+          c->m, rpb, c->rowptr.as<int64_t>(), c->col.as<int32_t>(), c->val.as<double>(), x, y, ar, ai, br, bi, bz,
+          err);
+    } else {
+      const size_t sm = csr_bulk_smem<false>();
+      INTI_CUDA(cudaFuncSetAttribute(&csr_bulk_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+      csr_bulk_kernel<false><<<grid, kBulkThreads, sm, ctx->stream>>>(
+          c->m, rpb, c->rowptr.as<int64_t>(), c->col.as<int32_t>(), c->val.as<double>(), x, y, ar, ai, br, bi, bz,
+          err);
+    }
   } else {
     csr_go<32>(ctx, c, x, y, ar, ai, br, bi, bz);
   }

@@ -3,6 +3,7 @@
 
 #include <atomic>
 #include <memory>
+#include <vector>
 
 #include "common.h"
 
@@ -41,10 +42,17 @@ struct inti_op {
   bool symm = false;
   int sym_nb = 0, sym_nitems = 0;
   inti::DevBuf sym_tab, zpart;
+  // panels of the work items (one unless the column partials of the whole
+  // operator would pass the partial budget), their running sums
+  std::vector<inti::SymPanel> sym_panels;
+  int64_t sym_zld = 0;
+  double sym_budget = 0.0;  // bytes of partials allowed, fixed at creation
+  inti::DevBuf sym_acc;
   // item shard of this operator (inti_op_set_shard): rank, ranks, and the
-  // rank's items (3 x n) followed by their ids
+  // rank's items (3 x n) followed by their ids; per panel (offset, count)
   int shard_rank = 0, shard_n = 1, shard_items = 0;
   inti::DevBuf shard_tab;
+  std::vector<int32_t> shard_panels;
   int64_t n_tiles = 1, tn_tiles = 1;
   // Derived operators kept for repeated solves: the FP32C twin used by the
   // mixed-precision GMRES, and (on a double layer) the combined-field operator

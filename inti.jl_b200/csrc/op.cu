@@ -20,9 +20,9 @@ static void req(bool c, int code, const std::string& m) {
   if (!c) throw Error(code, m);
 }
 
-inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
-                   const inti_quad* target, const inti_quad* source, const inti_csr* correction,
-                   int precision) {
+// The checks of op_create, without creating anything.
+static void op_validate(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im, const inti_quad* target,
+                        const inti_quad* source, const inti_csr* correction, int precision) {
   req(target && source, INTI_E_ARG, "target/source quadrature is NULL");
   req(target->ctx == ctx && source->ctx == ctx, INTI_E_STATE, "quadrature belongs to another context");
   req(pde == INTI_LAPLACE || pde == INTI_HELMHOLTZ, INTI_E_ARG, "unknown pde");
@@ -46,6 +46,13 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
     req(correction->dtype == (pde == INTI_HELMHOLTZ ? INTI_C128 : INTI_F64), INTI_E_ARG,
         "correction dtype must be F64 for Laplace and C128 for Helmholtz");
   }
+}
+
+inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
+                   const inti_quad* target, const inti_quad* source, const inti_csr* correction,
+                   int precision) {
+  op_validate(ctx, pde, kernel, k_re, k_im, target, source, correction, precision);
+  const int dim = source->dim;
   std::unique_ptr<inti_op> op(new inti_op());
   op->ctx = ctx;
   op->pde = pde;
@@ -140,10 +147,8 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   if (!cplx) req(c_dl[1] == 0.0 && c_sl[1] == 0.0, INTI_E_UNSUPPORTED,
                  "complex coefficients need a Helmholtz (complex) operator");
   // validate both halves like two ordinary operators
-  std::unique_ptr<inti_op> probe_d(op_create(ctx, pde, INTI_DL, k_re, k_im, target, source, corr_dl, precision));
-  std::unique_ptr<inti_op> probe_s(op_create(ctx, pde, INTI_SL, k_re, k_im, target, source, corr_sl, precision));
-  probe_d.reset();
-  probe_s.reset();
+  op_validate(ctx, pde, INTI_DL, k_re, k_im, target, source, corr_dl, precision);
+  op_validate(ctx, pde, INTI_SL, k_re, k_im, target, source, corr_sl, precision);
   std::unique_ptr<inti_op> op(new inti_op());
   op->ctx = ctx;
   op->pde = pde;
@@ -206,19 +211,77 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
   return t.release();
 }
 
-// Column partials of the symmetric form are nb x n values (N^2/256 at 2
-// targets per thread).  An operator takes the symmetric form while they fit
-// in a quarter of the device memory free at its creation and 64 GB (N of
-// about 1.4e6 real, 1e6 complex on an empty 180 GB device); larger ones keep
-// the one-sided kernel.  Writing and summing the partials costs O(N^2/256)
-// memory traffic against the O(N^2) pair evaluations they save.
-constexpr double kSymmMaxPartialBytes = 64.0e9;
+// The symmetric form keeps per work item a row partial (128*tpt values) and
+// per row block a column partial of each later node (nb x n values, N^2/512
+// at 4 targets per thread).  While both fit the partial budget (2 GB, and a
+// quarter of the device memory free at creation; the budget is the
+// context's, inti_ctx_set_partial_budget) the items run in one launch.  Beyond it the items are grouped into panels of source blocks: a
+// panel's launch writes the column partials of its own nodes only
+// (nb x panel width), a fold kernel adds them and the row partials into
+// running sums, and the next panel reuses the buffers.  Memory stays
+// O(N) + the budget; the pair evaluations are the same.
 constexpr double kSymmMaxFreeShare = 0.25;
+
+namespace {
+
+// Partial bytes of a symmetric plan with panels of pcols source blocks.
+double symm_partial_bytes(int64_t n, int tpt, int ch, int pcols, int pb) {
+  const int64_t bt = pair_symm_block(tpt);
+  const int64_t nb = std::max<int64_t>(1, (n + bt - 1) / bt);
+  const int64_t pc = std::max<int64_t>(1, std::min<int64_t>(pcols, nb));
+  const int64_t cw = std::max<int64_t>(1, std::min<int64_t>(ch, pc));
+  const double items = (double)nb * (double)((pc + cw - 1) / cw);  // per panel, at most
+  const double zl = pc >= nb ? (double)((n + 511) / 512 * 512) : (double)(pc * bt);
+  return ((double)nb * zl + items * (double)bt) * pb;
+}
+
+}  // namespace
+
+// Widest panel (in source blocks) whose partials fit `budget`; 0 if none does.
+int symm_panel_width(int64_t n, int tpt, int ch, int pb, double budget) {
+  const int64_t bt = pair_symm_block(tpt);
+  const int nb = (int)std::max<int64_t>(1, (n + bt - 1) / bt);
+  if (symm_partial_bytes(n, tpt, ch, nb, pb) <= budget) return nb;
+  int lo = 0, hi = nb - 1;  // largest pcols in [1, nb) that fits
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) / 2;
+    if (symm_partial_bytes(n, tpt, ch, mid, pb) <= budget) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Panel width and source blocks per item of a plan.  With several panels an
+// item spans at most an eighth of a panel, so that each panel's launch has
+// many items and a short tail.
+void symm_layout(int64_t n, int tpt, int ch, int pb, double budget, int& pcols, int& ch_eff) {
+  const int64_t bt = pair_symm_block(tpt);
+  const int nb = (int)std::max<int64_t>(1, (n + bt - 1) / bt);
+  ch_eff = std::max(1, ch);
+  pcols = std::max(1, symm_panel_width(n, tpt, ch_eff, pb, budget));
+  if (pcols >= nb) return;
+  for (int it = 0; it < 4; ++it) {
+    const int c = std::max(1, std::min(ch_eff, pcols / 8));
+    if (c == ch_eff) break;
+    ch_eff = c;
+    pcols = std::max(1, symm_panel_width(n, tpt, ch_eff, pb, budget));
+  }
+}
+
+double symm_budget(const inti_op* op) {
+  size_t free_b = 0, total_b = 0;
+  INTI_CUDA(cudaMemGetInfo(&free_b, &total_b));
+  return std::min(op->ctx->symm_budget,
+                  kSymmMaxFreeShare * (double)free_b + op->partial.bytes + op->zpart.bytes);
+}
 
 void op_symm_configure(inti_op* op, int tpt, int ch) {
   std::vector<int32_t> tab;
   int nb = 0, nitems = 0;
-  pair_symm_plan(op->source->n, tpt, ch, tab, nb, nitems);
+  const int pb = pair_partial_bytes(op->pde, op->precision);
+  int pcols = 1, ch_eff = 1;
+  symm_layout(op->source->n, tpt, ch, pb, op->sym_budget, pcols, ch_eff);
+  pair_symm_plan(op->source->n, tpt, ch_eff, pcols, tab, op->sym_panels, nb, nitems);
   INTI_CUDA(cudaStreamSynchronize(op->ctx->stream));  // no launch is reading the old table
   op->sym_tab.ensure(sizeof(int32_t) * tab.size());
   INTI_CUDA(cudaMemcpy(op->sym_tab.p, tab.data(), sizeof(int32_t) * tab.size(), cudaMemcpyHostToDevice));
@@ -226,10 +289,12 @@ void op_symm_configure(inti_op* op, int tpt, int ch) {
   op->sym_nitems = nitems;
   op->tpt = tpt;
   op->split = ch;
-  const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
   const int64_t npad = op->n_tiles * pair_tile(op->precision);
-  op->partial.ensure(pb * nitems * pair_symm_block(tpt));
-  op->zpart.ensure(pb * nb * npad);
+  const bool panels = op->sym_panels.size() > 1;
+  op->sym_zld = panels ? (int64_t)pcols * pair_symm_block(tpt) : npad;
+  op->partial.ensure((size_t)pb * nitems * pair_symm_block(tpt));
+  op->zpart.ensure((size_t)pb * nb * op->sym_zld);
+  if (panels) op->sym_acc.ensure(sizeof(double) * (op->pde == INTI_HELMHOLTZ ? 2 : 1) * op->source->n);
   if (op->shard_n > 1) op_set_shard(op, op->shard_rank, op->shard_n);  // the items changed
 }
 
@@ -241,14 +306,29 @@ void op_set_shard(inti_op* op, int rank, int nranks) {
   op->shard_rank = rank;
   op->shard_n = nranks;
   op->shard_items = 0;
+  op->shard_panels.clear();
   if (nranks == 1) return;
   std::vector<int32_t> tab;
+  std::vector<SymPanel> panels;
   int nb = 0, nitems = 0;
-  pair_symm_plan(op->source->n, op->tpt, op->split, tab, nb, nitems);
+  const int pb = pair_partial_bytes(op->pde, op->precision);
+  int pcols = 1, ch_eff = 1;
+  symm_layout(op->source->n, op->tpt, op->split, pb, op->sym_budget, pcols, ch_eff);
+  pair_symm_plan(op->source->n, op->tpt, ch_eff, pcols, tab, panels, nb, nitems);
+  // round robin over the items of each panel (largest first); ids are the
+  // panel-local item indices (the row-partial slots)
   std::vector<int32_t> items, ids;
-  for (int q = rank; q < nitems; q += nranks) {
-    for (int c = 0; c < 3; ++c) items.push_back(tab[3 * q + c]);
-    ids.push_back(q);
+  int global = 0;
+  for (const SymPanel& P : panels) {
+    op->shard_panels.push_back((int32_t)ids.size());
+    int count = 0;
+    for (int q = 0; q < P.nitems; ++q, ++global) {
+      if (global % nranks != rank) continue;
+      for (int c = 0; c < 3; ++c) items.push_back(tab[P.item_off + 3 * q + c]);
+      ids.push_back(q);
+      ++count;
+    }
+    op->shard_panels.push_back(count);
   }
   op->shard_items = (int)ids.size();
   items.insert(items.end(), ids.begin(), ids.end());
@@ -264,16 +344,18 @@ void op_symm_init(inti_op* op) {
   if (!ctx->symmetric || op->target != op->source) return;
   const int64_t n = op->source->n;
   const int tile = pair_tile(op->precision);
-  const int64_t bmax = pair_symm_block(4), bmin = pair_symm_block(2);
+  const int64_t bmax = pair_symm_block(4);
   const int64_t npad = (n + bmax - 1) / bmax * bmax;  // whole blocks for both node-block sizes
-  const double zbytes = (double)((n + bmin - 1) / bmin) * npad * pair_partial_bytes(op->pde, op->precision);
-  size_t free_b = 0, total_b = 0;
-  INTI_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  if (zbytes > std::min(kSymmMaxPartialBytes, kSymmMaxFreeShare * (double)free_b)) return;
+  op->sym_budget = symm_budget(op);
+  // the narrowest panel (one source block, 2 targets per thread) must fit
+  if (symm_panel_width(n, 2, 1, pair_partial_bytes(op->pde, op->precision), op->sym_budget) < 1) return;
   op->symm = true;
   op->n_tiles = npad / tile;
   op->packed.ensure((size_t)npad * pair_symm_record_bytes(op->pde, op->kind, op->dim, op->precision));
-  const int tpt = 2;
+  // untimed default shape: 4 targets per thread for FP32C (two target pairs
+  // of the paired-FP32 kernel; timed picks at C3: 4 / 5 blocks per item),
+  // 2 for FP64
+  const int tpt = op->precision == INTI_FP32C ? 4 : 2;
   op_symm_configure(op, tpt, pair_symm_default_ch(ctx, op->pde, op->kind, op->dim, op->precision, n, tpt));
 }
 

@@ -557,7 +557,8 @@ struct SymArgs {
   const int32_t* ids;     // row-partial slot of each CTA's item (NULL: the CTA index)
   const void* packed;
   void* ypart;            // [item][BT]
-  void* zpart;            // [nb][npad]
+  void* zpart;            // [nb][zld]: node j of the panel's columns at j - zcol0
+  int64_t zld, zcol0;     // one panel: npad and 0
   double k, kT, delta;
   const void* expi;
   int* err;
@@ -911,7 +912,7 @@ __global__ void __launch_bounds__(kBlock) pair_symm(SymArgs a) {
     }
     __syncthreads();  // the stage is read and this tile's column sums are in zb
     if (!diag) {
-      P* zp = static_cast<P*>(a.zpart) + (int64_t)I * a.npad + t * TILE;
+      P* zp = static_cast<P*>(a.zpart) + (int64_t)I * a.zld + (t * TILE - a.zcol0);
       for (int s = tid; s < TILE; s += kBlock) {
         R vr = zb[s * 2], vi = zb[s * 2 + 1];
 #pragma unroll
@@ -1119,7 +1120,7 @@ __global__ void __launch_bounds__(kBlock) pair_symm_x2(SymArgs a) {
     }
     __syncthreads();  // the stage is read and this tile's column sums are in zb
     if (!diag) {
-      float2* zp = static_cast<float2*>(a.zpart) + (int64_t)I * a.npad + t * TILE;
+      float2* zp = static_cast<float2*>(a.zpart) + (int64_t)I * a.zld + (t * TILE - a.zcol0);
       for (int s = tid; s < TILE; s += kBlock) {
         float vr = zb[s * 2];
 #pragma unroll
@@ -1141,6 +1142,68 @@ __global__ void __launch_bounds__(kBlock) pair_symm_x2(SymArgs a) {
 
 // Row sums of the symmetric form: the item partials of row block B and the
 // column partials of the row blocks above.
+// Running sums over panels: for node i of row block B (B < the panel's
+// rows), acc[i] += the panel's row partials of B's items (in order), then,
+// when B is one of the panel's source blocks, the column partials
+// zpart[r][i - col0*bt] of the row blocks r < B.
+struct SymFold {
+  int64_t m;
+  int bt;
+  const int32_t* rowptr;
+  const int32_t* rowitems;
+  const void* ypart;
+  const void* zpart;
+  int64_t zld;
+  int col0, ncols;
+  void* acc;
+};
+
+// Four threads per node: slice s sums the column partials of the row blocks
+// r = s, s + 4, ...; the slices are added in a fixed order (deterministic).
+constexpr int kFoldNodes = 64, kFoldSlices = 4;
+
+template <class P, bool CPLX>
+__global__ void __launch_bounds__(kFoldNodes * kFoldSlices) pair_symm_fold_kernel(SymFold f) {
+  __shared__ double2 part[kFoldSlices][kFoldNodes];
+  const int tn = threadIdx.x % kFoldNodes, sl = threadIdx.x / kFoldNodes;
+  const int64_t i = blockIdx.x * (int64_t)kFoldNodes + tn;
+  const bool live = i < f.m;
+  const int B = live ? (int)(i / f.bt) : 0, il = live ? (int)(i % f.bt) : 0;
+  const P* yp = static_cast<const P*>(f.ypart);
+  const P* zp = static_cast<const P*>(f.zpart);
+  double2 c = make_double2(0.0, 0.0);
+  if (live && B >= f.col0 && B < f.col0 + f.ncols) {
+    const int64_t jl = i - (int64_t)f.col0 * f.bt;
+    for (int r = sl; r < B; r += kFoldSlices) {
+      const double2 v = load_partial(zp + (int64_t)r * f.zld + jl);
+      c.x += v.x;
+      c.y += v.y;
+    }
+  }
+  part[sl][tn] = c;
+  __syncthreads();
+  if (sl != 0 || !live) return;
+  double sr = 0.0, si = 0.0;
+  if (CPLX) {
+    const double2 v = static_cast<const double2*>(f.acc)[i];
+    sr = v.x;
+    si = v.y;
+  } else {
+    sr = static_cast<const double*>(f.acc)[i];
+  }
+  for (int q = f.rowptr[B]; q < f.rowptr[B + 1]; ++q) {
+    const double2 v = load_partial(yp + (int64_t)f.rowitems[q] * f.bt + il);
+    sr += v.x;
+    si += v.y;
+  }
+  sr += (part[0][tn].x + part[1][tn].x) + (part[2][tn].x + part[3][tn].x);
+  si += (part[0][tn].y + part[1][tn].y) + (part[2][tn].y + part[3][tn].y);
+  if (CPLX)
+    static_cast<double2*>(f.acc)[i] = make_double2(sr, si);
+  else
+    static_cast<double*>(f.acc)[i] = sr;
+}
+
 struct SymEpi {
   int64_t npad;
   int bt;
@@ -1404,30 +1467,47 @@ int pair_symm_record_bytes(int pde, int kind, int dim, int precision) {
 
 int pair_symm_block(int tpt) { return kBlock * tpt; }
 
-void pair_symm_plan(int64_t n, int tpt, int ch, std::vector<int32_t>& table, int& nb, int& nitems) {
+void pair_symm_plan(int64_t n, int tpt, int ch, int pcols, std::vector<int32_t>& table,
+                    std::vector<SymPanel>& panels, int& nb, int& nitems) {
   const int bt = pair_symm_block(tpt);
   nb = (int)std::max<int64_t>(1, (n + bt - 1) / bt);
   ch = std::max(1, ch);
-  std::vector<std::array<int32_t, 3>> it;
-  for (int I = 0; I < nb; ++I)
-    for (int J0 = I; J0 < nb; J0 += ch) it.push_back({I, J0, std::min(J0 + ch, nb)});
-  std::stable_sort(it.begin(), it.end(), [](const std::array<int32_t, 3>& a, const std::array<int32_t, 3>& b) {
-    return a[2] - a[1] > b[2] - b[1];
-  });
-  nitems = (int)it.size();
-  table.assign((size_t)3 * nitems + nb + 1 + nitems, 0);
-  int32_t* items = table.data();
-  int32_t* rowptr = items + 3 * nitems;
-  int32_t* rowitems = rowptr + nb + 1;
-  for (int q = 0; q < nitems; ++q) {
-    items[3 * q] = it[q][0];
-    items[3 * q + 1] = it[q][1];
-    items[3 * q + 2] = it[q][2];
-    ++rowptr[it[q][0] + 1];
+  pcols = std::max(1, std::min(pcols, nb));
+  table.clear();
+  panels.clear();
+  nitems = 0;
+  for (int c0 = 0; c0 < nb; c0 += pcols) {
+    const int c1 = std::min(c0 + pcols, nb);
+    std::vector<std::array<int32_t, 3>> it;
+    for (int I = 0; I < c1; ++I)
+      for (int J0 = std::max(I, c0); J0 < c1; J0 += ch) it.push_back({I, J0, std::min(J0 + ch, c1)});
+    std::stable_sort(it.begin(), it.end(), [](const std::array<int32_t, 3>& a, const std::array<int32_t, 3>& b) {
+      return a[2] - a[1] > b[2] - b[1];
+    });
+    SymPanel P;
+    P.col0 = c0;
+    P.ncols = c1 - c0;
+    P.rows = c1;
+    P.nitems = (int)it.size();
+    P.item_off = (int)table.size();  // int32 offset of the items
+    P.rowptr_off = P.item_off + 3 * P.nitems;
+    P.rowitems_off = P.rowptr_off + P.rows + 1;
+    table.resize((size_t)P.rowitems_off + P.nitems, 0);
+    int32_t* items = table.data() + P.item_off;
+    int32_t* rowptr = table.data() + P.rowptr_off;
+    int32_t* rowitems = table.data() + P.rowitems_off;
+    for (int q = 0; q < P.nitems; ++q) {
+      items[3 * q] = it[q][0];
+      items[3 * q + 1] = it[q][1];
+      items[3 * q + 2] = it[q][2];
+      ++rowptr[it[q][0] + 1];
+    }
+    for (int I = 0; I < P.rows; ++I) rowptr[I + 1] += rowptr[I];
+    std::vector<int32_t> fill(rowptr, rowptr + P.rows);
+    for (int q = 0; q < P.nitems; ++q) rowitems[fill[it[q][0]]++] = q;
+    nitems = std::max(nitems, P.nitems);
+    panels.push_back(P);
   }
-  for (int I = 0; I < nb; ++I) rowptr[I + 1] += rowptr[I];
-  std::vector<int32_t> fill(rowptr, rowptr + nb);
-  for (int q = 0; q < nitems; ++q) rowitems[fill[it[q][0]]++] = q;
 }
 
 int pair_symm_default_ch(const inti_ctx* ctx, int pde, int kind, int dim, int precision, int64_t n, int tpt) {
@@ -1521,10 +1601,62 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
                             : &pair_symm<T::pde, T::kind, T::dim, R, TILE, 4>;
           }
           INTI_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-          ProfScope pp(ctx, "pair");
-          const int grid = L.sym_launch ? L.sym_launch_items : L.sym_nitems;
-          if (grid > 0) fn<<<(unsigned)grid, kBlock, sm, ctx->stream>>>(a);
-          launches = 2;
+          a.zld = npad;
+          a.zcol0 = 0;
+          if (L.sym_npanels <= 1) {
+            ProfScope pp(ctx, "pair");
+            const int grid = L.sym_launch ? L.sym_launch_items : L.sym_nitems;
+            if (grid > 0) fn<<<(unsigned)grid, kBlock, sm, ctx->stream>>>(a);
+            launches = 2;
+            return;
+          }
+          // panels one after another; after each, its partials are folded
+          // into the running sums (fixed order: panels ascending)
+          const int bt = pair_symm_block(L.tpt);
+          const bool cplx = T::pde == HELMHOLTZ;
+          INTI_CUDA(cudaMemsetAsync(L.sym_acc, 0, (size_t)L.m * (cplx ? 16 : 8), ctx->stream));
+          a.zld = L.sym_zld;
+          launches = 1;
+          for (int p = 0; p < L.sym_npanels; ++p) {
+            const SymPanel& P = L.sym_panels[p];
+            int grid = P.nitems;
+            a.items = L.sym_table + P.item_off;
+            a.ids = nullptr;
+            if (L.sym_launch) {
+              grid = L.sym_launch_panels[2 * p + 1];
+              a.items = L.sym_launch + 3 * L.sym_launch_panels[2 * p];
+              a.ids = L.sym_launch_ids + L.sym_launch_panels[2 * p];
+              INTI_CUDA(cudaMemsetAsync(L.partial, 0, L.sym_ypart_bytes, ctx->stream));
+              INTI_CUDA(cudaMemsetAsync(L.zpart, 0, L.sym_zpart_bytes, ctx->stream));
+            }
+            a.zcol0 = (int64_t)P.col0 * bt;
+            {
+              ProfScope pp(ctx, "pair");
+              if (grid > 0) fn<<<(unsigned)grid, kBlock, sm, ctx->stream>>>(a);
+            }
+            SymFold f;
+            f.m = std::min<int64_t>(L.m, (int64_t)P.rows * bt);
+            f.bt = bt;
+            f.rowptr = L.sym_table + P.rowptr_off;
+            f.rowitems = L.sym_table + P.rowitems_off;
+            f.ypart = L.partial;
+            f.zpart = L.zpart;
+            f.zld = L.sym_zld;
+            f.col0 = P.col0;
+            f.ncols = P.ncols;
+            f.acc = L.sym_acc;
+            const unsigned gf = (unsigned)((f.m + kFoldNodes - 1) / kFoldNodes);
+            const unsigned tf = kFoldNodes * kFoldSlices;
+            ProfScope pf(ctx, "epilogue");
+            if (std::is_same<R, float>::value) {
+              if (cplx) pair_symm_fold_kernel<float4, true><<<gf, tf, 0, ctx->stream>>>(f);
+              else pair_symm_fold_kernel<float2, false><<<gf, tf, 0, ctx->stream>>>(f);
+            } else {
+              if (cplx) pair_symm_fold_kernel<double2, true><<<gf, tf, 0, ctx->stream>>>(f);
+              else pair_symm_fold_kernel<double, false><<<gf, tf, 0, ctx->stream>>>(f);
+            }
+            launches += 2;
+          }
           return;
         }
       }
@@ -1583,6 +1715,18 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
   const unsigned gb = (unsigned)((L.m + tb - 1) / tb);
   const bool cplx = L.pde == HELMHOLTZ;
   ProfScope pe(ctx, "epilogue");
+  if (L.symm && L.sym_npanels > 1) {
+    // the panels' running sums hold the whole pair product
+    e.partial = L.sym_acc;
+    e.split = 1;
+    if (cplx)
+      pair_epilogue_kernel<double2, true><<<gb, tb, 0, ctx->stream>>>(e);
+    else
+      pair_epilogue_kernel<double, false><<<gb, tb, 0, ctx->stream>>>(e);
+    INTI_CUDA(cudaGetLastError());
+    ctx->launches += 1;
+    return 1;
+  }
   if (L.symm) {
     SymEpi se;
     se.npad = L.n_tiles * pair_tile(L.precision);

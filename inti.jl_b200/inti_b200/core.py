@@ -120,6 +120,12 @@ class Context:
         afterwards (on by default; see ``GpuOperator.tuning``)."""
         self.check(self.lib.inti_ctx_set_symmetric(self.handle, int(bool(enable))))
 
+    def set_partial_budget(self, nbytes: float) -> None:
+        """Bytes of partial sums a symmetric operator created afterwards may
+        hold before its work is split into panels run one after another
+        (0 restores the default, 2e9)."""
+        self.check(self.lib.inti_ctx_set_partial_budget(self.handle, float(nbytes)))
+
     def selftest_math(self) -> dict:
         """Accuracy of the device's fast rsqrt / e^{iθ} helpers (see the ABI)."""
         out = (C.c_double * 5)()
@@ -533,7 +539,8 @@ class GpuOperator(_Map):
         t, s = C.c_int32(), C.c_int32()
         self.ctx.check(self.ctx.lib.inti_op_tuning(self.handle, C.byref(t), C.byref(s)))
         return {"targets_per_thread": t.value, "split": s.value,
-                "symmetric": bool(self.ctx.lib.inti_op_symmetric(self.handle) == 1)}
+                "symmetric": bool(self.ctx.lib.inti_op_symmetric(self.handle) == 1),
+                "panels": int(self.ctx.lib.inti_op_panels(self.handle))}
 
     def set_shard(self, rank: int, nranks: int) -> None:
         """Compute only rank ``rank``'s share of the node pairs (symmetric

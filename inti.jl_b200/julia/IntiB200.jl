@@ -16,7 +16,8 @@ extension does (ext/IntiFMM3DExt.jl:12-33): node arrays are repacked as
 
 The C ABI is declared in include/inti_b200.h.  Julia was not available where
 this package was developed; the entry points it calls are exercised from
-Python (ctypes) by the repository's tests.
+Python (ctypes) by the repository's tests.  Package dependencies: Inti,
+LinearMaps and ChainRulesCore (the reverse rule of `A * σ`).
 """
 module IntiB200
 
