@@ -59,7 +59,7 @@ FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "lap
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one pair-kernel
 # launch per workload, from the ncu capture of that launch summarised in
 # profiles/ (the file named beside each entry); None where no capture exists.
-PAIR_TRAFFIC_BYTES = {"c2": (67.32e6, "profiles/pair_symm_helmholtz_sl_fp64_p2sphere62k.md")}
+PAIR_TRAFFIC_BYTES = {"c2": (66.74e6, "profiles/pair_symm_helmholtz_sl_fp64_p2sphere62k.md")}
 # Fallback HBM copy bandwidth (GB/s) when MEASURED_PEAKS.json is absent
 HBM_FALLBACK_GBS = 6650.0
 
