@@ -534,9 +534,15 @@ def bench_batch(args, ctx, peaks, torch) -> dict:
                       f"(C++ FP64 restatement of the reference's per-RHS matvec), {dt:.1f} s"}
     if not args.no_gmres:
         # scattering solves (I/2 + D - i k S) sigma = -u_inc for all 32 x 64 systems
-        g = {"rtol": 1e-10, "restart": 30, "systems": len(quads) * nrhs}
+        g = {"rtol": 1e-10, "restart": 30, "systems": len(quads) * nrhs,
+             "timing": "wall time of the whole solve call: right-hand sides and solutions in page-locked host "
+                       "buffers, copied in and out inside the call"}
+        # page-locked, column-major host buffers for the right-hand sides and the solutions
+        Bh = torch.empty((nrhs, B.n), dtype=torch.complex128, pin_memory=True).numpy().T
+        Xh = torch.empty((nrhs, B.n), dtype=torch.complex128, pin_memory=True).numpy().T
+        Bh[...] = -X
         for mode in ("mixed", "fp64"):
-            _, st = B.gmres(-X, shift=0.5, rtol=1e-10, restart=30, maxiter=300, mode=mode)
+            _, st = B.gmres(Bh, shift=0.5, rtol=1e-10, restart=30, maxiter=300, mode=mode, out=Xh)
             g[mode] = {"seconds": st["seconds"], "iterations": st["iterations"], "outer": st["outer"],
                        "fp64_applies": st["fp64_applies"], "tf32_applies": st["fp32_applies"],
                        "worst_relres_fp64": st["relres"], "converged": bool(st["converged"])}

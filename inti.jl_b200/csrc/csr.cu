@@ -164,11 +164,16 @@ __global__ void __launch_bounds__(kStreamThreads) csr_stream_kernel(
 // on a timeout the CTA records the error, waits once more for its copies
 // and leaves.
 constexpr int kBulkThreads = 256;
-constexpr int kBulkNnz = 2560;  // nonzeros staged per CTA
+// nonzeros staged per CTA (about 31 KB of shared memory either way, so that
+// seven or eight CTAs fit on an SM)
+template <bool CPLX>
+constexpr int bulk_nnz() {
+  return CPLX ? 1536 : 2560;
+}
 
 template <bool CPLX>
 constexpr size_t csr_bulk_smem() {
-  return (size_t)(kBulkNnz + 2) * (CPLX ? 16 : 8) + (size_t)(kBulkNnz + 4) * 4;
+  return (size_t)(bulk_nnz<CPLX>() + 2) * (CPLX ? 16 : 8) + (size_t)(bulk_nnz<CPLX>() + 4) * 4;
 }
 
 template <bool CPLX>
@@ -178,6 +183,7 @@ __global__ void __launch_bounds__(kBulkThreads) csr_bulk_kernel(
     double ai, double br, double bi, bool beta_zero, int* err) {
   constexpr int VB = CPLX ? 16 : 8;   // bytes per value
   constexpr int VA = 16 / VB;          // values per 16 bytes
+  constexpr int kBulkNnz = bulk_nnz<CPLX>();
   extern __shared__ __align__(16) unsigned char csm[];
   double* sval = reinterpret_cast<double*>(csm);
   int32_t* scol = reinterpret_cast<int32_t*>(csm + (size_t)(kBulkNnz + 2) * VB);
@@ -227,16 +233,44 @@ __global__ void __launch_bounds__(kBulkThreads) csr_bulk_kernel(
     } else {
       __syncthreads();
     }
-    // products in place
-    for (int64_t p = p0 + tid; p < p1; p += kBulkThreads) {
-      const int32_t j = scol[p - sc];
+    // products in place, in chunks: the thread's column indices first, then
+    // their gathers of x (in flight together), then the products
+    constexpr int PER = 5;
+    for (int64_t base = p0 + tid; base < p1; base += (int64_t)PER * kBulkThreads) {
+      int32_t js[PER];
+#pragma unroll
+      for (int u = 0; u < PER; ++u) {
+        const int64_t p = base + (int64_t)u * kBulkThreads;
+        js[u] = p < p1 ? scol[p - sc] : 0;
+      }
       if (CPLX) {
-        double2* v = reinterpret_cast<double2*>(sval) + (p - sv);
-        const double2 a = *v;
-        const double2 xv = __ldg(reinterpret_cast<const double2*>(x) + j);
-        *v = make_double2(fma(a.x, xv.x, -a.y * xv.y), fma(a.x, xv.y, a.y * xv.x));
+        double2 xs[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int64_t p = base + (int64_t)u * kBulkThreads;
+          xs[u] = p < p1 ? __ldg(reinterpret_cast<const double2*>(x) + js[u]) : make_double2(0.0, 0.0);
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int64_t p = base + (int64_t)u * kBulkThreads;
+          if (p < p1) {
+            double2* v = reinterpret_cast<double2*>(sval) + (p - sv);
+            const double2 a = *v;
+            *v = make_double2(fma(a.x, xs[u].x, -a.y * xs[u].y), fma(a.x, xs[u].y, a.y * xs[u].x));
+          }
+        }
       } else {
-        sval[p - sv] *= __ldg(x + j);
+        double xs[PER];
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int64_t p = base + (int64_t)u * kBulkThreads;
+          xs[u] = p < p1 ? __ldg(x + js[u]) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < PER; ++u) {
+          const int64_t p = base + (int64_t)u * kBulkThreads;
+          if (p < p1) sval[p - sv] *= xs[u];
+        }
       }
     }
     __syncthreads();
@@ -307,7 +341,8 @@ int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, cons
   const bool cplx = c->dtype == INTI_C128;
   if (mean <= 64) {
     // rows per CTA: fill ~90% of the staging buffers at the mean row length
-    const int rpb = (int)std::max<double>(1.0, std::min<double>(kBulkThreads, 0.9 * kBulkNnz / std::max(mean, 1.0)));
+    const int cap = cplx ? bulk_nnz<true>() : bulk_nnz<false>();
+    const int rpb = (int)std::max<double>(1.0, std::min<double>(kBulkThreads, 0.9 * cap / std::max(mean, 1.0)));
     const unsigned grid = (unsigned)((c->m + rpb - 1) / rpb);
     int* err = ctx->err_flag.as<int>();
     if (cplx) {

@@ -652,16 +652,30 @@ class BatchOperator:
         return Yo[:, 0] if single else Yo
 
     def gmres(self, B, *, shift=0.0, X0=None, rtol: float = 1e-10, restart: int = 30, maxiter: int = 300,
-              mode: str = "fp64"):
+              mode: str = "fp64", out=None):
         """Solve ``(shift·I + A_s + C_s) x = b`` for every surface and column
         in lockstep; returns ``(X, stats)`` with ``stats["relres"]`` the
-        per-system FP64 relative residuals ``(S, nrhs)``."""
+        per-system FP64 relative residuals ``(S, nrhs)``.  ``B`` that is
+        already complex128 and column-major is used without a copy; ``out``
+        (complex128, column-major, ``(N_total, nrhs)``) receives the solution
+        in place (page-locked buffers make the copies fast)."""
         B = np.asarray(B)
         single = B.ndim == 1
-        Bm = np.asfortranarray(_as_density(B.reshape(self.n, -1) if single else B, True, self.n))
+        Bm = B.reshape(self.n, -1) if single else B
+        if not (Bm.dtype == np.complex128 and Bm.flags.f_contiguous and Bm.shape[0] == self.n):
+            Bm = np.asfortranarray(_as_density(Bm, True, self.n))
         nrhs = Bm.shape[1]
-        X = np.zeros_like(Bm, order="F") if X0 is None else np.asfortranarray(
-            _as_density(np.asarray(X0).reshape(self.n, -1), True, self.n)).copy(order="F")
+        if out is not None:
+            X = out
+            if not (X.dtype == np.complex128 and X.flags.f_contiguous and X.shape == (self.n, nrhs)):
+                raise L.ArgumentError(L.E_ARG, "out must be a column-major complex128 array of shape (N_total, nrhs)")
+            if X0 is None:
+                X[...] = 0
+            else:
+                X[...] = np.asarray(X0).reshape(self.n, nrhs)
+        else:
+            X = np.zeros_like(Bm, order="F") if X0 is None else np.asfortranarray(
+                _as_density(np.asarray(X0).reshape(self.n, -1), True, self.n)).copy(order="F")
         rel = np.zeros(len(self.quads) * nrhs)
         st = L.GmresStats()
         m = {"fp64": L.GMRES_FP64, "mixed": L.GMRES_MIXED}[mode]

@@ -299,6 +299,17 @@ set_symmetric!(ctx::Context, flag::Bool) =
     check(ccall((:inti_ctx_set_symmetric, LIB), Cint, (Ptr{Cvoid}, Cint), ctx.ptr, flag), ctx.ptr)
 
 """
+    set_partial_budget!(ctx, bytes)
+
+Bytes of partial sums a symmetric operator created afterwards may hold
+(default 2e9; `0` restores it).  Larger operators run their work in panels,
+so their memory stays O(N) plus the budget; `panels(A)` reports the count.
+"""
+set_partial_budget!(ctx::Context, bytes::Real) =
+    check(ccall((:inti_ctx_set_partial_budget, LIB), Cint, (Ptr{Cvoid}, Float64), ctx.ptr, bytes), ctx.ptr)
+panels(A::B200Map) = Int(ccall((:inti_op_panels, LIB), Cint, (Ptr{Cvoid},), A.h.ptr))
+
+"""
     set_shard!(A::B200Map, rank, nranks)
 
 One process per GPU: `A` computes only rank `rank`'s share of the node pairs
