@@ -50,8 +50,10 @@ constexpr int TC_N = 2 * TC_R;           // real accumulator columns
 constexpr int TC_J = 32;                 // sources per stage
 constexpr int TC_K = 2 * TC_J;           // K elements per stage
 constexpr int TC_B_BYTES = TC_N * TC_K * 4;          // 32 KB
-constexpr int TC_S_FLOATS = 8;                       // x y z nx ny nz pad pad
-constexpr int TC_S_BYTES = TC_J * TC_S_FLOATS * 4;   // 1 KB
+// every value twice (x x y y | z z nx nx | ny ny nz nz | pad): each 16-byte
+// shared load gives the generator two ready operand pairs for its two rows
+constexpr int TC_S_FLOATS = 16;
+constexpr int TC_S_BYTES = TC_J * TC_S_FLOATS * 4;   // 2 KB
 // dynamic shared memory layout (bytes)
 // Ring depths: a bulk copy from L2 takes ~1500 cycles to land, longer than
 // a stage's MMAs, so densities are fetched TC_NB - 1 stages and source
@@ -242,12 +244,13 @@ __device__ __forceinline__ float2 tc_kernel(const float* x, const float4 s0, con
 // lane.  Each lane performs tc_kernel's operations in the same order, so the
 // values are the same bit for bit.
 template <int KIND>
-__device__ __forceinline__ void tc_kernel_x2(const float2 (&x)[3], const float4 s0, const float2 s1,
-                                             const TcConst& c, float2& k0, float2& k1) {
+__device__ __forceinline__ void tc_kernel_x2(const float2 (&x)[3], const float4 sa, const float4 sb,
+                                             const float4 sc, const TcConst& c, float2& k0, float2& k1) {
+  // sa = (x x y y), sb = (z z nx nx), sc = (ny ny nz nz) of the source
   const float2 m1 = make_float2(-1.f, -1.f);
-  const float2 r0 = __ffma2_rn(make_float2(s0.x, s0.x), m1, x[0]);  // x - s, one rounding
-  const float2 r1 = __ffma2_rn(make_float2(s0.y, s0.y), m1, x[1]);
-  const float2 r2 = __ffma2_rn(make_float2(s0.z, s0.z), m1, x[2]);
+  const float2 r0 = __ffma2_rn(make_float2(sa.x, sa.y), m1, x[0]);  // x - s, one rounding
+  const float2 r1 = __ffma2_rn(make_float2(sa.z, sa.w), m1, x[1]);
+  const float2 r2 = __ffma2_rn(make_float2(sb.x, sb.y), m1, x[2]);
   const float2 d2 = __ffma2_rn(r2, r2, __ffma2_rn(r1, r1, __fmul2_rn(r0, r0)));
   float2 ri;
   ri.x = d2.x > 1.0e-28f ? rsqrt_approx_f32(d2.x) : 0.0f;
@@ -263,8 +266,8 @@ __device__ __forceinline__ void tc_kernel_x2(const float2 (&x)[3], const float4 
     k1 = make_float2(re.y, im.y);
     return;
   }
-  const float2 rn = __ffma2_rn(r2, make_float2(s1.y, s1.y),
-                               __ffma2_rn(r1, make_float2(s1.x, s1.x), __fmul2_rn(r0, make_float2(s0.w, s0.w))));
+  const float2 rn = __ffma2_rn(r2, make_float2(sc.z, sc.w),
+                               __ffma2_rn(r1, make_float2(sc.x, sc.y), __fmul2_rn(r0, make_float2(sb.z, sb.w))));
   const float2 u = __fmul2_rn(rn, ri);
   if (KIND == CFI) {
     br = __fmul2_rn(u, __fmul2_rn(ri, ri));
@@ -451,10 +454,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) mrhs_tc_kernel(TcArgs a) {
 #pragma unroll
           for (int e = 0; e < 4; ++e) {
             const int j = j0 + jq + e;
-            const float4 s0 = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
-            const float2 s1 = *reinterpret_cast<const float2*>(S + j * TC_S_FLOATS + 4);
+            const float4 sa = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS);
+            const float4 sb = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS + 4);
+            const float4 sc = *reinterpret_cast<const float4*>(S + j * TC_S_FLOATS + 8);
             float2 k0, k1;
-            tc_kernel_x2<KIND>(xt, s0, s1, kc, k0, k1);
+            tc_kernel_x2<KIND>(xt, sa, sb, sc, kc, k0, k1);
             v[0][2 * e] = tf32_bits(k0.x);
             v[0][2 * e + 1] = tf32_bits(k0.y);
             v[1][2 * e] = tf32_bits(k1.x);
@@ -539,8 +543,8 @@ done:
   }
 }
 
-// Source records: x y z nx ny nz (FP32) per source, tiles of TC_J per
-// surface, zero-padded.
+// Source records (FP32) per source, every value twice: x x y y z z nx nx
+// ny ny nz nz and four pad floats; tiles of TC_J per surface, zero-padded.
 __global__ void tc_pack_sources(int nsurf, const int64_t* off, const int64_t* toff, const double* coords,
                                 const double* normals, float* out) {
   const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;  // padded source slot
@@ -550,18 +554,19 @@ __global__ void tc_pack_sources(int nsurf, const int64_t* off, const int64_t* to
   if (g >= toff[nsurf] * TC_J) return;
   const int64_t j = g - toff[s] * TC_J;
   const int64_t n = off[s + 1] - off[s];
-  float* o = out + g * TC_S_FLOATS;
+  float v[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (j < n) {
     const int64_t i = off[s] + j;
     for (int c = 0; c < 3; ++c) {
-      o[c] = (float)coords[3 * i + c];
-      o[3 + c] = normals ? (float)normals[3 * i + c] : 0.f;
+      v[c] = (float)coords[3 * i + c];
+      v[3 + c] = normals ? (float)normals[3 * i + c] : 0.f;
     }
-  } else {
-    for (int c = 0; c < 6; ++c) o[c] = 0.f;
   }
-  o[6] = 0.f;
-  o[7] = 0.f;
+  float4* o = reinterpret_cast<float4*>(out + g * TC_S_FLOATS);
+  o[0] = make_float4(v[0], v[0], v[1], v[1]);
+  o[1] = make_float4(v[2], v[2], v[3], v[3]);
+  o[2] = make_float4(v[4], v[4], v[5], v[5]);
+  o[3] = make_float4(0.f, 0.f, 0.f, 0.f);
 }
 
 // Density blocks: for column group cg and tile (surface s, local tile lt),
