@@ -193,11 +193,14 @@ __global__ void __launch_bounds__(kBulkThreads) csr_bulk_kernel(
   const int64_t p0 = rowptr[r0], p1 = rowptr[r1];
   const int tid = threadIdx.x;
   if (p1 - p0 <= kBulkNnz) {
-    const int64_t sv = p0 & ~(int64_t)(VA - 1), sc = p0 & ~(int64_t)3;  // slot origins
-    const int64_t va = (p0 + VA - 1) & ~(int64_t)(VA - 1), vb = p1 & ~(int64_t)(VA - 1);
-    const int64_t ca = (p0 + 3) & ~(int64_t)3, cb = p1 & ~(int64_t)3;
-    const uint32_t vbytes = vb > va ? (uint32_t)((vb - va) * VB) : 0u;
-    const uint32_t cbytes = cb > ca ? (uint32_t)((cb - ca) * 4) : 0u;
+    // 32-bit offsets within the block: element p0 + q sits at vals[q + lv],
+    // cols[q + lc]; the aligned interiors are q in [va, vb) and [ca, cb)
+    const int cnt = (int)(p1 - p0);
+    const int lv = (int)(p0 & (VA - 1)), lc = (int)(p0 & 3);
+    const int va = (VA - lv) & (VA - 1), vb = cnt - (int)((p0 + cnt) & (VA - 1));
+    const int ca = (4 - lc) & 3, cb = cnt - (int)((p0 + cnt) & 3);
+    const uint32_t vbytes = vb > va ? (uint32_t)(vb - va) * VB : 0u;
+    const uint32_t cbytes = cb > ca ? (uint32_t)(cb - ca) * 4u : 0u;
     const bool bulk = vbytes + cbytes > 0;
     if (tid == 0 && bulk) {
       mbar_init(&bar, 1);
@@ -207,19 +210,22 @@ __global__ void __launch_bounds__(kBulkThreads) csr_bulk_kernel(
     if (tid == 0 && bulk) {
       mbar_arrive_expect_tx(&bar, vbytes + cbytes);
       if (vbytes)
-        bulk_copy_g2s(reinterpret_cast<unsigned char*>(sval) + (va - sv) * VB,
-                      reinterpret_cast<const unsigned char*>(val) + va * VB, vbytes, &bar);
-      if (cbytes) bulk_copy_g2s(scol + (ca - sc), col + ca, cbytes, &bar);
+        bulk_copy_g2s(reinterpret_cast<unsigned char*>(sval) + (size_t)(va + lv) * VB,
+                      reinterpret_cast<const unsigned char*>(val + (p0 + va) * (VB / 8)), vbytes, &bar);
+      if (cbytes) bulk_copy_g2s(scol + ca + lc, col + p0 + ca, cbytes, &bar);
     }
-    // heads and tails outside the aligned interiors
-    for (int64_t p = p0 + tid; p < p1; p += kBulkThreads) {
-      if (p < va || p >= vb) {
-        if (CPLX)
-          reinterpret_cast<double2*>(sval)[p - sv] = reinterpret_cast<const double2*>(val)[p];
-        else
-          sval[p - sv] = val[p];
+    // heads and tails outside the aligned interiors (fewer than 16 bytes each)
+    if (tid < 16) {
+      const int q = tid < 8 ? tid : cnt - 16 + tid;  // the first and the last 8 elements
+      if (q >= 0 && q < cnt && !(tid >= 8 && q < 8)) {
+        if (q < va || q >= vb || vb <= va) {
+          if (CPLX)
+            reinterpret_cast<double2*>(sval)[q + lv] = reinterpret_cast<const double2*>(val)[p0 + q];
+          else
+            sval[q + lv] = val[p0 + q];
+        }
+        if (q < ca || q >= cb || cb <= ca) scol[q + lc] = col[p0 + q];
       }
-      if (p < ca || p >= cb) scol[p - sc] = col[p];
     }
     if (bulk) {
       const bool ok = mbar_wait_bounded(&bar, 0);
@@ -236,48 +242,48 @@ __global__ void __launch_bounds__(kBulkThreads) csr_bulk_kernel(
     // products in place, in chunks: the thread's column indices first, then
     // their gathers of x (in flight together), then the products
     constexpr int PER = 5;
-    for (int64_t base = p0 + tid; base < p1; base += (int64_t)PER * kBulkThreads) {
+    for (int base = tid; base < cnt; base += PER * kBulkThreads) {
       int32_t js[PER];
 #pragma unroll
       for (int u = 0; u < PER; ++u) {
-        const int64_t p = base + (int64_t)u * kBulkThreads;
-        js[u] = p < p1 ? scol[p - sc] : 0;
+        const int q = base + u * kBulkThreads;
+        js[u] = q < cnt ? scol[q + lc] : 0;
       }
       if (CPLX) {
         double2 xs[PER];
 #pragma unroll
         for (int u = 0; u < PER; ++u) {
-          const int64_t p = base + (int64_t)u * kBulkThreads;
-          xs[u] = p < p1 ? __ldg(reinterpret_cast<const double2*>(x) + js[u]) : make_double2(0.0, 0.0);
+          const int q = base + u * kBulkThreads;
+          xs[u] = q < cnt ? __ldg(reinterpret_cast<const double2*>(x) + js[u]) : make_double2(0.0, 0.0);
         }
 #pragma unroll
         for (int u = 0; u < PER; ++u) {
-          const int64_t p = base + (int64_t)u * kBulkThreads;
-          if (p < p1) {
-            double2* v = reinterpret_cast<double2*>(sval) + (p - sv);
-            const double2 a = *v;
-            *v = make_double2(fma(a.x, xs[u].x, -a.y * xs[u].y), fma(a.x, xs[u].y, a.y * xs[u].x));
+          const int q = base + u * kBulkThreads;
+          if (q < cnt) {
+            double2* v = reinterpret_cast<double2*>(sval) + (q + lv);
+            const double2 w = *v;
+            *v = make_double2(fma(w.x, xs[u].x, -w.y * xs[u].y), fma(w.x, xs[u].y, w.y * xs[u].x));
           }
         }
       } else {
         double xs[PER];
 #pragma unroll
         for (int u = 0; u < PER; ++u) {
-          const int64_t p = base + (int64_t)u * kBulkThreads;
-          xs[u] = p < p1 ? __ldg(x + js[u]) : 0.0;
+          const int q = base + u * kBulkThreads;
+          xs[u] = q < cnt ? __ldg(x + js[u]) : 0.0;
         }
 #pragma unroll
         for (int u = 0; u < PER; ++u) {
-          const int64_t p = base + (int64_t)u * kBulkThreads;
-          if (p < p1) sval[p - sv] *= xs[u];
+          const int q = base + u * kBulkThreads;
+          if (q < cnt) sval[q + lv] *= xs[u];
         }
       }
     }
     __syncthreads();
     for (int64_t row = r0 + tid; row < r1; row += kBulkThreads) {
-      const int64_t a = rowptr[row] - sv, b = rowptr[row + 1] - sv;
+      const int qa = (int)(rowptr[row] - p0) + lv, qb = (int)(rowptr[row + 1] - p0) + lv;
       double sr = 0.0, si = 0.0;
-      for (int64_t q = a; q < b; ++q) {
+      for (int q = qa; q < qb; ++q) {
         if (CPLX) {
           const double2 v = reinterpret_cast<const double2*>(sval)[q];
           sr += v.x;
