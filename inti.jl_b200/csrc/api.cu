@@ -127,13 +127,14 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
     L.sym_items = op->sym_tab.as<int32_t>();
     L.sym_rowptr = L.sym_items + 3 * op->sym_nitems;
     L.sym_rowitems = L.sym_rowptr + op->sym_nb + 1;
-    L.zpart = op->zpart.p;
+    L.partial = op->ctx->sym_ypart.p;  // the context's shared symmetric scratch
+    L.zpart = op->ctx->sym_zpart.p;
     L.sym_npanels = (int)op->sym_panels.size();
     if (L.sym_npanels > 1) {
       L.sym_panels = op->sym_panels.data();
       L.sym_table = op->sym_tab.as<int32_t>();
       L.sym_zld = op->sym_zld;
-      L.sym_acc = op->sym_acc.p;
+      L.sym_acc = op->ctx->sym_acc.p;
       const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
       L.sym_ypart_bytes = pb * op->sym_nitems * pair_symm_block(op->tpt);
       L.sym_zpart_bytes = pb * op->sym_nb * op->sym_zld;
@@ -158,8 +159,8 @@ void op_apply_device(inti_op* op, const double* x, double* y, const double* alph
     // (with panels pair_launch clears them before each panel)
     if (L.sym_npanels <= 1) {
       const size_t pb = (size_t)pair_partial_bytes(op->pde, op->precision);
-      INTI_CUDA(cudaMemsetAsync(op->partial.p, 0, pb * op->sym_nitems * pair_symm_block(op->tpt), op->ctx->stream));
-      INTI_CUDA(cudaMemsetAsync(op->zpart.p, 0, pb * op->sym_nb * op->n_tiles * pair_tile(op->precision),
+      INTI_CUDA(cudaMemsetAsync(L.partial, 0, pb * op->sym_nitems * pair_symm_block(op->tpt), op->ctx->stream));
+      INTI_CUDA(cudaMemsetAsync(L.zpart, 0, pb * op->sym_nb * op->n_tiles * pair_tile(op->precision),
                                 op->ctx->stream));
     }
     pair_launch(op->ctx, L);

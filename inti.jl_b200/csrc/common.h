@@ -95,6 +95,13 @@ struct inti_ctx {
   // bytes of row and column partials a symmetric operator may hold before
   // its work is split into panels (inti_ctx_set_partial_budget)
   double symm_budget = 2.0e9;
+  // Row partials, column partials and panel running sums of the symmetric
+  // form, shared by all of the context's symmetric operators: they are live
+  // only from an apply's pair launch to its epilogue, and every launch of a
+  // context goes to its one stream in call order (calls are serialised), so
+  // no two applies use them at the same time.  Sized for the largest
+  // operator (each within the partial budget).
+  inti::DevBuf sym_ypart, sym_zpart, sym_acc;
   // GMRES workspace kept between solves: Krylov basis, work vectors, the
   // reduction scratch and the staged right-hand side / solution.
   struct {

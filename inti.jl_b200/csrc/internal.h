@@ -41,13 +41,13 @@ struct inti_op {
   // column partials; split holds the source blocks per work item
   bool symm = false;
   int sym_nb = 0, sym_nitems = 0;
-  inti::DevBuf sym_tab, zpart;
+  inti::DevBuf sym_tab;
   // panels of the work items (one unless the column partials of the whole
-  // operator would pass the partial budget), their running sums
+  // operator would pass the partial budget); the partials and running sums
+  // themselves are the context's (sym_ypart, sym_zpart, sym_acc)
   std::vector<inti::SymPanel> sym_panels;
   int64_t sym_zld = 0;
   double sym_budget = 0.0;  // bytes of partials allowed, fixed at creation
-  inti::DevBuf sym_acc;
   // item shard of this operator (inti_op_set_shard): rank, ranks, and the
   // rank's items (3 x n) followed by their ids; per panel (offset, count)
   int shard_rank = 0, shard_n = 1, shard_items = 0;

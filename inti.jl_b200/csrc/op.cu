@@ -272,7 +272,7 @@ double symm_budget(const inti_op* op) {
   size_t free_b = 0, total_b = 0;
   INTI_CUDA(cudaMemGetInfo(&free_b, &total_b));
   return std::min(op->ctx->symm_budget,
-                  kSymmMaxFreeShare * (double)free_b + op->partial.bytes + op->zpart.bytes);
+                  kSymmMaxFreeShare * (double)free_b + op->ctx->sym_ypart.bytes + op->ctx->sym_zpart.bytes);
 }
 
 void op_symm_configure(inti_op* op, int tpt, int ch) {
@@ -292,9 +292,10 @@ void op_symm_configure(inti_op* op, int tpt, int ch) {
   const int64_t npad = op->n_tiles * pair_tile(op->precision);
   const bool panels = op->sym_panels.size() > 1;
   op->sym_zld = panels ? (int64_t)pcols * pair_symm_block(tpt) : npad;
-  op->partial.ensure((size_t)pb * nitems * pair_symm_block(tpt));
-  op->zpart.ensure((size_t)pb * nb * op->sym_zld);
-  if (panels) op->sym_acc.ensure(sizeof(double) * (op->pde == INTI_HELMHOLTZ ? 2 : 1) * op->source->n);
+  inti_ctx* ctx = op->ctx;
+  ctx->sym_ypart.ensure((size_t)pb * nitems * pair_symm_block(tpt));
+  ctx->sym_zpart.ensure((size_t)pb * nb * op->sym_zld);
+  if (panels) ctx->sym_acc.ensure(sizeof(double) * (op->pde == INTI_HELMHOLTZ ? 2 : 1) * op->source->n);
   if (op->shard_n > 1) op_set_shard(op, op->shard_rank, op->shard_n);  // the items changed
 }
 

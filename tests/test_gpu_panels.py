@@ -85,3 +85,32 @@ def test_panels_with_correction_alpha_beta_and_shards(ctx, pde):
 def test_partial_budget_rejects_negative(ctx):
     with pytest.raises(inti.ArgumentError):
         ctx.set_partial_budget(-1.0)
+
+
+def test_symmetric_operators_share_the_context_scratch(ctx):
+    """The symmetric form's partials belong to the context and are shared by
+    its operators: applies of different operators enqueued back to back on
+    the context's stream (no synchronisation in between), one of them in
+    panels, give the products each operator gives alone."""
+    import torch
+
+    q, op, k = _surface("helmholtz")
+    A = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp64", ctx)
+    ctx.set_partial_budget(2.5e5)
+    try:
+        B = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, None, "fp64", ctx)
+    finally:
+        ctx.set_partial_budget(0)
+    assert A.tuning["panels"] == 1 and B.tuning["panels"] > 2
+    sigma = density(len(q), True, 21)
+    ya, yb = A @ sigma, B @ sigma
+    dev = torch.device("cuda:0")
+    xs = torch.from_numpy(np.ascontiguousarray(sigma).view(np.float64).copy()).to(dev)
+    outs = [torch.zeros_like(xs) for _ in range(4)]
+    torch.cuda.synchronize()
+    for i, M in enumerate((A, B, A, B)):
+        M.apply_device(xs.data_ptr(), outs[i].data_ptr())
+    ctx.synchronize()
+    got = [o.cpu().numpy().view(np.complex128) for o in outs]
+    assert np.array_equal(got[0], ya) and np.array_equal(got[2], ya)
+    assert np.array_equal(got[1], yb) and np.array_equal(got[3], yb)
