@@ -231,3 +231,31 @@ def test_symmetric_fp32c_edge_sizes(ctx, n):
             assert np.all(got == 0)
         else:
             assert relerr(got, ref) < 5e-5
+
+
+@pytest.mark.parametrize("n", [1, 7, 257, 513, 1025])
+def test_symmetric_fp32c_helmholtz_edge_sizes(ctx, n):
+    """The FP32C Helmholtz symmetric kernel (SL, DL and the combined field
+    with complex coefficients) at node counts around its 256-source tiles
+    and 256/512-node blocks: padded records, targets straddling the end of
+    the nodes, a single node; against the oracle."""
+    r = np.random.default_rng(300 + n)
+    X = r.standard_normal((n, 3))
+    N = r.standard_normal((n, 3))
+    N /= np.linalg.norm(N, axis=1, keepdims=True)
+    q = inti.Quadrature(X, N, r.uniform(0.5, 1.5, n), 0)
+    x = density(n, True, 4)
+    k = 4.0
+    op = inti.Helmholtz(k=k, dim=3)
+    S = inti.GpuOperator(inti.SingleLayerKernel(op), q, q, None, "fp32c", ctx)
+    D = inti.GpuOperator(inti.DoubleLayerKernel(op), q, q, None, "fp32c", ctx)
+    CF = inti.CombinedFieldOperator(D, S, 1.0, -1j * k)
+    assert S.tuning["symmetric"] and D.tuning["symmetric"] and CF.tuning["symmetric"]
+    rs = oracle_apply(O.HELMHOLTZ, O.SL, k, q, q, x)
+    rd = oracle_apply(O.HELMHOLTZ, O.DL, k, q, q, x)
+    for A, ref in ((S, rs), (D, rd), (CF, rd - 1j * k * rs)):
+        got = A @ x
+        if n == 1:
+            assert np.all(got == 0)
+        else:
+            assert relerr(got, ref) < 5e-5
