@@ -60,6 +60,7 @@ FLOPS_PER_PAIR = {"helmholtz_sl": 24, "helmholtz_dl": 34, "laplace_sl": 11, "lap
 # launch per workload, from the ncu capture of that launch summarised in
 # profiles/ (the file named beside each entry); None where no capture exists.
 PAIR_TRAFFIC_BYTES = {"c2": (66.74e6, "profiles/pair_symm_helmholtz_sl_fp64_p2sphere62k.md")}
+CSR_TRAFFIC_BYTES = (527.0e6, "profiles/csr_bulk_kernel_dim_pattern_c3x20.md")
 # Fallback HBM copy bandwidth (GB/s) when MEASURED_PEAKS.json is absent
 HBM_FALLBACK_GBS = 6650.0
 
@@ -737,8 +738,10 @@ def bench_csr(args, ctx, torch) -> dict:
             "config": {"workload": "dim_pattern_c3x20_rows4018680_nq9", "nnz": m * nq,
                        "l2": "inputs larger than L2 (>= 470 MB per step)"},
             "roofline": {"bound": "hbm", "achieved": out["f64"]["gbs"], "peak": peak, "unit": "GB/s",
-                         "frac": out["f64"]["gbs"] / peak, "traffic": None, "kernel": "csr_kernel<8, real>",
-                         "peak_source": peak_src},
+                         "frac": out["f64"]["gbs"] / peak, "traffic": CSR_TRAFFIC_BYTES[0],
+                         "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                           f"{CSR_TRAFFIC_BYTES[1]}",
+                         "kernel": "csr_bulk_kernel<real>", "peak_source": peak_src},
             "complex": out["c128"], "real": out["f64"], "gpu_launches": out["f64"]["launches"]}
 
 
