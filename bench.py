@@ -919,7 +919,8 @@ def main() -> None:
     achieved = float(m_loc) * n * FLOPS_PER_PAIR[fkey] / (kern_ms * 1e-3) / 1e12
     peak = peaks["fp32_flops" if fp32 else "fp64_flops"] / 1e12
     shape = A.tuning
-    sym = bool(shape.get("symmetric"))
+    small = bool(shape.get("single_launch"))
+    sym = bool(shape.get("symmetric")) and not small
     if sym:  # diagonal node blocks evaluate every ordered pair, the others each unordered pair once
         bt = 128 * shape["targets_per_thread"]
         nb = -(-n // bt)
@@ -932,11 +933,14 @@ def main() -> None:
                 "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
                                    f"{PAIR_TRAFFIC_BYTES[args.workload][1]}"
                                    if args.workload in PAIR_TRAFFIC_BYTES else "no capture"),
-                "kernel": f"{'pair_symm' if sym else 'pair_forward'} ({fkey}, {'float' if fp32 else 'double'})",
+                "kernel": f"{'pair_small_kernel' if small else 'pair_symm' if sym else 'pair_forward'} "
+                          f"({fkey}, {'float' if fp32 else 'double'})",
                 "kernel_ms": kern_ms,
                 "flops_per_pair": FLOPS_PER_PAIR[fkey],
                 "form": ("symmetric: one kernel evaluation per unordered pair serves both products; achieved "
-                         "counts the metric's M*N ordered pairs" if sym else "one-sided"),
+                         "counts the metric's M*N ordered pairs" if sym else
+                         "single launch: pair sums and epilogue in one kernel after the pack" if small else
+                         "one-sided"),
                 "kernel_evaluations_per_step": evals,
                 "peak_source": f"{'FP32' if fp32 else 'FP64'} FMA throughput measured in this run "
                                "(inti_measure_peaks), of measured",

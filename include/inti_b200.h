@@ -214,6 +214,15 @@ int inti_ctx_set_symmetric(inti_ctx* ctx, int enable);  /* default on */
 int inti_op_symmetric(const inti_op* op);
 int inti_ctx_set_partial_budget(inti_ctx* ctx, double bytes);
 int inti_op_panels(const inti_op* op);
+/* Small FP64 operators (at most 2^20 target-source pairs, e.g. the 1,000-node
+ * kite) apply in a single-launch form: after the pack, one kernel forms the
+ * pair sums (each CTA 32 targets, its warps splitting the sources, a fixed
+ * order) together with the epilogue.  inti_ctx_set_single_launch(ctx, 0)
+ * makes operators created afterwards use the tiled kernels;
+ * inti_op_single_launch returns 1 when an operator uses the form.  No
+ * counterpart in the reference. */
+int inti_ctx_set_single_launch(inti_ctx* ctx, int enable);  /* default on */
+int inti_op_single_launch(const inti_op* op);
 /* Item shard of a symmetric operator for one process per GPU: after
  * inti_op_set_shard(op, r, P), inti_op_apply on rank r computes this rank's
  * share of the unordered node pairs (every P-th work item, largest first,

@@ -153,6 +153,10 @@ PairLaunch make_launch(inti_op* op, const double* xdev) {
 void op_apply_device(inti_op* op, const double* x, double* y, const double* alpha,
                      const double* beta) {
   PairLaunch L = make_launch(op, x);
+  if (op->small && op->shard_n == 1) {
+    pair_small(op->ctx, L, op->corr, x, y, alpha, beta);
+    return;
+  }
   if (op->shard_n > 1) {
     // this rank's items only: the partials of the others' items are zero, and
     // the correction and beta*y belong to rank 0 (the ranks' y are summed)
@@ -618,6 +622,16 @@ int inti_op_set_shard(inti_op* op, int rank, int nranks) {
 int inti_op_symmetric(const inti_op* op) {
   if (!op) return -INTI_E_ARG;
   return op->symm ? 1 : 0;
+}
+
+int inti_ctx_set_single_launch(inti_ctx* ctx, int enable) {
+  if (!ctx) return INTI_E_ARG;
+  return guarded(ctx, [&] { ctx->single_launch = enable != 0; });
+}
+
+int inti_op_single_launch(const inti_op* op) {
+  if (!op) return -INTI_E_ARG;
+  return op->small ? 1 : 0;
 }
 
 int inti_ctx_set_partial_budget(inti_ctx* ctx, double bytes) {

@@ -95,6 +95,9 @@ struct inti_ctx {
   // bytes of row and column partials a symmetric operator may hold before
   // its work is split into panels (inti_ctx_set_partial_budget)
   double symm_budget = 2.0e9;
+  // FP64 operators of at most kSmallPairs pairs created while this is set
+  // apply in the single-launch form (inti_ctx_set_single_launch)
+  bool single_launch = true;
   // Row partials, column partials and panel running sums of the symmetric
   // form, shared by all of the context's symmetric operators: they are live
   // only from an apply's pair launch to its epilogue, and every launch of a
@@ -251,6 +254,12 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
                   double* y, const double* alpha, const double* beta, const double* rowscale = nullptr);
 // Dense assembly of A.
 int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out);
+// Single-launch form of small FP64 products (pack, then the pair sums with
+// the epilogue in one kernel): operators of at most kSmallPairs pairs.
+constexpr double kSmallPairs = 1048576.0;
+bool pair_small_eligible(int precision, int64_t m, int64_t n);
+int pair_small(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x, double* y,
+               const double* alpha, const double* beta);
 
 // CSR: y = alpha*C*x + beta*y (alpha/beta complex pairs); transpose via col scatter.
 int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, const double* alpha,

@@ -39,6 +39,7 @@ struct inti_op {
   int tsplit = 1, ttpt = 4;  // A^T launch shape
   // symmetric form (target set == source set, pair_symm): plan table and
   // column partials; split holds the source blocks per work item
+  bool small = false;  // applies in the single-launch form (pair_small)
   bool symm = false;
   int sym_nb = 0, sym_nitems = 0;
   inti::DevBuf sym_tab;

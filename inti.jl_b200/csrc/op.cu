@@ -74,6 +74,7 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   op->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(op.get());
   op_autotune(op.get(), false);
+  op->small = ctx->single_launch && pair_small_eligible(precision, target->n, source->n);
   return op.release();
 }
 
@@ -177,6 +178,7 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   op->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(op.get());
   op_autotune(op.get(), false);
+  op->small = ctx->single_launch && pair_small_eligible(precision, target->n, source->n);
   return op.release();
 }
 

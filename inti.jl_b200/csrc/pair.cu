@@ -530,6 +530,60 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
 }
 
 // ---------------------------------------------------------------------------
+// Single-launch form for small FP64 operators (m*n up to kSmallPairs, e.g.
+// the 1,000-node kite): the pair sums and the epilogue in one kernel after
+// the pack.  The tiled kernels give such a problem only a few CTAs (ten for
+// a 1,000-node square operator) whose threads each run a long dependent
+// chain; here a CTA of kSmallWarps warps takes 32 targets (one per lane) and
+// its warps split the sources, so every SM has work and each thread's chain
+// is n/kSmallWarps sources.  The step is pair_step's (the one-sided
+// kernel's arithmetic); the warps' sums are added in a fixed order, then
+// the kernel constant, the correction row and alpha/beta as in the
+// epilogue.
+// ---------------------------------------------------------------------------
+constexpr int kSmallWarps = 8;
+
+template <int PDE, int KIND, int DIM>
+__global__ void __launch_bounds__(32 * kSmallWarps) pair_small_kernel(int64_t m, int64_t n, const double* tc,
+                                                                      const double* tn, const double* packed,
+                                                                      double k, double kT, double delta,
+                                                                      const double2* expi, EpiArgs e) {
+  using RC = Rec<PDE, KIND, DIM, double>;
+  constexpr bool CPLX = RC::cplx;
+  __shared__ double2 part[kSmallWarps][32];
+  __shared__ double2 tab[CPLX ? kExpiTable : 1];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t i = blockIdx.x * (int64_t)32 + lane;
+  if (CPLX)
+    for (int q = threadIdx.x; q < kExpiTable; q += 32 * kSmallWarps) tab[q] = expi[q];
+  __syncthreads();
+  double ar = 0.0, ai = 0.0;
+  if (i < m) {
+    Target<double, DIM, RC::tnormal> t;
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) t.x[c] = tc[DIM * i + c];
+    if constexpr (RC::tnormal) {
+#pragma unroll
+      for (int c = 0; c < DIM; ++c) t.n[c] = tn[DIM * i + c];
+    }
+    const int64_t per = (n + kSmallWarps - 1) / kSmallWarps;
+    const int64_t j0 = warp * per, j1 = j0 + per < n ? j0 + per : n;
+    for (int64_t j = j0; j < j1; ++j) pair_step<PDE, KIND, DIM, double>(t, packed + j * RC::n, kT, delta, k, tab, ar, ai);
+  }
+  part[warp][lane] = make_double2(ar, ai);
+  __syncthreads();
+  if (warp != 0 || i >= m) return;
+  double sr = 0.0, si = 0.0;
+#pragma unroll
+  for (int w = 0; w < kSmallWarps; ++w) {
+    sr += part[w][lane].x;
+    si += part[w][lane].y;
+  }
+  epilogue_finish<CPLX>(e, i, sr, si);
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric form for square operators (the target set is the source set),// ---------------------------------------------------------------------------
 // Symmetric form for square operators (the target set is the source set),
 // every kernel: single layer, double layer, combined field (3D), adjoint
 // double layer and hypersingular, in 3D and for the 2D Laplace kernels.
@@ -1763,6 +1817,46 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
   INTI_CUDA(cudaGetLastError());
   ctx->launches += 1;
   return 1;
+}
+
+bool pair_small_eligible(int precision, int64_t m, int64_t n) {
+  return precision == INTI_FP64 && (double)m * (double)n <= kSmallPairs && m > 0 && n > 0;
+}
+
+int pair_small(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x, double* y,
+               const double* alpha, const double* beta) {
+  EpiArgs e;
+  e.m = L.m;
+  e.split = 1;
+  e.partial = nullptr;
+  e.scale = pair_scale(L.pde, L.kind, L.dim);
+  e.rowptr = corr ? corr->rowptr.as<int64_t>() : nullptr;
+  e.col = corr ? corr->col.as<int32_t>() : nullptr;
+  e.val = corr ? corr->val.as<double>() : nullptr;
+  e.x = x;
+  e.y = y;
+  e.ar = alpha ? alpha[0] : 1.0;
+  e.ai = alpha ? alpha[1] : 0.0;
+  e.br = beta ? beta[0] : 0.0;
+  e.bi = beta ? beta[1] : 0.0;
+  e.beta_zero = (e.br == 0.0 && e.bi == 0.0);
+  dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
+    using T = decltype(tag);
+    const unsigned gp = (unsigned)((L.n + 255) / 256);
+    {
+      ProfScope ps(ctx, "pack");
+      pack_sources<T::pde, T::kind, T::dim, double><<<gp, 256, 0, ctx->stream>>>(
+          L.n, L.n, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
+          make_double2(L.c2[0], L.c2[1]), static_cast<double*>(L.packed));
+    }
+    ProfScope pp(ctx, "pair");
+    pair_small_kernel<T::pde, T::kind, T::dim><<<(unsigned)((L.m + 31) / 32), 32 * kSmallWarps, 0, ctx->stream>>>(
+        L.m, L.n, L.tcoords, L.tnormals, static_cast<const double*>(L.packed), L.k, L.k * kExpiTable / (2 * kPi),
+        2 * kPi / kExpiTable, T::pde == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, e);
+  });
+  INTI_CUDA(cudaGetLastError());
+  ctx->launches += 2;
+  return 2;
 }
 
 int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {

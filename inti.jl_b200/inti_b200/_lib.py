@@ -129,6 +129,8 @@ SIGNATURES = {
     "inti_op_symmetric": (C.c_int, [P]),
     "inti_ctx_set_partial_budget": (C.c_int, [P, C.c_double]),
     "inti_op_panels": (C.c_int, [P]),
+    "inti_ctx_set_single_launch": (C.c_int, [P, C.c_int]),
+    "inti_op_single_launch": (C.c_int, [P]),
     "inti_op_set_shard": (C.c_int, [P, C.c_int, C.c_int]),
     "inti_selftest_math": (C.c_int, [P, D]),
     "inti_batch_create": (C.c_int, [P, C.c_int32, PP, C.c_int, C.c_int, C.c_double, C.c_double, D, D, PP, PP, PP]),

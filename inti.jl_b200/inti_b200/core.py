@@ -120,6 +120,11 @@ class Context:
         afterwards (on by default; see ``GpuOperator.tuning``)."""
         self.check(self.lib.inti_ctx_set_symmetric(self.handle, int(bool(enable))))
 
+    def set_single_launch(self, enable: bool) -> None:
+        """Apply small FP64 operators (at most 2^20 pairs) created afterwards
+        in the single-launch form (on by default; see ``GpuOperator.tuning``)."""
+        self.check(self.lib.inti_ctx_set_single_launch(self.handle, int(bool(enable))))
+
     def set_partial_budget(self, nbytes: float) -> None:
         """Bytes of partial sums a symmetric operator created afterwards may
         hold before its work is split into panels run one after another
@@ -540,7 +545,8 @@ class GpuOperator(_Map):
         self.ctx.check(self.ctx.lib.inti_op_tuning(self.handle, C.byref(t), C.byref(s)))
         return {"targets_per_thread": t.value, "split": s.value,
                 "symmetric": bool(self.ctx.lib.inti_op_symmetric(self.handle) == 1),
-                "panels": int(self.ctx.lib.inti_op_panels(self.handle))}
+                "panels": int(self.ctx.lib.inti_op_panels(self.handle)),
+                "single_launch": bool(self.ctx.lib.inti_op_single_launch(self.handle) == 1)}
 
     def set_shard(self, rank: int, nranks: int) -> None:
         """Compute only rank ``rank``'s share of the node pairs (symmetric

@@ -144,9 +144,16 @@ def test_transpose_apply_off_surface_and_corrected(ctx, pde):
 def test_launch_counter_advances(ctx):
     q = SURF["kite"]
     A = inti.IntegralOperator(inti.DoubleLayerKernel(inti.Laplace(dim=2)), q, ctx=ctx)
+    assert A.tuning["single_launch"]
     before = ctx.launch_count
     A @ np.ones(len(q))
-    assert ctx.launch_count - before == 3  # pack, pair, epilogue
+    assert ctx.launch_count - before == 2  # pack, pair sums with the epilogue
+    tiled = inti.Context(0)
+    tiled.set_single_launch(False)
+    B = inti.IntegralOperator(inti.DoubleLayerKernel(inti.Laplace(dim=2)), q, ctx=tiled)
+    before = tiled.launch_count
+    B @ np.ones(len(q))
+    assert tiled.launch_count - before == 3  # pack, pair, epilogue
 
 
 def test_fast_special_functions_accuracy(ctx):

@@ -19,6 +19,16 @@ pytestmark = pytest.mark.gpu
 def one_sided():
     c = inti.Context(0)
     c.set_symmetric(False)
+    c.set_single_launch(False)  # the tiled one-sided kernel at every size
+    return c
+
+
+@pytest.fixture(scope="module")
+def tiled():
+    """The symmetric kernel at every size (small FP64 operators otherwise
+    take the single-launch form)."""
+    c = inti.Context(0)
+    c.set_single_launch(False)
     return c
 
 
@@ -132,7 +142,7 @@ def test_symmetric_gmres_matches_one_sided(ctx, one_sided):
 
 @pytest.mark.parametrize("n", [1, 7, 511, 512, 513, 1025])
 @pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
-def test_symmetric_edge_sizes(ctx, n, pde):
+def test_symmetric_edge_sizes(tiled, n, pde):
     """Node counts around the block size (512 or 256 nodes): a single node,
     a partial block, exact blocks and one node past them; points with
     arbitrary normals and weights (no element structure needed)."""
@@ -147,8 +157,8 @@ def test_symmetric_edge_sizes(ctx, n, pde):
     x = density(n, cplx, 2)
     op = inti.Laplace(dim=3) if pde == O.LAPLACE else inti.Helmholtz(k=3.0, dim=3)
     for K, okind in KERNELS.values():
-        A = inti.GpuOperator(K(op), q, q, None, "fp64", ctx)
-        assert A.tuning["symmetric"]
+        A = inti.GpuOperator(K(op), q, q, None, "fp64", tiled)
+        assert A.tuning["symmetric"] and not A.tuning["single_launch"]
         ref = oracle_apply(pde, okind, k, q, q, x)
         got = A @ x
         if n == 1:
@@ -190,7 +200,7 @@ def test_symmetric_2d_laplace(ctx, one_sided, kname, prec):
 
 
 @pytest.mark.parametrize("n", [1, 7, 257, 513])
-def test_symmetric_2d_edge_sizes(ctx, n):
+def test_symmetric_2d_edge_sizes(tiled, n):
     r = np.random.default_rng(100 + n)
     X = r.standard_normal((n, 2))
     N = r.standard_normal((n, 2))
@@ -198,8 +208,8 @@ def test_symmetric_2d_edge_sizes(ctx, n):
     q = inti.Quadrature(X, N, r.uniform(0.5, 1.5, n), 0)
     x = density(n, False, 3)
     for K, okind in KERNELS.values():
-        A = inti.GpuOperator(K(inti.Laplace(dim=2)), q, q, None, "fp64", ctx)
-        assert A.tuning["symmetric"]
+        A = inti.GpuOperator(K(inti.Laplace(dim=2)), q, q, None, "fp64", tiled)
+        assert A.tuning["symmetric"] and not A.tuning["single_launch"]
         got = A @ x
         if n == 1:
             assert np.all(got == 0)
