@@ -371,7 +371,8 @@ int inti_apply_noalloc(int pde, int kernel, int dim, double k, int precision, in
  * reciprocal square root over [1e-27, 1e27]; out[1], out[2] max absolute
  * error of the FP64 e^{i theta} for theta <= 25 and theta <= 1000; out[3]
  * the same for the FP32 form, theta <= 25; out[4] max relative error of the
- * FP64 x^{-3/2} over [1e-27, 1e27].  out holds 5 doubles. */
+ * FP64 x^{-3/2} over [1e-27, 1e27]; out[5] max relative error of the FP64
+ * reciprocal over [1e-27, 1e27].  out holds 6 doubles. */
 int inti_selftest_math(inti_ctx* ctx, double* out);
 
 #ifdef __cplusplus

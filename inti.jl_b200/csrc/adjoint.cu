@@ -105,7 +105,7 @@ __global__ void __launch_bounds__(kAdjBlock) adjoint_sources(
             }
           }
         } else {
-          const double id2 = keep ? 1.0 / d2 : 0.0;
+          const double id2 = keep ? rcp_fast(d2) : 0.0;
           if (KIND == SL) {
             s[u] = fma(gi, keep ? log(d2) : 0.0, s[u]);  // scaled by -1/(4 pi) at the end
 #pragma unroll

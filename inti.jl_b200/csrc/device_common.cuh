@@ -195,6 +195,21 @@ __device__ __forceinline__ double rsqrt_fast(double x) {
 }
 __device__ __forceinline__ float rsqrt_fast(float x) { return rsqrt_approx_f32(x); }
 
+__device__ __forceinline__ double rcp_approx_f64(double x) {
+  double r;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+  return r;
+}
+
+// 1/x to ~1 ulp for normal x > 0 (NaN for x == 0): the hardware estimate y
+// refined by one third-order Newton step for f(y) = 1/y - x,
+// y' = y (1 + e + e^2) with e = 1 - x y, which cubes the relative error.
+__device__ __forceinline__ double rcp_fast(double x) {
+  const double y = rcp_approx_f64(x);
+  const double e = fma(-x, y, 1.0);
+  return fma(y, fma(e, e, e), y);
+}
+
 // x^{-3/2} to a few ulp for normal x > 0 (NaN for x == 0).
 __device__ __forceinline__ double rsqrt_cube_fast(double x) {
   const double y = rsqrt_approx_f64(x);

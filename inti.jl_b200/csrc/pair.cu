@@ -21,6 +21,7 @@
 //    carries no O(N eps) growth.
 //  * The epilogue applies the kernel constant, alpha/beta, and the CSR
 //    correction row in the same pass (the fused near-field correction).
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -61,6 +62,48 @@ struct Rec {
   static constexpr bool tnormal = (KIND == ADL || KIND == HS);
 };
 
+// Record of source j (zero past n: a zero charge at the origin, which adds
+// nothing to any target).
+template <int PDE, int KIND, int DIM, class R>
+__device__ __forceinline__ void build_record(int64_t j, int64_t n, const double* __restrict__ xs,
+                                             const double* __restrict__ ns, const double* __restrict__ w,
+                                             const double* __restrict__ sigma, double2 c1, double2 c2,
+                                             R (&rec)[Rec<PDE, KIND, DIM, R>::n]) {
+  using RC = Rec<PDE, KIND, DIM, R>;
+#pragma unroll
+  for (int c = 0; c < RC::n; ++c) rec[c] = R(0);
+  if (j >= n) return;
+#pragma unroll
+  for (int c = 0; c < DIM; ++c) rec[c] = R(xs[DIM * j + c]);
+  const double wj = w[j];
+  double qr, qi = 0.0;
+  if (RC::cplx) {
+    qr = wj * sigma[2 * j];
+    qi = wj * sigma[2 * j + 1];
+  } else {
+    qr = wj * sigma[j];
+  }
+  if (RC::charge2) {
+    // monopole charge c2*q after the dipole block
+    const double mr = c2.x * qr - c2.y * qi, mi = c2.x * qi + c2.y * qr;
+    rec[DIM + (RC::cplx ? 2 : 1) * DIM] = R(mr);
+    if (RC::cplx) rec[DIM + 2 * DIM + 1] = R(mi);
+    const double dr = c1.x * qr - c1.y * qi, di = c1.x * qi + c1.y * qr;
+    qr = dr;
+    qi = di;
+  }
+  if (RC::dipole) {
+#pragma unroll
+    for (int c = 0; c < DIM; ++c) {
+      rec[DIM + c] = R(qr * ns[DIM * j + c]);
+      if (RC::cplx) rec[2 * DIM + c] = R(qi * ns[DIM * j + c]);
+    }
+  } else {
+    rec[DIM] = R(qr);
+    if (RC::cplx) rec[DIM + 1] = R(qi);
+  }
+}
+
 template <int PDE, int KIND, int DIM, class R>
 __global__ void pack_sources(int64_t n, int64_t npad, const double* __restrict__ xs,
                              const double* __restrict__ ns, const double* __restrict__ w,
@@ -70,39 +113,7 @@ __global__ void pack_sources(int64_t n, int64_t npad, const double* __restrict__
   const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   if (j >= npad) return;
   R rec[RC::n];
-#pragma unroll
-  for (int c = 0; c < RC::n; ++c) rec[c] = R(0);
-  if (j < n) {
-#pragma unroll
-    for (int c = 0; c < DIM; ++c) rec[c] = R(xs[DIM * j + c]);
-    const double wj = w[j];
-    double qr, qi = 0.0;
-    if (RC::cplx) {
-      qr = wj * sigma[2 * j];
-      qi = wj * sigma[2 * j + 1];
-    } else {
-      qr = wj * sigma[j];
-    }
-    if (RC::charge2) {
-      // monopole charge c2*q after the dipole block
-      const double mr = c2.x * qr - c2.y * qi, mi = c2.x * qi + c2.y * qr;
-      rec[DIM + (RC::cplx ? 2 : 1) * DIM] = R(mr);
-      if (RC::cplx) rec[DIM + 2 * DIM + 1] = R(mi);
-      const double dr = c1.x * qr - c1.y * qi, di = c1.x * qi + c1.y * qr;
-      qr = dr;
-      qi = di;
-    }
-    if (RC::dipole) {
-#pragma unroll
-      for (int c = 0; c < DIM; ++c) {
-        rec[DIM + c] = R(qr * ns[DIM * j + c]);
-        if (RC::cplx) rec[2 * DIM + c] = R(qi * ns[DIM * j + c]);
-      }
-    } else {
-      rec[DIM] = R(qr);
-      if (RC::cplx) rec[DIM + 1] = R(qi);
-    }
-  }
+  build_record<PDE, KIND, DIM, R>(j, n, xs, ns, w, sigma, c1, c2, rec);
   R* o = out + j * RC::n;
 #pragma unroll
   for (int c = 0; c < RC::n; ++c) o[c] = rec[c];
@@ -119,6 +130,7 @@ struct MathOps<double> {
   using R2 = double2;
   static __device__ __forceinline__ double rsq(double v) { return rsqrt_fast(v); }
   static __device__ __forceinline__ double rsq3(double v) { return rsqrt_cube_fast(v); }
+  static __device__ __forceinline__ double rcp(double v) { return rcp_fast(v); }
   static __device__ __forceinline__ double lg(double v) { return log(v); }
   static __device__ __forceinline__ bool keep(double d2) { return pair_keep(d2); }
 };
@@ -127,6 +139,7 @@ struct MathOps<float> {
   using R2 = float2;
   static __device__ __forceinline__ float rsq(float v) { return rsqrt_fast(v); }
   static __device__ __forceinline__ float rsq3(float v) { return rsqrt_cube_fast(v); }
+  static __device__ __forceinline__ float rcp(float v) { return 1.0f / v; }
   static __device__ __forceinline__ float lg(float v) { return __logf(v); }
   static __device__ __forceinline__ bool keep(float d2) { return d2 > 1.0e-28f; }
 };
@@ -170,7 +183,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
 #pragma unroll
       for (int c = 1; c < DIM; ++c) rp = fma(r[c], s[DIM + c], rp);
       if (DIM == 2) {
-        const R ri = keep ? R(1) / d2 : R(0);
+        const R ri = keep ? M::rcp(d2) : R(0);
         ar = fma(rp, ri, ar);
       } else if (KIND == CF) {
         const R ri = keep ? M::rsq(d2) : R(0);
@@ -185,7 +198,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
       for (int c = 1; c < DIM; ++c) rn = fma(r[c], t.n[c], rn);
       const R q = s[DIM];
       if (DIM == 2) {
-        const R ri = keep ? R(1) / d2 : R(0);
+        const R ri = keep ? M::rcp(d2) : R(0);
         ar = fma(rn * q, ri, ar);
       } else {
         ar = fma(rn * q, keep ? M::rsq3(d2) : R(0), ar);
@@ -199,7 +212,7 @@ __device__ __forceinline__ void pair_step(const Target<R, DIM, Rec<PDE, KIND, DI
         np = fma(t.n[c], s[DIM + c], np);
       }
       if (DIM == 2) {
-        const R id2 = keep ? R(1) / d2 : R(0);
+        const R id2 = keep ? M::rcp(d2) : R(0);
         ar = fma(id2, fma(R(-2) * rn * rp, id2, np), ar);
       } else {
         const R ri = keep ? M::rsq(d2) : R(0);
@@ -471,6 +484,29 @@ struct EpiArgs {
   const int* err = nullptr;          // when set and nonzero (a pair kernel timed out): y gets NaN
 };
 
+// y[i] before the product (read only when beta != 0).
+template <bool CPLX>
+__device__ __forceinline__ double2 epilogue_y_old(const EpiArgs& e, int64_t i) {
+  return CPLX ? reinterpret_cast<const double2*>(e.y)[i] : make_double2(e.y[i], 0.0);
+}
+
+// y[i] = alpha * (sr, si) + beta * yo, yo the old y[i].
+template <bool CPLX>
+__device__ __forceinline__ void epilogue_store(const EpiArgs& e, int64_t i, double sr, double si, double2 yo) {
+  if (CPLX) {
+    double yr = e.ar * sr - e.ai * si, yi = e.ar * si + e.ai * sr;
+    if (!e.beta_zero) {
+      yr += e.br * yo.x - e.bi * yo.y;
+      yi += e.br * yo.y + e.bi * yo.x;
+    }
+    reinterpret_cast<double2*>(e.y)[i] = make_double2(yr, yi);
+  } else {
+    double yr = e.ar * sr;
+    if (!e.beta_zero) yr += e.br * yo.x;
+    e.y[i] = yr;
+  }
+}
+
 // Kernel constant, correction row, alpha/beta and the store for row i, given
 // the row's pair sum (sr, si).
 template <bool CPLX>
@@ -492,19 +528,7 @@ __device__ __forceinline__ void epilogue_finish(const EpiArgs& e, int64_t i, dou
       }
     }
   }
-  if (CPLX) {
-    double yr = e.ar * sr - e.ai * si, yi = e.ar * si + e.ai * sr;
-    if (!e.beta_zero) {
-      const double2 yo = reinterpret_cast<const double2*>(e.y)[i];
-      yr += e.br * yo.x - e.bi * yo.y;
-      yi += e.br * yo.y + e.bi * yo.x;
-    }
-    reinterpret_cast<double2*>(e.y)[i] = make_double2(yr, yi);
-  } else {
-    double yr = e.ar * sr;
-    if (!e.beta_zero) yr += e.br * e.y[i];
-    e.y[i] = yr;
-  }
+  epilogue_store<CPLX>(e, i, sr, si, e.beta_zero ? make_double2(0.0, 0.0) : epilogue_y_old<CPLX>(e, i));
 }
 
 template <class P, bool CPLX>
@@ -531,55 +555,156 @@ __global__ void pair_epilogue_kernel(EpiArgs e) {
 
 // ---------------------------------------------------------------------------
 // Single-launch form for small FP64 operators (m*n up to kSmallPairs, e.g.
-// the 1,000-node kite): the pair sums and the epilogue in one kernel after
-// the pack.  The tiled kernels give such a problem only a few CTAs (ten for
-// a 1,000-node square operator) whose threads each run a long dependent
-// chain; here a CTA of kSmallWarps warps takes 32 targets (one per lane) and
-// its warps split the sources, so every SM has work and each thread's chain
-// is n/kSmallWarps sources.  The step is pair_step's (the one-sided
-// kernel's arithmetic); the warps' sums are added in a fixed order, then
-// the kernel constant, the correction row and alpha/beta as in the
-// epilogue.
+// the 1,000-node kite): one kernel per product, no pack.  The tiled kernels
+// give such a problem a handful of CTAs whose threads each run a long chain
+// of dependent global loads, so the launch is latency-bound.  Here a
+// cluster of S CTAs takes 32 targets (one per lane); CTA s of the cluster
+// takes the s-th slice of the sources, builds their records in shared memory
+// from the raw nodes (build_record, kSmallTile at a time), and its warps
+// split each staged tile.  S is chosen on the host so that the clusters
+// fill the SMs.  The correction row of a target is split over the same
+// S * kSmallWarps threads (entry p0 + s*kSmallWarps + warp, then strides of
+// S*kSmallWarps); the first kSmallCorr entries of a thread are fetched before
+// the pair loop so their latency hides behind it.  The warps' pair and
+// correction sums are added in a fixed order, then the slices' sums, read
+// by CTA 0 of the cluster from its peers' shared memory (distributed shared
+// memory), in slice order; CTA 0 then applies the kernel constant to the
+// pair sum, adds the correction sum and alpha/beta.  The step is
+// pair_step's (the one-sided kernel's arithmetic).
 // ---------------------------------------------------------------------------
 constexpr int kSmallWarps = 8;
+constexpr int kSmallTile = 32 * kSmallWarps;  // sources staged per pass, one per thread
+constexpr int kSmallMaxSlices = 8;            // portable cluster size
+constexpr int kSmallCorr = 2;                 // correction entries per thread fetched ahead
+
+struct SmallSources {
+  const double *xs, *ns, *w, *sigma;
+  double2 c1, c2;
+};
 
 template <int PDE, int KIND, int DIM>
 __global__ void __launch_bounds__(32 * kSmallWarps) pair_small_kernel(int64_t m, int64_t n, const double* tc,
-                                                                      const double* tn, const double* packed,
+                                                                      const double* tn, SmallSources src,
                                                                       double k, double kT, double delta,
                                                                       const double2* expi, EpiArgs e) {
+  namespace cg = cooperative_groups;
   using RC = Rec<PDE, KIND, DIM, double>;
   constexpr bool CPLX = RC::cplx;
-  __shared__ double2 part[kSmallWarps][32];
+  // the staged records; after the last tile, the warps' sums (pair, correction)
+  __shared__ __align__(16) double recs[kSmallTile * RC::n];
+  __shared__ double4 slice_sum[32];
   __shared__ double2 tab[CPLX ? kExpiTable : 1];
+  static_assert(kSmallTile * RC::n >= 4 * 32 * kSmallWarps, "the sums reuse the record buffer");
+  cg::cluster_group cl = cg::this_cluster();
+  const int64_t slices = cl.num_blocks(), slice = cl.block_rank();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int64_t i = blockIdx.x * (int64_t)32 + lane;
+  const int64_t i = (blockIdx.x / slices) * 32 + lane;
+  const bool lead = slice == 0 && warp == 0;
   if (CPLX)
     for (int q = threadIdx.x; q < kExpiTable; q += 32 * kSmallWarps) tab[q] = expi[q];
-  __syncthreads();
-  double ar = 0.0, ai = 0.0;
+  Target<double, DIM, RC::tnormal> t;
+  int64_t p = 0, p1 = 0;  // this thread's next correction entry, row end
+  double2 yo = make_double2(0.0, 0.0);
   if (i < m) {
-    Target<double, DIM, RC::tnormal> t;
 #pragma unroll
     for (int c = 0; c < DIM; ++c) t.x[c] = tc[DIM * i + c];
     if constexpr (RC::tnormal) {
 #pragma unroll
       for (int c = 0; c < DIM; ++c) t.n[c] = tn[DIM * i + c];
     }
-    const int64_t per = (n + kSmallWarps - 1) / kSmallWarps;
-    const int64_t j0 = warp * per, j1 = j0 + per < n ? j0 + per : n;
-    for (int64_t j = j0; j < j1; ++j) pair_step<PDE, KIND, DIM, double>(t, packed + j * RC::n, kT, delta, k, tab, ar, ai);
+    if (e.rowptr) {
+      p = e.rowptr[i] + slice * kSmallWarps + warp;
+      p1 = e.rowptr[i + 1];
+    }
+    if (lead && !e.beta_zero) yo = epilogue_y_old<CPLX>(e, i);
   }
-  part[warp][lane] = make_double2(ar, ai);
-  __syncthreads();
-  if (warp != 0 || i >= m) return;
-  double sr = 0.0, si = 0.0;
+  const int64_t pstride = slices * kSmallWarps;
+  const int64_t per = (n + slices - 1) / slices;
+  const int64_t j0 = slice * per, j1 = j0 + per < n ? j0 + per : n;
+  double ar = 0.0, ai = 0.0;
+  int32_t cc[kSmallCorr];
+  double2 cv[kSmallCorr];
+  for (int64_t base = j0; base < j1; base += kSmallTile) {
+    const int cnt = (int)(j1 - base < kSmallTile ? j1 - base : kSmallTile);
+    __syncthreads();  // the previous tile is consumed
+    if (threadIdx.x < cnt) {
+      double rec[RC::n];
+      build_record<PDE, KIND, DIM, double>(base + threadIdx.x, n, src.xs, src.ns, src.w, src.sigma, src.c1,
+                                           src.c2, rec);
+      double2* o = reinterpret_cast<double2*>(recs + threadIdx.x * RC::n);
 #pragma unroll
-  for (int w = 0; w < kSmallWarps; ++w) {
-    sr += part[w][lane].x;
-    si += part[w][lane].y;
+      for (int c = 0; c < RC::n / 2; ++c) o[c] = make_double2(rec[2 * c], rec[2 * c + 1]);
+    }
+    if (base == j0) {
+      // correction entries fetched ahead (their values are used after the pair loop)
+#pragma unroll
+      for (int u = 0; u < kSmallCorr; ++u) {
+        const int64_t pu = p + u * pstride;
+        cc[u] = pu < p1 ? e.col[pu] : -1;
+        cv[u] = pu < p1 ? (CPLX ? reinterpret_cast<const double2*>(e.val)[pu] : make_double2(e.val[pu], 0.0))
+                        : make_double2(0.0, 0.0);
+      }
+    }
+    __syncthreads();
+    if (i < m) {
+      const int pw = (cnt + kSmallWarps - 1) / kSmallWarps;
+      const int q0 = warp * pw, q1 = q0 + pw < cnt ? q0 + pw : cnt;
+      for (int q = q0; q < q1; ++q) pair_step<PDE, KIND, DIM, double>(t, recs + q * RC::n, kT, delta, k, tab, ar, ai);
+    }
   }
-  epilogue_finish<CPLX>(e, i, sr, si);
+  if (j0 >= j1) {  // an empty slice still fetches its correction entries
+#pragma unroll
+    for (int u = 0; u < kSmallCorr; ++u) {
+      const int64_t pu = p + u * pstride;
+      cc[u] = pu < p1 ? e.col[pu] : -1;
+      cv[u] = pu < p1 ? (CPLX ? reinterpret_cast<const double2*>(e.val)[pu] : make_double2(e.val[pu], 0.0))
+                      : make_double2(0.0, 0.0);
+    }
+  }
+  double cr = 0.0, ci = 0.0;
+  auto corr_add = [&](int32_t j, double2 v) {
+    if (CPLX) {
+      const double2 xv = reinterpret_cast<const double2*>(e.x)[j];
+      cr = fma(v.x, xv.x, fma(-v.y, xv.y, cr));
+      ci = fma(v.x, xv.y, fma(v.y, xv.x, ci));
+    } else {
+      cr = fma(v.x, e.x[j], cr);
+    }
+  };
+#pragma unroll
+  for (int u = 0; u < kSmallCorr; ++u)
+    if (cc[u] >= 0) corr_add(cc[u], cv[u]);
+  for (int64_t pu = p + kSmallCorr * pstride; pu < p1; pu += pstride)
+    corr_add(e.col[pu], CPLX ? reinterpret_cast<const double2*>(e.val)[pu] : make_double2(e.val[pu], 0.0));
+  __syncthreads();  // every warp is done with the records: reuse them for the sums
+  double4* part = reinterpret_cast<double4*>(recs);  // [warp][lane]
+  part[warp * 32 + lane] = make_double4(ar, ai, cr, ci);
+  __syncthreads();
+  if (warp == 0) {
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+    for (int w = 0; w < kSmallWarps; ++w) {
+      const double4 v = part[w * 32 + lane];
+      acc.x += v.x;
+      acc.y += v.y;
+      acc.z += v.z;
+      acc.w += v.w;
+    }
+    slice_sum[lane] = acc;
+  }
+  cl.sync();  // every slice's sums are in its shared memory
+  if (lead && i < m) {
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
+    for (int r = 0; r < (int)slices; ++r) {
+      const double4 v = *cl.map_shared_rank(&slice_sum[lane], r);
+      acc.x += v.x;
+      acc.y += v.y;
+      acc.z += v.z;
+      acc.w += v.w;
+    }
+    epilogue_store<CPLX>(e, i, fma(acc.x, e.scale, acc.z), fma(acc.y, e.scale, acc.w), yo);
+  }
+  cl.sync();  // the peers' shared memory stays valid until CTA 0 has read it
 }
 
 // ---------------------------------------------------------------------------
@@ -692,7 +817,7 @@ __device__ __forceinline__ void pair_sym_step_2d(const R* __restrict__ t, const 
     if (COL) zr = fma(l, t[2], zr);
     return;
   }
-  const R id2 = keep ? R(1) / d2 : R(0);
+  const R id2 = keep ? M::rcp(d2) : R(0);
   if (KIND == DL) {
     ar = fma(fma(r1, s[3], r0 * s[2]), id2, ar);
     if (COL) zr = fma(-fma(r1, t[3], r0 * t[2]), id2, zr);
@@ -1823,6 +1948,13 @@ bool pair_small_eligible(int precision, int64_t m, int64_t n) {
   return precision == INTI_FP64 && (double)m * (double)n <= kSmallPairs && m > 0 && n > 0;
 }
 
+static int pair_small_slices(int num_sms, int64_t m, int64_t n) {
+  const int64_t rows = (m + 31) / 32;
+  int s = 1;
+  while (s < kSmallMaxSlices && rows * 2 * s <= num_sms && n >= (int64_t)64 * 2 * s) s *= 2;
+  return s;
+}
+
 int pair_small(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x, double* y,
                const double* alpha, const double* beta) {
   EpiArgs e;
@@ -1840,23 +1972,32 @@ int pair_small(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const d
   e.br = beta ? beta[0] : 0.0;
   e.bi = beta ? beta[1] : 0.0;
   e.beta_zero = (e.br == 0.0 && e.bi == 0.0);
+  const SmallSources src{L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
+                         make_double2(L.c2[0], L.c2[1])};
+  const int slices = pair_small_slices(ctx->num_sms, L.m, L.n);
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = slices;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)((L.m + 31) / 32 * slices));
+  cfg.blockDim = dim3(32 * kSmallWarps);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = ctx->stream;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  const double2* expi = L.pde == HELMHOLTZ ? expi_table_f64(ctx) : nullptr;
+  const double kT = L.k * kExpiTable / (2 * kPi), delta = 2 * kPi / kExpiTable;
   dispatch(L.pde, L.kind, L.dim, [&](auto tag) {
     using T = decltype(tag);
-    const unsigned gp = (unsigned)((L.n + 255) / 256);
-    {
-      ProfScope ps(ctx, "pack");
-      pack_sources<T::pde, T::kind, T::dim, double><<<gp, 256, 0, ctx->stream>>>(
-          L.n, L.n, L.scoords, L.snormals, L.sweights, L.x, make_double2(L.c1[0], L.c1[1]),
-          make_double2(L.c2[0], L.c2[1]), static_cast<double*>(L.packed));
-    }
     ProfScope pp(ctx, "pair");
-    pair_small_kernel<T::pde, T::kind, T::dim><<<(unsigned)((L.m + 31) / 32), 32 * kSmallWarps, 0, ctx->stream>>>(
-        L.m, L.n, L.tcoords, L.tnormals, static_cast<const double*>(L.packed), L.k, L.k * kExpiTable / (2 * kPi),
-        2 * kPi / kExpiTable, T::pde == HELMHOLTZ ? expi_table_f64(ctx) : nullptr, e);
+    INTI_CUDA(cudaLaunchKernelEx(&cfg, pair_small_kernel<T::pde, T::kind, T::dim>, (int64_t)L.m, (int64_t)L.n,
+                                 L.tcoords, L.tnormals, src, (double)L.k, kT, delta, expi, e));
   });
   INTI_CUDA(cudaGetLastError());
-  ctx->launches += 2;
-  return 2;
+  ctx->launches += 1;
+  return 1;
 }
 
 int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out) {

@@ -95,7 +95,7 @@ void measure_peaks(inti_ctx* ctx, double* fp64, double* fp32, double* mufu) {
 }
 
 // Evaluates the pair loops' fast special functions on given inputs.
-__global__ void math_probe(int n, const double* x, double* rs, double* rs3, const double* u,
+__global__ void math_probe(int n, const double* x, double* rs, double* rs3, double* rc, const double* u,
                            const double2* tab64, const float2* tab32, double2* e64, float2* e32) {
   __shared__ double2 t64[kExpiTable];
   __shared__ float2 t32[kExpiTable];
@@ -108,6 +108,7 @@ __global__ void math_probe(int n, const double* x, double* rs, double* rs3, cons
   if (i >= n) return;
   rs[i] = rsqrt_fast(x[i]);
   rs3[i] = rsqrt_cube_fast(x[i]);
+  rc[i] = rcp_fast(x[i]);
   double c, s;
   expi_table_eval(u[i], 1.0, t64, 2 * kPi / kExpiTable, c, s);
   e64[i] = make_double2(c, s);
@@ -132,36 +133,40 @@ void selftest_math(inti_ctx* ctx, double* out) {
     const double th = i < n / 2 ? 25.0 * rnd() : 1000.0 * rnd();
     u[i] = th * kExpiTable / (2 * kPi);
   }
-  DevBuf dx, drs, drs3, du, d64, d32;
+  DevBuf dx, drs, drs3, drc, du, d64, d32;
   dx.ensure(8 * n);
   drs.ensure(8 * n);
   drs3.ensure(8 * n);
+  drc.ensure(8 * n);
   du.ensure(8 * n);
   d64.ensure(16 * n);
   d32.ensure(8 * n);
   INTI_CUDA(cudaMemcpy(dx.p, x.data(), 8 * n, cudaMemcpyHostToDevice));
   INTI_CUDA(cudaMemcpy(du.p, u.data(), 8 * n, cudaMemcpyHostToDevice));
   math_probe<<<n / 256, 256, 0, ctx->stream>>>(n, dx.as<double>(), drs.as<double>(), drs3.as<double>(),
-                                               du.as<double>(),
+                                               drc.as<double>(), du.as<double>(),
                                                expi_table_f64(ctx), expi_table_f32(ctx),
                                                d64.as<double2>(), d32.as<float2>());
   ctx->launches++;
   INTI_CUDA(cudaGetLastError());
   INTI_CUDA(cudaStreamSynchronize(ctx->stream));
-  std::vector<double> rs(n), rs3(n);
+  std::vector<double> rs(n), rs3(n), rc(n);
   std::vector<double2> e64(n);
   std::vector<float2> e32(n);
   INTI_CUDA(cudaMemcpy(rs.data(), drs.p, 8 * n, cudaMemcpyDeviceToHost));
   INTI_CUDA(cudaMemcpy(rs3.data(), drs3.p, 8 * n, cudaMemcpyDeviceToHost));
+  INTI_CUDA(cudaMemcpy(rc.data(), drc.p, 8 * n, cudaMemcpyDeviceToHost));
   INTI_CUDA(cudaMemcpy(e64.data(), d64.p, 16 * n, cudaMemcpyDeviceToHost));
   INTI_CUDA(cudaMemcpy(e32.data(), d32.p, 8 * n, cudaMemcpyDeviceToHost));
-  double m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0;
+  double m0 = 0, m1 = 0, m2 = 0, m3 = 0, m4 = 0, m5 = 0;
   const long double delta = (long double)(2 * kPi / kExpiTable);
   for (int i = 0; i < n; ++i) {
     const long double ref = 1.0L / sqrtl((long double)x[i]);
     m0 = std::max(m0, (double)fabsl(((long double)rs[i] - ref) / ref));
     const long double ref3 = ref * ref * ref;
     m4 = std::max(m4, (double)fabsl(((long double)rs3[i] - ref3) / ref3));
+    const long double refr = 1.0L / (long double)x[i];
+    m5 = std::max(m5, (double)fabsl(((long double)rc[i] - refr) / refr));
     const long double th = (long double)u[i] * delta;
     const double err64 = (double)std::max(fabsl(e64[i].x - cosl(th)), fabsl(e64[i].y - sinl(th)));
     const double err32 = (double)std::max(fabsl(e32[i].x - cosl(th)), fabsl(e32[i].y - sinl(th)));
@@ -177,6 +182,7 @@ void selftest_math(inti_ctx* ctx, double* out) {
   out[2] = m2;
   out[3] = m3;
   out[4] = m4;
+  out[5] = m5;
 }
 
 }  // namespace inti

@@ -132,11 +132,12 @@ class Context:
         self.check(self.lib.inti_ctx_set_partial_budget(self.handle, float(nbytes)))
 
     def selftest_math(self) -> dict:
-        """Accuracy of the device's fast rsqrt / e^{iθ} helpers (see the ABI)."""
-        out = (C.c_double * 5)()
+        """Accuracy of the device's fast rsqrt / reciprocal / e^{iθ} helpers (see the ABI)."""
+        out = (C.c_double * 6)()
         self.check(self.lib.inti_selftest_math(self.handle, out))
         return {"rsqrt_f64_maxrel": out[0], "expi_f64_maxabs_25": out[1], "expi_f64_maxabs_1000": out[2],
-                "expi_f32_maxabs_25": out[3], "rsqrt_cube_f64_maxrel": out[4]}
+                "expi_f32_maxabs_25": out[3], "rsqrt_cube_f64_maxrel": out[4],
+                "rcp_f64_maxrel": out[5]}
 
     def measure_peaks(self) -> dict:
         a, b, c, t = C.c_double(), C.c_double(), C.c_double(), C.c_double()

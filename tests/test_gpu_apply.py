@@ -147,7 +147,7 @@ def test_launch_counter_advances(ctx):
     assert A.tuning["single_launch"]
     before = ctx.launch_count
     A @ np.ones(len(q))
-    assert ctx.launch_count - before == 2  # pack, pair sums with the epilogue
+    assert ctx.launch_count - before == 1  # one kernel: records, pair sums, epilogue
     tiled = inti.Context(0)
     tiled.set_single_launch(False)
     B = inti.IntegralOperator(inti.DoubleLayerKernel(inti.Laplace(dim=2)), q, ctx=tiled)
@@ -157,10 +157,11 @@ def test_launch_counter_advances(ctx):
 
 
 def test_fast_special_functions_accuracy(ctx):
-    """The pair loops' rsqrt, x^{-3/2} and e^{iθ} against extended precision."""
+    """The pair loops' rsqrt, x^{-3/2}, reciprocal and e^{iθ} against extended precision."""
     r = ctx.selftest_math()
     assert r["rsqrt_f64_maxrel"] < 4e-16, r
     assert r["rsqrt_cube_f64_maxrel"] < 8e-16, r
+    assert r["rcp_f64_maxrel"] < 3e-16, r
     assert r["expi_f64_maxabs_25"] < 8e-16, r
     assert r["expi_f64_maxabs_1000"] < 2e-13, r
     assert r["expi_f32_maxabs_25"] < 4e-6, r
