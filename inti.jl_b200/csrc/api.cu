@@ -85,11 +85,14 @@ namespace inti {
 void noalloc_error_set(const char* msg) { g_thread_error = msg; }
 
 void sync_and_check(inti_ctx* ctx) {
+  // the flag comes back with the stream's other work: one round trip per call
+  INTI_CUDA(cudaMemcpyAsync(ctx->err_host, ctx->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   INTI_CUDA(cudaStreamSynchronize(ctx->stream));
-  int flag = 0;
-  INTI_CUDA(cudaMemcpy(&flag, ctx->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost));
+  const int flag = *ctx->err_host;
   if (flag) {
-    INTI_CUDA(cudaMemset(ctx->err_flag.p, 0, sizeof(int)));
+    *ctx->err_host = 0;
+    INTI_CUDA(cudaMemsetAsync(ctx->err_flag.p, 0, sizeof(int), ctx->stream));
+    INTI_CUDA(cudaStreamSynchronize(ctx->stream));
     throw Error(INTI_E_TIMEOUT, "a device-side bounded wait ran out (code " + std::to_string(flag) + ")");
   }
 }
@@ -322,6 +325,8 @@ int inti_ctx_create(int device, void* stream, inti_ctx** out) {
     INTI_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
     c->err_flag.ensure(sizeof(int));
     INTI_CUDA(cudaMemset(c->err_flag.p, 0, sizeof(int)));
+    INTI_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&c->err_host), sizeof(int), cudaHostAllocDefault));
+    *c->err_host = 0;
     *out = c.release();
   });
 }
@@ -337,6 +342,8 @@ int inti_ctx_destroy(inti_ctx* ctx) {
     }
     ctx->spans.clear();
     ctx->err_flag.release();
+    if (ctx->err_host) cudaFreeHost(ctx->err_host);
+    ctx->err_host = nullptr;
     for (inti::DevBuf* d : {&ctx->krylov.V, &ctx->krylov.w, &ctx->krylov.r, &ctx->krylov.e, &ctx->krylov.w_outer,
                             &ctx->krylov.partial, &ctx->krylov.h, &ctx->krylov.y, &ctx->krylov.nrm, &ctx->krylov.b,
                             &ctx->krylov.x, &ctx->expi64, &ctx->expi32, &ctx->dimwork.d_xs, &ctx->dimwork.g0,

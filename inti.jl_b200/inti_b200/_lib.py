@@ -180,7 +180,16 @@ def dptr(a) -> int | None:
     return a.ctypes.data
 
 
+_ONE = (C.c_double * 2)(1.0, 0.0)
+_ZERO = (C.c_double * 2)(0.0, 0.0)
+
+
 def cpair(z) -> C.Array:
-    """A complex scalar as the (re, im) double pair the ABI takes."""
+    """A complex scalar as the (re, im) double pair the ABI takes (the ABI
+    only reads it, so 1 and 0 share one array each)."""
+    if z == 1:
+        return _ONE
+    if z == 0:
+        return _ZERO
     z = complex(z)
     return (C.c_double * 2)(z.real, z.imag)

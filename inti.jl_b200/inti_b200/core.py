@@ -487,6 +487,16 @@ class GpuOperator(_Map):
         m, n = self.shape
         if transpose:
             m, n = n, m
+        fn = self.ctx.lib.inti_op_apply_transpose if transpose else self.ctx.lib.inti_op_apply
+        dt = self.dtype
+        if (type(x) is np.ndarray and x.ndim == 1 and x.shape[0] == n and x.dtype == dt and x.flags.c_contiguous
+                and (y is None or (type(y) is np.ndarray and y.ndim == 1 and y.shape[0] == m and y.dtype == dt
+                                   and y.flags.c_contiguous and y.flags.writeable))):
+            # one contiguous column of the operator's type: no conversions
+            if y is None:
+                y, beta = np.empty(m, dt), 0.0
+            self.ctx.check(fn(self.handle, x.ctypes.data, n, y.ctypes.data, m, 1, L.cpair(alpha), L.cpair(beta), 0))
+            return y
         x = np.asarray(x)
         single = x.ndim == 1
         if x.shape[0] != n:
@@ -499,7 +509,6 @@ class GpuOperator(_Map):
             beta = 0.0
         else:
             Y = np.asfortranarray(np.asarray(y, dtype=self.dtype).reshape(m, -1))
-        fn = self.ctx.lib.inti_op_apply_transpose if transpose else self.ctx.lib.inti_op_apply
         self.ctx.check(fn(self.handle, L.dptr(X), n, L.dptr(Y), m, nrhs, L.cpair(alpha), L.cpair(beta), 0))
         out = Y[:, 0] if single else Y
         if y is not None:
