@@ -215,10 +215,12 @@ int inti_op_symmetric(const inti_op* op);
 int inti_ctx_set_partial_budget(inti_ctx* ctx, double bytes);
 int inti_op_panels(const inti_op* op);
 /* Small FP64 operators (at most 2^20 target-source pairs, e.g. the 1,000-node
- * kite) apply in a single-launch form: after the pack, one kernel forms the
- * pair sums (each CTA 32 targets, its warps splitting the sources, a fixed
- * order) together with the epilogue.  inti_ctx_set_single_launch(ctx, 0)
- * makes operators created afterwards use the tiled kernels;
+ * kite) apply in a single-launch form: one kernel per product builds the
+ * source records, forms the pair sums (a cluster of up to 8 CTAs per 32
+ * targets, the CTAs and their warps splitting the sources, sums in a fixed
+ * order), adds the correction rows and applies alpha/beta.  Transposed and
+ * item-sharded applies keep the tiled kernels.  inti_ctx_set_single_launch(ctx,
+ * 0) makes operators created afterwards use the tiled kernels;
  * inti_op_single_launch returns 1 when an operator uses the form.  No
  * counterpart in the reference. */
 int inti_ctx_set_single_launch(inti_ctx* ctx, int enable);  /* default on */

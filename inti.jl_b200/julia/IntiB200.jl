@@ -310,6 +310,17 @@ set_partial_budget!(ctx::Context, bytes::Real) =
 panels(A::B200Map) = Int(ccall((:inti_op_panels, LIB), Cint, (Ptr{Cvoid},), A.h.ptr))
 
 """
+    set_single_launch!(ctx, flag)
+
+Small FP64 operators (at most 2^20 pairs) created afterwards apply with one
+kernel launch per product (`true`, the default) or with the tiled kernels;
+`single_launch(A)` reports the form of an operator.
+"""
+set_single_launch!(ctx::Context, flag::Bool) =
+    check(ccall((:inti_ctx_set_single_launch, LIB), Cint, (Ptr{Cvoid}, Cint), ctx.ptr, flag), ctx.ptr)
+single_launch(A::B200Map) = ccall((:inti_op_single_launch, LIB), Cint, (Ptr{Cvoid},), A.h.ptr) == 1
+
+"""
     set_shard!(A::B200Map, rank, nranks)
 
 One process per GPU: `A` computes only rank `rank`'s share of the node pairs
