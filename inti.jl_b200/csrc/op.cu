@@ -78,66 +78,7 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   return op.release();
 }
 
-// c1*C_dl + c2*C_sl with the union of the two patterns (host merge, once).
-std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, const double* ca,
-                                                   const inti_csr* b, const double* cb, int64_t m,
-                                                   int64_t n, bool cplx) {
-  const int comps = cplx ? 2 : 1;
-  struct Host {
-    std::vector<int64_t> rp;
-    std::vector<int32_t> col;
-    std::vector<double> val;
-  };
-  auto fetch = [&](const inti_csr* c) {
-    Host h;
-    h.rp.assign(m + 1, 0);
-    if (!c) return h;
-    h.col.resize(c->nnz);
-    h.val.resize((size_t)c->nnz * comps);
-    INTI_CUDA(cudaMemcpy(h.rp.data(), c->rowptr.p, sizeof(int64_t) * (m + 1), cudaMemcpyDeviceToHost));
-    INTI_CUDA(cudaMemcpy(h.col.data(), c->col.p, sizeof(int32_t) * c->nnz, cudaMemcpyDeviceToHost));
-    INTI_CUDA(cudaMemcpy(h.val.data(), c->val.p, sizeof(double) * comps * c->nnz, cudaMemcpyDeviceToHost));
-    return h;
-  };
-  INTI_CUDA(cudaStreamSynchronize(ctx->stream));
-  const Host A = fetch(a), B = fetch(b);
-  std::vector<int64_t> rp(m + 1, 0);
-  std::vector<int32_t> col;
-  std::vector<double> val;
-  col.reserve(A.col.size() + B.col.size());
-  val.reserve((A.col.size() + B.col.size()) * comps);
-  auto scaled = [&](const Host& H, int64_t p, const double* c, double* out) {
-    const double vr = H.val[p * comps], vi = cplx ? H.val[p * comps + 1] : 0.0;
-    out[0] = c[0] * vr - c[1] * vi;
-    out[1] = c[0] * vi + c[1] * vr;
-  };
-  for (int64_t i = 0; i < m; ++i) {
-    int64_t pa = A.rp[i], pb = B.rp[i];
-    const int64_t ea = A.rp[i + 1], eb = B.rp[i + 1];
-    while (pa < ea || pb < eb) {
-      const int32_t ja = pa < ea ? A.col[pa] : INT32_MAX, jb = pb < eb ? B.col[pb] : INT32_MAX;
-      const int32_t j = std::min(ja, jb);
-      double v[2] = {0, 0}, t[2];
-      if (ja == j) {
-        scaled(A, pa++, ca, t);
-        v[0] += t[0];
-        v[1] += t[1];
-      }
-      if (jb == j) {
-        scaled(B, pb++, cb, t);
-        v[0] += t[0];
-        v[1] += t[1];
-      }
-      col.push_back(j);
-      val.push_back(v[0]);
-      if (cplx) val.push_back(v[1]);
-    }
-    rp[i + 1] = (int64_t)col.size();
-  }
-  return std::unique_ptr<inti_csr>(csr_create_host(ctx, m, n, (int64_t)col.size(), rp.data(), col.data(),
-                                                   val.data(), cplx ? INTI_C128 : INTI_F64));
-}
-
+// c1*C_dl + c2*C_sl with the union of the two patterns (merged on the device, once).
 inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, const inti_quad* target,
                             const inti_quad* source, const inti_csr* corr_dl, const inti_csr* corr_sl,
                             const double* c_dl, const double* c_sl, int precision) {
