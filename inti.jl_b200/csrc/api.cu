@@ -342,6 +342,7 @@ int inti_ctx_destroy(inti_ctx* ctx) {
     }
     ctx->spans.clear();
     ctx->err_flag.release();
+    ctx->scan_tmp.release();
     if (ctx->err_host) cudaFreeHost(ctx->err_host);
     ctx->err_host = nullptr;
     for (inti::DevBuf* d : {&ctx->krylov.V, &ctx->krylov.w, &ctx->krylov.r, &ctx->krylov.e, &ctx->krylov.w_outer,

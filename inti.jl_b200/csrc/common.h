@@ -77,6 +77,7 @@ struct inti_ctx {
   int64_t launches = 0;
   inti::DevBuf err_flag;  // device int: nonzero when a bounded wait ran out
   int* err_host = nullptr;  // page-locked copy of err_flag, read after a stream sync
+  inti::DevBuf scan_tmp;    // device-scan scratch (correction merges), kept between calls
   inti::DevBuf expi64, expi32;  // e^{i m delta} tables of the Helmholtz pair loops
   // per-kernel-class event timing (inti_ctx_set_profiling)
   bool profiling = false;

@@ -110,15 +110,14 @@ std::unique_ptr<inti_csr> merge_corrections(inti_ctx* ctx, const inti_csr* a, co
   int64_t* rp = out->rowptr.as<int64_t>();
   INTI_CUDA(cudaMemsetAsync(rp, 0, sizeof(int64_t), ctx->stream));
   const unsigned grid = (unsigned)std::max<int64_t>(1, (m + 255) / 256);
-  DevBuf scratch;
   if (m > 0) {
     // counts in rp[1..m], then their inclusive scan in place
     csr_merge_count<<<grid, 256, 0, ctx->stream>>>(m, A, B, rp + 1);
     ctx->launches++;
     size_t tmp = 0;
     INTI_CUDA(cub::DeviceScan::InclusiveSum(nullptr, tmp, rp + 1, rp + 1, m, ctx->stream));
-    scratch.ensure(tmp);
-    INTI_CUDA(cub::DeviceScan::InclusiveSum(scratch.p, tmp, rp + 1, rp + 1, m, ctx->stream));
+    ctx->scan_tmp.ensure(tmp);
+    INTI_CUDA(cub::DeviceScan::InclusiveSum(ctx->scan_tmp.p, tmp, rp + 1, rp + 1, m, ctx->stream));
     ctx->launches++;
   }
   int64_t nnz = 0;

@@ -66,13 +66,17 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   const int64_t tile = pair_tile(precision);
   op->n_tiles = std::max<int64_t>(1, (source->n + tile - 1) / tile);
   op->split = pair_plan_split(ctx, pde, kernel, dim, precision, target->n, source->n);
-  op->packed.ensure((size_t)op->n_tiles * tile * pair_record_bytes(pde, kernel, dim, precision));
-  op->partial.ensure((size_t)op->split * target->n * pair_partial_bytes(pde, precision));
   const int comps = pde == INTI_HELMHOLTZ ? 2 : 1;
   const int64_t big = std::max(target->n, source->n);
   op->xbuf.ensure(sizeof(double) * comps * big);
   op->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(op.get());
+  if (!op->symm) {
+    // the one-sided records and partials (the symmetric form packs its own
+    // records and keeps its partials in the context)
+    op->packed.ensure((size_t)op->n_tiles * tile * pair_record_bytes(pde, kernel, dim, precision));
+    op->partial.ensure((size_t)op->split * target->n * pair_partial_bytes(pde, precision));
+  }
   op_autotune(op.get(), false);
   op->small = ctx->single_launch && pair_small_eligible(precision, target->n, source->n);
   return op.release();
@@ -111,13 +115,15 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   const int64_t tile = pair_tile(precision);
   op->n_tiles = std::max<int64_t>(1, (source->n + tile - 1) / tile);
   op->split = pair_plan_split(ctx, pde, CF, 3, precision, target->n, source->n);
-  op->packed.ensure((size_t)op->n_tiles * tile * pair_record_bytes(pde, CF, 3, precision));
-  op->partial.ensure((size_t)op->split * target->n * pair_partial_bytes(pde, precision));
   const int comps = cplx ? 2 : 1;
   const int64_t big = std::max(target->n, source->n);
   op->xbuf.ensure(sizeof(double) * comps * big);
   op->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(op.get());
+  if (!op->symm) {
+    op->packed.ensure((size_t)op->n_tiles * tile * pair_record_bytes(pde, CF, 3, precision));
+    op->partial.ensure((size_t)op->split * target->n * pair_partial_bytes(pde, precision));
+  }
   op_autotune(op.get(), false);
   op->small = ctx->single_launch && pair_small_eligible(precision, target->n, source->n);
   return op.release();
@@ -143,13 +149,15 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
   const int64_t tile = pair_tile(precision);
   t->n_tiles = std::max<int64_t>(1, (op->source->n + tile - 1) / tile);
   t->split = pair_plan_split(op->ctx, op->pde, op->kind, op->dim, precision, op->target->n, op->source->n);
-  t->packed.ensure((size_t)t->n_tiles * tile * pair_record_bytes(op->pde, op->kind, op->dim, precision));
-  t->partial.ensure((size_t)t->split * op->target->n * pair_partial_bytes(op->pde, precision));
   const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
   const int64_t big = std::max(op->target->n, op->source->n);
   t->xbuf.ensure(sizeof(double) * comps * big);
   t->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(t.get());
+  if (!t->symm) {
+    t->packed.ensure((size_t)t->n_tiles * tile * pair_record_bytes(op->pde, op->kind, op->dim, precision));
+    t->partial.ensure((size_t)t->split * op->target->n * pair_partial_bytes(op->pde, precision));
+  }
   op_autotune(t.get(), false);
   return t.release();
 }
