@@ -268,31 +268,6 @@ inti_csr* csr_create_host(inti_ctx* ctx, int64_t m, int64_t n, int64_t nnz,
   return csr_from_host(ctx, m, n, nnz, rowptr, col, val, dtype);
 }
 
-// Host transpose of a CSR already on the device (for A^T applies).
-std::unique_ptr<inti_csr> csr_transpose(inti_ctx* ctx, const inti_csr* c) {
-  const int comps = c->dtype == INTI_C128 ? 2 : 1;
-  std::vector<int64_t> rp(c->m + 1);
-  std::vector<int32_t> col(c->nnz);
-  std::vector<double> val((size_t)c->nnz * comps);
-  d2h(ctx, rp.data(), c->rowptr.p, sizeof(int64_t) * (c->m + 1));
-  d2h(ctx, col.data(), c->col.p, sizeof(int32_t) * c->nnz);
-  d2h(ctx, val.data(), c->val.p, sizeof(double) * comps * c->nnz);
-  INTI_CUDA(cudaStreamSynchronize(ctx->stream));
-  std::vector<int64_t> trp(c->n + 1, 0);
-  for (int64_t p = 0; p < c->nnz; ++p) trp[col[p] + 1]++;
-  for (int64_t j = 0; j < c->n; ++j) trp[j + 1] += trp[j];
-  std::vector<int64_t> fill(trp.begin(), trp.end() - 1);
-  std::vector<int32_t> tcol(c->nnz);
-  std::vector<double> tval((size_t)c->nnz * comps);
-  for (int64_t i = 0; i < c->m; ++i)
-    for (int64_t p = rp[i]; p < rp[i + 1]; ++p) {
-      const int64_t q = fill[col[p]]++;
-      tcol[q] = (int32_t)i;
-      for (int k = 0; k < comps; ++k) tval[q * comps + k] = val[p * comps + k];
-    }
-  return std::unique_ptr<inti_csr>(
-      csr_from_host(ctx, c->n, c->m, c->nnz, trp.data(), tcol.data(), tval.data(), c->dtype));
-}
 
 }  // namespace inti
 

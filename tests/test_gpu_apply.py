@@ -141,6 +141,28 @@ def test_transpose_apply_off_surface_and_corrected(ctx, pde):
     assert relerr(got, alpha * (full.T @ g) + beta * y0) < 1e-12
 
 
+@pytest.mark.parametrize("pde", [O.LAPLACE, O.HELMHOLTZ])
+def test_transpose_of_rectangular_correction(ctx, pde):
+    """Off-surface targets with their DIM correction (a rectangular CSR, built
+    and transposed on the device) through the transposed apply."""
+    import scipy.sparse as sp
+
+    q = SURF["ellipsoid"]
+    tgt = inti.points(0.9 * q.coords[::3])
+    op = inti.Laplace(dim=3) if pde == O.LAPLACE else inti.Helmholtz(k=4.0, dim=3)
+    k = 0.0 if pde == O.LAPLACE else 4.0
+    cplx = pde == O.HELMHOLTZ
+    S, D = inti.single_double_layer(op=op, target=tgt, source=q, ctx=ctx,
+                                    correction={"method": "dim", "target_location": "inside"})
+    for A, kind, tn in ((D, O.DL, None), (S, O.SL, None)):
+        rp, col, val = A.correction.arrays()
+        full = O.assemble(pde, kind, k, tgt.coords, tn, q.coords, q.normals, q.weights) + \
+            sp.csr_matrix((val, col, rp), shape=A.shape).toarray()
+        g = density(len(tgt), cplx, 3)
+        assert relerr(A.rmatvec(g), full.T @ g) < 1e-12
+        assert np.array_equal(A.rmatvec(g), A.rmatvec(g))  # deterministic
+
+
 def test_launch_counter_advances(ctx):
     q = SURF["kite"]
     A = inti.IntegralOperator(inti.DoubleLayerKernel(inti.Laplace(dim=2)), q, ctx=ctx)
