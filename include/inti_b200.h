@@ -214,8 +214,8 @@ int inti_ctx_set_symmetric(inti_ctx* ctx, int enable);  /* default on */
 int inti_op_symmetric(const inti_op* op);
 int inti_ctx_set_partial_budget(inti_ctx* ctx, double bytes);
 int inti_op_panels(const inti_op* op);
-/* Small FP64 operators (at most 2^20 target-source pairs, e.g. the 1,000-node
- * kite) apply in a single-launch form: one kernel per product builds the
+/* Small FP64 operators (at most 2^20 target-source pairs and 65,536 sources,
+ * e.g. the 1,000-node kite) apply in a single-launch form: one kernel per product builds the
  * source records, forms the pair sums (a cluster of up to 8 CTAs per 32
  * targets, the CTAs and their warps splitting the sources, sums in a fixed
  * order), adds the correction rows and applies alpha/beta.  Transposed and

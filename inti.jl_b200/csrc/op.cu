@@ -344,10 +344,14 @@ void op_autotune(inti_op* op, bool measure) {
     INTI_CUDA(cudaEventCreate(&e1));
     float best = -1.0f;
     std::pair<int, int> pick(op->tpt, op->split);
+    int warmed = 0;
     for (auto& c : cand) {
       op_symm_configure(op, c.first, c.second);
       PairLaunch L = make_launch(op, op->xbuf.as<double>());
-      pair_launch(ctx, L);  // warm-up of this shape
+      if (c.first != warmed) {  // one warm-up per kernel (targets per thread); the others reuse it
+        pair_launch(ctx, L);
+        warmed = c.first;
+      }
       INTI_CUDA(cudaEventRecord(e0, ctx->stream));
       pair_launch(ctx, L);
       INTI_CUDA(cudaEventRecord(e1, ctx->stream));
@@ -397,12 +401,16 @@ void op_autotune(inti_op* op, bool measure) {
   cudaEvent_t e0, e1;
   INTI_CUDA(cudaEventCreate(&e0));
   INTI_CUDA(cudaEventCreate(&e1));
-  pair_launch(ctx, L);  // warm-up with the heuristic shape
   float best = -1.0f;
   std::pair<int, int> pick(op->tpt, op->split);
+  int warmed = 0;
   for (auto& c : cand) {
     L.tpt = c.first;
     L.split = c.second;
+    if (c.first != warmed) {  // one warm-up per kernel (targets per thread)
+      pair_launch(ctx, L);
+      warmed = c.first;
+    }
     INTI_CUDA(cudaEventRecord(e0, ctx->stream));
     pair_launch(ctx, L);
     INTI_CUDA(cudaEventRecord(e1, ctx->stream));

@@ -1945,7 +1945,8 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
 }
 
 bool pair_small_eligible(int precision, int64_t m, int64_t n) {
-  return precision == INTI_FP64 && (double)m * (double)n <= kSmallPairs && m > 0 && n > 0;
+  // sources capped so that a thread's chain (n / (8 slices * 8 warps)) stays short
+  return precision == INTI_FP64 && (double)m * (double)n <= kSmallPairs && m > 0 && n > 0 && n <= 65536;
 }
 
 static int pair_small_slices(int num_sms, int64_t m, int64_t n) {

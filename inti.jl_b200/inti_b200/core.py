@@ -121,7 +121,7 @@ class Context:
         self.check(self.lib.inti_ctx_set_symmetric(self.handle, int(bool(enable))))
 
     def set_single_launch(self, enable: bool) -> None:
-        """Apply small FP64 operators (at most 2^20 pairs) created afterwards
+        """Apply small FP64 operators (at most 2^20 pairs, 65,536 sources) created afterwards
         in the single-launch form (on by default; see ``GpuOperator.tuning``)."""
         self.check(self.lib.inti_ctx_set_single_launch(self.handle, int(bool(enable))))
 

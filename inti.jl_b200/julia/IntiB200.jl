@@ -312,7 +312,7 @@ panels(A::B200Map) = Int(ccall((:inti_op_panels, LIB), Cint, (Ptr{Cvoid},), A.h.
 """
     set_single_launch!(ctx, flag)
 
-Small FP64 operators (at most 2^20 pairs) created afterwards apply with one
+Small FP64 operators (at most 2^20 pairs, 65,536 sources) created afterwards apply with one
 kernel launch per product (`true`, the default) or with the tiled kernels;
 `single_launch(A)` reports the form of an operator.
 """

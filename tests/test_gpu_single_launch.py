@@ -121,3 +121,16 @@ def test_c1_kite_single_launch(ctx):
     assert ctx.launch_count - before == 1
     ref = oracle_apply(O.LAPLACE, O.DL, 0.0, q, q, sigma) + O.csr_apply(*D.correction.arrays(), sigma)
     assert relerr(y, ref) < 1e-12
+
+
+def test_single_launch_eligibility(ctx):
+    """FP64 only, at most 2^20 pairs and 65,536 sources."""
+    lap = inti.Laplace(dim=3)
+    small, many = _points(8, 3, 1), _points(70000, 3, 2)
+    assert inti.GpuOperator(inti.SingleLayerKernel(lap), small, _points(1024, 3, 3), None, "fp64", ctx).tuning[
+        "single_launch"]
+    assert not inti.GpuOperator(inti.SingleLayerKernel(lap), small, many, None, "fp64", ctx).tuning["single_launch"]
+    q = _points(1025, 3, 4)  # 1,050,625 pairs
+    assert not inti.GpuOperator(inti.SingleLayerKernel(lap), q, q, None, "fp64", ctx).tuning["single_launch"]
+    q = _points(300, 3, 5)
+    assert not inti.GpuOperator(inti.SingleLayerKernel(lap), q, q, None, "fp32c", ctx).tuning["single_launch"]
