@@ -686,6 +686,10 @@ static int apply_common(inti_op* op, const double* x, int64_t ldx, double* y, in
       const double* xd = xr;
       double* yd = yr;
       if (!on_device) {
+        // host staging, made on the first host-pointer apply
+        const size_t big = sizeof(double) * comps * std::max(op->target->n, op->source->n);
+        op->xbuf.ensure(big);
+        op->ybuf.ensure(big);
         h2d(ctx, op->xbuf.p, xr, sizeof(double) * comps * nin);
         if (!bz) h2d(ctx, op->ybuf.p, yr, sizeof(double) * comps * nout);
         xd = op->xbuf.as<double>();

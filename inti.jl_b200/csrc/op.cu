@@ -66,10 +66,6 @@ inti_op* op_create(inti_ctx* ctx, int pde, int kernel, double k_re, double k_im,
   const int64_t tile = pair_tile(precision);
   op->n_tiles = std::max<int64_t>(1, (source->n + tile - 1) / tile);
   op->split = pair_plan_split(ctx, pde, kernel, dim, precision, target->n, source->n);
-  const int comps = pde == INTI_HELMHOLTZ ? 2 : 1;
-  const int64_t big = std::max(target->n, source->n);
-  op->xbuf.ensure(sizeof(double) * comps * big);
-  op->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(op.get());
   if (!op->symm) {
     // the one-sided records and partials (the symmetric form packs its own
@@ -115,10 +111,6 @@ inti_op* op_create_combined(inti_ctx* ctx, int pde, double k_re, double k_im, co
   const int64_t tile = pair_tile(precision);
   op->n_tiles = std::max<int64_t>(1, (source->n + tile - 1) / tile);
   op->split = pair_plan_split(ctx, pde, CF, 3, precision, target->n, source->n);
-  const int comps = cplx ? 2 : 1;
-  const int64_t big = std::max(target->n, source->n);
-  op->xbuf.ensure(sizeof(double) * comps * big);
-  op->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(op.get());
   if (!op->symm) {
     op->packed.ensure((size_t)op->n_tiles * tile * pair_record_bytes(pde, CF, 3, precision));
@@ -149,10 +141,6 @@ inti_op* op_clone_precision(const inti_op* op, int precision) {
   const int64_t tile = pair_tile(precision);
   t->n_tiles = std::max<int64_t>(1, (op->source->n + tile - 1) / tile);
   t->split = pair_plan_split(op->ctx, op->pde, op->kind, op->dim, precision, op->target->n, op->source->n);
-  const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
-  const int64_t big = std::max(op->target->n, op->source->n);
-  t->xbuf.ensure(sizeof(double) * comps * big);
-  t->ybuf.ensure(sizeof(double) * comps * big);
   op_symm_init(t.get());
   if (!t->symm) {
     t->packed.ensure((size_t)t->n_tiles * tile * pair_record_bytes(op->pde, op->kind, op->dim, precision));
@@ -234,7 +222,8 @@ void op_symm_configure(inti_op* op, int tpt, int ch) {
   symm_layout(op->source->n, tpt, ch, pb, op->sym_budget, pcols, ch_eff);
   pair_symm_plan(op->source->n, tpt, ch_eff, pcols, tab, op->sym_panels, nb, nitems);
   INTI_CUDA(cudaStreamSynchronize(op->ctx->stream));  // no launch is reading the old table
-  op->sym_tab.ensure(sizeof(int32_t) * tab.size());
+  // half again as much room: a re-configuration (a tuned shape) then rarely reallocates
+  if (op->sym_tab.bytes < sizeof(int32_t) * tab.size()) op->sym_tab.ensure(sizeof(int32_t) * tab.size() * 3 / 2);
   INTI_CUDA(cudaMemcpy(op->sym_tab.p, tab.data(), sizeof(int32_t) * tab.size(), cudaMemcpyHostToDevice));
   op->sym_nb = nb;
   op->sym_nitems = nitems;
@@ -244,7 +233,8 @@ void op_symm_configure(inti_op* op, int tpt, int ch) {
   const bool panels = op->sym_panels.size() > 1;
   op->sym_zld = panels ? (int64_t)pcols * pair_symm_block(tpt) : npad;
   inti_ctx* ctx = op->ctx;
-  ctx->sym_ypart.ensure((size_t)pb * nitems * pair_symm_block(tpt));
+  const size_t yb = (size_t)pb * nitems * pair_symm_block(tpt);
+  if (ctx->sym_ypart.bytes < yb) ctx->sym_ypart.ensure(yb + yb / 4);
   ctx->sym_zpart.ensure((size_t)pb * nb * op->sym_zld);
   if (panels) ctx->sym_acc.ensure(sizeof(double) * (op->pde == INTI_HELMHOLTZ ? 2 : 1) * op->source->n);
   if (op->shard_n > 1) op_set_shard(op, op->shard_rank, op->shard_n);  // the items changed
@@ -338,6 +328,7 @@ void op_autotune(inti_op* op, bool measure) {
         if (std::find(cand.begin(), cand.end(), std::make_pair(tpt, ch)) == cand.end()) cand.emplace_back(tpt, ch);
     }
     const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
+    op->xbuf.ensure(sizeof(double) * comps * std::max(m, n));
     INTI_CUDA(cudaMemsetAsync(op->xbuf.p, 0, sizeof(double) * comps * n, ctx->stream));
     cudaEvent_t e0, e1;
     INTI_CUDA(cudaEventCreate(&e0));
@@ -396,6 +387,7 @@ void op_autotune(inti_op* op, bool measure) {
   op->partial.ensure((size_t)smax * m * pbytes);
   // the pair kernel's cost does not depend on the density: time it on zeros
   const int comps = op->pde == INTI_HELMHOLTZ ? 2 : 1;
+  op->xbuf.ensure(sizeof(double) * comps * std::max(m, n));
   INTI_CUDA(cudaMemsetAsync(op->xbuf.p, 0, sizeof(double) * comps * n, ctx->stream));
   PairLaunch L = make_launch(op, op->xbuf.as<double>());
   cudaEvent_t e0, e1;
