@@ -285,6 +285,16 @@ int inti_gmres(inti_ctx* ctx, int32_t nterms, inti_op* const* ops, const double*
                const double* shift, const double* b, double* x, double rtol,
                int32_t restart, int32_t maxiter, int32_t mode, int on_device,
                double* history, inti_gmres_stats* stats);
+/* Systems of at most max_unknowns unknowns (default 8192) run each Arnoldi
+ * step's orthogonalisation (both Gram-Schmidt passes), the new basis vector
+ * and the Givens update in one single-CTA kernel after the operator
+ * application, and the host checks the residual once per four steps (the
+ * steps enqueued after convergence leave the iterate alone; their operator
+ * applications still run and are counted); larger systems use the multi-CTA
+ * kernels and read the Hessenberg column back every step.  0 turns the
+ * small-system form off.  Both forms give the same iterates up to rounding.
+ * No counterpart in the reference (its examples call IterativeSolvers). */
+int inti_ctx_set_gmres_small(inti_ctx* ctx, int64_t max_unknowns);
 
 /* ---- adjoint: gradients of J(u), u = A sigma (Laplace, on-the-fly) ------ */
 /* Given the cotangent g = dJ/du (m values) and the density sigma (n values),

@@ -322,7 +322,7 @@ int inti_ctx_destroy(inti_ctx* ctx) {
     ctx->err_host = nullptr;
     for (inti::DevBuf* d : {&ctx->krylov.V, &ctx->krylov.w, &ctx->krylov.r, &ctx->krylov.e, &ctx->krylov.w_outer,
                             &ctx->krylov.partial, &ctx->krylov.h, &ctx->krylov.y, &ctx->krylov.nrm, &ctx->krylov.b,
-                            &ctx->krylov.x, &ctx->expi64, &ctx->expi32, &ctx->dimwork.d_xs, &ctx->dimwork.g0,
+                            &ctx->krylov.x, &ctx->krylov.small, &ctx->expi64, &ctx->expi32, &ctx->dimwork.d_xs, &ctx->dimwork.g0,
                             &ctx->dimwork.g1, &ctx->dimwork.theta, &ctx->dimwork.part, &ctx->dimwork.mu})
       d->release();
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -605,6 +605,14 @@ int inti_op_set_shard(inti_op* op, int rank, int nranks) {
 int inti_op_symmetric(const inti_op* op) {
   if (!op) return -INTI_E_ARG;
   return op->symm ? 1 : 0;
+}
+
+int inti_ctx_set_gmres_small(inti_ctx* ctx, int64_t max_unknowns) {
+  if (!ctx) return INTI_E_ARG;
+  return guarded(ctx, [&] {
+    require(max_unknowns >= 0, INTI_E_ARG, "max_unknowns must be >= 0");
+    ctx->krylov_small = max_unknowns;
+  });
 }
 
 int inti_ctx_set_single_launch(inti_ctx* ctx, int enable) {

@@ -100,6 +100,10 @@ struct inti_ctx {
   // FP64 operators of at most kSmallPairs pairs created while this is set
   // apply in the single-launch form (inti_ctx_set_single_launch)
   bool single_launch = true;
+  // GMRES on systems of at most this many unknowns runs each Arnoldi step's
+  // orthogonalisation and Givens update in one single-CTA kernel
+  // (inti_ctx_set_gmres_small; 0 turns it off)
+  int64_t krylov_small = 8192;
   // Row partials, column partials and panel running sums of the symmetric
   // form, shared by all of the context's symmetric operators: they are live
   // only from an apply's pair launch to its epilogue, and every launch of a
@@ -110,7 +114,7 @@ struct inti_ctx {
   // GMRES workspace kept between solves: Krylov basis, work vectors, the
   // reduction scratch and the staged right-hand side / solution.
   struct {
-    inti::DevBuf V, w, r, e, w_outer, partial, h, y, nrm, b, x;
+    inti::DevBuf V, w, r, e, w_outer, partial, h, y, nrm, b, x, small;
   } krylov;
   // DIM construction workspace kept between constructions: source points,
   // traces, Theta, its partial sums, green multipliers.

@@ -15,7 +15,12 @@
 // Orthogonalisation is classical Gram-Schmidt applied twice (CGS2): two
 // fused multi-dot / update kernel pairs per step, deterministic block
 // reductions.  The small Hessenberg least-squares problem (Givens rotations)
-// runs on the host from one device->host copy per step.
+// runs on the host from one device->host copy per step.  Small systems
+// (n <= 8192 unknowns by default) take a whole step after the operator application in
+// one single-CTA kernel (both CGS passes, the norm, the new basis vector and
+// the Givens update on the device) and the host looks at the residuals once
+// per kArnoldiBatch steps, so a step costs two or three launches and no
+// round trip.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -146,6 +151,144 @@ __global__ void axpby(int64_t n, double ar, double ai, const double* x, double b
   }
 }
 
+constexpr int kArnoldiThreads = 1024;
+constexpr int kArnoldiBatch = 4;
+
+// Device state of a small-system Arnoldi cycle: the rotated Hessenberg
+// matrix R ((restart+1) x restart, column-major), the Givens rotations, the
+// rotated right-hand side g, the residual estimate after each step and
+// flags[0] = stop (converged or breakdown), flags[1] = steps done.
+struct ArnoldiState {
+  double2 *R, *cs, *sn, *g;
+  double* res;
+  int* flags;
+};
+
+__device__ __forceinline__ double2 c_add(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 c_conj(double2 a) { return make_double2(a.x, -a.y); }
+
+template <bool C>
+__device__ __forceinline__ double2 load_c(const double* v, int64_t i) {
+  return C ? reinterpret_cast<const double2*>(v)[i] : make_double2(v[i], 0.0);
+}
+
+// Step j of a small-system cycle, after w = L v_j: w is orthogonalised
+// against v_0..v_j twice (CGS2; sums in a fixed order), v_{j+1} = w/|w|,
+// and thread 0 applies the earlier rotations to the new Hessenberg column,
+// forms rotation j, and records |g[j+1]|.  A stopped cycle leaves later
+// steps as no-ops.  Dynamic shared memory: 2 * (restart + 1) double2.
+template <bool C>
+__global__ void __launch_bounds__(kArnoldiThreads) arnoldi_small_step(int64_t n, int j, int restart, double* V,
+                                                                      double* w, double tol_abs, ArnoldiState st) {
+  extern __shared__ double2 hbuf[];
+  __shared__ double2 red[kArnoldiThreads / 32][8];
+  __shared__ double hn_s;
+  if (st.flags[0]) return;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int comps = C ? 2 : 1;
+  double2* hsum = hbuf;               // [restart + 1]
+  double2* hp = hbuf + restart + 1;   // [restart + 1]
+  for (int k = tid; k <= j; k += kArnoldiThreads) hsum[k] = make_double2(0.0, 0.0);
+  for (int pass = 0; pass < 2; ++pass) {
+    for (int k0 = 0; k0 <= j; k0 += 8) {
+      double2 acc[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) acc[u] = make_double2(0.0, 0.0);
+      for (int64_t i = tid; i < n; i += kArnoldiThreads) {
+        const double2 wi = load_c<C>(w, i);
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+          if (k0 + u <= j) acc[u] = c_add(acc[u], cjm(load_c<C>(V + (int64_t)comps * n * (k0 + u), i), wi));
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        acc[u].x = warp_sum(acc[u].x);
+        acc[u].y = warp_sum(acc[u].y);
+      }
+      if (lane == 0)
+#pragma unroll
+        for (int u = 0; u < 8; ++u) red[warp][u] = acc[u];
+      __syncthreads();
+      if (tid < 8 && k0 + tid <= j) {
+        double2 t = make_double2(0.0, 0.0);
+        for (int q = 0; q < kArnoldiThreads / 32; ++q) t = c_add(t, red[q][tid]);
+        hp[k0 + tid] = t;
+      }
+      __syncthreads();
+    }
+    // w -= V hp (each thread updates the entries it reads)
+    for (int64_t i = tid; i < n; i += kArnoldiThreads) {
+      double2 a = load_c<C>(w, i);
+      for (int k = 0; k <= j; ++k) {
+        const double2 p = cm(load_c<C>(V + (int64_t)comps * n * k, i), hp[k]);
+        a.x -= p.x;
+        a.y -= p.y;
+      }
+      if (C)
+        reinterpret_cast<double2*>(w)[i] = a;
+      else
+        w[i] = a.x;
+    }
+    for (int k = tid; k <= j; k += kArnoldiThreads) hsum[k] = c_add(hsum[k], hp[k]);
+    __syncthreads();
+  }
+  double s2 = 0.0;
+  for (int64_t i = tid; i < n; i += kArnoldiThreads) {
+    const double2 a = load_c<C>(w, i);
+    s2 = fma(a.x, a.x, fma(a.y, a.y, s2));
+  }
+  s2 = warp_sum(s2);
+  if (lane == 0) red[warp][0].x = s2;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int q = 0; q < kArnoldiThreads / 32; ++q) t += red[q][0].x;
+    hn_s = sqrt(fmax(t, 0.0));
+  }
+  __syncthreads();
+  const double hn = hn_s;
+  if (hn > 0.0) {
+    double* vn = V + (int64_t)comps * n * (j + 1);
+    const double inv = 1.0 / hn;
+    for (int64_t i = tid; i < n; i += kArnoldiThreads) {
+      if (C) {
+        const double2 a = reinterpret_cast<const double2*>(w)[i];
+        reinterpret_cast<double2*>(vn)[i] = make_double2(a.x * inv, a.y * inv);
+      } else {
+        vn[i] = w[i] * inv;
+      }
+    }
+  }
+  if (tid == 0) {
+    double2* col = hsum;  // column j of H, then rotated in place (row j + 1 = hn)
+    col[j + 1] = make_double2(hn, 0.0);
+    for (int i = 0; i < j; ++i) {
+      const double2 a = col[i], b = col[i + 1], c = st.cs[i], sg = st.sn[i];
+      col[i] = c_add(cm(c_conj(c), a), cm(c_conj(sg), b));
+      const double2 t1 = cm(sg, a), t2 = cm(c, b);
+      col[i + 1] = make_double2(t2.x - t1.x, t2.y - t1.y);
+    }
+    const double2 a = col[j], b = col[j + 1];
+    const double den = sqrt(a.x * a.x + a.y * a.y + b.x * b.x + b.y * b.y);
+    const double2 cj = den == 0.0 ? make_double2(1.0, 0.0) : make_double2(a.x / den, a.y / den);
+    const double2 sj = den == 0.0 ? make_double2(0.0, 0.0) : make_double2(b.x / den, b.y / den);
+    st.cs[j] = cj;
+    st.sn[j] = sj;
+    col[j] = make_double2(den, 0.0);
+    const double2 gj = st.g[j];
+    const double2 ng = cm(sj, gj);
+    st.g[j + 1] = make_double2(-ng.x, -ng.y);
+    st.g[j] = cm(c_conj(cj), gj);
+    double2* Rj = st.R + (int64_t)(restart + 1) * j;
+    for (int i = 0; i <= j; ++i) Rj[i] = col[i];
+    const double2 gn = st.g[j + 1];
+    const double res = sqrt(gn.x * gn.x + gn.y * gn.y);
+    st.res[j] = res;
+    st.flags[1] = j + 1;
+    if (res <= tol_abs || hn == 0.0) st.flags[0] = 1;
+  }
+}
+
 struct Solver {
   inti_ctx* ctx;
   int64_t n;
@@ -210,6 +353,72 @@ struct Solver {
     return std::sqrt(std::max(v.x, 0.0));
   }
 
+  bool small_cycle(int restart) const { return n <= ctx->krylov_small && restart <= 1000; }
+
+  // One Arnoldi cycle of a small system with v_0 = V[0] normalised and
+  // g = (beta, 0, ...): steps of one operator application and one
+  // arnoldi_small_step each, kArnoldiBatch at a time between host checks.
+  // Fills H (rows 0..j-1 of the rotated Hessenberg matrix, row-major with
+  // `restart` columns) and g[0..j], and returns the steps j kept; steps
+  // enqueued after the cycle stopped are no-ops.
+  int arnoldi_cycle_small(bool fp32, double* V, double* w, double beta, double tol_abs, int restart, int maxit,
+                          int& it, double& res, bool& done, double* history, double bnorm_for_history,
+                          int hist_offset, std::vector<cplx>& H, std::vector<cplx>& g) {
+    const size_t nR = (size_t)(restart + 1) * restart;
+    const size_t bytes = sizeof(double2) * (nR + 2 * (size_t)restart + (restart + 1)) + sizeof(double) * restart +
+                         2 * sizeof(int);
+    DevBuf& sb = ctx->krylov.small;
+    sb.ensure(bytes);
+    ArnoldiState st;
+    st.R = sb.as<double2>();
+    st.cs = st.R + nR;
+    st.sn = st.cs + restart;
+    st.g = st.sn + restart;
+    st.res = reinterpret_cast<double*>(st.g + restart + 1);
+    st.flags = reinterpret_cast<int*>(st.res + restart);
+    INTI_CUDA(cudaMemsetAsync(st.g, 0, sizeof(double2) * (restart + 1), ctx->stream));
+    INTI_CUDA(cudaMemsetAsync(st.flags, 0, 2 * sizeof(int), ctx->stream));
+    const double2 g0 = make_double2(beta, 0.0);
+    INTI_CUDA(cudaMemcpyAsync(st.g, &g0, sizeof(double2), cudaMemcpyHostToDevice, ctx->stream));
+    const size_t smem = sizeof(double2) * 2 * (restart + 1);
+    std::vector<double> rh(restart);
+    int flags[2] = {0, 0};
+    int j = 0;
+    while (j < restart && it < maxit && !done) {
+      const int batch = std::min({kArnoldiBatch, restart - j, maxit - it});
+      for (int b = 0; b < batch; ++b) {
+        apply(fp32, V + (size_t)comps * n * (j + b), w);
+        if (C)
+          arnoldi_small_step<true><<<1, kArnoldiThreads, smem, ctx->stream>>>(n, j + b, restart, V, w, tol_abs, st);
+        else
+          arnoldi_small_step<false><<<1, kArnoldiThreads, smem, ctx->stream>>>(n, j + b, restart, V, w, tol_abs, st);
+        ctx->launches++;
+      }
+      INTI_CUDA(cudaMemcpyAsync(rh.data() + j, st.res + j, sizeof(double) * batch, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+      INTI_CUDA(cudaMemcpyAsync(flags, st.flags, 2 * sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+      INTI_CUDA(cudaStreamSynchronize(ctx->stream));
+      const int now = flags[1];  // steps done in this cycle
+      for (; j < now; ++j) {
+        ++it;
+        res = rh[j];
+        if (history) history[hist_offset + it] = res / bnorm_for_history;
+      }
+      if (flags[0]) done = true;
+    }
+    if (j > 0) {
+      std::vector<double2> Rh((size_t)(restart + 1) * j), gh(j + 1);
+      INTI_CUDA(cudaMemcpyAsync(Rh.data(), st.R, sizeof(double2) * Rh.size(), cudaMemcpyDeviceToHost, ctx->stream));
+      INTI_CUDA(cudaMemcpyAsync(gh.data(), st.g, sizeof(double2) * (j + 1), cudaMemcpyDeviceToHost, ctx->stream));
+      INTI_CUDA(cudaStreamSynchronize(ctx->stream));
+      for (int c = 0; c < j; ++c)
+        for (int r = 0; r <= c; ++r)
+          H[(size_t)r * restart + c] = cplx(Rh[(size_t)(restart + 1) * c + r].x, Rh[(size_t)(restart + 1) * c + r].y);
+      for (int r = 0; r <= j; ++r) g[r] = cplx(gh[r].x, gh[r].y);
+    }
+    return j;
+  }
+
   // GMRES(restart) on L (fp32 selects the operators) for L e = rhs, e0 = x.
   // Stops at ||rhs - L x|| <= tol_abs (estimated by the Arnoldi recurrence)
   // or after maxit steps.  Returns the steps used; est receives the final
@@ -247,7 +456,11 @@ struct Solver {
       g[0] = beta;
       int j = 0;
       bool done = false;
-      for (; j < restart && it < maxit; ++j) {
+      if (small_cycle(restart)) {
+        j = arnoldi_cycle_small(fp32, V, w, beta, tol_abs, restart, maxit, it, res, done, history,
+                                bnorm_for_history, hist_offset, H, g);
+      }
+      for (; !small_cycle(restart) && j < restart && it < maxit; ++j) {
         double* vj = V + (size_t)comps * n * j;
         apply(fp32, vj, w);
         // CGS2

@@ -130,6 +130,7 @@ SIGNATURES = {
     "inti_ctx_set_partial_budget": (C.c_int, [P, C.c_double]),
     "inti_op_panels": (C.c_int, [P]),
     "inti_ctx_set_single_launch": (C.c_int, [P, C.c_int]),
+    "inti_ctx_set_gmres_small": (C.c_int, [P, I64]),
     "inti_op_single_launch": (C.c_int, [P]),
     "inti_op_set_shard": (C.c_int, [P, C.c_int, C.c_int]),
     "inti_selftest_math": (C.c_int, [P, D]),

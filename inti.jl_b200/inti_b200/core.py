@@ -125,6 +125,12 @@ class Context:
         in the single-launch form (on by default; see ``GpuOperator.tuning``)."""
         self.check(self.lib.inti_ctx_set_single_launch(self.handle, int(bool(enable))))
 
+    def set_gmres_small(self, max_unknowns: int) -> None:
+        """GMRES on systems of at most ``max_unknowns`` unknowns (default
+        8192) runs each Arnoldi step in one single-CTA kernel with a host
+        check every four steps; 0 turns that form off."""
+        self.check(self.lib.inti_ctx_set_gmres_small(self.handle, int(max_unknowns)))
+
     def set_partial_budget(self, nbytes: float) -> None:
         """Bytes of partial sums a symmetric operator created afterwards may
         hold before its work is split into panels run one after another

@@ -321,6 +321,16 @@ set_single_launch!(ctx::Context, flag::Bool) =
 single_launch(A::B200Map) = ccall((:inti_op_single_launch, LIB), Cint, (Ptr{Cvoid},), A.h.ptr) == 1
 
 """
+    set_gmres_small!(ctx, max_unknowns)
+
+GMRES on systems of at most `max_unknowns` unknowns (default 8192) runs each
+Arnoldi step in one single-CTA kernel and checks the residual every four
+steps; `0` turns that form off.
+"""
+set_gmres_small!(ctx::Context, max_unknowns::Integer) =
+    check(ccall((:inti_ctx_set_gmres_small, LIB), Cint, (Ptr{Cvoid}, Int64), ctx.ptr, max_unknowns), ctx.ptr)
+
+"""
     set_shard!(A::B200Map, rank, nranks)
 
 One process per GPU: `A` computes only rank `rank`'s share of the node pairs

@@ -96,3 +96,29 @@ def test_gmres_repeated_solves_reuse_derived_operators(ctx):
     Lx = 0.5 * x4 + D @ x4 - 1j * k * (S2 @ x4)
     assert st4["converged"] == 1 and np.linalg.norm(b - Lx) / np.linalg.norm(b) < 2e-10
     assert not np.allclose(x3, x4)
+
+
+@pytest.mark.parametrize("mode", ["fp64", "mixed"])
+def test_gmres_small_form_matches_multi_kernel_form(ctx, mode):
+    """The single-CTA Arnoldi step (systems of at most 8192 unknowns) and the
+    multi-CTA kernels with a host Givens update give the same iterates up to
+    rounding, real and complex, across restarts."""
+    q, S, D = laplace_problem(ctx)
+    qh = inti.p2_sphere_quadrature(3)
+    Sh, Dh = inti.single_double_layer(op=inti.Helmholtz(k=2.0, dim=3), target=qh, source=qh,
+                                      correction={"method": "dim"}, ctx=ctx)
+    cases = [(D - 0.5 * inti.I, density(len(q), False, 13)), (0.5 * inti.I + Dh - 2j * Sh, density(len(qh), True, 14))]
+    for L, b in cases:
+        for restart in (4, 50):
+            out = []
+            for small in (8192, 0):
+                ctx.set_gmres_small(small)
+                try:
+                    out.append(inti.gmres(L, b, rtol=1e-10, restart=restart, maxiter=400, mode=mode, history=True))
+                finally:
+                    ctx.set_gmres_small(8192)
+            (x1, st1), (x0, st0) = out
+            assert st1["converged"] == 1 and st0["converged"] == 1
+            assert abs(st1["iterations"] - st0["iterations"]) <= 1, (st1, st0)
+            assert relerr(x1, x0) < 1e-8
+            assert st1["relres"] <= 1e-10
