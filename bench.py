@@ -345,6 +345,40 @@ def gmres_c2_cfie(ctx) -> dict:
     return out
 
 
+def gmres_c1(ctx, S_unused, D, q, cpu: bool) -> dict:
+    """The interior Dirichlet problem of the C1 kite, (-I/2 + D) sigma = g with
+    g the trace of a point source outside (docs/src/examples/poisson.jl:160-168),
+    FP64 GMRES to 1e-10 on the GPU (the small-system Arnoldi form), first solve
+    and repeat; beside it the oracle's FP64 GMRES (C++ on-the-fly row sums on
+    all host cores) on the same system."""
+    import inti_b200 as inti
+
+    xs = np.array([3.0, 2.0])
+    b = -np.log(np.linalg.norm(q.coords - xs, axis=1)) / (2 * np.pi)
+    L = D - 0.5 * inti.I
+    _, st = inti.gmres(L, b, rtol=1e-10, restart=100, maxiter=500)
+    reps = [inti.gmres(L, b, rtol=1e-10, restart=100, maxiter=500)[1]["seconds"] for _ in range(5)]
+    out = {"workload": "laplace2d_interior_dirichlet(-0.5I+D)_kite_N1000_dim", "rtol": 1e-10,
+           "fp64": {"seconds": st["seconds"], "seconds_repeat": statistics.median(reps),
+                    "iterations": st["iterations"], "fp64_applies": st["fp64_applies"], "relres_fp64": st["relres"],
+                    "converged": bool(st["converged"])},
+           "timing": "wall time of the whole solve call (b up, x back); repeat = median of 5"}
+    if cpu:
+        sys.path.insert(0, str(ROOT / "oracle"))
+        import oracle as O
+
+        nt = host_cores()
+        dD = D.correction.arrays()
+        O.gmres(O.LAPLACE, 0.0, q.coords, q.normals, q.weights, -0.5, [(O.DL, 1.0, dD)], b, rtol=1e-10,
+                restart=100, maxiter=500, nthreads=nt)
+        t0 = time.perf_counter()
+        _, sto = O.gmres(O.LAPLACE, 0.0, q.coords, q.normals, q.weights, -0.5, [(O.DL, 1.0, dD)], b, rtol=1e-10,
+                         restart=100, maxiter=500, nthreads=nt)
+        out["cpu_fp64"] = {"seconds": time.perf_counter() - t0, "iterations": sto["iterations"], "cores": nt,
+                           "kind": "port", "sample": "the whole solve (C++ FP64 restatement, on-the-fly row sums)"}
+    return out
+
+
 def gmres_c3(ctx, cpu_seconds: float | None = None) -> dict:
     """Combined-field Laplace solve on the ellipsoid (N = 200,934).  With
     cpu_seconds, also the CPU estimate of the same FP64 solve: the oracle's
@@ -1010,6 +1044,8 @@ def main() -> None:
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_sample(q, S, sigma, args.cpu_seconds, host_cores())
+    if not args.no_gmres and world == 1 and args.workload == "c1":
+        line["gmres"] = gmres_c1(ctx, None, S, q, not args.no_cpu)
     if not args.no_gmres and world == 1 and args.workload == "c2":
         line["gmres"] = gmres_c3(ctx, None if args.no_cpu else min(args.cpu_seconds, 10.0))
         line["gmres_helmholtz"] = gmres_c2_cfie(ctx)
