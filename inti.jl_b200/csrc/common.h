@@ -34,16 +34,27 @@ struct Error : std::runtime_error {
       throw ::inti::Error(INTI_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
+// Device blocks are taken from, and given back to, a per-device cache of
+// released blocks (devmem.cu): creating and destroying operators then rarely
+// goes back to the driver, whose allocation latency on a busy host ranges
+// from microseconds to tens of milliseconds.  Giving a block back waits for
+// its device to be idle, as cudaFree does, so a block handed out again is
+// never still in use.
+void* dev_alloc(size_t nbytes, int* device, size_t* got);  // throws Error(INTI_E_NOMEM)
+void dev_release(void* p, size_t bytes, int device);
+size_t dev_cache_bytes(int device);  // bytes held free in the cache
+
 // Device allocation owned by a handle.
 struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
+  int device = 0;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (p) cudaFree(p);
+    if (p) dev_release(p, bytes, device);
     p = nullptr;
     bytes = 0;
   }
@@ -51,13 +62,7 @@ struct DevBuf {
     if (nbytes <= bytes && p) return;
     release();
     if (nbytes == 0) nbytes = 16;
-    cudaError_t e = cudaMalloc(&p, nbytes);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      throw Error(INTI_E_NOMEM, std::string("cudaMalloc(") + std::to_string(nbytes) +
-                                    "): " + cudaGetErrorString(e));
-    }
-    bytes = nbytes;
+    p = dev_alloc(nbytes, &device, &bytes);
   }
   template <class T>
   T* as() const {
