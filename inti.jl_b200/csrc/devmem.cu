@@ -19,7 +19,7 @@
 namespace inti {
 namespace {
 
-constexpr size_t kCacheCap = (size_t)16 << 30;
+constexpr size_t kCacheCap = (size_t)8 << 30;
 constexpr size_t kSlack = (size_t)2 << 20;
 
 struct DeviceCache {

@@ -202,3 +202,28 @@ def test_combined_field_operator(ctx, prec, tol):
         ref = cD * (oracle_apply(pde, O.DL, k, q, q, x) + O.csr_apply(*dD, x)) + \
             cS * (oracle_apply(pde, O.SL, k, q, q, x) + O.csr_apply(*dS, x))
         assert relerr(C @ x, ref) < tol, (op, prec)
+
+
+def test_released_device_blocks_are_reused(ctx):
+    """Operators created and destroyed again and again take their device
+    blocks from the cache of released blocks: device memory in use stays
+    flat after the first round."""
+    import gc
+
+    import torch
+
+    q = inti.ellipsoid_quadrature(12, 5)  # 7,776 nodes
+    op = inti.Helmholtz(k=3.0, dim=3)
+    x = density(len(q), True, 3)
+    used = []
+    for _ in range(4):
+        S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+        CF = inti.CombinedFieldOperator(D, S, 1.0, -3.0j)
+        y = CF @ x
+        del S, D, CF
+        gc.collect()
+        ctx.synchronize()
+        free, total = torch.cuda.mem_get_info()
+        used.append(total - free)
+    assert max(used[1:]) - min(used[1:]) < (64 << 20), used
+    assert np.all(np.isfinite(y))
