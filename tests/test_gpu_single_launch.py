@@ -134,3 +134,27 @@ def test_single_launch_eligibility(ctx):
     assert not inti.GpuOperator(inti.SingleLayerKernel(lap), q, q, None, "fp64", ctx).tuning["single_launch"]
     q = _points(300, 3, 5)
     assert not inti.GpuOperator(inti.SingleLayerKernel(lap), q, q, None, "fp32c", ctx).tuning["single_launch"]
+
+
+@pytest.mark.parametrize("case", ["laplace2d", "laplace3d", "helmholtz3d"])
+def test_single_launch_derivative_kernels_with_correction(ctx, tiled, case):
+    """ADL and HS with their derivative DIM corrections, complex alpha/beta on
+    the Helmholtz kernels: the single-launch form against the tiled kernels
+    with the same correction arrays."""
+    if case == "laplace2d":
+        q, op, cplx = inti.kite_quadrature(120, 9), inti.Laplace(dim=2), False  # 600 nodes
+    elif case == "laplace3d":
+        q, op, cplx = inti.ellipsoid_quadrature(3, 5), inti.Laplace(dim=3), False  # 486 nodes
+    else:
+        q, op, cplx = inti.p2_sphere_quadrature(4), inti.Helmholtz(k=3.0, dim=3), True  # 768 nodes
+    K, H = inti.adj_double_layer_hypersingular(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    x, y0 = density(len(q), cplx, 21), density(len(q), cplx, 22)
+    alpha, beta = (0.5 - 0.25j, 1.5 + 0.5j) if cplx else (0.5, 1.5)
+    for A, K_ in ((K, inti.AdjointDoubleLayerKernel), (H, inti.HyperSingularKernel)):
+        assert A.tuning["single_launch"]
+        rp, col, val = A.correction.arrays()
+        ct = inti.CorrectionMatrix.from_csr(rp, col, val, A.shape, ctx=tiled)
+        B = inti.GpuOperator(K_(op), q, q, ct, "fp64", tiled)
+        got = A.mul(y0.copy(), x, alpha=alpha, beta=beta)
+        assert relerr(got, B.mul(y0.copy(), x, alpha=alpha, beta=beta)) < 1e-12, K_
+        assert np.array_equal(got, A.mul(y0.copy(), x, alpha=alpha, beta=beta))
