@@ -386,6 +386,12 @@ int inti_apply_noalloc(int pde, int kernel, int dim, double k, int precision, in
  * FP64 x^{-3/2} over [1e-27, 1e27]; out[5] max relative error of the FP64
  * reciprocal over [1e-27, 1e27].  out holds 6 doubles. */
 int inti_selftest_math(inti_ctx* ctx, double* out);
+/* Runs the device-side bounded wait of the pair kernels on an mbarrier that
+ * nothing arrives at: the wait gives up after its poll limit, records the
+ * timeout in the context's flag and the kernel returns, so this returns
+ * INTI_E_TIMEOUT and the context stays usable (the flag is cleared).  For
+ * tests of the timeout path; no counterpart in the reference. */
+int inti_selftest_wait_timeout(inti_ctx* ctx);
 
 #ifdef __cplusplus
 }

@@ -864,6 +864,11 @@ int inti_selftest_math(inti_ctx* ctx, double* out) {
   return guarded(ctx, [&] { selftest_math(ctx, out); });
 }
 
+int inti_selftest_wait_timeout(inti_ctx* ctx) {
+  if (!ctx) return INTI_E_ARG;
+  return guarded(ctx, [&] { selftest_wait_timeout(ctx); });
+}
+
 int inti_measure_peaks(inti_ctx* ctx, double* fp64_flops, double* fp32_flops, double* mufu_ops) {
   if (!ctx || !fp64_flops || !fp32_flops || !mufu_ops) return INTI_E_ARG;
   return guarded(ctx, [&] { measure_peaks(ctx, fp64_flops, fp32_flops, mufu_ops); });

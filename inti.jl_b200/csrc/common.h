@@ -34,15 +34,15 @@ struct Error : std::runtime_error {
       throw ::inti::Error(INTI_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(_e)); \
   } while (0)
 
-// Device blocks are taken from, and given back to, a per-device cache of
-// released blocks (devmem.cu): creating and destroying operators then rarely
-// goes back to the driver, whose allocation latency on a busy host ranges
-// from microseconds to tens of milliseconds.  Giving a block back waits for
-// its device to be idle, as cudaFree does, so a block handed out again is
-// never still in use.
+// Device blocks are taken from, and given back to, a per-device CUDA memory
+// pool that keeps released memory (devmem.cu): creating and destroying
+// operators then rarely goes back to the driver, whose allocation latency on
+// a busy host ranges from microseconds to tens of milliseconds.  Giving a
+// block back waits for its device to be idle, as cudaFree does, so memory
+// handed out again is never still in use.
 void* dev_alloc(size_t nbytes, int* device, size_t* got);  // throws Error(INTI_E_NOMEM)
 void dev_release(void* p, size_t bytes, int device);
-size_t dev_cache_bytes(int device);  // bytes held free in the cache
+size_t dev_cache_bytes(int device);  // bytes the pool holds free
 
 // Device allocation owned by a handle.
 struct DevBuf {

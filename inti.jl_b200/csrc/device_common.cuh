@@ -132,9 +132,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Upper bound on polls of one barrier phase (each poll may suspend the
-// thread for a hardware-chosen interval); far beyond any healthy copy.
-constexpr uint32_t kWaitLimit = 1u << 22;
+// Upper bound on polls of one barrier phase.  Each poll that finds the phase
+// incomplete may suspend the thread for a hardware-chosen interval (about
+// 4 us on the B200: 2^22 polls took 16.6 s), so 2^18 polls give up after
+// about a second, far beyond any healthy copy or MMA.
+constexpr uint32_t kWaitLimit = 1u << 18;
 
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity) {
   for (uint32_t it = 0; it < kWaitLimit; ++it)

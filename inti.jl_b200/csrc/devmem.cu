@@ -1,40 +1,52 @@
-// Cache of released device blocks behind DevBuf (declared in common.h).
+// Device memory behind DevBuf (declared in common.h).
 //
-// A released block is kept, per device and by size, and handed out again for
-// a request it covers without too much waste (at most twice the request, or
-// 2 MiB more).  Releasing waits for the device to be idle (what cudaFree
-// does), so a reused block has no work in flight.  An allocation that fails
-// empties the device's cache and tries once more.  At most kCacheCap bytes
-// per device are kept; beyond that a released block goes back to the driver.
-// The cache is never torn down: the process's exit returns the memory.
+// Blocks under kPoolMax bytes come from a per-device CUDA memory pool that
+// keeps released memory and sub-allocates from what it holds; the pool
+// reserves kPoolReserve bytes when it is created.  Creating and destroying
+// operators then rarely goes back to the driver, whose latency for a first
+// allocation of a few megabytes ranges from microseconds to tens of
+// milliseconds on a busy host.  Larger blocks (the symmetric form's partial
+// pools, Krylov bases, DIM work arrays: made once per context or solve) go
+// to cudaMalloc, which maps them in well under a millisecond, where growing
+// the pool by a gigabyte took 0.4 s.
+//
+// Pool allocations are made on a private stream of the pool and waited for,
+// so a block is ready for every stream when dev_alloc returns.  Releasing
+// first waits for the device to be idle (what cudaFree does), so memory
+// handed out again has no work in flight.  Above kCacheCap bytes of released
+// memory the pool returns the excess to the driver at its next
+// synchronisation.  An allocation that fails trims the pool to nothing and
+// tries once more.  The pools are never torn down: the process's exit
+// returns the memory.
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <map>
 #include <mutex>
 #include <string>
-#include <vector>
 
 #include "common.h"
 
 namespace inti {
 namespace {
 
-constexpr size_t kCacheCap = (size_t)8 << 30;
-constexpr size_t kSlack = (size_t)2 << 20;
+constexpr uint64_t kCacheCap = (uint64_t)8 << 30;
+constexpr size_t kPoolMax = (size_t)64 << 20;
+constexpr size_t kPoolReserve = (size_t)256 << 20;
 
-struct DeviceCache {
-  std::multimap<size_t, void*> free;  // size -> block
-  size_t bytes = 0;
+struct DevicePool {
+  cudaMemPool_t pool = nullptr;
+  cudaStream_t stream = nullptr;
 };
 
-struct Cache {
+struct Pools {
   std::mutex mu;
-  std::map<int, DeviceCache> dev;
+  std::map<int, DevicePool> dev;
 };
 
-Cache& cache() {
-  static Cache* c = new Cache();  // never destroyed: freeing at process exit is the driver's job
-  return *c;
+Pools& pools() {
+  static Pools* p = new Pools();  // never destroyed: freeing at process exit is the driver's job
+  return *p;
 }
 
 struct SetDevice {
@@ -50,70 +62,98 @@ struct SetDevice {
   }
 };
 
+// The pool of device d (created on first use, with d current).
+DevicePool& pool_for(int d) {
+  Pools& ps = pools();
+  std::lock_guard<std::mutex> lk(ps.mu);
+  DevicePool& p = ps.dev[d];
+  if (!p.pool) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = d;
+    INTI_CUDA(cudaMemPoolCreate(&p.pool, &props));
+    uint64_t threshold = kCacheCap;
+    INTI_CUDA(cudaMemPoolSetAttribute(p.pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    INTI_CUDA(cudaStreamCreateWithFlags(&p.stream, cudaStreamNonBlocking));
+    void* warm = nullptr;  // reserve kPoolReserve bytes now, kept by the release threshold
+    if (cudaMallocFromPoolAsync(&warm, kPoolReserve, p.pool, p.stream) == cudaSuccess) {
+      cudaFreeAsync(warm, p.stream);
+      cudaStreamSynchronize(p.stream);
+    } else {
+      cudaGetLastError();
+    }
+  }
+  return p;
+}
+
 }  // namespace
 
 void* dev_alloc(size_t nbytes, int* device, size_t* got) {
   int d = 0;
   INTI_CUDA(cudaGetDevice(&d));
   *device = d;
-  Cache& c = cache();
-  {
-    std::lock_guard<std::mutex> lk(c.mu);
-    DeviceCache& dc = c.dev[d];
-    auto it = dc.free.lower_bound(nbytes);
-    if (it != dc.free.end() && (it->first <= 2 * nbytes || it->first - nbytes <= kSlack)) {
-      void* p = it->second;
-      *got = it->first;
-      dc.bytes -= it->first;
-      dc.free.erase(it);
-      return p;
-    }
-  }
-  void* p = nullptr;
-  cudaError_t e = cudaMalloc(&p, nbytes);
-  if (e != cudaSuccess) {
-    cudaGetLastError();  // clear the allocation error
-    std::vector<void*> drop;
-    {
-      std::lock_guard<std::mutex> lk(c.mu);
-      DeviceCache& dc = c.dev[d];
-      for (auto& kv : dc.free) drop.push_back(kv.second);
-      dc.free.clear();
-      dc.bytes = 0;
-    }
-    for (void* q : drop) cudaFree(q);
-    e = cudaMalloc(&p, nbytes);
+  void* ptr = nullptr;
+  if (nbytes >= kPoolMax) {
+    cudaError_t e = cudaMalloc(&ptr, nbytes);
     if (e != cudaSuccess) {
       cudaGetLastError();
-      throw Error(INTI_E_NOMEM, std::string("cudaMalloc(") + std::to_string(nbytes) + "): " + cudaGetErrorString(e));
+      {
+        std::lock_guard<std::mutex> lk(pools().mu);
+        auto it = pools().dev.find(d);
+        if (it != pools().dev.end() && it->second.pool) {
+          cudaDeviceSynchronize();
+          cudaMemPoolTrimTo(it->second.pool, 0);
+        }
+      }
+      e = cudaMalloc(&ptr, nbytes);
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(INTI_E_NOMEM, std::string("cudaMalloc(") + std::to_string(nbytes) + "): " + cudaGetErrorString(e));
+      }
+    }
+    *got = nbytes;
+    return ptr;
+  }
+  DevicePool& p = pool_for(d);
+  cudaError_t e = cudaMallocFromPoolAsync(&ptr, nbytes, p.pool, p.stream);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // clear the allocation error
+    cudaDeviceSynchronize();
+    cudaMemPoolTrimTo(p.pool, 0);
+    e = cudaMallocFromPoolAsync(&ptr, nbytes, p.pool, p.stream);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      throw Error(INTI_E_NOMEM, std::string("device allocation of ") + std::to_string(nbytes) +
+                                    " bytes: " + cudaGetErrorString(e));
     }
   }
+  INTI_CUDA(cudaStreamSynchronize(p.stream));  // ready for every stream
   *got = nbytes;
-  return p;
+  return ptr;
 }
 
-void dev_release(void* p, size_t bytes, int device) {
-  if (!p) return;
+void dev_release(void* ptr, size_t bytes, int device) {
+  if (!ptr) return;
   SetDevice sd(device);
-  cudaDeviceSynchronize();  // no work of any stream still uses the block
-  Cache& c = cache();
-  {
-    std::lock_guard<std::mutex> lk(c.mu);
-    DeviceCache& dc = c.dev[device];
-    if (dc.bytes + bytes <= kCacheCap) {
-      dc.free.emplace(bytes, p);
-      dc.bytes += bytes;
-      return;
-    }
+  if (bytes >= kPoolMax) {
+    cudaFree(ptr);
+    return;
   }
-  cudaFree(p);
+  cudaDeviceSynchronize();  // no work of any stream still uses the block
+  DevicePool& p = pool_for(device);
+  cudaFreeAsync(ptr, p.stream);
 }
 
 size_t dev_cache_bytes(int device) {
-  Cache& c = cache();
-  std::lock_guard<std::mutex> lk(c.mu);
-  auto it = c.dev.find(device);
-  return it == c.dev.end() ? 0 : it->second.bytes;
+  Pools& ps = pools();
+  std::lock_guard<std::mutex> lk(ps.mu);
+  auto it = ps.dev.find(device);
+  if (it == ps.dev.end() || !it->second.pool) return 0;
+  uint64_t reserved = 0, used = 0;
+  cudaMemPoolGetAttribute(it->second.pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+  cudaMemPoolGetAttribute(it->second.pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  return reserved > used ? (size_t)(reserved - used) : 0;
 }
 
 }  // namespace inti

@@ -428,6 +428,8 @@ struct Solver {
             bool x_is_zero, bool final_true_residual) {
     double* V = vec(ctx->krylov.V, restart + 1);
     double* w = vec(ctx->krylov.w);
+    // the dot-product partials for the widest step, so no step reallocates
+    ctx->krylov.partial.ensure(sizeof(double2) * (size_t)nblk * (restart + 2));
     DevBuf& hbuf = ctx->krylov.h;
     DevBuf& ybuf = ctx->krylov.y;
     hbuf.ensure(sizeof(double2) * (restart + 2) * 2);

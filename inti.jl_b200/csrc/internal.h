@@ -119,5 +119,6 @@ void grad_sources(inti_op* op, const double* g, const double* sigma, double* dsi
 void measure_peaks(inti_ctx* ctx, double* fp64, double* fp32, double* mufu);
 void measure_peak_tf32(inti_ctx* ctx, double* tf32_flops);
 void selftest_math(inti_ctx* ctx, double* out);
+void selftest_wait_timeout(inti_ctx* ctx);
 
 }  // namespace inti

@@ -210,7 +210,7 @@ void symm_layout(int64_t n, int tpt, int ch, int pb, double budget, int& pcols, 
 double symm_budget(const inti_op* op) {
   size_t free_b = 0, total_b = 0;
   INTI_CUDA(cudaMemGetInfo(&free_b, &total_b));
-  free_b += dev_cache_bytes(op->ctx->device);  // released blocks held for reuse count as free
+  free_b += dev_cache_bytes(op->ctx->device);  // released memory the pool holds counts as free
   return std::min(op->ctx->symm_budget,
                   kSymmMaxFreeShare * (double)free_b + op->ctx->sym_ypart.bytes + op->ctx->sym_zpart.bytes);
 }

@@ -10,6 +10,7 @@
 
 #include "common.h"
 #include "device_common.cuh"
+#include "internal.h"
 
 namespace inti {
 
@@ -115,6 +116,26 @@ __global__ void math_probe(int n, const double* x, double* rs, double* rs3, doub
   float cf, sf;
   expi_table_eval((float)u[i], 1.0f, t32, (float)(2 * kPi / kExpiTable), cf, sf);
   e32[i] = make_float2(cf, sf);
+}
+
+// A bounded wait that runs out: one thread waits for the first phase of an
+// mbarrier that nothing arrives at, with the pair kernels' own bounded wait,
+// and records the timeout in the context's flag as they do.
+__global__ void wait_timeout_probe(int* err) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0)) atomicExch(err, kErrWaitTimeout);
+}
+
+void selftest_wait_timeout(inti_ctx* ctx) {
+  wait_timeout_probe<<<1, 32, 0, ctx->stream>>>(ctx->err_flag.as<int>());
+  ctx->launches++;
+  INTI_CUDA(cudaGetLastError());
+  sync_and_check(ctx);  // throws INTI_E_TIMEOUT and clears the flag
 }
 
 void selftest_math(inti_ctx* ctx, double* out) {

@@ -134,6 +134,7 @@ SIGNATURES = {
     "inti_op_single_launch": (C.c_int, [P]),
     "inti_op_set_shard": (C.c_int, [P, C.c_int, C.c_int]),
     "inti_selftest_math": (C.c_int, [P, D]),
+    "inti_selftest_wait_timeout": (C.c_int, [P]),
     "inti_batch_create": (C.c_int, [P, C.c_int32, PP, C.c_int, C.c_int, C.c_double, C.c_double, D, D, PP, PP, PP]),
     "inti_batch_apply": (C.c_int, [P, C.c_int, P, I64, P, I64, C.c_int32, D, D, C.c_int]),
     "inti_batch_gmres": (C.c_int, [P, D, P, P, I64, C.c_int32, C.c_double, C.c_int32, C.c_int32, C.c_int32, C.c_int,

@@ -227,3 +227,25 @@ def test_released_device_blocks_are_reused(ctx):
         used.append(total - free)
     assert max(used[1:]) - min(used[1:]) < (64 << 20), used
     assert np.all(np.isfinite(y))
+
+
+def test_bounded_wait_timeout_is_reported_and_context_survives(ctx):
+    """A device-side bounded wait that runs out (an mbarrier nothing arrives
+    at) ends its kernel with INTI_E_TIMEOUT in the context's flag; the call
+    reports it, and the context keeps working with the flag cleared."""
+    import time
+
+    from inti_b200 import _lib as L
+
+    t0 = time.perf_counter()
+    status = ctx.lib.inti_selftest_wait_timeout(ctx.handle)
+    elapsed = time.perf_counter() - t0
+    assert status == L.E_TIMEOUT
+    assert b"bounded wait" in ctx.lib.inti_last_error(ctx.handle)
+    assert elapsed < 30.0, elapsed
+    print(f"bounded wait ran out after {elapsed:.3f} s")
+    q = SURF["ellipsoid"]
+    A = inti.GpuOperator(inti.SingleLayerKernel(inti.Laplace(dim=3)), q, q, None, "fp64", ctx)
+    x = density(len(q), False, 4)
+    assert relerr(A @ x, oracle_apply(O.LAPLACE, O.SL, 0.0, q, q, x)) < 1e-12
+    ctx.synchronize()  # no stale timeout
