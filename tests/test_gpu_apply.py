@@ -205,9 +205,10 @@ def test_combined_field_operator(ctx, prec, tol):
 
 
 def test_released_device_blocks_are_reused(ctx):
-    """Operators created and destroyed again and again take their device
-    blocks from the cache of released blocks: device memory in use stays
-    flat after the first round."""
+    """Operators created and destroyed again and again reuse the device
+    memory released by the previous round (the memory pool for small blocks,
+    cudaMalloc/cudaFree for large ones): device memory in use stays flat
+    after the first round."""
     import gc
 
     import torch
