@@ -218,8 +218,10 @@ int inti_op_panels(const inti_op* op);
  * e.g. the 1,000-node kite) apply in a single-launch form: one kernel per product builds the
  * source records, forms the pair sums (a cluster of up to 8 CTAs per 32
  * targets, the CTAs and their warps splitting the sources, sums in a fixed
- * order), adds the correction rows and applies alpha/beta.  Transposed and
- * item-sharded applies keep the tiled kernels.  inti_ctx_set_single_launch(ctx,
+ * order), adds the correction rows and applies alpha/beta.  Transposed
+ * products of small square operators run the same kernel with the transposed
+ * kernel and the transposed correction; item-sharded applies keep the tiled
+ * kernels.  inti_ctx_set_single_launch(ctx,
  * 0) makes operators created afterwards use the tiled kernels;
  * inti_op_single_launch returns 1 when an operator uses the form.  No
  * counterpart in the reference. */

@@ -182,6 +182,15 @@ void op_apply_device(inti_op* op, const double* x, double* y, const double* alph
 
 void op_apply_transpose_device(inti_op* op, const double* x, double* y, const double* alpha,
                                const double* beta) {
+  if (op->symm && op->small && op->shard_n == 1) {
+    // small square operator: the transposed kernel with unit source weights
+    // in the single-launch form, row j scaled by w_j, the transposed correction
+    PairLaunch L = make_launch(op, x);
+    L.kind = transposed_kind(op->kind);
+    L.sweights = op->tones.as<double>();
+    pair_small(op->ctx, L, op->corrT.get(), x, y, alpha, beta, op->source->weights.as<double>());
+    return;
+  }
   if (op->symm) {
     // square operator: the symmetric product of the transposed kernel with
     // unit weights on the same node blocks, work items and partial buffers

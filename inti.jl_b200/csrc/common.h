@@ -265,12 +265,14 @@ int pair_epilogue(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, cons
                   double* y, const double* alpha, const double* beta, const double* rowscale = nullptr);
 // Dense assembly of A.
 int pair_assemble(inti_ctx* ctx, const PairLaunch& L, double* out);
-// Single-launch form of small FP64 products (pack, then the pair sums with
-// the epilogue in one kernel): operators of at most kSmallPairs pairs.
+// Single-launch form of small FP64 products (one cluster kernel: source
+// records, pair sums, correction rows, alpha/beta): operators of at most
+// kSmallPairs pairs.  rowscale (nullable) scales row i's pair sum, as the
+// epilogue does for transposed products (the source weights).
 constexpr double kSmallPairs = 1048576.0;
 bool pair_small_eligible(int precision, int64_t m, int64_t n);
 int pair_small(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x, double* y,
-               const double* alpha, const double* beta);
+               const double* alpha, const double* beta, const double* rowscale = nullptr);
 
 // CSR: y = alpha*C*x + beta*y (alpha/beta complex pairs); transpose via col scatter.
 int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, const double* alpha,

@@ -702,7 +702,8 @@ __global__ void __launch_bounds__(32 * kSmallWarps) pair_small_kernel(int64_t m,
       acc.z += v.z;
       acc.w += v.w;
     }
-    epilogue_store<CPLX>(e, i, fma(acc.x, e.scale, acc.z), fma(acc.y, e.scale, acc.w), yo);
+    const double sc = e.rowscale ? e.scale * e.rowscale[i] : e.scale;
+    epilogue_store<CPLX>(e, i, fma(acc.x, sc, acc.z), fma(acc.y, sc, acc.w), yo);
   }
   cl.sync();  // the peers' shared memory stays valid until CTA 0 has read it
 }
@@ -1957,8 +1958,9 @@ static int pair_small_slices(int num_sms, int64_t m, int64_t n) {
 }
 
 int pair_small(inti_ctx* ctx, const PairLaunch& L, const inti_csr* corr, const double* x, double* y,
-               const double* alpha, const double* beta) {
+               const double* alpha, const double* beta, const double* rowscale) {
   EpiArgs e;
+  e.rowscale = rowscale;
   e.m = L.m;
   e.split = 1;
   e.partial = nullptr;

@@ -158,3 +158,37 @@ def test_single_launch_derivative_kernels_with_correction(ctx, tiled, case):
         got = A.mul(y0.copy(), x, alpha=alpha, beta=beta)
         assert relerr(got, B.mul(y0.copy(), x, alpha=alpha, beta=beta)) < 1e-12, K_
         assert np.array_equal(got, A.mul(y0.copy(), x, alpha=alpha, beta=beta))
+
+
+@pytest.mark.parametrize("case", ["laplace2d", "laplace3d", "helmholtz3d"])
+def test_single_launch_transpose(ctx, tiled, case):
+    """Transposed products of small square operators (every kernel, with the
+    DIM correction, complex alpha/beta) in the single-launch form: the
+    transposed kernel with unit source weights and each row scaled by its
+    weight, against the tiled kernels and the dense oracle transpose."""
+    import scipy.sparse as sp
+
+    if case == "laplace2d":
+        q, op, cplx, pde, k = inti.kite_quadrature(120, 9), inti.Laplace(dim=2), False, O.LAPLACE, 0.0
+    elif case == "laplace3d":
+        q, op, cplx, pde, k = inti.ellipsoid_quadrature(3, 5), inti.Laplace(dim=3), False, O.LAPLACE, 0.0
+    else:
+        q, op, cplx, pde, k = inti.p2_sphere_quadrature(4), inti.Helmholtz(k=3.0, dim=3), True, O.HELMHOLTZ, 3.0
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    K, H = inti.adj_double_layer_hypersingular(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    g, y0 = density(len(q), cplx, 31), density(len(q), cplx, 32)
+    alpha, beta = (0.5 - 0.25j, 1.5 + 0.5j) if cplx else (0.5, 1.5)
+    for A, kind, K_ in ((S, O.SL, inti.SingleLayerKernel), (D, O.DL, inti.DoubleLayerKernel),
+                        (K, O.ADL, inti.AdjointDoubleLayerKernel), (H, O.HS, inti.HyperSingularKernel)):
+        assert A.tuning["single_launch"]
+        rp, col, val = A.correction.arrays()
+        dense = O.assemble(pde, kind, k, q.coords, q.normals, q.coords, q.normals, q.weights) + \
+            sp.csr_matrix((val, col, rp), shape=A.shape).toarray()
+        got = A._apply(g, y=y0.copy(), alpha=alpha, beta=beta, transpose=True)
+        assert relerr(got, alpha * (dense.T @ g) + beta * y0) < 1e-12, kind
+        B = inti.GpuOperator(K_(op), q, q, inti.CorrectionMatrix.from_csr(rp, col, val, A.shape, ctx=tiled),
+                             "fp64", tiled)
+        assert relerr(got, B._apply(g, y=y0.copy(), alpha=alpha, beta=beta, transpose=True)) < 1e-12, kind
+        before = ctx.launch_count
+        A.rmatvec(g)
+        assert ctx.launch_count - before == 1
