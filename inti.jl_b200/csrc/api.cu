@@ -307,6 +307,7 @@ int inti_ctx_create(int device, void* stream, inti_ctx** out) {
       c->own_stream = true;
     }
     INTI_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    dev_prepare(device);  // the memory pool and its reservation: set-up cost here, not in a first product
     c->err_flag.ensure(sizeof(int));
     INTI_CUDA(cudaMemset(c->err_flag.p, 0, sizeof(int)));
     INTI_CUDA(cudaHostAlloc(reinterpret_cast<void**>(&c->err_host), sizeof(int), cudaHostAllocDefault));

@@ -43,6 +43,7 @@ struct Error : std::runtime_error {
 void* dev_alloc(size_t nbytes, int* device, size_t* got);  // throws Error(INTI_E_NOMEM)
 void dev_release(void* p, size_t bytes, int device);
 size_t dev_cache_bytes(int device);  // bytes the pool holds free
+void dev_prepare(int device);        // create the device's pool now (context creation)
 
 // Device allocation owned by a handle.
 struct DevBuf {

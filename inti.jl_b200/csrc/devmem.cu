@@ -145,6 +145,11 @@ void dev_release(void* ptr, size_t bytes, int device) {
   cudaFreeAsync(ptr, p.stream);
 }
 
+void dev_prepare(int device) {
+  SetDevice sd(device);
+  pool_for(device);
+}
+
 size_t dev_cache_bytes(int device) {
   Pools& ps = pools();
   std::lock_guard<std::mutex> lk(ps.mu);
