@@ -122,3 +122,38 @@ def test_gmres_small_form_matches_multi_kernel_form(ctx, mode):
             assert abs(st1["iterations"] - st0["iterations"]) <= 1, (st1, st0)
             assert relerr(x1, x0) < 1e-8
             assert st1["relres"] <= 1e-10
+
+
+@pytest.mark.parametrize("small", [8192, 0])
+def test_gmres_iteration_cap_across_batches_and_restarts(ctx, small):
+    """maxiter reached inside a batch of small-system steps and across a
+    restart: exactly maxiter iterations, reported as not converged, in both
+    forms."""
+    q, S, D = laplace_problem(ctx, 3)
+    L = D - 0.5 * inti.I
+    b = density(len(q), False, 17)
+    ctx.set_gmres_small(small)
+    try:
+        for restart, maxiter in ((5, 6), (3, 7), (4, 4)):
+            x, st = inti.gmres(L, b, rtol=1e-15, restart=restart, maxiter=maxiter, history=True)
+            assert st["converged"] == 0 and st["iterations"] == maxiter, (restart, maxiter, st)
+            assert np.all(np.isfinite(x))
+            h = st["history"]
+            assert len(h) >= maxiter + 1 and np.all(np.isfinite(h[: maxiter + 1]))
+    finally:
+        ctx.set_gmres_small(8192)
+
+
+@pytest.mark.parametrize("small", [8192, 0])
+def test_gmres_lucky_breakdown(ctx, small):
+    """L = I + 0·S: the first Krylov step breaks down (the new vector is
+    zero), which ends the cycle with the exact solution in both forms."""
+    q, S, D = laplace_problem(ctx, 3)
+    b = density(len(q), False, 19)
+    ctx.set_gmres_small(small)
+    try:
+        x, st = inti.gmres(1.0 * inti.I + 0.0 * S, b, rtol=1e-12, restart=10, maxiter=50)
+    finally:
+        ctx.set_gmres_small(8192)
+    assert st["converged"] == 1 and st["iterations"] == 1, st
+    assert relerr(x, b) < 1e-14
