@@ -84,7 +84,11 @@ enum { INTI_GMRES_FP64 = 0, INTI_GMRES_MIXED = 1 };
 int inti_version(void);
 
 /* ---- context ----------------------------------------------------------- */
-/* stream: a cudaStream_t to run on, or NULL for a library-owned stream. */
+/* stream: a cudaStream_t to run on, or NULL for a library-owned stream.
+ * The library's device buffers come from a per-device memory pool for blocks
+ * under 64 MB (made by the first context on a device, 256 MB reserved then,
+ * released memory kept up to 8 GB for reuse; the pool lives until exit) and
+ * from cudaMalloc for larger blocks. */
 int inti_ctx_create(int device, void* stream, inti_ctx** out);
 int inti_ctx_destroy(inti_ctx* ctx);
 /* Message of the last failure on ctx (or of the calling thread when ctx is
