@@ -85,9 +85,14 @@ namespace inti {
 void noalloc_error_set(const char* msg) { g_thread_error = msg; }
 
 void sync_and_check(inti_ctx* ctx) {
+  if (!ctx->flag_armed) {  // nothing enqueued since the last check can have raised the flag
+    INTI_CUDA(cudaStreamSynchronize(ctx->stream));
+    return;
+  }
   // the flag comes back with the stream's other work: one round trip per call
   INTI_CUDA(cudaMemcpyAsync(ctx->err_host, ctx->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   INTI_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx->flag_armed = false;
   const int flag = *ctx->err_host;
   if (flag) {
     *ctx->err_host = 0;

@@ -83,6 +83,9 @@ struct inti_ctx {
   int64_t launches = 0;
   inti::DevBuf err_flag;  // device int: nonzero when a bounded wait ran out
   int* err_host = nullptr;  // page-locked copy of err_flag, read after a stream sync
+  // set when a kernel that can raise err_flag (one with bounded waits) is
+  // enqueued; a synchronising call reads the flag back only then
+  bool flag_armed = false;
   inti::DevBuf scan_tmp;    // device-scan scratch (correction merges), kept between calls
   inti::DevBuf expi64, expi32;  // e^{i m delta} tables of the Helmholtz pair loops
   // per-kernel-class event timing (inti_ctx_set_profiling)

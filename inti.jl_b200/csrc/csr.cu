@@ -351,6 +351,7 @@ int csr_apply(inti_ctx* ctx, const inti_csr* c, const double* x, double* y, cons
     const int rpb = (int)std::max<double>(1.0, std::min<double>(kBulkThreads, 0.9 * cap / std::max(mean, 1.0)));
     const unsigned grid = (unsigned)((c->m + rpb - 1) / rpb);
     int* err = ctx->err_flag.as<int>();
+    ctx->flag_armed = true;
     if (cplx) {
       const size_t sm = csr_bulk_smem<true>();
       INTI_CUDA(cudaFuncSetAttribute(&csr_bulk_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

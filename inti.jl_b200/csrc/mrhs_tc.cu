@@ -654,6 +654,7 @@ void measure_peak_tf32(inti_ctx* ctx, double* tf32_flops) {
   cudaEvent_t e0, e1;
   INTI_CUDA(cudaEventCreate(&e0));
   INTI_CUDA(cudaEventCreate(&e1));
+  ctx->flag_armed = true;
   tc_peak_probe<<<ctx->num_sms, 128, TC_B_BYTES, ctx->stream>>>(rounds, ctx->err_flag.as<int>());  // warm-up
   INTI_CUDA(cudaEventRecord(e0, ctx->stream));
   tc_peak_probe<<<ctx->num_sms, 128, TC_B_BYTES, ctx->stream>>>(rounds, ctx->err_flag.as<int>());
@@ -793,6 +794,7 @@ static void tc_run(inti_batch* b, const BatchArgs& a, const int32_t* item_surf, 
   t.beta_zero = a.beta_zero;
   t.counter = b->tc_counter.as<int>();
   t.err = ctx->err_flag.as<int>();
+  ctx->flag_armed = true;
   INTI_CUDA(cudaMemsetAsync(b->tc_counter.p, 0, sizeof(int), ctx->stream));
   auto launch = [&](auto kern) {
     ProfScope pk(ctx, "batch_tc");

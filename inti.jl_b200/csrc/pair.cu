@@ -1770,6 +1770,7 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
           a.delta = 2 * kPi / kExpiTable;
           a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
           a.err = L.err_flag;
+          ctx->flag_armed = true;
           size_t sm;
           void (*fn)(SymArgs);
           if constexpr (symm_x2<T, R>()) {
@@ -1854,6 +1855,7 @@ int pair_launch(inti_ctx* ctx, const PairLaunch& L) {
       a.delta = 2 * kPi / kExpiTable;
       a.expi = std::is_same<R, float>::value ? (const void*)expi_table_f32(ctx) : (const void*)expi_table_f64(ctx);
       a.err = L.err_flag;
+      ctx->flag_armed = true;
       const size_t sm = fwd_smem<T, R>();
       auto fn = L.tpt == 2 ? &pair_forward<T::pde, T::kind, T::dim, R, TILE, 2>
                            : &pair_forward<T::pde, T::kind, T::dim, R, TILE, 4>;

@@ -132,6 +132,7 @@ __global__ void wait_timeout_probe(int* err) {
 }
 
 void selftest_wait_timeout(inti_ctx* ctx) {
+  ctx->flag_armed = true;
   wait_timeout_probe<<<1, 32, 0, ctx->stream>>>(ctx->err_flag.as<int>());
   ctx->launches++;
   INTI_CUDA(cudaGetLastError());
