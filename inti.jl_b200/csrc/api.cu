@@ -661,6 +661,29 @@ int inti_op_info(const inti_op* op, int64_t* m, int64_t* n, int* dtype) {
   return INTI_OK;
 }
 
+// Host-pointer applies of small vectors in page-locked host memory that the
+// device can address (cudaHostAlloc, or cudaHostRegister on a system with
+// unified addressing) skip the copy engines, whose round trip costs several
+// microseconds per copy: one small kernel reads x into the device staging
+// buffer, and the product writes y straight into the host buffer (each row
+// once; read once when beta != 0).
+constexpr size_t kZeroCopyMax = (size_t)64 << 10;
+
+static void* device_view(const void* p, size_t bytes) {
+  if (bytes > kZeroCopyMax) return nullptr;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return a.type == cudaMemoryTypeHost ? a.devicePointer : nullptr;
+}
+
+__global__ void copy_doubles(int64_t n, const double* __restrict__ src, double* __restrict__ dst) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
 static int apply_common(inti_op* op, const double* x, int64_t ldx, double* y, int64_t ldy,
                         int32_t nrhs, const double* alpha, const double* beta, int on_device,
                         bool transpose) {
@@ -708,21 +731,36 @@ static int apply_common(inti_op* op, const double* x, int64_t ldx, double* y, in
       double* yr = y + (size_t)r * ldy * comps;
       const double* xd = xr;
       double* yd = yr;
+      bool direct = false;  // y written in place in mapped host memory
       if (!on_device) {
         // host staging, made on the first host-pointer apply
         const size_t big = sizeof(double) * comps * std::max(op->target->n, op->source->n);
         op->xbuf.ensure(big);
         op->ybuf.ensure(big);
-        h2d(ctx, op->xbuf.p, xr, sizeof(double) * comps * nin);
-        if (!bz) h2d(ctx, op->ybuf.p, yr, sizeof(double) * comps * nout);
-        xd = op->xbuf.as<double>();
-        yd = op->ybuf.as<double>();
+        const size_t bx = sizeof(double) * comps * nin, by = sizeof(double) * comps * nout;
+        const void* xv = device_view(xr, bx);
+        void* yv = xv ? device_view(yr, by) : nullptr;
+        if (xv && yv) {
+          const int64_t cnt = (int64_t)comps * nin;
+          copy_doubles<<<(unsigned)std::min<int64_t>(64, (cnt + 255) / 256), 256, 0, ctx->stream>>>(
+              cnt, static_cast<const double*>(xv), op->xbuf.as<double>());
+          INTI_CUDA(cudaGetLastError());
+          ctx->launches++;
+          xd = op->xbuf.as<double>();
+          yd = static_cast<double*>(yv);
+          direct = true;
+        } else {
+          h2d(ctx, op->xbuf.p, xr, bx);
+          if (!bz) h2d(ctx, op->ybuf.p, yr, by);
+          xd = op->xbuf.as<double>();
+          yd = op->ybuf.as<double>();
+        }
       }
       if (transpose)
         op_apply_transpose_device(op, xd, yd, alpha, beta);
       else
         op_apply_device(op, xd, yd, alpha, beta);
-      if (!on_device) d2h(ctx, yr, op->ybuf.p, sizeof(double) * comps * nout);
+      if (!on_device && !direct) d2h(ctx, yr, op->ybuf.p, sizeof(double) * comps * nout);
     }
     if (!on_device) sync_and_check(ctx);
   });

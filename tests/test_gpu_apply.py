@@ -250,3 +250,32 @@ def test_bounded_wait_timeout_is_reported_and_context_survives(ctx):
     x = density(len(q), False, 4)
     assert relerr(A @ x, oracle_apply(O.LAPLACE, O.SL, 0.0, q, q, x)) < 1e-12
     ctx.synchronize()  # no stale timeout
+
+
+@pytest.mark.parametrize("case", ["kite", "ellipsoid", "helmholtz"])
+def test_pinned_host_vectors_match_pageable(ctx, case):
+    """Host-pointer applies of small vectors in page-locked memory (read by a
+    copy kernel, y written in place in host memory) give the same bits as
+    pageable buffers (copied by the copy engines): products and transposes,
+    beta = 0 and beta != 0."""
+    import torch
+
+    if case == "kite":
+        q, op, cplx = inti.kite_quadrature(200, 9), inti.Laplace(dim=2), False  # single-launch form
+    elif case == "ellipsoid":
+        q, op, cplx = inti.ellipsoid_quadrature(8, 5), inti.Laplace(dim=3), False  # 3,456 nodes, tiled
+    else:
+        q, op, cplx = inti.p2_sphere_quadrature(8), inti.Helmholtz(k=3.0, dim=3), True  # 3,072 nodes
+    S, D = inti.single_double_layer(op=op, target=q, source=q, correction={"method": "dim"}, ctx=ctx)
+    dt = torch.complex128 if cplx else torch.float64
+    x = density(len(q), cplx, 41)
+    y0 = density(len(q), cplx, 42)
+    alpha, beta = (0.5 - 0.25j, 1.5 + 0.5j) if cplx else (0.5, 1.5)
+    for A in (S, D):
+        px = torch.from_numpy(x.copy()).pin_memory().numpy()
+        for transpose in (False, True):
+            for b in (0.0, beta):
+                py = torch.from_numpy(y0.copy()).to(dt).pin_memory().numpy()
+                got = A._apply(px, y=py, alpha=alpha, beta=b, transpose=transpose)
+                want = A._apply(x.copy(), y=y0.copy(), alpha=alpha, beta=b, transpose=transpose)
+                assert np.array_equal(got, want), (case, transpose, b)
