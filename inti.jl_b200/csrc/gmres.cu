@@ -172,14 +172,16 @@ __device__ __forceinline__ double2 load_c(const double* v, int64_t i) {
   return C ? reinterpret_cast<const double2*>(v)[i] : make_double2(v[i], 0.0);
 }
 
-// Step j of a small-system cycle, after w = L v_j: w is orthogonalised
+// Step j of a small-system cycle, after w = sum_t coef_t A_t v_j (the shift
+// is added here, w += shift * v_j, saving a launch per step): w is orthogonalised
 // against v_0..v_j twice (CGS2; sums in a fixed order), v_{j+1} = w/|w|,
 // and thread 0 applies the earlier rotations to the new Hessenberg column,
 // forms rotation j, and records |g[j+1]|.  A stopped cycle leaves later
 // steps as no-ops.  Dynamic shared memory: 2 * (restart + 1) double2.
 template <bool C>
 __global__ void __launch_bounds__(kArnoldiThreads) arnoldi_small_step(int64_t n, int j, int restart, double* V,
-                                                                      double* w, double tol_abs, ArnoldiState st) {
+                                                                      double* w, double2 shift, double tol_abs,
+                                                                      ArnoldiState st) {
   extern __shared__ double2 hbuf[];
   __shared__ double2 red[kArnoldiThreads / 32][8];
   __shared__ double hn_s;
@@ -189,6 +191,18 @@ __global__ void __launch_bounds__(kArnoldiThreads) arnoldi_small_step(int64_t n,
   double2* hsum = hbuf;               // [restart + 1]
   double2* hp = hbuf + restart + 1;   // [restart + 1]
   for (int k = tid; k <= j; k += kArnoldiThreads) hsum[k] = make_double2(0.0, 0.0);
+  if (shift.x != 0.0 || shift.y != 0.0) {  // each thread its own entries, as in the passes below
+    const double* vj = V + (int64_t)comps * n * j;
+    for (int64_t i = tid; i < n; i += kArnoldiThreads) {
+      if (C) {
+        const double2 a = reinterpret_cast<const double2*>(w)[i];
+        const double2 p = cm(shift, reinterpret_cast<const double2*>(vj)[i]);
+        reinterpret_cast<double2*>(w)[i] = make_double2(a.x + p.x, a.y + p.y);
+      } else {
+        w[i] += shift.x * vj[i];
+      }
+    }
+  }
   for (int pass = 0; pass < 2; ++pass) {
     for (int k0 = 0; k0 <= j; k0 += 8) {
       double2 acc[8];
@@ -324,6 +338,16 @@ struct Solver {
     }
     (fp32 ? fp32_applies : fp64_applies)++;
   }
+  // out = sum_t coef_t A_t v (no shift term; the small-system step adds it)
+  void apply_unshifted(bool fp32, const double* v, double* out) {
+    auto& ops = fp32 ? ops32 : ops64;
+    for (size_t t = 0; t < ops.size(); ++t) {
+      const double al[2] = {coefs[t].real(), coefs[t].imag()};
+      const double be[2] = {t == 0 ? 0.0 : 1.0, 0.0};
+      op_apply_device(ops[t], v, out, al, be);
+    }
+    (fp32 ? fp32_applies : fp64_applies)++;
+  }
   // h[0:kcount] (=|+=) V^H w  (device)
   void dots(const double* V, int64_t ldv, int kcount, const double* w, double2* h, bool acc) {
     DevBuf& partial = ctx->krylov.partial;
@@ -387,11 +411,14 @@ struct Solver {
     while (j < restart && it < maxit && !done) {
       const int batch = std::min({kArnoldiBatch, restart - j, maxit - it});
       for (int b = 0; b < batch; ++b) {
-        apply(fp32, V + (size_t)comps * n * (j + b), w);
+        apply_unshifted(fp32, V + (size_t)comps * n * (j + b), w);
+        const double2 sh = make_double2(shift.real(), shift.imag());
         if (C)
-          arnoldi_small_step<true><<<1, kArnoldiThreads, smem, ctx->stream>>>(n, j + b, restart, V, w, tol_abs, st);
+          arnoldi_small_step<true><<<1, kArnoldiThreads, smem, ctx->stream>>>(n, j + b, restart, V, w, sh, tol_abs,
+                                                                               st);
         else
-          arnoldi_small_step<false><<<1, kArnoldiThreads, smem, ctx->stream>>>(n, j + b, restart, V, w, tol_abs, st);
+          arnoldi_small_step<false><<<1, kArnoldiThreads, smem, ctx->stream>>>(n, j + b, restart, V, w, sh,
+                                                                                tol_abs, st);
         ctx->launches++;
       }
       INTI_CUDA(cudaMemcpyAsync(rh.data() + j, st.res + j, sizeof(double) * batch, cudaMemcpyDeviceToHost,
